@@ -1,0 +1,379 @@
+#!/usr/bin/env python3
+"""Benchmark of the D3Q19 moving-boundary step (GLUPS and fraction of the HBM roofline).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
+
+One JSON line on rank 0.  A "step" is one lattice-Boltzmann time step of the
+whole workload (geometry, links, bounce-back, loads, fused stream+collide,
+body update).  ``value`` is device-timed (CUDA events on the library's stream)
+with the populations resident in HBM; ``e2e`` runs the same steps through the
+C ABI one call at a time with the body state written from pinned host memory
+and the step's loads read back every step.  ``roofline`` uses the fused
+stream+collide kernel's own CUDA-event launch times and its algorithmic
+traffic of 38 * s bytes per cell (19 reads + 19 writes of s-byte populations).
+
+Workloads (lattice units):
+  ellipsoid_channel  256x128x128, ellipsoid (24,12,12) at x=64, inflow 0.05,
+                     nu 0.005, RR3, interpolated links, velocity inlet /
+                     zero-gradient outlet / periodic y,z (default)
+  flapping_plates    512x256x256, two 64x12x2 plates as 2x8192 triangles,
+                     stroke 60 sin, pitch 45 cos, T = 4000, nu 0.004, TRT
+  shear_wave         64^3 periodic, nu 0.01, magic 1/4 (L2-resident)
+Multi-GPU: the step does not shard here (one GPU per lattice), so N GPUs run N
+independent replicas; ``value`` is the aggregate and ``scaling`` is weak.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "numi-gpu-physics_b200"))
+
+FALLBACK_HBM_GBS = 6650.0
+WORKLOAD_DEFAULT = "ellipsoid_channel"
+
+
+def build_case(name: str, storage: int):
+    import bfx._lib as L
+    import bfx.cases as cases
+    if name == "ellipsoid_channel":
+        cfg, rows, body, mesh = cases.ellipsoid_channel(storage=storage)
+        desc = ("ellipsoid_channel 256x128x128 semi-axes (24,12,12) at x=64, inflow u_x=0.05 velocity inlet, "
+                "zero-gradient outflow, periodic y/z, nu=0.005, RR3, interpolated bounce-back")
+        collision = "rr3"
+    elif name == "flapping_plates":
+        cfg, rows, body, mesh = cases.flapping_plates(storage=storage)
+        desc = ("flapping_plates 512x256x256 two 64x12x2 flat plates (2x8192 triangles), stroke 60deg sin, "
+                "pitch 45deg cos, T=4000, nu=0.004, TRT, ray-root links rebuilt each step")
+        collision = "trt"
+    elif name == "shear_wave":
+        cfg, rows, body, mesh = cases.shear_wave(n=64, viscosity=0.01, magic=0.25, axis="z", storage=storage)
+        desc = "shear_wave 64^3 periodic, u_x=0.01 sin(2 pi z/64), nu=0.01, magic 1/4, TRT (L2-resident)"
+        collision = "trt"
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return cfg, rows, body, mesh, desc, collision
+
+
+def make_lattice(name, storage, device):
+    import bfx._lib as L
+    from bfx.simulation import Lattice, bird_struct
+    from bfx.simulation import default_config  # noqa: F401
+    cfg, rows, body, mesh, desc, coll = build_case(name, storage)
+    cfg.device = device
+    bs = None
+    if body is not None:
+        bs = L.BodyState()
+        bs.position[:] = list(body[0])
+        bs.orientation[:] = list(body[1])
+        bs.velocity[:] = list(body[2])
+        bs.omega_body[:] = list(body[3])
+    lat = Lattice(cfg, bird_struct(rows) if rows is not None else None, bs, mesh)
+    return lat, cfg, desc, coll
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic(workload: str, storage_name: str):
+    """Per-launch DRAM bytes of the fused kernel from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    try:
+        for ln in open(path):
+            parts = ln.split()
+            if len(parts) >= 3 and not ln.startswith("#") and parts[0] == workload and parts[1] == storage_name:
+                return float(parts[2])
+    except OSError:
+        pass
+    return None
+
+
+def time_steps(lat, steps, warmup):
+    """Device time of `steps` steps (CUDA events on the library stream) plus kernel stats."""
+    lat.advance(warmup, batch_size=max(warmup, 1))
+    lat.set_kernel_timing(True)
+    l0 = lat.launch_count()
+    lat.timer_begin()
+    lat.advance(steps, batch_size=steps)
+    ms = lat.timer_end()
+    l1 = lat.launch_count()
+    kms, klaunch = lat.kernel_timing()
+    lat.set_kernel_timing(False)
+    return ms, l1 - l0, kms, klaunch
+
+
+def e2e_steps(lat, steps):
+    """Per-step C-ABI calls with host buffers: body state in (pinned), loads out."""
+    import ctypes as ct
+    import bfx._lib as L
+    try:
+        import torch
+        pinned_in = torch.empty(ct.sizeof(L.BodyState), dtype=torch.uint8).pin_memory()
+        pinned_out = torch.empty(ct.sizeof(L.Loads), dtype=torch.uint8).pin_memory()
+        body = L.BodyState.from_address(pinned_in.data_ptr())
+        loads = L.Loads.from_address(pinned_out.data_ptr())
+    except Exception:  # pinned memory unavailable: plain host structs
+        body, loads = L.BodyState(), L.Loads()
+    cur = lat.body()
+    ct.memmove(ct.addressof(body), ct.addressof(cur), ct.sizeof(L.BodyState))
+    lib = lat.lib
+    lat.timer_begin()
+    for _ in range(steps):
+        rc = lib.bfx_set_body(lat.handle, ct.byref(body))
+        rc |= lib.bfx_advance(lat.handle, 1, 1, 0, None, 0, None)
+        rc |= lib.bfx_last_loads(lat.handle, ct.byref(loads))
+        if rc:
+            raise RuntimeError(L.last_error(lat.handle))
+    ms = lat.timer_end()
+    return ms, ct.sizeof(L.BodyState), ct.sizeof(L.Loads)
+
+
+def force_history(name, storage, steps, device):
+    """Per-step force (N) of `steps` steps from the start, recorded on the device."""
+    lat, cfg, _, _ = make_lattice(name, storage, device)
+    _, samples = lat.advance(steps, batch_size=steps, record_samples=True)
+    f = np.array([[samples[i].force[0], samples[i].force[1], samples[i].force[2]] for i in range(steps)])
+    lat.close()
+    return f
+
+
+def cpu_port_rate(name, seconds_budget=12.0, max_steps=64):
+    """The oracle (CPU restatement of the reference path) on the same workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle as O  # noqa: F401  (checker library, CPU baseline only)
+    from helpers import oracle_twin
+    cfg, rows, body, mesh, desc, _ = build_case(name, 0)
+    osim = oracle_twin(cfg, rows, body, mesh)
+    osim.step()
+    t0 = time.perf_counter()
+    steps = 0
+    while steps < max_steps:
+        osim.step()
+        steps += 1
+        if time.perf_counter() - t0 > seconds_budget:
+            break
+    dt = time.perf_counter() - t0
+    cells = cfg.nx * cfg.ny * cfg.nz
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return cells * steps / dt / 1e9, steps, threads, dt
+
+
+def run_reference_arm(args, rank, world):
+    name = args.workload
+    if rank != 0:
+        return 0
+    cfg, rows, body, mesh, desc, coll = build_case(name, 0)
+    budget = 150.0
+    per_step_budget = budget / max(args.steps + args.warmup, 1)
+    rate, steps, cores, dt = cpu_port_rate(name, seconds_budget=min(60.0, per_step_budget * args.steps),
+                                           max_steps=max(1, args.steps))
+    cells = cfg.nx * cfg.ny * cfg.nz
+    line = {
+        "impl": "reference", "metric": "D3Q19 GLUPS", "value": rate, "unit": "GLUPS", "n_gpus": world,
+        "steps": steps, "warmup": 1, "ms_per_step": dt * 1000.0 / max(steps, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": desc, "lattice": [cfg.nx, cfg.ny, cfg.nz], "collision": coll, "storage": "f32"},
+        "cpu_baseline": {"value": rate, "unit": "GLUPS", "cores": cores, "kind": "port",
+                         "sample": f"{steps} full steps of the {name} workload ({cells} cells) on the CPU "
+                                   f"restatement of the reference step (oracle/, C + OpenMP)"},
+        "e2e": {"value": rate, "unit": "GLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--workload", default=WORKLOAD_DEFAULT)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    if args.impl == "reference":
+        rc = run_reference_arm(args, rank, world)
+        if dist is not None:
+            dist.destroy_process_group()
+        return rc
+
+    import bfx._lib as L
+    lat, cfg, desc, coll = make_lattice(args.workload, L.STORAGE_F32, local)
+    cells = cfg.nx * cfg.ny * cfg.nz
+
+    def barrier():
+        if dist is not None:
+            import torch
+            torch.cuda.synchronize()
+            dist.barrier()
+
+    barrier()
+    with ClockSampler(local) as clocks:
+        ms, launches, kms, klaunch = time_steps(lat, args.steps, args.warmup)
+    barrier()
+    if dist is not None:
+        import torch
+        t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * cells * args.steps / (ms / 1000.0) / 1e9
+    e2e_n = min(args.steps, 200)
+    e2e_ms, h2d, d2h = e2e_steps(lat, e2e_n)
+    if dist is not None:
+        import torch
+        t = torch.tensor([e2e_ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * cells * e2e_n / (e2e_ms / 1000.0) / 1e9
+    lat.close()
+
+    peak, peak_kind = measured_peak()
+    bytes_per_launch = cells * 38 * 4
+    kernel_s = kms / max(klaunch, 1) / 1000.0
+    achieved = bytes_per_launch / kernel_s / 1e9
+    traffic = profiled_traffic(args.workload, "f32")
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "peak_kind": f"of {peak_kind}", "kernel": "k_bulk (fused AA stream+collide)",
+                "bytes_per_launch": bytes_per_launch, "kernel_ms": kernel_s * 1000.0}
+
+    line = {
+        "metric": "D3Q19 GLUPS", "value": value, "unit": "GLUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": desc, "lattice": [cfg.nx, cfg.ny, cfg.nz], "collision": coll, "storage": "f32",
+                   "l2": f"inputs larger than L2 ({19 * cells * 4 / 1e6:.1f} MB of populations)"
+                   if 19 * cells * 4 > 126e6 else "L2-resident working set",
+                   "parallelism": f"replicas{world}"},
+        "e2e": {"value": e2e_value, "unit": "GLUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": e2e_n, "calls": "bfx_set_body + bfx_advance(1) + bfx_last_loads per step"},
+        "roofline": roofline,
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+    }
+
+    if rank == 0 and not args.no_variants:
+        variants = {}
+        hist_steps = 400 if args.workload != "flapping_plates" else 4000
+        ref = force_history(args.workload, L.STORAGE_F64, hist_steps, local)
+        half = hist_steps // 2
+        ref_mean = ref[half:].mean(axis=0)
+        for st in (L.STORAGE_F32, L.STORAGE_F16_DEVIATION, L.STORAGE_BF16_DEVIATION):
+            nm = L.STORAGE_NAMES[st]
+            if st != L.STORAGE_F32:
+                vlat, _, _, _ = make_lattice(args.workload, st, local)
+                vms, _, vkms, vkl = time_steps(vlat, args.steps, args.warmup)
+                vlat.close()
+                s = L.STORAGE_BYTES[st]
+                vach = cells * 38 * s / (vkms / max(vkl, 1) / 1000.0) / 1e9
+                variants[nm] = {"value": cells * args.steps / (vms / 1000.0) / 1e9, "unit": "GLUPS",
+                                "roofline_frac": vach / peak, "achieved_gbs": vach,
+                                "speedup_vs_f32": (cells * args.steps / (vms / 1000.0) / 1e9) / value * world}
+            else:
+                variants[nm] = {"value": value / world, "unit": "GLUPS", "roofline_frac": roofline["frac"]}
+            f = force_history(args.workload, st, hist_steps, local)
+            mean = f[half:].mean(axis=0)
+            scale = max(np.linalg.norm(ref_mean), 1e-30)
+            variants[nm]["force_error_vs_f64"] = float(np.linalg.norm(mean - ref_mean) / scale)
+            variants[nm]["force_window_steps"] = [half, hist_steps]
+        line["variants"] = variants
+
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, steps, cores, dt = cpu_port_rate(args.workload)
+        line["cpu_baseline"] = {"value": rate, "unit": "GLUPS", "cores": cores, "kind": "port",
+                                "sample": f"{steps} full steps of the same workload on the CPU restatement "
+                                          f"(oracle/, C + OpenMP, {dt:.1f} s)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,310 @@
+/*
+ * bfx — B200-native D3Q19 lattice-Boltzmann step with moving articulated
+ * boundaries.  Plain C ABI (no CUDA or torch types): opaque handle, plain
+ * pointers and sizes, integer status codes.
+ *
+ * This library replaces the Metal execution path of BirdFlowMetal's
+ * BirdFlowSimulation (Numi2/numi-gpu-physics,
+ * Sources/BirdFlowMetal/BirdFlowSimulation.swift).  Each entry point below
+ * names the reference interface it stands in for.  The reference has no plugin
+ * protocol: its boundary is the concrete class, and its non-Metal branch
+ * (BirdFlowSimulation.swift:2105-2182) is where a Linux backend calls this ABI.
+ *
+ * Threading: one handle owns one CUDA stream; calls on one handle must be
+ * serialised by the caller (the reference class is @unchecked Sendable with
+ * caller-serialised calls, BirdFlowSimulation.swift:410-478).  Independent
+ * handles may be used from different threads.
+ *
+ * Errors: every function returns a bfx_status.  After a GPU failure the
+ * handle is terminally invalid and later calls return BFX_ERR_INVALIDATED,
+ * mirroring BirdFlowSimulation.invalidate (BirdFlowSimulation.swift:2059-2095).
+ * bfx_last_error() returns the message of the last failure.
+ */
+#ifndef BFX_H
+#define BFX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BFX_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define BFX_API __attribute__((visibility("default")))
+#else
+#define BFX_API
+#endif
+
+typedef struct bfx_sim bfx_sim;
+
+/* Mirrors BirdFlowError (Sources/BirdFlowMetal/BirdFlowError.swift:3-55) and
+ * BirdFlowConfigurationError (Sources/BirdFlowCore/SimulationConfiguration.swift:3-24). */
+typedef enum bfx_status {
+    BFX_OK = 0,
+    BFX_ERR_DEVICE_UNAVAILABLE = 1, /* deviceUnavailable / metalUnavailable */
+    BFX_ERR_ALLOCATION = 2,         /* allocationFailed */
+    BFX_ERR_INVALID_ADVANCE = 3,    /* invalidAdvanceRequest */
+    BFX_ERR_KERNEL = 4,             /* commandBufferFailed */
+    BFX_ERR_SAFETY = 5,             /* runtimeSafetyViolation */
+    BFX_ERR_INVALIDATED = 6,        /* simulationStateInvalidated */
+    BFX_ERR_INVALID_CONFIG = 7,     /* BirdFlowConfigurationError */
+    BFX_ERR_INVALID_ARGUMENT = 8,
+    BFX_ERR_CAPACITY = 9            /* caller buffer or link list too small */
+} bfx_status;
+
+/* Collision operator.  The reference selects these through caseParameters.w
+ * thresholds inside stepFluidTRT (BF.metal:2544-2555, 2906-2912). */
+typedef enum bfx_collision {
+    BFX_COLLISION_TRT = 0,           /* BF.metal:3063-3093 */
+    BFX_COLLISION_TRT_LIMITER = 1,   /* symmetric positivity limiter, BF.metal:3094-3174 */
+    BFX_COLLISION_REGULARIZED = 2,   /* projected regularized BGK, BF.metal:2917-3062 */
+    BFX_COLLISION_RR3 = 3            /* recursive regularized, third order, BF.metal:2917-3062 */
+} bfx_collision;
+
+/* Moving-wall bounce-back rule (BF.metal:2727-2806). */
+typedef enum bfx_wall_rule {
+    BFX_WALL_HALFWAY = 0,
+    BFX_WALL_INTERPOLATED = 1
+} bfx_wall_rule;
+
+/* Population storage.  Collision arithmetic is FP32 for the first three and
+ * FP64 for BFX_STORAGE_F64 (the reference run for error statements). */
+typedef enum bfx_storage {
+    BFX_STORAGE_F32 = 0,
+    BFX_STORAGE_F16_DEVIATION = 1,   /* f - w_q in IEEE half, scaled by 2^12 */
+    BFX_STORAGE_BF16_DEVIATION = 2,  /* f - w_q in bfloat16 */
+    BFX_STORAGE_F64 = 3
+} bfx_storage;
+
+/* Domain face rule for populations pulled from outside the lattice.
+ * FARFIELD is the reference rule (BF.metal:2696-2725); PERIODIC is per axis
+ * (both faces of the axis must say so); VELOCITY and OUTFLOW are additions. */
+typedef enum bfx_face_bc {
+    BFX_BC_FARFIELD = 0,  /* equilibrium(far density, far velocity) */
+    BFX_BC_PERIODIC = 1,
+    BFX_BC_VELOCITY = 2,  /* equilibrium(far density, face_velocity[face]) */
+    BFX_BC_OUTFLOW = 3    /* zero gradient: copy what the interior neighbour receives */
+} bfx_face_bc;
+
+typedef enum bfx_geometry_kind {
+    BFX_GEOMETRY_NONE = 0,       /* all fluid */
+    BFX_GEOMETRY_BIRD = 1,       /* analytic bird: ellipsoid body, tapered wings, tail (BF.metal:816-938) */
+    BFX_GEOMETRY_ELLIPSOID = 2,  /* body ellipsoid alone, link fractions by bisection (BF.metal:1144-1175 rule) */
+    BFX_GEOMETRY_MESH = 3        /* articulated triangle mesh (BF.metal:1638-2076) */
+} bfx_geometry_kind;
+
+/* Link fraction rule for mesh geometry. */
+typedef enum bfx_link_rule {
+    BFX_LINK_LINEAR = 0,  /* q = d_f / (d_f - d_s) from signed distances (BF.metal:2044-2076) */
+    BFX_LINK_RAY_ROOT = 1 /* bracketed root of the wall distance along the link */
+} bfx_link_rule;
+
+typedef enum bfx_init {
+    BFX_INIT_EQUILIBRIUM = 0,   /* initializePopulations, BF.metal:2078-2103 */
+    BFX_INIT_SHEAR_WAVE_Y = 1,  /* initializeShearWave, BF.metal:2132-2162: u_x = A sin(2 pi y / N_y) */
+    BFX_INIT_SHEAR_WAVE_Z = 2   /* same wave along z */
+} bfx_init;
+
+/* Simulation parameters: the lattice-unit content of SimulationConfiguration
+ * and LatticeScaling (SimulationConfiguration.swift:55-315) as packed into
+ * GPUUniforms (Sources/BirdFlowMetal/GPUData.swift:4-80). */
+typedef struct bfx_config {
+    uint32_t nx, ny, nz;
+    int32_t device;                 /* CUDA device ordinal */
+    float origin[3];                /* domainOriginMeters */
+    float cell_size;                /* cellSizeMeters (dx) */
+    float time_step;                /* timeStepSeconds (dt) */
+    float velocity_to_lattice;      /* dt/dx */
+    float force_to_physical;        /* rho dx^4 / dt^2 */
+    float _reserved0;
+    float omega_plus, omega_minus;  /* 1/tau+, 1/tau- */
+    float sponge_strength;
+    float sponge_width;             /* cells */
+    float far_field[4];             /* lattice velocity xyz, density w */
+    float gravity[3];               /* m/s^2 */
+    uint32_t body_substeps;         /* 1...64 */
+    int32_t face_bc[6];             /* bfx_face_bc for -x,+x,-y,+y,-z,+z */
+    float face_velocity[6][3];      /* lattice velocity of BFX_BC_VELOCITY faces */
+    int32_t collision;              /* bfx_collision */
+    int32_t wall_rule;              /* bfx_wall_rule */
+    int32_t storage;                /* bfx_storage */
+    int32_t geometry;               /* bfx_geometry_kind */
+    int32_t link_rule;              /* bfx_link_rule (mesh) */
+    int32_t force_estimator;        /* 0..6; 6 = production conservative estimator */
+    int32_t load_component;         /* 0 both, 1 link exchange only, 2 topology only */
+    int32_t selected_part;          /* 0 = all parts */
+    uint32_t free_flight;
+    uint32_t accumulate_loads;
+    uint32_t moving_wall_local_density; /* integration.y: pre-step local density in the wall term */
+    uint32_t static_geometry;       /* geometry does not move: classify and build links once */
+    int32_t init;                   /* bfx_init */
+    uint32_t link_capacity;         /* 0 = automatic */
+    float init_amplitude;           /* shear-wave amplitude (lattice velocity) */
+    float mesh_half_thickness;      /* meters */
+} bfx_config;
+
+typedef struct bfx_float4 { float v[4]; } bfx_float4;
+
+/* GPUBirdParameters (Sources/BirdFlowMetal/GPUData.swift:82-178), 13 float4. */
+typedef struct bfx_bird {
+    bfx_float4 body_radii_mass;     /* body radii xyz (m), mass (kg) */
+    bfx_float4 inertia;             /* principal inertia xyz */
+    bfx_float4 wing_geometry0;      /* span, root chord, tip chord, thickness */
+    bfx_float4 wing_geometry1;      /* sweep, root offset xyz */
+    bfx_float4 tail_geometry;       /* length, half width, thickness, - */
+    bfx_float4 wing_kinematics0;    /* frequency Hz, stroke amplitude, stroke bias, pitch mean */
+    bfx_float4 wing_kinematics1;    /* pitch amplitude, pitch phase, -, - */
+    bfx_float4 safety_geometry;     /* conservative local half extent xyz, bounding radius */
+    bfx_float4 safety_limits;       /* max prescribed wing speed, Mach limit */
+    bfx_float4 left_wing_mass_com;  /* mass, centre of mass from hinge (chord, span, normal) */
+    bfx_float4 left_wing_inertia;   /* principal inertia xyz, w = 1 when present */
+    bfx_float4 right_wing_mass_com;
+    bfx_float4 right_wing_inertia;
+} bfx_bird;
+
+/* BirdBodyState (Sources/BirdFlowCore/BirdModel.swift:53-68), FP64. */
+typedef struct bfx_body_state {
+    double position[3];
+    double orientation[4];          /* body-to-world quaternion x, y, z, w */
+    double velocity[3];
+    double omega_body[3];
+} bfx_body_state;
+
+/* Articulated triangle mesh: vertex coordinates in the frame of their segment
+ * (0 = body frame, relative to the body origin; 1 = left wing frame and
+ * 2 = right wing frame, as (chord, span, normal) offsets from the wing root). */
+typedef struct bfx_mesh {
+    const float* local_vertices;    /* 3 * vertex_count */
+    const uint8_t* vertex_segment;  /* vertex_count */
+    uint32_t vertex_count;
+    const uint32_t* triangles;      /* 3 * triangle_count vertex indices */
+    const uint8_t* triangle_part;   /* part id 1..63 per triangle */
+    uint32_t triangle_count;
+} bfx_mesh;
+
+/* ForceTorque (Sources/BirdFlowCore/Diagnostics.swift) plus step diagnostics. */
+typedef struct bfx_loads {
+    double force[3];                /* N, FP64 momentum-exchange sum */
+    double torque[3];               /* N m about the body position */
+    double force_lattice[3];
+    double limiter_activations;     /* cells where the positivity limiter engaged */
+    double max_restriction;
+    int64_t link_count;
+    int64_t covered_count;
+    int64_t uncovered_count;
+} bfx_loads;
+
+/* RunSample (Sources/BirdFlowMetal/GPUFieldObservation.swift; GPURunSample GPUData.swift:457-501). */
+typedef struct bfx_run_sample {
+    double time;
+    double position[3];
+    double orientation[4];
+    double velocity[3];
+    double omega_body[3];
+    double force[3];
+    double torque[3];
+    float left_hinge_force[3];
+    float left_hinge_torque[3];
+    float right_hinge_force[3];
+    float right_hinge_torque[3];
+    uint64_t step;
+} bfx_run_sample;
+
+/* GPURuntimeSafetyRecord (BF.metal:80-83): metrics = max Mach, min clearance,
+ * Mach and clearance at the first event; event = step (lo, hi), flags
+ * (1 Mach, 2 clearance, 4 non-finite), reserved. */
+typedef struct bfx_safety_record {
+    float metrics[4];
+    uint32_t event[4];
+} bfx_safety_record;
+
+typedef struct bfx_snapshot_data {  /* SimulationSnapshot (Diagnostics.swift) */
+    uint64_t step;
+    double time;
+    bfx_body_state body;
+    bfx_loads loads;
+} bfx_snapshot_data;
+
+enum {
+    BFX_ADVANCE_CAPTURE_FIELDS = 1,   /* FieldCaptureMode.required: rho/u on the last step */
+    BFX_ADVANCE_RECORD_SAMPLES = 2    /* recordRunSamples */
+};
+
+typedef struct bfx_advance_result { /* AdvanceResult (GPUFieldObservation.swift) */
+    uint64_t steps_done;
+    uint32_t field_frame_published;
+    uint32_t safety_passed;
+    bfx_safety_record safety;
+} bfx_advance_result;
+
+BFX_API const char* bfx_version(void);
+BFX_API int bfx_abi_version(void);
+BFX_API int bfx_device_count(int* count);
+
+/* BirdFlowSimulation.init(configuration:bird:initialBodyState:) (BirdFlowSimulation.swift:480-644).
+ * bird/body may be NULL for BFX_GEOMETRY_NONE; mesh is required for BFX_GEOMETRY_MESH. */
+BFX_API int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_state* body,
+               const bfx_mesh* mesh, bfx_sim** out);
+BFX_API void bfx_destroy(bfx_sim* sim);
+
+/* advance(steps:batchSize:fieldCapture:recordRunSamples:) (BirdFlowSimulation.swift:688-799).
+ * samples may be NULL unless BFX_ADVANCE_RECORD_SAMPLES is set (capacity >= steps). */
+BFX_API int bfx_advance(bfx_sim* sim, uint64_t steps, uint32_t batch_size, uint32_t flags,
+                bfx_run_sample* samples, size_t sample_capacity, bfx_advance_result* result);
+
+/* snapshot() (BirdFlowSimulation.swift:1087) */
+BFX_API int bfx_snapshot(bfx_sim* sim, bfx_snapshot_data* out);
+/* copyMacroscopicFields() (BirdFlowSimulation.swift:1109): the fields captured by
+ * the last advance with BFX_ADVANCE_CAPTURE_FIELDS (density[n], velocity[3n]). */
+BFX_API int bfx_copy_fields(bfx_sim* sim, float* density, float* velocity_xyz, size_t cells);
+/* copyGaugePressureFieldPascals() (BirdFlowSimulation.swift:1132) */
+BFX_API int bfx_copy_gauge_pressure(bfx_sim* sim, float pressure_scale_pascals, float* out, size_t cells);
+/* runtimeSafetyReport() (BirdFlowSimulation.swift:1766) */
+BFX_API int bfx_runtime_safety(bfx_sim* sim, bfx_safety_record* out);
+BFX_API int bfx_last_loads(bfx_sim* sim, bfx_loads* out);
+/* Canonical post-collision populations f*_q(x), direction-major [19][n] in FP32
+ * (the reference's populationsIn layout, Docs/NUMERICS.md:33-37). */
+BFX_API int bfx_copy_populations(bfx_sim* sim, float* out, size_t count);
+BFX_API int bfx_set_populations(bfx_sim* sim, const float* in, size_t count);
+/* Current occupancy (part id per cell) and wall field (xyz lattice velocity, w distance). */
+BFX_API int bfx_copy_mask(bfx_sim* sim, uint8_t* out, size_t cells);
+BFX_API int bfx_copy_wall(bfx_sim* sim, float* out4, size_t cells);
+/* Cut links of the last step (fluid cell, direction, link fraction), in the
+ * deterministic order of the compaction. */
+BFX_API int bfx_copy_links(bfx_sim* sim, uint32_t* cell, uint8_t* direction, float* fraction, size_t capacity,
+                   size_t* count);
+/* Global mass and momentum of fluid cells in FP64 (measureFluidMassMomentum, BF.metal:4272-4297). */
+BFX_API int bfx_fluid_mass_momentum(bfx_sim* sim, double out[4]);
+/* Raw restart state (saveCheckpoint / init(checkpointURL:), BirdFlowSimulation.swift:1214-1298, 1920-2024):
+ * bfx_save_state with buf == NULL reports the size. */
+BFX_API int bfx_save_state(bfx_sim* sim, void* buf, size_t capacity, size_t* size);
+BFX_API int bfx_restore_state(bfx_sim* sim, const void* buf, size_t size);
+/* Body state (FP64) read/write between advances. */
+BFX_API int bfx_get_body(bfx_sim* sim, bfx_body_state* out);
+BFX_API int bfx_set_body(bfx_sim* sim, const bfx_body_state* in);
+/* Step counter and time (stepIndex, timeSeconds). */
+BFX_API int bfx_step_index(bfx_sim* sim, uint64_t* step, double* time);
+/* Device timing of the fused stream-collide kernel: when enabled, CUDA events on
+ * the simulation's stream bracket every launch; total milliseconds and launch
+ * count since enabling. */
+BFX_API int bfx_set_kernel_timing(bfx_sim* sim, int enabled);
+BFX_API int bfx_kernel_timing(bfx_sim* sim, double* total_ms, uint64_t* launches);
+/* Region timer on the simulation's stream: bfx_timer_begin records a CUDA event,
+ * bfx_timer_end records a second one, waits for it and returns the elapsed
+ * device time in milliseconds. */
+BFX_API int bfx_timer_begin(bfx_sim* sim);
+BFX_API int bfx_timer_end(bfx_sim* sim, double* elapsed_ms);
+/* Total kernel launches issued by the library on this handle. */
+BFX_API int bfx_launch_count(bfx_sim* sim, uint64_t* launches);
+/* Bytes of device memory held by the handle. */
+BFX_API int bfx_device_bytes(bfx_sim* sim, uint64_t* bytes);
+/* Message of the last failure on this handle (or of the last failed create when sim is NULL). */
+BFX_API int bfx_last_error(bfx_sim* sim, char* buf, size_t capacity);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BFX_H */

@@ -1,0 +1,336 @@
+"""Python host mirror of BirdFlowSimulation over the bfx C ABI.
+
+``Lattice`` is a thin owner of one ``bfx_sim`` handle, configured with the raw
+``bfx_config`` fields (lattice units).  ``BirdFlowSimulation`` mirrors the
+reference class (Sources/BirdFlowMetal/BirdFlowSimulation.swift:410-2096):
+same construction from a ``SimulationConfiguration`` + ``BirdParameters`` +
+``BirdBodyState``, same ``advance(steps, batch_size, field_capture,
+record_run_samples)`` semantics and the same error kinds (``BirdFlowError``).
+"""
+from __future__ import annotations
+
+import ctypes as ct
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib as L
+from .config import BirdBodyState, BirdParameters, SimulationConfiguration
+
+
+class BirdFlowError(RuntimeError):
+    """BirdFlowError (Sources/BirdFlowMetal/BirdFlowError.swift:3-55) with the C status code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{L.STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+        self.kind = L.STATUS_NAMES.get(status, str(status))
+
+
+def _check(status: int, handle=None):
+    if status != L.BFX_OK:
+        raise BirdFlowError(status, L.last_error(handle))
+
+
+def _fp(a):
+    return a.ctypes.data_as(ct.POINTER(ct.c_float))
+
+
+@dataclass
+class AdvanceResult:
+    """AdvanceResult (Sources/BirdFlowMetal/GPUFieldObservation.swift)."""
+    run_samples: list = field(default_factory=list)
+    field_frame_published: bool = False
+    runtime_safety: dict | None = None
+
+
+def default_config(nx: int, ny: int, nz: int, **kw) -> L.Config:
+    c = L.Config()
+    c.nx, c.ny, c.nz = nx, ny, nz
+    c.device = 0
+    c.cell_size = 1.0
+    c.time_step = 1.0
+    c.velocity_to_lattice = 1.0
+    c.force_to_physical = 1.0
+    c.omega_plus = c.omega_minus = 1.0
+    c.sponge_width = 4.0
+    c.far_field[:] = [0.0, 0.0, 0.0, 1.0]
+    c.body_substeps = 1
+    c.accumulate_loads = 1
+    c.force_estimator = 6
+    for k, v in kw.items():
+        cur = getattr(c, k)
+        if isinstance(cur, ct.Array):
+            if isinstance(v, (list, tuple)) and len(v) and isinstance(v[0], (list, tuple)):
+                for i, row in enumerate(v):
+                    cur[i][:] = list(row)
+            else:
+                cur[:] = list(v)
+        else:
+            setattr(c, k, v)
+    return c
+
+
+def bird_struct(rows) -> L.Bird:
+    b = L.Bird()
+    for name, row in zip(L.BIRD_FIELDS, rows):
+        getattr(b, name).v[:] = [float(x) for x in row]
+    return b
+
+
+def body_struct(state: BirdBodyState | None) -> L.BodyState:
+    s = L.BodyState()
+    if state is None:
+        s.orientation[:] = [0.0, 0.0, 0.0, 1.0]
+        return s
+    s.position[:] = list(state.position_meters)
+    s.orientation[:] = list(state.orientation_body_to_world)
+    s.velocity[:] = list(state.linear_velocity_meters_per_second)
+    s.omega_body[:] = list(state.angular_velocity_body_radians_per_second)
+    return s
+
+
+class Lattice:
+    """One simulation handle on the GPU (bfx_create / bfx_destroy)."""
+
+    def __init__(self, config: L.Config, bird: L.Bird | None = None, body: L.BodyState | None = None,
+                 mesh: dict | None = None):
+        self.lib = L.load()
+        self.config = config
+        self.n = int(config.nx) * int(config.ny) * int(config.nz)
+        self._mesh_keep = None
+        mesh_ptr = None
+        if mesh is not None:
+            local = np.ascontiguousarray(mesh["local"], np.float32)
+            seg = np.ascontiguousarray(mesh["segment"], np.uint8)
+            tris = np.ascontiguousarray(mesh["tris"], np.uint32)
+            parts = np.ascontiguousarray(mesh["tri_part"], np.uint8)
+            self._mesh_keep = (local, seg, tris, parts)
+            m = L.Mesh()
+            m.local_vertices = local.ctypes.data_as(ct.POINTER(ct.c_float))
+            m.vertex_segment = seg.ctypes.data_as(ct.POINTER(ct.c_uint8))
+            m.vertex_count = local.shape[0]
+            m.triangles = tris.ctypes.data_as(ct.POINTER(ct.c_uint32))
+            m.triangle_part = parts.ctypes.data_as(ct.POINTER(ct.c_uint8))
+            m.triangle_count = tris.shape[0]
+            mesh_ptr = ct.byref(m)
+            self._mesh_struct = m
+        handle = ct.c_void_p()
+        st = self.lib.bfx_create(ct.byref(config), ct.byref(bird) if bird is not None else None,
+                                 ct.byref(body) if body is not None else None, mesh_ptr, ct.byref(handle))
+        _check(st, None)
+        self.handle = handle
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.bfx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- stepping ---------------------------------------------------------
+    def advance(self, steps: int, batch_size: int = 32, capture_fields: bool = False, record_samples: bool = False):
+        flags = (L.ADVANCE_CAPTURE_FIELDS if capture_fields else 0) | (L.ADVANCE_RECORD_SAMPLES if record_samples else 0)
+        samples = (L.RunSample * max(steps, 1))() if record_samples else None
+        res = L.AdvanceResult()
+        st = self.lib.bfx_advance(self.handle, steps, batch_size, flags, samples, steps if record_samples else 0,
+                                  ct.byref(res))
+        _check(st, self.handle)
+        return res, samples
+
+    # -- read-back ----------------------------------------------------------
+    def populations(self) -> np.ndarray:
+        out = np.empty(19 * self.n, np.float32)
+        _check(self.lib.bfx_copy_populations(self.handle, _fp(out), out.size), self.handle)
+        return out.reshape(19, self.config.nz, self.config.ny, self.config.nx)
+
+    def set_populations(self, pops: np.ndarray):
+        a = np.ascontiguousarray(pops, np.float32).ravel()
+        _check(self.lib.bfx_set_populations(self.handle, _fp(a), a.size), self.handle)
+
+    def fields(self):
+        rho = np.empty(self.n, np.float32)
+        vel = np.empty(3 * self.n, np.float32)
+        _check(self.lib.bfx_copy_fields(self.handle, _fp(rho), _fp(vel), self.n), self.handle)
+        return rho, vel.reshape(-1, 3)
+
+    def mask(self) -> np.ndarray:
+        out = np.empty(self.n, np.uint8)
+        _check(self.lib.bfx_copy_mask(self.handle, out.ctypes.data_as(ct.POINTER(ct.c_uint8)), self.n), self.handle)
+        return out
+
+    def wall(self) -> np.ndarray:
+        out = np.empty(4 * self.n, np.float32)
+        _check(self.lib.bfx_copy_wall(self.handle, _fp(out), self.n), self.handle)
+        return out.reshape(-1, 4)
+
+    def links(self):
+        count = ct.c_size_t()
+        _check(self.lib.bfx_copy_links(self.handle, None, None, None, 0, ct.byref(count)), self.handle)
+        n = count.value
+        cell = np.empty(max(n, 1), np.uint32)
+        d = np.empty(max(n, 1), np.uint8)
+        q = np.empty(max(n, 1), np.float32)
+        _check(self.lib.bfx_copy_links(self.handle, cell.ctypes.data_as(ct.POINTER(ct.c_uint32)),
+                                       d.ctypes.data_as(ct.POINTER(ct.c_uint8)), _fp(q), n, ct.byref(count)),
+               self.handle)
+        return cell[:n], d[:n], q[:n]
+
+    def loads(self) -> L.Loads:
+        out = L.Loads()
+        _check(self.lib.bfx_last_loads(self.handle, ct.byref(out)), self.handle)
+        return out
+
+    def snapshot(self) -> L.Snapshot:
+        out = L.Snapshot()
+        _check(self.lib.bfx_snapshot(self.handle, ct.byref(out)), self.handle)
+        return out
+
+    def safety(self) -> L.SafetyRecord:
+        out = L.SafetyRecord()
+        _check(self.lib.bfx_runtime_safety(self.handle, ct.byref(out)), self.handle)
+        return out
+
+    def body(self) -> L.BodyState:
+        out = L.BodyState()
+        _check(self.lib.bfx_get_body(self.handle, ct.byref(out)), self.handle)
+        return out
+
+    def set_body(self, body: L.BodyState):
+        _check(self.lib.bfx_set_body(self.handle, ct.byref(body)), self.handle)
+
+    def mass_momentum(self) -> np.ndarray:
+        out = np.zeros(4, np.float64)
+        _check(self.lib.bfx_fluid_mass_momentum(self.handle, out.ctypes.data_as(ct.POINTER(ct.c_double))), self.handle)
+        return out
+
+    def step_index(self):
+        step = ct.c_uint64()
+        t = ct.c_double()
+        _check(self.lib.bfx_step_index(self.handle, ct.byref(step), ct.byref(t)), self.handle)
+        return step.value, t.value
+
+    def save_state(self) -> bytes:
+        size = ct.c_size_t()
+        _check(self.lib.bfx_save_state(self.handle, None, 0, ct.byref(size)), self.handle)
+        buf = ct.create_string_buffer(size.value)
+        _check(self.lib.bfx_save_state(self.handle, buf, size.value, ct.byref(size)), self.handle)
+        return buf.raw
+
+    def restore_state(self, data: bytes):
+        buf = ct.create_string_buffer(data, len(data))
+        _check(self.lib.bfx_restore_state(self.handle, buf, len(data)), self.handle)
+
+    def set_kernel_timing(self, enabled: bool):
+        _check(self.lib.bfx_set_kernel_timing(self.handle, int(enabled)), self.handle)
+
+    def kernel_timing(self):
+        ms = ct.c_double()
+        n = ct.c_uint64()
+        _check(self.lib.bfx_kernel_timing(self.handle, ct.byref(ms), ct.byref(n)), self.handle)
+        return ms.value, n.value
+
+    def timer_begin(self):
+        _check(self.lib.bfx_timer_begin(self.handle), self.handle)
+
+    def timer_end(self) -> float:
+        ms = ct.c_double()
+        _check(self.lib.bfx_timer_end(self.handle, ct.byref(ms)), self.handle)
+        return ms.value
+
+    def launch_count(self) -> int:
+        n = ct.c_uint64()
+        _check(self.lib.bfx_launch_count(self.handle, ct.byref(n)), self.handle)
+        return n.value
+
+    def device_bytes(self) -> int:
+        n = ct.c_uint64()
+        _check(self.lib.bfx_device_bytes(self.handle, ct.byref(n)), self.handle)
+        return n.value
+
+
+class BirdFlowSimulation:
+    """BirdFlowSimulation (BirdFlowSimulation.swift:410-2096) on the CUDA backend.
+
+    Production defaults of the reference: analytic bird geometry, halfway
+    moving bounce-back, TRT collision, estimator 6, far-field + sponge faces.
+    ``storage``, ``collision``, ``wall_rule`` expose the typed operator
+    selection that the reference overloads onto caseParameters.w.
+    """
+
+    def __init__(self, configuration: SimulationConfiguration, bird: BirdParameters,
+                 initial_body_state: BirdBodyState, *, storage: int = L.STORAGE_F32,
+                 collision: int = L.COLLISION_TRT, device: int = 0):
+        bird.validate(configuration)
+        self.configuration = configuration
+        self.bird = bird
+        sc = configuration.scaling
+        far = configuration.far_field_velocity_meters_per_second
+        v2l = sc.velocity_to_lattice
+        cfg = default_config(
+            configuration.grid.x, configuration.grid.y, configuration.grid.z,
+            device=device, origin=configuration.domain_origin_meters, cell_size=sc.cell_size_meters,
+            time_step=sc.time_step_seconds, velocity_to_lattice=v2l, force_to_physical=sc.force_to_physical,
+            omega_plus=sc.omega_plus, omega_minus=sc.omega_minus, sponge_strength=configuration.sponge_strength,
+            sponge_width=float(configuration.sponge_width_cells),
+            far_field=[float(np.float32(far[0]) * np.float32(v2l)), float(np.float32(far[1]) * np.float32(v2l)),
+                       float(np.float32(far[2]) * np.float32(v2l)), 1.0],
+            gravity=configuration.gravity_meters_per_second_squared, body_substeps=configuration.body_substeps,
+            collision=collision, wall_rule=L.WALL_HALFWAY, storage=storage, geometry=L.GEOMETRY_BIRD,
+            free_flight=int(configuration.free_flight), accumulate_loads=1)
+        self.lattice = Lattice(cfg, bird_struct(bird.packed()), body_struct(initial_body_state))
+        self.step_index = 0
+        self.time_seconds = 0.0
+
+    def advance(self, steps: int, batch_size: int = 32, field_capture: str = "required",
+                record_run_samples: bool = False) -> AdvanceResult:
+        if steps < 0 or batch_size <= 0:
+            raise BirdFlowError(3, f"invalid advance request steps={steps} batchSize={batch_size}")
+        if steps == 0:
+            return AdvanceResult(runtime_safety=self.runtime_safety_report() if self.configuration.free_flight else None)
+        capture = field_capture in ("required", "latest")
+        res, samples = self.lattice.advance(steps, batch_size, capture, record_run_samples)
+        self.step_index, self.time_seconds = self.lattice.step_index()
+        out = AdvanceResult(field_frame_published=bool(res.field_frame_published))
+        if record_run_samples:
+            out.run_samples = [samples[i] for i in range(steps)]
+        if self.configuration.free_flight:
+            out.runtime_safety = self.runtime_safety_report()
+        return out
+
+    def snapshot(self):
+        return self.lattice.snapshot()
+
+    def copy_macroscopic_fields(self):
+        return self.lattice.fields()
+
+    def copy_gauge_pressure_field_pascals(self):
+        rho, _ = self.lattice.fields()
+        sc = self.configuration.scaling
+        return (np.float32(1.0 / 3.0) * (rho - np.float32(1.0)) * np.float32(sc.pressure_scale_pascals)).astype(np.float32)
+
+    def runtime_safety_report(self) -> dict:
+        r = self.lattice.safety()
+        return {"maximum_mach": r.metrics[0], "minimum_clearance_meters": r.metrics[1],
+                "first_violation_step": (r.event[1] << 32) | r.event[0] if r.event[2] else None,
+                "flags": int(r.event[2]), "passed": r.event[2] == 0}
+
+    def save_checkpoint(self) -> bytes:
+        return self.lattice.save_state()
+
+    def restore_checkpoint(self, data: bytes):
+        self.lattice.restore_state(data)
+        self.step_index, self.time_seconds = self.lattice.step_index()
+
+    def close(self):
+        self.lattice.close()

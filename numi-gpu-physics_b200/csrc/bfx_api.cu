@@ -1,0 +1,1027 @@
+// C-ABI runtime of the bfx library: owns the device buffers of one
+// simulation, encodes the per-step kernel sequence on one CUDA stream, and
+// implements the BirdFlowSimulation surface (Sources/BirdFlowMetal/
+// BirdFlowSimulation.swift) behind plain-C entry points (include/bfx.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/bfx.h"
+#include "bfx_internal.h"
+
+using namespace bfx;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+size_t storage_bytes(int storage) {
+    switch (storage) {
+    case BFX_STORAGE_F16_DEVIATION:
+    case BFX_STORAGE_BF16_DEVIATION: return 2;
+    case BFX_STORAGE_F64: return 8;
+    default: return 4;
+    }
+}
+
+uint64_t fnv1a(const void* data, size_t n, uint64_t h = 1469598103934665603ull) {
+    const unsigned char* p = (const unsigned char*)data;
+    for (size_t i = 0; i < n; ++i) {
+        h ^= p[i];
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+}  // namespace
+
+struct bfx_sim {
+    bfx_config cfg{};
+    bfx_bird bird{};
+    bool has_bird = false;
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    GridDesc g{};
+    FluidParams fp{};
+    BoxDesc box{};
+    size_t elem = 4;
+    void* pops = nullptr;
+    void* spill = nullptr;
+    void* ghost = nullptr;
+    uint8_t* mask[2] = {nullptr, nullptr};
+    int cur = 0;
+    float4* wall = nullptr;
+    float* density = nullptr;
+    float4* velocity = nullptr;
+    DeviceState* dstate = nullptr;
+    bfx_bird* dbird = nullptr;
+    // mesh
+    float* mesh_local = nullptr;
+    uint8_t* mesh_segment = nullptr;
+    uint32_t* mesh_tris = nullptr;
+    uint8_t* mesh_tri_part = nullptr;
+    float4* mesh_pos = nullptr;
+    float4* mesh_vel = nullptr;
+    unsigned long long* keys = nullptr;
+    uint32_t nverts = 0, ntris = 0;
+    // links and reductions
+    uint32_t* link_cell = nullptr;
+    uint32_t* link_meta = nullptr;
+    float* link_q = nullptr;
+    uint32_t link_capacity = 0;
+    uint32_t* block_counts = nullptr;
+    uint32_t* block_offsets = nullptr;
+    int box_blocks = 0;
+    double* topo_partials = nullptr;
+    double* link_partials = nullptr;
+    int apply_blocks = 0;
+    double* mm_partials = nullptr;
+    double* mm_result = nullptr;
+    int mm_blocks = 0;
+    float* scratch_f32 = nullptr;  // canonical read-out staging (lazily)
+    bfx_run_sample* dsamples = nullptr;
+    size_t dsamples_cap = 0;
+    // state
+    int rep_s = 0;
+    uint64_t step = 0;
+    bool invalid = false;
+    bool fields_valid = false;
+    std::string err;
+    uint64_t launches = 0;
+    uint64_t device_bytes = 0;
+    // kernel timing
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_start, ev_stop;
+    size_t ev_used = 0;
+    double timing_ms = 0.0;
+    uint64_t timing_launches = 0;
+    std::vector<void*> allocations;
+    cudaEvent_t region[2] = {nullptr, nullptr};
+
+    bool geometry() const { return cfg.geometry != BFX_GEOMETRY_NONE; }
+    bool moving() const { return geometry() && !cfg.static_geometry; }
+};
+
+namespace {
+
+int fail(bfx_sim* s, int code, const std::string& msg) {
+    if (s) {
+        s->err = msg;
+        if (code == BFX_ERR_KERNEL || code == BFX_ERR_SAFETY) s->invalid = true;
+    } else {
+        g_create_error = msg;
+    }
+    return code;
+}
+
+int cuda_fail(bfx_sim* s, cudaError_t e, const char* what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    if (s) {
+        s->err = m;
+        s->invalid = true;
+    } else {
+        g_create_error = m;
+    }
+    return e == cudaErrorMemoryAllocation ? BFX_ERR_ALLOCATION : BFX_ERR_KERNEL;
+}
+
+template <class T>
+cudaError_t dalloc(bfx_sim* s, T** p, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc((void**)p, bytes);
+    if (e == cudaSuccess) {
+        s->allocations.push_back((void*)*p);
+        s->device_bytes += bytes;
+        cudaMemsetAsync(*p, 0, bytes, s->stream);
+    }
+    return e;
+}
+
+FluidBuffers fluid_buffers(bfx_sim* s, uint8_t* mask) {
+    FluidBuffers b;
+    b.pops = s->pops;
+    b.spill = s->spill;
+    b.ghost = s->ghost;
+    b.mask = mask;
+    b.wall = s->wall;
+    b.density = s->density;
+    b.velocity = s->velocity;
+    b.state = s->dstate;
+    return b;
+}
+
+GeomBuffers geom_buffers(bfx_sim* s, uint8_t* mprev, uint8_t* mnext) {
+    GeomBuffers b;
+    b.bird = s->dbird;
+    b.mask_prev = mprev;
+    b.mask_next = mnext;
+    b.wall = s->wall;
+    b.mesh_local = s->mesh_local;
+    b.mesh_segment = s->mesh_segment;
+    b.mesh_tris = s->mesh_tris;
+    b.mesh_tri_part = s->mesh_tri_part;
+    b.mesh_pos = s->mesh_pos;
+    b.mesh_vel = s->mesh_vel;
+    b.keys = s->keys;
+    b.nverts = s->nverts;
+    b.ntris = s->ntris;
+    b.half_thickness = s->cfg.mesh_half_thickness;
+    b.link_cell = s->link_cell;
+    b.link_meta = s->link_meta;
+    b.link_q = s->link_q;
+    b.link_capacity = s->link_capacity;
+    b.block_counts = s->block_counts;
+    b.block_offsets = s->block_offsets;
+    b.box_blocks = s->box_blocks;
+    b.topo_partials = s->topo_partials;
+    b.link_partials = s->link_partials;
+    b.apply_blocks = s->apply_blocks;
+    b.state = s->dstate;
+    return b;
+}
+
+// Classification + link build for the geometry at the current state.
+void encode_geometry_build(bfx_sim* s, int init, uint8_t* mprev, uint8_t* mnext) {
+    GeomBuffers gb = geom_buffers(s, mprev, mnext);
+    launch_prepare(s->cfg.geometry, s->cfg.time_step, s->g, s->fp, s->box, gb, init, s->stream);
+    launch_classify(s->cfg.geometry, init ? 0 : 1, s->g, s->fp, s->box, gb, s->stream);
+    s->launches += 1 + (s->cfg.geometry == BFX_GEOMETRY_MESH ? 4 : 1);
+}
+
+void encode_links(bfx_sim* s, uint8_t* mprev, uint8_t* mnext) {
+    GeomBuffers gb = geom_buffers(s, mprev, mnext);
+    launch_boundary_scan(s->cfg.storage, s->rep_s, s->g, s->fp, s->box, gb, fluid_buffers(s, mnext), s->stream);
+    launch_links_emit(s->cfg.geometry, s->cfg.link_rule, s->g, s->fp, s->box, gb, s->stream);
+    s->launches += 3;
+}
+
+void timing_begin(bfx_sim* s) {
+    if (!s->timing) return;
+    if (s->ev_used >= s->ev_start.size()) {
+        cudaEvent_t a, b;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        s->ev_start.push_back(a);
+        s->ev_stop.push_back(b);
+    }
+    cudaEventRecord(s->ev_start[s->ev_used], s->stream);
+}
+void timing_end(bfx_sim* s) {
+    if (!s->timing) return;
+    cudaEventRecord(s->ev_stop[s->ev_used], s->stream);
+    ++s->ev_used;
+}
+void timing_collect(bfx_sim* s) {
+    for (size_t i = 0; i < s->ev_used; ++i) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, s->ev_start[i], s->ev_stop[i]) == cudaSuccess) {
+            s->timing_ms += ms;
+            s->timing_launches += 1;
+        }
+    }
+    s->ev_used = 0;
+}
+
+// One time step (BirdFlowSimulation.encodeBatch body, BirdFlowSimulation.swift:1374-1437).
+void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint64_t sample_index) {
+    uint8_t* mprev = s->mask[s->cur];
+    uint8_t* mnext = s->moving() ? s->mask[s->cur ^ 1] : s->mask[s->cur];
+    if (s->moving()) {
+        encode_geometry_build(s, 0, mprev, mnext);
+    }
+    FluidBuffers fb = fluid_buffers(s, s->geometry() ? mnext : nullptr);
+    if (s->fp.any_outflow) {
+        launch_ghost(s->cfg.storage, s->rep_s, s->g, s->fp, fb, s->stream);
+        s->launches += 1;
+    }
+    if (s->geometry()) {
+        GeomBuffers gb = geom_buffers(s, mprev, mnext);
+        if (s->moving()) encode_links(s, mprev, mnext);
+        launch_links_apply(s->cfg.storage, s->rep_s, s->g, s->fp, gb, fb, s->stream);
+        launch_reduce_loads(gb, s->moving() ? 1 : 0, s->stream);
+        s->launches += 2;
+    }
+    timing_begin(s);
+    launch_bulk(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, capture, s->stream);
+    timing_end(s);
+    s->launches += 1;
+    GeomBuffers gb = geom_buffers(s, mprev, mnext);
+    launch_integrate(s->g, s->fp, gb, s->cfg.gravity[0], s->cfg.gravity[1], s->cfg.gravity[2],
+                     (int)s->cfg.body_substeps, s->cfg.free_flight && s->has_bird ? 1 : 0, s->stream);
+    s->launches += 1;
+    if (sample_slot_base) {
+        launch_record_sample(gb, sample_slot_base, sample_index, s->cfg.time_step, s->stream);
+        s->launches += 1;
+    }
+    s->rep_s ^= 1;
+    if (s->moving()) s->cur ^= 1;
+}
+
+int sync_check(bfx_sim* s, const char* what) {
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(s, e, what);
+    timing_collect(s);
+    return BFX_OK;
+}
+
+int validate_config(const bfx_config* c, const bfx_bird* bird, const bfx_mesh* mesh) {
+    if (c->nx < 4 || c->ny < 4 || c->nz < 4) return fail(nullptr, BFX_ERR_INVALID_CONFIG, "each grid dimension must be at least 4 cells");
+    uint64_t n = (uint64_t)c->nx * c->ny * c->nz;
+    if (n > 0xFFFFFFFFull) return fail(nullptr, BFX_ERR_INVALID_CONFIG, "the total cell count must fit in 32 bits");
+    for (int a = 0; a < 3; ++a) {
+        int lo = c->face_bc[2 * a], hi = c->face_bc[2 * a + 1];
+        if (lo < 0 || lo > 3 || hi < 0 || hi > 3)
+            return fail(nullptr, BFX_ERR_INVALID_CONFIG, "face boundary rule out of range");
+        if ((lo == BFX_BC_PERIODIC) != (hi == BFX_BC_PERIODIC))
+            return fail(nullptr, BFX_ERR_INVALID_CONFIG, "a periodic axis needs both faces periodic");
+    }
+    if (c->collision < 0 || c->collision > 3) return fail(nullptr, BFX_ERR_INVALID_CONFIG, "unknown collision operator");
+    if (c->storage < 0 || c->storage > 3) return fail(nullptr, BFX_ERR_INVALID_CONFIG, "unknown storage format");
+    if (c->geometry < 0 || c->geometry > 3) return fail(nullptr, BFX_ERR_INVALID_CONFIG, "unknown geometry kind");
+    if (c->wall_rule < 0 || c->wall_rule > 1) return fail(nullptr, BFX_ERR_INVALID_CONFIG, "unknown wall rule");
+    if (c->force_estimator < 0 || c->force_estimator > 6)
+        return fail(nullptr, BFX_ERR_INVALID_CONFIG, "force estimator must be 0...6");
+    if (c->load_component < 0 || c->load_component > 2)
+        return fail(nullptr, BFX_ERR_INVALID_CONFIG, "load component must be 0, 1 or 2");
+    if (c->selected_part < 0 || c->selected_part > 63) return fail(nullptr, BFX_ERR_INVALID_CONFIG, "selected part out of range");
+    if (!(c->omega_plus > 0.0f && c->omega_plus < 2.0f) || !(c->omega_minus > 0.0f && c->omega_minus < 2.0f))
+        return fail(nullptr, BFX_ERR_INVALID_CONFIG, "relaxation rates must lie in (0, 2)");
+    if (!(c->cell_size > 0.0f) || !(c->time_step > 0.0f))
+        return fail(nullptr, BFX_ERR_INVALID_CONFIG, "cell size and time step must be positive");
+    if (!(c->sponge_strength >= 0.0f && c->sponge_strength <= 1.0f))
+        return fail(nullptr, BFX_ERR_INVALID_CONFIG, "sponge strength must be in [0, 1]");
+    if (c->body_substeps < 1 || c->body_substeps > 64)
+        return fail(nullptr, BFX_ERR_INVALID_CONFIG, "bodySubsteps must be in 1...64");
+    float far2 = c->far_field[0] * c->far_field[0] + c->far_field[1] * c->far_field[1] + c->far_field[2] * c->far_field[2];
+    if (std::sqrt(far2) / std::sqrt(1.0f / 3.0f) > 0.15f)
+        return fail(nullptr, BFX_ERR_INVALID_CONFIG, "far-field lattice Mach number above 0.15");
+    if (c->geometry != BFX_GEOMETRY_NONE && bird == nullptr)
+        return fail(nullptr, BFX_ERR_INVALID_CONFIG, "a geometry needs bird parameters");
+    if (c->geometry == BFX_GEOMETRY_MESH && (mesh == nullptr || mesh->triangle_count == 0 || mesh->vertex_count == 0))
+        return fail(nullptr, BFX_ERR_INVALID_CONFIG, "mesh geometry needs a non-empty mesh");
+    if (c->geometry == BFX_GEOMETRY_BIRD && c->wall_rule == BFX_WALL_INTERPOLATED)
+        return fail(nullptr, BFX_ERR_INVALID_CONFIG, "the analytic bird provides halfway links only");
+    if (c->geometry == BFX_GEOMETRY_MESH && !(c->mesh_half_thickness > 0.0f))
+        return fail(nullptr, BFX_ERR_INVALID_CONFIG, "mesh half thickness must be positive");
+    if (c->free_flight && bird == nullptr) return fail(nullptr, BFX_ERR_INVALID_CONFIG, "free flight needs bird parameters");
+    if (c->free_flight && c->static_geometry)
+        return fail(nullptr, BFX_ERR_INVALID_CONFIG, "a free-flying body cannot be static geometry");
+    if (mesh && mesh->triangles) {
+        for (uint32_t i = 0; i < 3 * mesh->triangle_count; ++i)
+            if (mesh->triangles[i] >= mesh->vertex_count)
+                return fail(nullptr, BFX_ERR_INVALID_CONFIG, "triangle index out of range");
+        for (uint32_t i = 0; i < mesh->vertex_count; ++i)
+            if (mesh->vertex_segment[i] > 2) return fail(nullptr, BFX_ERR_INVALID_CONFIG, "vertex segment must be 0, 1 or 2");
+        for (uint32_t i = 0; i < mesh->triangle_count; ++i)
+            if (mesh->triangle_part[i] == 0 || mesh->triangle_part[i] > 63)
+                return fail(nullptr, BFX_ERR_INVALID_CONFIG, "triangle part must be 1...63");
+    }
+    return BFX_OK;
+}
+
+// Conservative radius (m) of everything the geometry kernels may mark solid,
+// measured from the body origin.
+float geometry_radius(const bfx_config* c, const bfx_bird* b, const bfx_mesh* m) {
+    const float* br = b->body_radii_mass.v;
+    const float* tg = b->tail_geometry.v;
+    const float* w0 = b->wing_geometry0.v;
+    const float* w1 = b->wing_geometry1.v;
+    float body = std::sqrt(br[0] * br[0] + br[1] * br[1] + br[2] * br[2]);
+    if (c->geometry == BFX_GEOMETRY_ELLIPSOID) return std::max(br[0], std::max(br[1], br[2])) + 2.0f * c->cell_size;
+    float root = std::sqrt(w1[1] * w1[1] + w1[2] * w1[2] + w1[3] * w1[3]);
+    if (c->geometry == BFX_GEOMETRY_BIRD) {
+        float tx = br[0] + tg[0], ty = std::max(br[1], tg[1]), tz = br[2] + 0.5f * tg[2];
+        float tail = std::sqrt(tx * tx + ty * ty + tz * tz);
+        float wing = root + w0[0] + std::fabs(w1[0]) + 0.5f * std::max(w0[1], w0[2]) + 0.5f * w0[3];
+        return std::max(body, std::max(tail, wing)) + 2.0f * c->cell_size;
+    }
+    float r = 0.0f;
+    for (uint32_t i = 0; i < m->vertex_count; ++i) {
+        const float* l = m->local_vertices + 3 * i;
+        float d = std::sqrt(l[0] * l[0] + l[1] * l[1] + l[2] * l[2]);
+        if (m->vertex_segment[i] != 0) d += root;
+        r = std::max(r, d);
+    }
+    return r + c->mesh_half_thickness + 2.0f * c->cell_size;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* bfx_version(void) { return "bfx 0.1.0 (sm_100a)"; }
+int bfx_abi_version(void) { return BFX_ABI_VERSION; }
+
+int bfx_device_count(int* count) {
+    if (!count) return BFX_ERR_INVALID_ARGUMENT;
+    int c = 0;
+    cudaError_t e = cudaGetDeviceCount(&c);
+    *count = e == cudaSuccess ? c : 0;
+    return e == cudaSuccess ? BFX_OK : BFX_ERR_DEVICE_UNAVAILABLE;
+}
+
+void bfx_destroy(bfx_sim* s) {
+    if (!s) return;
+    if (s->stream) {
+        cudaSetDevice(s->device);
+        cudaStreamSynchronize(s->stream);
+    }
+    for (void* p : s->allocations) cudaFree(p);
+    for (auto e : s->ev_start) cudaEventDestroy(e);
+    for (auto e : s->ev_stop) cudaEventDestroy(e);
+    for (auto e : s->region)
+        if (e) cudaEventDestroy(e);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_state* body, const bfx_mesh* mesh,
+               bfx_sim** out) {
+    if (!config || !out) return fail(nullptr, BFX_ERR_INVALID_ARGUMENT, "config and out must not be null");
+    *out = nullptr;
+    int rc = validate_config(config, bird, mesh);
+    if (rc != BFX_OK) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(nullptr, BFX_ERR_DEVICE_UNAVAILABLE, "no CUDA device is available");
+    if (config->device < 0 || config->device >= ndev)
+        return fail(nullptr, BFX_ERR_DEVICE_UNAVAILABLE, "CUDA device ordinal out of range");
+
+    bfx_sim* s = new bfx_sim();
+    s->cfg = *config;
+    s->device = config->device;
+    cudaSetDevice(s->device);
+    cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, s->device);
+    cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        bfx_destroy(s);
+        return cuda_fail(nullptr, e, "stream creation");
+    }
+    if (bird) {
+        s->bird = *bird;
+        s->has_bird = true;
+    }
+    const bfx_config& c = s->cfg;
+    // grid
+    GridDesc& g = s->g;
+    g.nx = (int)c.nx;
+    g.ny = (int)c.ny;
+    g.nz = (int)c.nz;
+    g.per_x = c.face_bc[0] == BFX_BC_PERIODIC;
+    g.per_y = c.face_bc[2] == BFX_BC_PERIODIC;
+    g.per_z = c.face_bc[4] == BFX_BC_PERIODIC;
+    g.n = (int64_t)g.nx * g.ny * g.nz;
+    g.nxy = (int64_t)g.nx * g.ny;
+    int64_t face_cells[6] = {(int64_t)g.ny * g.nz, (int64_t)g.ny * g.nz, (int64_t)g.nx * g.nz,
+                             (int64_t)g.nx * g.nz, (int64_t)g.nx * g.ny, (int64_t)g.nx * g.ny};
+    int64_t off = 0;
+    for (int f = 0; f < 6; ++f) {
+        g.spill_off[f] = off;
+        g.ghost_off[f] = off;
+        off += 5 * face_cells[f];
+    }
+    g.spill_total = off;
+    // fluid parameters
+    FluidParams& fp = s->fp;
+    for (int k = 0; k < 3; ++k) fp.origin[k] = c.origin[k];
+    fp.dx = c.cell_size;
+    fp.dt = c.time_step;
+    fp.v2l = c.velocity_to_lattice;
+    fp.f2p = c.force_to_physical;
+    fp.omega_p = c.omega_plus;
+    fp.omega_m = c.omega_minus;
+    fp.sponge_strength = c.sponge_strength;
+    fp.sponge_width = c.sponge_width;
+    for (int k = 0; k < 4; ++k) fp.far[k] = c.far_field[k];
+    fp.any_outflow = 0;
+    for (int f = 0; f < 6; ++f) {
+        fp.face_bc[f] = c.face_bc[f];
+        for (int k = 0; k < 3; ++k) fp.face_u[f][k] = c.face_velocity[f][k];
+        if (c.face_bc[f] == BFX_BC_OUTFLOW) fp.any_outflow = 1;
+    }
+    fp.collision = c.collision;
+    fp.interpolated = c.wall_rule == BFX_WALL_INTERPOLATED;
+    fp.load_component = c.load_component;
+    fp.force_mode = c.force_estimator;
+    fp.selected_part = c.selected_part;
+    fp.local_density = c.moving_wall_local_density ? 1 : 0;
+    fp.accumulate = c.accumulate_loads ? 1 : 0;
+    fp.has_sponge = c.sponge_strength > 0.0f ? 1 : 0;
+
+    s->elem = storage_bytes(c.storage);
+    size_t pop_bytes = (size_t)19 * (size_t)g.n * s->elem;
+#define BFX_ALLOC(ptr, bytes)                                   \
+    do {                                                        \
+        cudaError_t ee = dalloc(s, &(ptr), (bytes));            \
+        if (ee != cudaSuccess) {                                \
+            int code = cuda_fail(nullptr, ee, "device allocation"); \
+            bfx_destroy(s);                                     \
+            return code;                                        \
+        }                                                       \
+    } while (0)
+    BFX_ALLOC(s->pops, pop_bytes);
+    BFX_ALLOC(s->spill, (size_t)g.spill_total * s->elem);
+    if (fp.any_outflow) BFX_ALLOC(s->ghost, (size_t)g.spill_total * s->elem);
+    BFX_ALLOC(s->density, (size_t)g.n * sizeof(float));
+    BFX_ALLOC(s->velocity, (size_t)g.n * sizeof(float4));
+    BFX_ALLOC(s->dstate, sizeof(DeviceState));
+    s->mm_blocks = 4 * s->sm_count;
+    BFX_ALLOC(s->mm_partials, (size_t)s->mm_blocks * 4 * sizeof(double));
+    BFX_ALLOC(s->mm_result, 4 * sizeof(double));
+
+    // host-side initial device state
+    DeviceState hs;
+    std::memset(&hs, 0, sizeof(hs));
+    hs.body[6] = 1.0;
+    if (body) {
+        for (int k = 0; k < 3; ++k) hs.body[k] = body->position[k];
+        for (int k = 0; k < 4; ++k) hs.body[3 + k] = body->orientation[k];
+        for (int k = 0; k < 3; ++k) hs.body[7 + k] = body->velocity[k];
+        for (int k = 0; k < 3; ++k) hs.body[10 + k] = body->omega_body[k];
+    }
+    hs.safety_metrics[0] = 0.0f;
+    hs.safety_metrics[1] = INFINITY;
+
+    if (s->geometry()) {
+        BFX_ALLOC(s->mask[0], (size_t)g.n);
+        BFX_ALLOC(s->mask[1], (size_t)g.n);
+        BFX_ALLOC(s->wall, (size_t)g.n * sizeof(float4));
+        BFX_ALLOC(s->dbird, sizeof(bfx_bird));
+        cudaMemcpyAsync(s->dbird, &s->bird, sizeof(bfx_bird), cudaMemcpyHostToDevice, s->stream);
+        // geometry box
+        float r = geometry_radius(&c, &s->bird, mesh);
+        int half = (int)std::ceil(r / c.cell_size) + 4;
+        int ext = 2 * half + 2;
+        s->box.sx = std::min(ext, g.nx);
+        s->box.sy = std::min(ext, g.ny);
+        s->box.sz = std::min(ext, g.nz);
+        s->box.cells = (int64_t)s->box.sx * s->box.sy * s->box.sz;
+        s->box_blocks = box_block_count(s->box);
+        BFX_ALLOC(s->block_counts, (size_t)s->box_blocks * sizeof(uint32_t));
+        BFX_ALLOC(s->block_offsets, (size_t)s->box_blocks * sizeof(uint32_t));
+        BFX_ALLOC(s->topo_partials, (size_t)s->box_blocks * 8 * sizeof(double));
+        s->apply_blocks = 4 * s->sm_count;
+        BFX_ALLOC(s->link_partials, (size_t)s->apply_blocks * 8 * sizeof(double));
+        uint64_t cap = c.link_capacity ? c.link_capacity
+                                       : std::max<uint64_t>(1u << 18, std::min<uint64_t>((uint64_t)s->box.cells, 1u << 24));
+        s->link_capacity = (uint32_t)cap;
+        BFX_ALLOC(s->link_cell, cap * sizeof(uint32_t));
+        BFX_ALLOC(s->link_meta, cap * sizeof(uint32_t));
+        BFX_ALLOC(s->link_q, cap * sizeof(float));
+        if (c.geometry == BFX_GEOMETRY_MESH) {
+            s->nverts = mesh->vertex_count;
+            s->ntris = mesh->triangle_count;
+            BFX_ALLOC(s->mesh_local, (size_t)s->nverts * 3 * sizeof(float));
+            BFX_ALLOC(s->mesh_segment, (size_t)s->nverts);
+            BFX_ALLOC(s->mesh_tris, (size_t)s->ntris * 3 * sizeof(uint32_t));
+            BFX_ALLOC(s->mesh_tri_part, (size_t)s->ntris);
+            BFX_ALLOC(s->mesh_pos, (size_t)s->nverts * sizeof(float4));
+            BFX_ALLOC(s->mesh_vel, (size_t)s->nverts * sizeof(float4));
+            BFX_ALLOC(s->keys, (size_t)s->box.cells * sizeof(unsigned long long));
+            cudaMemcpyAsync(s->mesh_local, mesh->local_vertices, (size_t)s->nverts * 3 * sizeof(float),
+                            cudaMemcpyHostToDevice, s->stream);
+            cudaMemcpyAsync(s->mesh_segment, mesh->vertex_segment, s->nverts, cudaMemcpyHostToDevice, s->stream);
+            cudaMemcpyAsync(s->mesh_tris, mesh->triangles, (size_t)s->ntris * 3 * sizeof(uint32_t),
+                            cudaMemcpyHostToDevice, s->stream);
+            cudaMemcpyAsync(s->mesh_tri_part, mesh->triangle_part, s->ntris, cudaMemcpyHostToDevice, s->stream);
+        }
+    }
+#undef BFX_ALLOC
+    cudaMemcpyAsync(s->dstate, &hs, sizeof(hs), cudaMemcpyHostToDevice, s->stream);
+
+    // initial geometry (BirdFlowSimulation.encodeInitialization, BirdFlowSimulation.swift:1300-1357)
+    if (s->geometry()) {
+        if (c.geometry == BFX_GEOMETRY_MESH) {
+            launch_fill_wall(s->wall, g.n, 16.0f, s->stream);
+            s->launches += 1;
+        }
+        encode_geometry_build(s, 1, s->mask[1], s->mask[0]);
+    }
+    launch_init(c.storage, c.init, c.init_amplitude, g, fp, fluid_buffers(s, s->geometry() ? s->mask[0] : nullptr),
+                s->stream);
+    s->launches += 1;
+    if (s->geometry() && !s->moving()) encode_links(s, s->mask[0], s->mask[0]);
+    s->rep_s = 0;
+    s->cur = 0;
+    s->fields_valid = true;
+    int sc = sync_check(s, "initialisation");
+    if (sc != BFX_OK) {
+        g_create_error = s->err;
+        bfx_destroy(s);
+        return sc;
+    }
+    if (s->geometry() && !s->moving()) {
+        DeviceState st;
+        cudaMemcpy(&st, s->dstate, sizeof(st), cudaMemcpyDeviceToHost);
+        if (st.link_overflow) {
+            g_create_error = "the cut-link list exceeds its capacity; raise link_capacity";
+            bfx_destroy(s);
+            return BFX_ERR_CAPACITY;
+        }
+    }
+    *out = s;
+    return BFX_OK;
+}
+
+#define BFX_GUARD(s)                                             \
+    do {                                                         \
+        if (!(s)) return BFX_ERR_INVALID_ARGUMENT;               \
+        if ((s)->invalid) return BFX_ERR_INVALIDATED;            \
+        cudaSetDevice((s)->device);                              \
+    } while (0)
+
+int bfx_advance(bfx_sim* s, uint64_t steps, uint32_t batch_size, uint32_t flags, bfx_run_sample* samples,
+                size_t sample_capacity, bfx_advance_result* result) {
+    BFX_GUARD(s);
+    if (batch_size == 0) return fail(s, BFX_ERR_INVALID_ADVANCE, "batch size must be positive");
+    const bool record = (flags & BFX_ADVANCE_RECORD_SAMPLES) != 0;
+    const bool capture = (flags & BFX_ADVANCE_CAPTURE_FIELDS) != 0;
+    if (record && (samples == nullptr || sample_capacity < steps))
+        return fail(s, BFX_ERR_CAPACITY, "run-sample buffer smaller than the step count");
+    if (record && steps > s->dsamples_cap) {
+        void* p = nullptr;
+        cudaError_t e = cudaMalloc(&p, steps * sizeof(bfx_run_sample));
+        if (e != cudaSuccess) return cuda_fail(s, e, "run-sample allocation");
+        if (s->dsamples) {
+            cudaFree(s->dsamples);
+            s->allocations.erase(std::find(s->allocations.begin(), s->allocations.end(), (void*)s->dsamples));
+        }
+        s->dsamples = (bfx_run_sample*)p;
+        s->dsamples_cap = steps;
+        s->allocations.push_back(p);
+    }
+    uint64_t done = 0;
+    while (done < steps) {
+        uint64_t count = std::min<uint64_t>(batch_size, steps - done);
+        for (uint64_t k = 0; k < count; ++k) {
+            bool last = done + k + 1 == steps;
+            encode_step(s, capture && last ? 1 : 0, record ? s->dsamples : nullptr, done + k);
+        }
+        cudaError_t le = cudaGetLastError();
+        if (le != cudaSuccess) return cuda_fail(s, le, "kernel launch");
+        done += count;
+        if (s->cfg.free_flight || s->moving() || done == steps) {
+            int rc = sync_check(s, "advance");
+            if (rc != BFX_OK) return rc;
+            DeviceState st;
+            cudaMemcpy(&st, s->dstate, sizeof(st), cudaMemcpyDeviceToHost);
+            s->step = st.step;
+            if (st.link_overflow) return fail(s, BFX_ERR_KERNEL, "the cut-link list exceeded its capacity; raise link_capacity");
+            if (s->cfg.free_flight && st.safety_event[2] != 0) {
+                if (result) {
+                    result->steps_done = done;
+                    result->safety_passed = 0;
+                    std::memcpy(result->safety.metrics, st.safety_metrics, sizeof(st.safety_metrics));
+                    std::memcpy(result->safety.event, st.safety_event, sizeof(st.safety_event));
+                }
+                return fail(s, BFX_ERR_SAFETY, "runtime safety violation (Mach, clearance or non-finite state)");
+            }
+        }
+    }
+    if (capture) s->fields_valid = true;
+    if (record && steps > 0) {
+        cudaError_t e = cudaMemcpy(samples, s->dsamples, steps * sizeof(bfx_run_sample), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return cuda_fail(s, e, "run-sample read-back");
+    }
+    if (result) {
+        DeviceState st;
+        cudaMemcpy(&st, s->dstate, sizeof(st), cudaMemcpyDeviceToHost);
+        result->steps_done = steps;
+        result->field_frame_published = capture ? 1 : 0;
+        result->safety_passed = st.safety_event[2] == 0 ? 1 : 0;
+        std::memcpy(result->safety.metrics, st.safety_metrics, sizeof(st.safety_metrics));
+        std::memcpy(result->safety.event, st.safety_event, sizeof(st.safety_event));
+    }
+    return BFX_OK;
+}
+
+static int read_state(bfx_sim* s, DeviceState* st) {
+    int rc = sync_check(s, "read-back");
+    if (rc != BFX_OK) return rc;
+    cudaError_t e = cudaMemcpy(st, s->dstate, sizeof(*st), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(s, e, "state read-back");
+    return BFX_OK;
+}
+
+static void loads_from_state(const bfx_sim* s, const DeviceState& st, bfx_loads* out) {
+    std::memset(out, 0, sizeof(*out));
+    for (int k = 0; k < 3; ++k) {
+        out->force_lattice[k] = st.loads_lattice[k];
+        out->force[k] = st.loads_lattice[k] * (double)s->fp.f2p;
+        out->torque[k] = st.loads_torque[k];
+    }
+    out->limiter_activations = st.limiter_count;
+    float r;
+    std::memcpy(&r, &st.limiter_max_bits, 4);
+    out->max_restriction = r;
+    out->link_count = st.link_count;
+    out->covered_count = st.covered_count;
+    out->uncovered_count = st.uncovered_count;
+}
+
+int bfx_last_loads(bfx_sim* s, bfx_loads* out) {
+    BFX_GUARD(s);
+    if (!out) return BFX_ERR_INVALID_ARGUMENT;
+    DeviceState st;
+    int rc = read_state(s, &st);
+    if (rc != BFX_OK) return rc;
+    loads_from_state(s, st, out);
+    return BFX_OK;
+}
+
+int bfx_snapshot(bfx_sim* s, bfx_snapshot_data* out) {
+    BFX_GUARD(s);
+    if (!out) return BFX_ERR_INVALID_ARGUMENT;
+    DeviceState st;
+    int rc = read_state(s, &st);
+    if (rc != BFX_OK) return rc;
+    out->step = st.step;
+    out->time = (double)(float)((double)st.step * (double)s->cfg.time_step);
+    for (int k = 0; k < 3; ++k) out->body.position[k] = st.body[k];
+    for (int k = 0; k < 4; ++k) out->body.orientation[k] = st.body[3 + k];
+    for (int k = 0; k < 3; ++k) out->body.velocity[k] = st.body[7 + k];
+    for (int k = 0; k < 3; ++k) out->body.omega_body[k] = st.body[10 + k];
+    loads_from_state(s, st, &out->loads);
+    return BFX_OK;
+}
+
+int bfx_copy_fields(bfx_sim* s, float* density, float* velocity_xyz, size_t cells) {
+    BFX_GUARD(s);
+    if (cells < (size_t)s->g.n) return fail(s, BFX_ERR_CAPACITY, "field buffers smaller than the lattice");
+    int rc = sync_check(s, "fields");
+    if (rc != BFX_OK) return rc;
+    if (density) cudaMemcpy(density, s->density, (size_t)s->g.n * sizeof(float), cudaMemcpyDeviceToHost);
+    if (velocity_xyz) {
+        std::vector<float> v4((size_t)s->g.n * 4);
+        cudaMemcpy(v4.data(), s->velocity, v4.size() * sizeof(float), cudaMemcpyDeviceToHost);
+        for (int64_t i = 0; i < s->g.n; ++i) {
+            velocity_xyz[3 * i] = v4[4 * i];
+            velocity_xyz[3 * i + 1] = v4[4 * i + 1];
+            velocity_xyz[3 * i + 2] = v4[4 * i + 2];
+        }
+    }
+    return BFX_OK;
+}
+
+int bfx_copy_gauge_pressure(bfx_sim* s, float pressure_scale_pascals, float* out, size_t cells) {
+    BFX_GUARD(s);
+    if (!out || cells < (size_t)s->g.n) return fail(s, BFX_ERR_CAPACITY, "pressure buffer smaller than the lattice");
+    int rc = bfx_copy_fields(s, out, nullptr, cells);
+    if (rc != BFX_OK) return rc;
+    // LatticeScaling.gaugePressurePascals (SimulationConfiguration.swift:189-196)
+    for (int64_t i = 0; i < s->g.n; ++i) out[i] = (1.0f / 3.0f) * (out[i] - 1.0f) * pressure_scale_pascals;
+    return BFX_OK;
+}
+
+int bfx_runtime_safety(bfx_sim* s, bfx_safety_record* out) {
+    BFX_GUARD(s);
+    if (!out) return BFX_ERR_INVALID_ARGUMENT;
+    DeviceState st;
+    int rc = read_state(s, &st);
+    if (rc != BFX_OK) return rc;
+    std::memcpy(out->metrics, st.safety_metrics, sizeof(out->metrics));
+    std::memcpy(out->event, st.safety_event, sizeof(out->event));
+    return BFX_OK;
+}
+
+static int ensure_scratch(bfx_sim* s) {
+    if (s->scratch_f32) return BFX_OK;
+    cudaError_t e = cudaMalloc(&s->scratch_f32, (size_t)19 * s->g.n * sizeof(float));
+    if (e != cudaSuccess) return cuda_fail(s, e, "read-out staging allocation");
+    s->allocations.push_back(s->scratch_f32);
+    return BFX_OK;
+}
+
+int bfx_copy_populations(bfx_sim* s, float* out, size_t count) {
+    BFX_GUARD(s);
+    if (!out || count < (size_t)19 * s->g.n) return fail(s, BFX_ERR_CAPACITY, "population buffer smaller than 19 * cells");
+    int rc = ensure_scratch(s);
+    if (rc != BFX_OK) return rc;
+    launch_readout(s->cfg.storage, s->rep_s, s->g, fluid_buffers(s, nullptr), s->scratch_f32, s->stream);
+    s->launches += 1;
+    rc = sync_check(s, "population read-out");
+    if (rc != BFX_OK) return rc;
+    cudaError_t e = cudaMemcpy(out, s->scratch_f32, (size_t)19 * s->g.n * sizeof(float), cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? BFX_OK : cuda_fail(s, e, "population copy");
+}
+
+int bfx_set_populations(bfx_sim* s, const float* in, size_t count) {
+    BFX_GUARD(s);
+    if (!in || count < (size_t)19 * s->g.n) return fail(s, BFX_ERR_CAPACITY, "population buffer smaller than 19 * cells");
+    int rc = ensure_scratch(s);
+    if (rc != BFX_OK) return rc;
+    cudaMemcpyAsync(s->scratch_f32, in, (size_t)19 * s->g.n * sizeof(float), cudaMemcpyHostToDevice, s->stream);
+    launch_writein(s->cfg.storage, s->rep_s, s->g, fluid_buffers(s, nullptr), s->scratch_f32, s->stream);
+    s->launches += 1;
+    return sync_check(s, "population write-in");
+}
+
+int bfx_copy_mask(bfx_sim* s, uint8_t* out, size_t cells) {
+    BFX_GUARD(s);
+    if (!out || cells < (size_t)s->g.n) return fail(s, BFX_ERR_CAPACITY, "mask buffer smaller than the lattice");
+    int rc = sync_check(s, "mask");
+    if (rc != BFX_OK) return rc;
+    if (!s->geometry()) {
+        std::memset(out, 0, (size_t)s->g.n);
+        return BFX_OK;
+    }
+    cudaMemcpy(out, s->mask[s->cur], (size_t)s->g.n, cudaMemcpyDeviceToHost);
+    for (int64_t i = 0; i < s->g.n; ++i) out[i] &= 0x3F;  // part id bits
+    return BFX_OK;
+}
+
+int bfx_copy_wall(bfx_sim* s, float* out4, size_t cells) {
+    BFX_GUARD(s);
+    if (!out4 || cells < (size_t)s->g.n) return fail(s, BFX_ERR_CAPACITY, "wall buffer smaller than the lattice");
+    int rc = sync_check(s, "wall");
+    if (rc != BFX_OK) return rc;
+    if (!s->geometry()) {
+        std::memset(out4, 0, (size_t)s->g.n * 16);
+        return BFX_OK;
+    }
+    cudaMemcpy(out4, s->wall, (size_t)s->g.n * sizeof(float4), cudaMemcpyDeviceToHost);
+    return BFX_OK;
+}
+
+int bfx_copy_links(bfx_sim* s, uint32_t* cell, uint8_t* direction, float* fraction, size_t capacity, size_t* count) {
+    BFX_GUARD(s);
+    if (!count) return BFX_ERR_INVALID_ARGUMENT;
+    DeviceState st;
+    int rc = read_state(s, &st);
+    if (rc != BFX_OK) return rc;
+    size_t n = s->geometry() ? (size_t)std::min<int64_t>(st.link_count, s->link_capacity) : 0;
+    *count = n;
+    if (!cell && !direction && !fraction) return BFX_OK;
+    if (capacity < n) return fail(s, BFX_ERR_CAPACITY, "link buffers smaller than the link count");
+    if (n == 0) return BFX_OK;
+    std::vector<uint32_t> meta(n);
+    if (cell) cudaMemcpy(cell, s->link_cell, n * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    cudaMemcpy(meta.data(), s->link_meta, n * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    if (direction)
+        for (size_t i = 0; i < n; ++i) direction[i] = (uint8_t)(meta[i] & 0xFF);
+    if (fraction) cudaMemcpy(fraction, s->link_q, n * sizeof(float), cudaMemcpyDeviceToHost);
+    return BFX_OK;
+}
+
+int bfx_fluid_mass_momentum(bfx_sim* s, double out[4]) {
+    BFX_GUARD(s);
+    if (!out) return BFX_ERR_INVALID_ARGUMENT;
+    launch_mass_momentum(s->cfg.storage, s->rep_s, s->g, fluid_buffers(s, s->geometry() ? s->mask[s->cur] : nullptr),
+                         s->mm_partials, s->mm_blocks, s->mm_result, s->stream);
+    s->launches += 2;
+    int rc = sync_check(s, "mass/momentum");
+    if (rc != BFX_OK) return rc;
+    cudaMemcpy(out, s->mm_result, 4 * sizeof(double), cudaMemcpyDeviceToHost);
+    return BFX_OK;
+}
+
+// Restart state: header, device state, populations (storage format), spill
+// planes, both masks and the wall field, followed by an FNV-1a checksum.
+struct StateHeader {
+    char magic[8];
+    uint32_t version;
+    uint32_t storage;
+    uint32_t nx, ny, nz;
+    int32_t rep_s, cur;
+    uint32_t geometry;
+    uint64_t payload;
+};
+
+static size_t state_size(const bfx_sim* s) {
+    size_t n = sizeof(StateHeader) + sizeof(DeviceState) + (size_t)19 * s->g.n * s->elem +
+               (size_t)s->g.spill_total * s->elem;
+    if (s->geometry()) n += 2 * (size_t)s->g.n + (size_t)s->g.n * sizeof(float4);
+    return n + sizeof(uint64_t);
+}
+
+int bfx_save_state(bfx_sim* s, void* buf, size_t capacity, size_t* size) {
+    BFX_GUARD(s);
+    size_t need = state_size(s);
+    if (size) *size = need;
+    if (!buf) return BFX_OK;
+    if (capacity < need) return fail(s, BFX_ERR_CAPACITY, "state buffer too small");
+    int rc = sync_check(s, "save state");
+    if (rc != BFX_OK) return rc;
+    char* p = (char*)buf;
+    StateHeader h;
+    std::memset(&h, 0, sizeof(h));
+    std::memcpy(h.magic, "BFXSTATE", 8);
+    h.version = 1;
+    h.storage = (uint32_t)s->cfg.storage;
+    h.nx = s->cfg.nx;
+    h.ny = s->cfg.ny;
+    h.nz = s->cfg.nz;
+    h.rep_s = s->rep_s;
+    h.cur = s->cur;
+    h.geometry = (uint32_t)s->cfg.geometry;
+    h.payload = need - sizeof(StateHeader) - sizeof(uint64_t);
+    std::memcpy(p, &h, sizeof(h));
+    p += sizeof(h);
+    cudaMemcpy(p, s->dstate, sizeof(DeviceState), cudaMemcpyDeviceToHost);
+    p += sizeof(DeviceState);
+    cudaMemcpy(p, s->pops, (size_t)19 * s->g.n * s->elem, cudaMemcpyDeviceToHost);
+    p += (size_t)19 * s->g.n * s->elem;
+    cudaMemcpy(p, s->spill, (size_t)s->g.spill_total * s->elem, cudaMemcpyDeviceToHost);
+    p += (size_t)s->g.spill_total * s->elem;
+    if (s->geometry()) {
+        cudaMemcpy(p, s->mask[0], (size_t)s->g.n, cudaMemcpyDeviceToHost);
+        p += s->g.n;
+        cudaMemcpy(p, s->mask[1], (size_t)s->g.n, cudaMemcpyDeviceToHost);
+        p += s->g.n;
+        cudaMemcpy(p, s->wall, (size_t)s->g.n * sizeof(float4), cudaMemcpyDeviceToHost);
+        p += (size_t)s->g.n * sizeof(float4);
+    }
+    uint64_t sum = fnv1a(buf, need - sizeof(uint64_t));
+    std::memcpy(p, &sum, sizeof(sum));
+    return sync_check(s, "save state");
+}
+
+int bfx_restore_state(bfx_sim* s, const void* buf, size_t size) {
+    BFX_GUARD(s);
+    if (!buf) return BFX_ERR_INVALID_ARGUMENT;
+    size_t need = state_size(s);
+    if (size != need) return fail(s, BFX_ERR_INVALID_ARGUMENT, "state size does not match this simulation");
+    StateHeader h;
+    std::memcpy(&h, buf, sizeof(h));
+    if (std::memcmp(h.magic, "BFXSTATE", 8) != 0 || h.version != 1 || h.storage != (uint32_t)s->cfg.storage ||
+        h.nx != s->cfg.nx || h.ny != s->cfg.ny || h.nz != s->cfg.nz || h.geometry != (uint32_t)s->cfg.geometry)
+        return fail(s, BFX_ERR_INVALID_ARGUMENT, "state header does not match this simulation");
+    uint64_t sum;
+    std::memcpy(&sum, (const char*)buf + need - sizeof(uint64_t), sizeof(sum));
+    if (sum != fnv1a(buf, need - sizeof(uint64_t))) return fail(s, BFX_ERR_INVALID_ARGUMENT, "state checksum mismatch");
+    const char* p = (const char*)buf + sizeof(h);
+    cudaMemcpy(s->dstate, p, sizeof(DeviceState), cudaMemcpyHostToDevice);
+    p += sizeof(DeviceState);
+    cudaMemcpy(s->pops, p, (size_t)19 * s->g.n * s->elem, cudaMemcpyHostToDevice);
+    p += (size_t)19 * s->g.n * s->elem;
+    cudaMemcpy(s->spill, p, (size_t)s->g.spill_total * s->elem, cudaMemcpyHostToDevice);
+    p += (size_t)s->g.spill_total * s->elem;
+    if (s->geometry()) {
+        cudaMemcpy(s->mask[0], p, (size_t)s->g.n, cudaMemcpyHostToDevice);
+        p += s->g.n;
+        cudaMemcpy(s->mask[1], p, (size_t)s->g.n, cudaMemcpyHostToDevice);
+        p += s->g.n;
+        cudaMemcpy(s->wall, p, (size_t)s->g.n * sizeof(float4), cudaMemcpyHostToDevice);
+    }
+    s->rep_s = h.rep_s;
+    s->cur = h.cur;
+    if (s->geometry() && !s->moving()) {
+        // rebuild the static link list for the restored representation
+        encode_links(s, s->mask[s->cur], s->mask[s->cur]);
+    }
+    DeviceState st;
+    int rc = read_state(s, &st);
+    if (rc != BFX_OK) return rc;
+    s->step = st.step;
+    return BFX_OK;
+}
+
+int bfx_get_body(bfx_sim* s, bfx_body_state* out) {
+    BFX_GUARD(s);
+    if (!out) return BFX_ERR_INVALID_ARGUMENT;
+    DeviceState st;
+    int rc = read_state(s, &st);
+    if (rc != BFX_OK) return rc;
+    for (int k = 0; k < 3; ++k) out->position[k] = st.body[k];
+    for (int k = 0; k < 4; ++k) out->orientation[k] = st.body[3 + k];
+    for (int k = 0; k < 3; ++k) out->velocity[k] = st.body[7 + k];
+    for (int k = 0; k < 3; ++k) out->omega_body[k] = st.body[10 + k];
+    return BFX_OK;
+}
+
+int bfx_set_body(bfx_sim* s, const bfx_body_state* in) {
+    BFX_GUARD(s);
+    if (!in) return BFX_ERR_INVALID_ARGUMENT;
+    double b[13];
+    for (int k = 0; k < 3; ++k) b[k] = in->position[k];
+    for (int k = 0; k < 4; ++k) b[3 + k] = in->orientation[k];
+    for (int k = 0; k < 3; ++k) b[7 + k] = in->velocity[k];
+    for (int k = 0; k < 3; ++k) b[10 + k] = in->omega_body[k];
+    int rc = sync_check(s, "set body");
+    if (rc != BFX_OK) return rc;
+    cudaMemcpy((char*)s->dstate + offsetof(DeviceState, body), b, sizeof(b), cudaMemcpyHostToDevice);
+    return BFX_OK;
+}
+
+int bfx_step_index(bfx_sim* s, uint64_t* step, double* time) {
+    BFX_GUARD(s);
+    DeviceState st;
+    int rc = read_state(s, &st);
+    if (rc != BFX_OK) return rc;
+    if (step) *step = st.step;
+    if (time) *time = (double)(float)((double)st.step * (double)s->cfg.time_step);
+    return BFX_OK;
+}
+
+int bfx_set_kernel_timing(bfx_sim* s, int enabled) {
+    BFX_GUARD(s);
+    int rc = sync_check(s, "timing");
+    if (rc != BFX_OK) return rc;
+    s->timing = enabled != 0;
+    s->timing_ms = 0.0;
+    s->timing_launches = 0;
+    s->ev_used = 0;
+    return BFX_OK;
+}
+
+int bfx_kernel_timing(bfx_sim* s, double* total_ms, uint64_t* launches) {
+    BFX_GUARD(s);
+    int rc = sync_check(s, "timing");
+    if (rc != BFX_OK) return rc;
+    if (total_ms) *total_ms = s->timing_ms;
+    if (launches) *launches = s->timing_launches;
+    return BFX_OK;
+}
+
+int bfx_timer_begin(bfx_sim* s) {
+    BFX_GUARD(s);
+    if (!s->region[0]) {
+        cudaEventCreate(&s->region[0]);
+        cudaEventCreate(&s->region[1]);
+    }
+    cudaError_t e = cudaEventRecord(s->region[0], s->stream);
+    return e == cudaSuccess ? BFX_OK : cuda_fail(s, e, "timer begin");
+}
+
+int bfx_timer_end(bfx_sim* s, double* elapsed_ms) {
+    BFX_GUARD(s);
+    if (!elapsed_ms || !s->region[0]) return BFX_ERR_INVALID_ARGUMENT;
+    cudaEventRecord(s->region[1], s->stream);
+    cudaError_t e = cudaEventSynchronize(s->region[1]);
+    if (e != cudaSuccess) return cuda_fail(s, e, "timer end");
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, s->region[0], s->region[1]);
+    *elapsed_ms = ms;
+    timing_collect(s);
+    return BFX_OK;
+}
+
+int bfx_launch_count(bfx_sim* s, uint64_t* launches) {
+    if (!s || !launches) return BFX_ERR_INVALID_ARGUMENT;
+    *launches = s->launches;
+    return BFX_OK;
+}
+
+int bfx_device_bytes(bfx_sim* s, uint64_t* bytes) {
+    if (!s || !bytes) return BFX_ERR_INVALID_ARGUMENT;
+    *bytes = s->device_bytes;
+    return BFX_OK;
+}
+
+int bfx_last_error(bfx_sim* s, char* buf, size_t capacity) {
+    const std::string& m = s ? s->err : g_create_error;
+    if (!buf || capacity == 0) return BFX_ERR_INVALID_ARGUMENT;
+    size_t n = std::min(capacity - 1, m.size());
+    std::memcpy(buf, m.data(), n);
+    buf[n] = 0;
+    return BFX_OK;
+}
+
+}  // extern "C"

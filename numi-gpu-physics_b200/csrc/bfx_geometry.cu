@@ -1,0 +1,1260 @@
+// Moving-boundary kernels of the D3Q19 step: pose preparation, cell
+// classification (analytic bird, ellipsoid, articulated triangle mesh), cut-link
+// compaction, interpolated moving-wall bounce-back with momentum exchange,
+// cover/uncover topology impulses, FP64 load reduction and the FP64 6-DOF
+// update.  Each kernel cites the reference kernel it restates
+// (Sources/BirdFlowMetal/Metal/BirdFlow.metal, "BF.metal").
+//
+// Geometry work is confined to a box that follows the body (its extent is
+// fixed at creation from the conservative body radius plus a 4-cell margin,
+// its origin is recomputed on the device every step), so a step costs
+// O(box) here and O(lattice) only in the fused fluid kernel.
+#include "bfx_device.cuh"
+#include "bfx_internal.h"
+
+namespace bfx {
+
+struct GeomArgs {
+    Grid g;
+    Spill sp;
+    FluidParams fp;
+    int bx, by, bz;          // box extent
+    int64_t box_cells;
+    GeomBuffers b;
+    void* pops;
+    void* spill;
+};
+
+// ---------------------------------------------------------------------------
+// float3 helpers with the reference's operation order.
+// ---------------------------------------------------------------------------
+struct V3 {
+    float x, y, z;
+};
+__device__ __forceinline__ V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+__device__ __forceinline__ V3 v3(const float4& a) { return V3{a.x, a.y, a.z}; }
+__device__ __forceinline__ V3 operator+(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ V3 operator-(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ V3 operator*(V3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ V3 cross(V3 a, V3 b) {
+    return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float length(V3 a) { return sqrtf(dot(a, a)); }
+__device__ __forceinline__ float mixf(float a, float b, float t) { return a + (b - a) * t; }
+__device__ __forceinline__ float clampf(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); }
+__device__ __forceinline__ float4 f4(V3 a, float w) { return make_float4(a.x, a.y, a.z, w); }
+
+__device__ __forceinline__ V3 cell_world(const FluidParams& fp, int x, int y, int z) {
+    return v3(fp.origin[0] + ((float)x + 0.5f) * fp.dx, fp.origin[1] + ((float)y + 0.5f) * fp.dx,
+              fp.origin[2] + ((float)z + 0.5f) * fp.dx);
+}
+
+// Quaternions (x, y, z, w).  Normalisation divides by the correctly rounded
+// norm so host and device agree bit for bit.
+__device__ __forceinline__ float4 qnormalize(float4 q) {
+    float n2 = q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w;
+    if (n2 > 1.0e-20f) {
+        float n = sqrtf(n2);
+        return make_float4(q.x / n, q.y / n, q.z / n, q.w / n);
+    }
+    return make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+}
+__device__ __forceinline__ V3 qrotate(float4 q, V3 v) {
+    V3 qv = v3(q.x, q.y, q.z);
+    V3 t = cross(qv, v);
+    t = v3(t.x * 2.0f, t.y * 2.0f, t.z * 2.0f);
+    V3 c2 = cross(qv, t);
+    return v3(v.x + q.w * t.x + c2.x, v.y + q.w * t.y + c2.y, v.z + q.w * t.z + c2.z);
+}
+__device__ __forceinline__ V3 qunrotate(float4 q, V3 v) { return qrotate(make_float4(-q.x, -q.y, -q.z, q.w), v); }
+// rotateAroundAxis: BF.metal:466-473
+__device__ __forceinline__ V3 rotate_axis(V3 v, V3 axis, float angle) {
+    float s = bfx_sinf(angle), c = bfx_cosf(angle);
+    V3 cr = cross(axis, v);
+    float d = dot(axis, v);
+    return v3(v.x * c + cr.x * s + axis.x * d * (1.0f - c), v.y * c + cr.y * s + axis.y * d * (1.0f - c),
+              v.z * c + cr.z * s + axis.z * d * (1.0f - c));
+}
+__device__ __forceinline__ V3 normalize3(V3 v) {
+    float l = length(v);
+    return v3(v.x / l, v.y / l, v.z / l);
+}
+
+struct WingFrame {
+    V3 root, chord, span, normal, rel;
+    float tip_twist, tip_rate;
+};
+
+// makeWingFrame: BF.metal:611-684
+__device__ void make_wing_frame(float side, float stroke, float stroke_rate, float pitch, float pitch_rate,
+                                const bfx_bird& bird, V3 pos, float4 orient, WingFrame& fr) {
+    float4 o = qnormalize(orient);
+    V3 bx = qrotate(o, v3(1, 0, 0)), by = qrotate(o, v3(0, 1, 0)), bz = qrotate(o, v3(0, 0, 1));
+    V3 root_local = v3(bird.wing_geometry1.v[1], side * bird.wing_geometry1.v[2], bird.wing_geometry1.v[3]);
+    V3 rr = qrotate(o, root_local);
+    V3 root = pos + rr;
+    float signed_stroke = side * stroke;
+    V3 span_after = rotate_axis(v3(side * by.x, side * by.y, side * by.z), bx, signed_stroke);
+    V3 normal_after = rotate_axis(v3(side * bz.x, side * bz.y, side * bz.z), bx, signed_stroke);
+    V3 span = rotate_axis(span_after, normal_after, 0.0f);
+    V3 chord_before = rotate_axis(bx, normal_after, 0.0f);
+    float signed_pitch = side * pitch;
+    V3 chord = rotate_axis(chord_before, span, signed_pitch);
+    V3 normal = rotate_axis(normal_after, span, signed_pitch);
+    fr.root = root;
+    fr.chord = normalize3(chord);
+    fr.span = normalize3(span);
+    fr.normal = normalize3(normal);
+    float sr = side * stroke_rate, pr = side * pitch_rate;
+    fr.rel = v3(bx.x * sr + normal_after.x * 0.0f + fr.span.x * pr, bx.y * sr + normal_after.y * 0.0f + fr.span.y * pr,
+                bx.z * sr + normal_after.z * 0.0f + fr.span.z * pr);
+    fr.tip_twist = side * 0.0f;
+    fr.tip_rate = side * 0.0f;
+}
+
+// ---------------------------------------------------------------------------
+// prepareBirdGeometry (BF.metal:686-814) + updateWingInertialReaction
+// (BF.metal:6493-6572) + the geometry box origin.  One thread.
+// ---------------------------------------------------------------------------
+__device__ void wing_momentum(V3 root, V3 chord, V3 span, V3 normal, V3 rel, const float* mc, const float* inertia,
+                              V3 body_pos, V3& lin, V3& ang) {
+    V3 co = v3(chord.x * mc[1] + span.x * mc[2] + normal.x * mc[3], chord.y * mc[1] + span.y * mc[2] + normal.y * mc[3],
+               chord.z * mc[1] + span.z * mc[2] + normal.z * mc[3]);
+    V3 cv = cross(rel, co);
+    lin = v3(mc[0] * cv.x, mc[0] * cv.y, mc[0] * cv.z);
+    float a = inertia[0] * dot(rel, chord), b = inertia[1] * dot(rel, span), c = inertia[2] * dot(rel, normal);
+    V3 spin = v3(chord.x * a + span.x * b + normal.x * c, chord.y * a + span.y * b + normal.y * c,
+                 chord.z * a + span.z * b + normal.z * c);
+    V3 arm = v3(root.x + co.x - body_pos.x, root.y + co.y - body_pos.y, root.z + co.z - body_pos.z);
+    V3 cr = cross(arm, lin);
+    ang = cr + spin;
+}
+
+__global__ void k_prepare(const GeomArgs a, int init, float dt, float box_radius) {
+    DeviceState* st = a.b.state;
+    const bfx_bird& bird = *a.b.bird;
+    uint64_t absolute = init ? 0 : st->step + 1;
+    float time = (float)((double)absolute * (double)dt);
+    V3 pos = v3((float)st->body[0], (float)st->body[1], (float)st->body[2]);
+    float4 orient = make_float4((float)st->body[3], (float)st->body[4], (float)st->body[5], (float)st->body[6]);
+    V3 vel = v3((float)st->body[7], (float)st->body[8], (float)st->body[9]);
+    V3 omb = v3((float)st->body[10], (float)st->body[11], (float)st->body[12]);
+    float af = 2.0f * 3.14159265358979323846f * bird.wing_kinematics0.v[0];
+    float phase = af * time;
+    float stroke = bird.wing_kinematics0.v[2] + bird.wing_kinematics0.v[1] * bfx_sinf(phase);
+    float stroke_rate = af * bird.wing_kinematics0.v[1] * bfx_cosf(phase);
+    float pitch = bird.wing_kinematics0.v[3] + bird.wing_kinematics1.v[0] * bfx_sinf(phase + bird.wing_kinematics1.v[1]);
+    float pitch_rate = af * bird.wing_kinematics1.v[0] * bfx_cosf(phase + bird.wing_kinematics1.v[1]);
+    WingFrame l, r;
+    make_wing_frame(1.0f, stroke, stroke_rate, pitch, pitch_rate, bird, pos, orient, l);
+    make_wing_frame(-1.0f, stroke, stroke_rate, pitch, pitch_rate, bird, pos, orient, r);
+    float4 o = qnormalize(orient);
+    Prepared& p = st->prep;
+    p.body_position = f4(pos, 0.0f);
+    p.orientation = o;
+    p.linear_velocity = f4(vel, 0.0f);
+    const float* br = bird.body_radii_mass.v;
+    const float* tg = bird.tail_geometry.v;
+    const float* wg0 = bird.wing_geometry0.v;
+    const float* wg1 = bird.wing_geometry1.v;
+    float body_radius = length(v3(br[0], br[1], br[2]));
+    float tail_radius = length(v3(br[0] + tg[0], fmaxf(br[1], tg[1]), br[2] + 0.5f * tg[2]));
+    float root_radius = length(v3(wg1[1], wg1[2], wg1[3]));
+    float wing_radius = root_radius + wg0[0] + fabsf(wg1[0]) + 0.5f * fmaxf(wg0[1], wg0[2]) + 0.5f * wg0[3];
+    float geometry_radius = fmaxf(body_radius, fmaxf(tail_radius, wing_radius)) + 2.0f * a.fp.dx;
+    p.omega_body_world = f4(qrotate(o, omb), geometry_radius);
+    p.left_root = f4(l.root, 0.0f);
+    p.left_chord = f4(l.chord, l.tip_twist);
+    p.left_span = f4(l.span, 0.0f);
+    p.left_normal = f4(l.normal, 0.0f);
+    p.left_angular_velocity = f4(l.rel, l.tip_rate);
+    p.right_root = f4(r.root, 0.0f);
+    p.right_chord = f4(r.chord, r.tip_twist);
+    p.right_span = f4(r.span, 0.0f);
+    p.right_normal = f4(r.normal, 0.0f);
+    p.right_angular_velocity = f4(r.rel, r.tip_rate);
+
+    // wing inertial reaction
+    if (bird.left_wing_inertia.v[3] < 0.5f || bird.right_wing_inertia.v[3] < 0.5f) {
+        for (int k = 0; k < 16; ++k) {
+            st->wing_prev[k] = 0.0f;
+            st->wing_reaction[k] = 0.0f;
+        }
+    } else {
+        V3 cur[4];
+        wing_momentum(l.root, l.chord, l.span, l.normal, l.rel, bird.left_wing_mass_com.v, bird.left_wing_inertia.v,
+                      pos, cur[0], cur[1]);
+        wing_momentum(r.root, r.chord, r.span, r.normal, r.rel, bird.right_wing_mass_com.v, bird.right_wing_inertia.v,
+                      pos, cur[2], cur[3]);
+        float inv = 1.0f / dt;
+        for (int j = 0; j < 4; ++j) {
+            if (init) {
+                st->wing_reaction[4 * j] = st->wing_reaction[4 * j + 1] = st->wing_reaction[4 * j + 2] = 0.0f;
+            } else {
+                st->wing_reaction[4 * j] = -(cur[j].x - st->wing_prev[4 * j]) * inv;
+                st->wing_reaction[4 * j + 1] = -(cur[j].y - st->wing_prev[4 * j + 1]) * inv;
+                st->wing_reaction[4 * j + 2] = -(cur[j].z - st->wing_prev[4 * j + 2]) * inv;
+            }
+            st->wing_reaction[4 * j + 3] = 0.0f;
+            st->wing_prev[4 * j] = cur[j].x;
+            st->wing_prev[4 * j + 1] = cur[j].y;
+            st->wing_prev[4 * j + 2] = cur[j].z;
+            st->wing_prev[4 * j + 3] = 0.0f;
+        }
+    }
+
+    // geometry box: centred on the body origin, clamped into the lattice
+    int ext[3] = {a.bx, a.by, a.bz};
+    int dims[3] = {a.g.nx, a.g.ny, a.g.nz};
+    float c[3] = {pos.x, pos.y, pos.z};
+    for (int k = 0; k < 3; ++k) {
+        float cc = (c[k] - a.fp.origin[k]) / a.fp.dx - 0.5f;
+        int lo = (int)floorf(cc) - ext[k] / 2;
+        lo = lo < 0 ? 0 : lo;
+        lo = lo > dims[k] - ext[k] ? dims[k] - ext[k] : lo;
+        st->box_origin[k] = lo < 0 ? 0 : lo;
+    }
+    (void)box_radius;
+}
+
+// ---------------------------------------------------------------------------
+// Signed distances: sdEllipsoid / sdTaperedWing / sdTail (BF.metal:486-533).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float sd_ellipsoid(V3 p, V3 r) {
+    V3 a = v3(p.x / r.x, p.y / r.y, p.z / r.z);
+    V3 r2 = v3(r.x * r.x, r.y * r.y, r.z * r.z);
+    V3 b = v3(p.x / r2.x, p.y / r2.y, p.z / r2.z);
+    float k0 = length(a);
+    float k1 = length(b);
+    return k1 > 1.0e-12f ? k0 * (k0 - 1.0f) / k1 : -fminf(r.x, fminf(r.y, r.z));
+}
+__device__ __forceinline__ float sd_box_tail(float qx, float qy, float qz) {
+    return length(v3(fmaxf(qx, 0.0f), fmaxf(qy, 0.0f), fmaxf(qz, 0.0f))) + fminf(fmaxf(qx, fmaxf(qy, qz)), 0.0f);
+}
+__device__ __forceinline__ float sd_tapered_wing(V3 l, float span, float root_chord, float tip_chord, float thickness,
+                                                 float sweep) {
+    float sf = clampf(l.y / fmaxf(span, 1.0e-6f), 0.0f, 1.0f);
+    float chord = mixf(root_chord, tip_chord, sf);
+    float cc = -sweep * sf;
+    float dx = fabsf(l.x - cc) - 0.5f * chord;
+    float dy = fmaxf(-l.y, l.y - span);
+    float dz = fabsf(l.z) - 0.5f * thickness;
+    return sd_box_tail(dx, dy, dz);
+}
+__device__ __forceinline__ float sd_tail(V3 bl, V3 br, const float* tg) {
+    float len = tg[0], hw = tg[1], th = tg[2];
+    float xr = -(bl.x + br.x);
+    float fr = clampf(xr / fmaxf(len, 1.0e-6f), 0.0f, 1.0f);
+    float lhw = mixf(0.35f * hw, hw, fr);
+    float dx = fmaxf(-xr, xr - len);
+    float dy = fabsf(bl.y) - lhw;
+    float dz = fabsf(bl.z + 0.15f * br.z) - 0.5f * th;
+    return sd_box_tail(dx, dy, dz);
+}
+
+__device__ __forceinline__ bool box_cell(const GeomArgs& a, int& x, int& y, int& z, int64_t& bidx) {
+    int lx = blockIdx.x * blockDim.x + threadIdx.x;
+    int ly = blockIdx.y * blockDim.y + threadIdx.y;
+    int lz = blockIdx.z;
+    if (lx >= a.bx || ly >= a.by || lz >= a.bz) return false;
+    const int32_t* o = a.b.state->box_origin;
+    x = o[0] + lx;
+    y = o[1] + ly;
+    z = o[2] + lz;
+    bidx = (int64_t)lx + (int64_t)a.bx * ((int64_t)ly + (int64_t)a.by * lz);
+    return x < a.g.nx && y < a.g.ny && z < a.g.nz;
+}
+
+__device__ __forceinline__ uint8_t topo_flags(uint8_t part, uint8_t prev_part, int has_prev) {
+    if (!has_prev) return part;
+    if (part && !prev_part) return (uint8_t)(part | kCovered);
+    if (!part && prev_part) return kUncovered;
+    return part;
+}
+
+// buildBirdGeometry: BF.metal:816-938
+__global__ void k_classify_bird(const GeomArgs a, int has_prev) {
+    int x, y, z;
+    int64_t bidx;
+    if (!box_cell(a, x, y, z, bidx)) return;
+    const Prepared& p = a.b.state->prep;
+    const bfx_bird& bird = *a.b.bird;
+    const int64_t gid = flat(a.g, x, y, z);
+    V3 world = cell_world(a.fp, x, y, z);
+    V3 rb = world - v3(p.body_position);
+    uint8_t prev_part = a.b.mask_prev[gid] & kPartMask;
+    bool was_solid = has_prev && prev_part != 0;
+    float gr = p.omega_body_world.w;
+    if (!was_solid && dot(rb, rb) > gr * gr) {
+        a.b.mask_next[gid] = topo_flags(0, prev_part, has_prev);
+        a.b.wall[gid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        return;
+    }
+    V3 bl = qunrotate(p.orientation, rb);
+    V3 base = v3(p.linear_velocity) + cross(v3(p.omega_body_world), rb);
+    float best = sd_ellipsoid(bl, v3(bird.body_radii_mass.v[0], bird.body_radii_mass.v[1], bird.body_radii_mass.v[2]));
+    V3 bestv = base;
+    uint8_t part = 1;
+    for (int wing = 0; wing < 2; ++wing) {
+        const float4* fr = wing == 0 ? &p.left_root : &p.right_root;
+        V3 root = v3(fr[0]), chord = v3(fr[1]), span = v3(fr[2]), normal = v3(fr[3]), rel = v3(fr[4]);
+        float tip_twist = fr[1].w, tip_rate = fr[4].w;
+        V3 rp = world - root;
+        V3 lu = v3(dot(rp, chord), dot(rp, span), dot(rp, normal));
+        float sf = clampf(lu.y / fmaxf(bird.wing_geometry0.v[0], 1.0e-6f), 0.0f, 1.0f);
+        float twist = tip_twist * sf;
+        float tc = bfx_cosf(twist), ts = bfx_sinf(twist);
+        V3 loc = v3(tc * lu.x + ts * lu.z, lu.y, -ts * lu.x + tc * lu.z);
+        float d = sd_tapered_wing(loc, bird.wing_geometry0.v[0], bird.wing_geometry0.v[1], bird.wing_geometry0.v[2],
+                                  bird.wing_geometry0.v[3], bird.wing_geometry1.v[0]);
+        if (d < best) {
+            best = d;
+            V3 c1 = cross(rel, rp);
+            float k = sf * tip_rate;
+            V3 sw = v3(span.x * k, span.y * k, span.z * k);
+            V3 arm = v3(world.x - (root.x + span.x * lu.y), world.y - (root.y + span.y * lu.y),
+                        world.z - (root.z + span.z * lu.y));
+            V3 c2 = cross(sw, arm);
+            bestv = v3(base.x + c1.x + c2.x, base.y + c1.y + c2.y, base.z + c1.z + c2.z);
+            part = wing == 0 ? 2 : 3;
+        }
+    }
+    float td = sd_tail(bl, v3(bird.body_radii_mass.v[0], bird.body_radii_mass.v[1], bird.body_radii_mass.v[2]),
+                       bird.tail_geometry.v);
+    if (td < best) {
+        best = td;
+        bestv = base;
+        part = 4;
+    }
+    uint8_t solid_part = best <= 0.0f ? part : (uint8_t)0;
+    a.b.mask_next[gid] = topo_flags(solid_part, prev_part, has_prev);
+    a.b.wall[gid] = make_float4(bestv.x * a.fp.v2l, bestv.y * a.fp.v2l, bestv.z * a.fp.v2l, 0.0f);
+}
+
+// Body ellipsoid alone (part 1); w holds the implicit value.
+__device__ __forceinline__ float ellipsoid_implicit(const Prepared& p, const bfx_bird& bird, V3 w) {
+    V3 rb = w - v3(p.body_position);
+    V3 bl = qunrotate(p.orientation, rb);
+    return sd_ellipsoid(bl, v3(bird.body_radii_mass.v[0], bird.body_radii_mass.v[1], bird.body_radii_mass.v[2]));
+}
+
+__global__ void k_classify_ellipsoid(const GeomArgs a, int has_prev) {
+    int x, y, z;
+    int64_t bidx;
+    if (!box_cell(a, x, y, z, bidx)) return;
+    const Prepared& p = a.b.state->prep;
+    const bfx_bird& bird = *a.b.bird;
+    const int64_t gid = flat(a.g, x, y, z);
+    float r = fmaxf(bird.body_radii_mass.v[0], fmaxf(bird.body_radii_mass.v[1], bird.body_radii_mass.v[2])) +
+              2.0f * a.fp.dx;
+    V3 world = cell_world(a.fp, x, y, z);
+    V3 rb = world - v3(p.body_position);
+    uint8_t prev_part = a.b.mask_prev[gid] & kPartMask;
+    bool was_solid = has_prev && prev_part != 0;
+    if (!was_solid && dot(rb, rb) > r * r) {
+        a.b.mask_next[gid] = topo_flags(0, prev_part, has_prev);
+        a.b.wall[gid] = make_float4(0.0f, 0.0f, 0.0f, r);
+        return;
+    }
+    float imp = ellipsoid_implicit(p, bird, world);
+    V3 cr = cross(v3(p.omega_body_world), rb);
+    a.b.mask_next[gid] = topo_flags(imp <= 0.0f ? 1 : 0, prev_part, has_prev);
+    a.b.wall[gid] = make_float4((p.linear_velocity.x + cr.x) * a.fp.v2l, (p.linear_velocity.y + cr.y) * a.fp.v2l,
+                                (p.linear_velocity.z + cr.z) * a.fp.v2l, imp);
+}
+
+// ---------------------------------------------------------------------------
+// Triangle mesh (BF.metal:1529-1583 closest point, 1638-1686 raster,
+// 1697-1738 / 1978-2039 resolve).  Keys are 64-bit: quantised distance
+// (1/65536 cell) in the high word, triangle id in the low word, so meshes are
+// not limited to the reference's 4,096 triangles and ties stay deterministic.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ V3 closest_point(V3 p, V3 a, V3 b, V3 c, V3& bary) {
+    V3 ab = b - a, ac = c - a, ap = p - a;
+    float d1 = dot(ab, ap), d2 = dot(ac, ap);
+    if (d1 <= 0.0f && d2 <= 0.0f) {
+        bary = v3(1, 0, 0);
+        return a;
+    }
+    V3 bp = p - b;
+    float d3 = dot(ab, bp), d4 = dot(ac, bp);
+    if (d3 >= 0.0f && d4 <= d3) {
+        bary = v3(0, 1, 0);
+        return b;
+    }
+    float vc = d1 * d4 - d3 * d2;
+    if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
+        float v = d1 / (d1 - d3);
+        bary = v3(1.0f - v, v, 0);
+        return v3(a.x + v * ab.x, a.y + v * ab.y, a.z + v * ab.z);
+    }
+    V3 cp = p - c;
+    float d5 = dot(ab, cp), d6 = dot(ac, cp);
+    if (d6 >= 0.0f && d5 <= d6) {
+        bary = v3(0, 0, 1);
+        return c;
+    }
+    float vb = d5 * d2 - d1 * d6;
+    if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
+        float w = d2 / (d2 - d6);
+        bary = v3(1.0f - w, 0, w);
+        return v3(a.x + w * ac.x, a.y + w * ac.y, a.z + w * ac.z);
+    }
+    float va = d3 * d6 - d5 * d4;
+    if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f) {
+        float w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+        bary = v3(0, 1.0f - w, w);
+        return v3(b.x + w * (c.x - b.x), b.y + w * (c.y - b.y), b.z + w * (c.z - b.z));
+    }
+    float inv = 1.0f / fmaxf(va + vb + vc, 1.0e-20f);
+    float v = vb * inv, w = vc * inv;
+    bary = v3(1.0f - v - w, v, w);
+    return v3(a.x + ab.x * v + ac.x * w, a.y + ab.y * v + ac.y * w, a.z + ab.z * v + ac.z * w);
+}
+
+// Articulated vertex placement: segment 0 rides the body frame, 1 / 2 the left
+// / right wing frames (the indexed surface preparation of BF.metal:1589-1622,
+// driven by the rigid frames instead of keyframes).
+__global__ void k_mesh_prepare(const GeomArgs a) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.b.nverts) return;
+    const Prepared& p = a.b.state->prep;
+    V3 l = v3(a.b.mesh_local[3 * i], a.b.mesh_local[3 * i + 1], a.b.mesh_local[3 * i + 2]);
+    V3 w, v;
+    uint8_t seg = a.b.mesh_segment[i];
+    if (seg == 0) {
+        V3 r = qrotate(p.orientation, l);
+        w = v3(p.body_position.x + r.x, p.body_position.y + r.y, p.body_position.z + r.z);
+        V3 cr = cross(v3(p.omega_body_world), r);
+        v = v3(p.linear_velocity.x + cr.x, p.linear_velocity.y + cr.y, p.linear_velocity.z + cr.z);
+    } else {
+        const float4* fr = seg == 1 ? &p.left_root : &p.right_root;
+        w = v3(fr[0].x + fr[1].x * l.x + fr[2].x * l.y + fr[3].x * l.z,
+               fr[0].y + fr[1].y * l.x + fr[2].y * l.y + fr[3].y * l.z,
+               fr[0].z + fr[1].z * l.x + fr[2].z * l.y + fr[3].z * l.z);
+        V3 rb = v3(w.x - p.body_position.x, w.y - p.body_position.y, w.z - p.body_position.z);
+        V3 cr = cross(v3(p.omega_body_world), rb);
+        V3 rr = v3(w.x - fr[0].x, w.y - fr[0].y, w.z - fr[0].z);
+        V3 cw = cross(v3(fr[4]), rr);
+        v = v3(p.linear_velocity.x + cr.x + cw.x, p.linear_velocity.y + cr.y + cw.y,
+               p.linear_velocity.z + cr.z + cw.z);
+    }
+    a.b.mesh_pos[i] = f4(w, 0.0f);
+    a.b.mesh_vel[i] = make_float4(v.x * a.fp.v2l, v.y * a.fp.v2l, v.z * a.fp.v2l, 0.0f);
+}
+
+__global__ void k_mesh_clear(const GeomArgs a) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < a.box_cells) a.b.keys[i] = 0xFFFFFFFFFFFFFFFFull;
+}
+
+__device__ __forceinline__ void tri_vertices(const GeomArgs& a, uint32_t t, V3& A, V3& B, V3& C) {
+    A = v3(a.b.mesh_pos[a.b.mesh_tris[3 * t]]);
+    B = v3(a.b.mesh_pos[a.b.mesh_tris[3 * t + 1]]);
+    C = v3(a.b.mesh_pos[a.b.mesh_tris[3 * t + 2]]);
+}
+
+__global__ void k_mesh_raster(const GeomArgs a) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.b.ntris) return;
+    V3 A, B, C;
+    tri_vertices(a, t, A, B, C);
+    const float cs = a.fp.dx;
+    const float guard = a.b.half_thickness + 2.0f * cs;
+    int lo[3], hi[3];
+    const int dims[3] = {a.g.nx, a.g.ny, a.g.nz};
+    const int ext[3] = {a.bx, a.by, a.bz};
+    const int32_t* o = a.b.state->box_origin;
+    float mn[3] = {fminf(A.x, fminf(B.x, C.x)), fminf(A.y, fminf(B.y, C.y)), fminf(A.z, fminf(B.z, C.z))};
+    float mx[3] = {fmaxf(A.x, fmaxf(B.x, C.x)), fmaxf(A.y, fmaxf(B.y, C.y)), fmaxf(A.z, fmaxf(B.z, C.z))};
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = (int)floorf(((mn[k] - guard) - a.fp.origin[k]) / cs - 0.5f);
+        hi[k] = (int)ceilf(((mx[k] + guard) - a.fp.origin[k]) / cs - 0.5f);
+        lo[k] = lo[k] < 0 ? 0 : (lo[k] > dims[k] - 1 ? dims[k] - 1 : lo[k]);
+        hi[k] = hi[k] < 0 ? 0 : (hi[k] > dims[k] - 1 ? dims[k] - 1 : hi[k]);
+        // confine to the geometry box (the key array is box-local)
+        lo[k] = lo[k] < o[k] ? o[k] : lo[k];
+        hi[k] = hi[k] > o[k] + ext[k] - 1 ? o[k] + ext[k] - 1 : hi[k];
+    }
+    for (int z = lo[2]; z <= hi[2]; ++z)
+        for (int y = lo[1]; y <= hi[1]; ++y)
+            for (int x = lo[0]; x <= hi[0]; ++x) {
+                V3 w = cell_world(a.fp, x, y, z), bary;
+                V3 cp = closest_point(w, A, B, C, bary);
+                float dc = length(w - cp) / cs;
+                float bin = roundf(dc * 65536.0f);
+                unsigned long long ub = bin >= 4294967295.0f ? 0xFFFFFFFFull : (unsigned long long)bin;
+                unsigned long long key = (ub << 32) | (unsigned long long)t;
+                int64_t bi = (int64_t)(x - o[0]) + (int64_t)a.bx * ((int64_t)(y - o[1]) + (int64_t)a.by * (z - o[2]));
+                atomicMin(&a.b.keys[bi], key);
+            }
+}
+
+__global__ void k_mesh_resolve(const GeomArgs a, int has_prev) {
+    int x, y, z;
+    int64_t bidx;
+    if (!box_cell(a, x, y, z, bidx)) return;
+    const int64_t gid = flat(a.g, x, y, z);
+    uint8_t prev_part = a.b.mask_prev[gid] & kPartMask;
+    unsigned long long key = a.b.keys[bidx];
+    uint32_t t = (uint32_t)(key & 0xFFFFFFFFull);
+    if (key == 0xFFFFFFFFFFFFFFFFull || t >= a.b.ntris) {
+        a.b.mask_next[gid] = topo_flags(0, prev_part, has_prev);
+        a.b.wall[gid] = make_float4(0.0f, 0.0f, 0.0f, 16.0f);
+        return;
+    }
+    V3 w = cell_world(a.fp, x, y, z);
+    V3 A, B, C, bary;
+    tri_vertices(a, t, A, B, C);
+    V3 cp = closest_point(w, A, B, C, bary);
+    float4 va = a.b.mesh_vel[a.b.mesh_tris[3 * t]], vb = a.b.mesh_vel[a.b.mesh_tris[3 * t + 1]],
+           vc = a.b.mesh_vel[a.b.mesh_tris[3 * t + 2]];
+    V3 v = v3(bary.x * va.x + bary.y * vb.x + bary.z * vc.x, bary.x * va.y + bary.y * vb.y + bary.z * vc.y,
+              bary.x * va.z + bary.y * vb.z + bary.z * vc.z);
+    float sd = length(w - cp) - a.b.half_thickness;
+    uint8_t part = sd <= 0.0f ? a.b.mesh_tri_part[t] : (uint8_t)0;
+    a.b.mask_next[gid] = topo_flags(part, prev_part, has_prev);
+    a.b.wall[gid] = make_float4(v.x, v.y, v.z, sd / a.fp.dx);
+}
+
+__global__ void k_fill_wall_w(float4* wall, int64_t n, float w) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) wall[i] = make_float4(0.0f, 0.0f, 0.0f, w);
+}
+
+// ---------------------------------------------------------------------------
+// Link predicate and link fractions.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool persistent_fluid(uint8_t m_next, uint8_t m_prev) {
+    return (m_next & (kPartMask | kUncovered)) == 0 && (m_prev & kPartMask) == 0;
+}
+// Solid source of link (x, q) or -1.
+__device__ __forceinline__ int64_t link_source(const Grid& g, const uint8_t* mask_next, int x, int y, int z, int q,
+                                               int& sx, int& sy, int& sz) {
+    sx = x - cx(q);
+    sy = y - cy(q);
+    sz = z - cz(q);
+    if (!wrap(g, sx, sy, sz)) return -1;
+    int64_t s = flat(g, sx, sy, sz);
+    return (mask_next[s] & kPartMask) ? s : -1;
+}
+
+// Ten-iteration bisection from the fluid node toward the solid node on the
+// ellipsoid implicit (the prescribedWingLinkFraction rule, BF.metal:1144-1175).
+__device__ float ellipsoid_link_fraction(const GeomArgs& a, int fx, int fy, int fz, int sx, int sy, int sz) {
+    const Prepared& p = a.b.state->prep;
+    const bfx_bird& bird = *a.b.bird;
+    V3 fw = cell_world(a.fp, fx, fy, fz), sw = cell_world(a.fp, sx, sy, sz);
+    float lo = 0.0f, hi = 1.0f;
+    for (int it = 0; it < 10; ++it) {
+        float mid = 0.5f * (lo + hi);
+        V3 s = v3(mixf(fw.x, sw.x, mid), mixf(fw.y, sw.y, mid), mixf(fw.z, sw.z, mid));
+        if (ellipsoid_implicit(p, bird, s) > 0.0f) lo = mid;
+        else hi = mid;
+    }
+    return clampf(0.5f * (lo + hi), 1.0e-4f, 1.0f);
+}
+
+__device__ __forceinline__ float tri_distance(const GeomArgs& a, uint32_t t, V3 w) {
+    V3 A, B, C, bary;
+    tri_vertices(a, t, A, B, C);
+    V3 cp = closest_point(w, A, B, C, bary);
+    return length(w - cp);
+}
+
+__device__ __forceinline__ unsigned long long box_key(const GeomArgs& a, int x, int y, int z) {
+    const int32_t* o = a.b.state->box_origin;
+    int lx = x - o[0], ly = y - o[1], lz = z - o[2];
+    if (lx < 0 || ly < 0 || lz < 0 || lx >= a.bx || ly >= a.by || lz >= a.bz) return 0xFFFFFFFFFFFFFFFFull;
+    return a.b.keys[(int64_t)lx + (int64_t)a.bx * ((int64_t)ly + (int64_t)a.by * lz)];
+}
+
+// Wall position along the link as the bracketed root of
+// min(d_A, d_B) - h, A and B the winning triangles of the two end cells.
+__device__ float mesh_ray_root(const GeomArgs& a, int fx, int fy, int fz, int sx, int sy, int sz) {
+    V3 fw = cell_world(a.fp, fx, fy, fz), sw = cell_world(a.fp, sx, sy, sz);
+    unsigned long long kf = box_key(a, fx, fy, fz), ks = box_key(a, sx, sy, sz);
+    uint32_t ta = (uint32_t)(ks & 0xFFFFFFFFull);
+    uint32_t tb = kf == 0xFFFFFFFFFFFFFFFFull ? ta : (uint32_t)(kf & 0xFFFFFFFFull);
+    if (ta >= a.b.ntris) return 0.5f;
+    if (tb >= a.b.ntris) tb = ta;
+    const float h = a.b.half_thickness;
+    float lo = 0.0f, hi = 1.0f;
+    bool found = false;
+    for (int i = 1; i <= 8; ++i) {
+        float t = (float)i * 0.125f;
+        V3 s = v3(mixf(fw.x, sw.x, t), mixf(fw.y, sw.y, t), mixf(fw.z, sw.z, t));
+        float gv = fminf(tri_distance(a, ta, s), tri_distance(a, tb, s)) - h;
+        if (gv <= 0.0f) {
+            hi = t;
+            found = true;
+            break;
+        }
+        lo = t;
+    }
+    if (!found) return 1.0f;
+    for (int it = 0; it < 24; ++it) {
+        float mid = 0.5f * (lo + hi);
+        V3 s = v3(mixf(fw.x, sw.x, mid), mixf(fw.y, sw.y, mid), mixf(fw.z, sw.z, mid));
+        float gv = fminf(tri_distance(a, ta, s), tri_distance(a, tb, s)) - h;
+        if (gv <= 0.0f) hi = mid;
+        else lo = mid;
+    }
+    return clampf(0.5f * (lo + hi), 1.0e-4f, 1.0f);
+}
+
+// ---------------------------------------------------------------------------
+// Block reductions in a fixed order (deterministic).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int linear_tid() { return threadIdx.x + blockDim.x * threadIdx.y; }
+
+// Fixed-order tree over the (up to 256) threads of a block; every thread
+// receives the block total.
+template <int K>
+__device__ __forceinline__ void block_sum(double (&v)[K], double (*sh)[256]) {
+    const int t = linear_tid();
+    const int nt = blockDim.x * blockDim.y;
+    for (int k = 0; k < K; ++k) sh[k][t] = v[k];
+    for (int k = 0; k < K; ++k)
+        if (t + nt < 256) sh[k][t + nt] = 0.0;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (t < s)
+            for (int k = 0; k < K; ++k) sh[k][t] += sh[k][t + s];
+        __syncthreads();
+    }
+    for (int k = 0; k < K; ++k) v[k] = sh[k][0];
+    __syncthreads();
+}
+
+// FP64 load contribution: lattice force fl applied at point pt (both in the
+// precision the step computes in), torque about the FP64 body position.
+template <class R>
+__device__ __forceinline__ void add_load(double (&acc)[8], R flx, R fly, R flz, R ptx, R pty, R ptz,
+                                         const double* body, float f2p) {
+    double fp[3] = {(double)flx * (double)f2p, (double)fly * (double)f2p, (double)flz * (double)f2p};
+    double r[3] = {(double)ptx - body[0], (double)pty - body[1], (double)ptz - body[2]};
+    acc[0] += (double)flx;
+    acc[1] += (double)fly;
+    acc[2] += (double)flz;
+    acc[3] += r[1] * fp[2] - r[2] * fp[1];
+    acc[4] += r[2] * fp[0] - r[0] * fp[2];
+    acc[5] += r[0] * fp[1] - r[1] * fp[0];
+}
+
+// ---------------------------------------------------------------------------
+// Topology impulses (BF.metal:2557-2609 covered, 2616-2666 uncovered) and the
+// per-block cut-link count.  Reads populations only; runs before any link write.
+// ---------------------------------------------------------------------------
+template <class S>
+__global__ void __launch_bounds__(256) k_boundary_scan(const GeomArgs a, int rep_s) {
+    __shared__ double sh[8][256];
+    using R = typename S::R;
+    const FluidParams& fp = a.fp;
+    const int sel = fp.interpolated;
+    const int mode = sel ? fp.force_mode : 6;
+    const int include_topo = !sel || fp.load_component != 1;
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    uint32_t links = 0;
+    int x, y, z;
+    int64_t bidx;
+    if (box_cell(a, x, y, z, bidx)) {
+        const Grid& g = a.g;
+        const int64_t gid = flat(g, x, y, z);
+        const uint8_t m1 = a.b.mask_next[gid];
+        const uint8_t m0 = a.b.mask_prev[gid];
+        const typename S::T* A = (const typename S::T*)a.pops;
+        const typename S::T* spill = (const typename S::T*)a.spill;
+        const double* body = a.b.state->body;
+        const V3 world = cell_world(fp, x, y, z);
+        if ((m1 & kCovered) && fp.accumulate && include_topo) {
+            // newly covered: previous fluid momentum (minus the wall-moving density for estimators 0-5)
+            R pd = 0, pmx = 0, pmy = 0, pmz = 0;
+            for (int q = 0; q < 19; ++q) {
+                R prev = canon_load<S>(A, g, a.sp, spill, rep_s, q, x, y, z);
+                pd += prev;
+                pmx += prev * (R)cx(q);
+                pmy += prev * (R)cy(q);
+                pmz += prev * (R)cz(q);
+            }
+            float4 w = a.b.wall[gid];
+            R ix = pmx, iy = pmy, iz = pmz;
+            if (mode != 6) {
+                ix = pmx - pd * (R)w.x;
+                iy = pmy - pd * (R)w.y;
+                iz = pmz - pd * (R)w.z;
+            }
+            add_load<R>(acc, ix, iy, iz, (R)world.x, (R)world.y, (R)world.z, body, fp.f2p);
+            acc[6] += 1.0;
+        } else if ((m1 & kUncovered) && fp.accumulate && include_topo && mode == 6) {
+            // newly uncovered: refill momentum plus the moving-domain stencil
+            float4 w = a.b.wall[gid];
+            R mx = 0, my = 0, mz = 0;
+            for (int q = 0; q < 19; ++q) {
+                R v = feq_rt<R>(q, R(1), (R)w.x, (R)w.y, (R)w.z);
+                mx += v * (R)cx(q);
+                my += v * (R)cy(q);
+                mz += v * (R)cz(q);
+            }
+            R tx = -mx, ty = -my, tz = -mz;
+            for (int q = 1; q < 19; ++q) {
+                int bx = x + cx(q), by = y + cy(q), bz = z + cz(q);
+                if (!inside(g, bx, by, bz)) continue;
+                int64_t nb = flat(g, bx, by, bz);
+                if (!((a.b.mask_prev[nb] & kPartMask) == 0 && (a.b.mask_next[nb] & kPartMask) == 0)) continue;
+                R old_out = canon_load<S>(A, g, a.sp, spill, rep_s, q, x, y, z);
+                R sup_in = canon_load<S>(A, g, a.sp, spill, rep_s, opp(q), bx, by, bz);
+                R sum = old_out + sup_in;
+                tx -= sum * (R)cx(q);
+                ty -= sum * (R)cy(q);
+                tz -= sum * (R)cz(q);
+            }
+            add_load<R>(acc, tx, ty, tz, (R)world.x, (R)world.y, (R)world.z, body, fp.f2p);
+            acc[7] += 1.0;
+        }
+        if (persistent_fluid(m1, m0)) {
+            for (int q = 1; q < 19; ++q) {
+                int sx, sy, sz;
+                if (link_source(g, a.b.mask_next, x, y, z, q, sx, sy, sz) >= 0) ++links;
+            }
+        }
+    }
+    block_sum<8>(acc, sh);
+    __shared__ uint32_t wcount[8];
+    uint32_t wl = links;
+    for (int o = 16; o > 0; o >>= 1) wl += __shfl_down_sync(0xffffffffu, wl, o);
+    const int t = linear_tid();
+    if ((t & 31) == 0) wcount[t >> 5] = wl;
+    __syncthreads();
+    const int block = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    if (t == 0) {
+        uint32_t tot = 0;
+        for (int w = 0; w < 8; ++w) tot += wcount[w];
+        a.b.block_counts[block] = tot;
+        for (int k = 0; k < 8; ++k) a.b.topo_partials[8 * block + k] = acc[k];
+    }
+}
+
+// Exclusive scan of the per-block link counts (one block, fixed order).
+__global__ void k_scan(const GeomArgs a) {
+    __shared__ uint32_t sh[1024];
+    const int nb = a.b.box_blocks;
+    const int per = (nb + 1023) / 1024;
+    const int t = threadIdx.x;
+    uint32_t local = 0;
+    for (int i = 0; i < per; ++i) {
+        int idx = t * per + i;
+        if (idx < nb) local += a.b.block_counts[idx];
+    }
+    sh[t] = local;
+    __syncthreads();
+    for (int s = 1; s < 1024; s <<= 1) {
+        uint32_t v = t >= s ? sh[t - s] : 0;
+        __syncthreads();
+        sh[t] += v;
+        __syncthreads();
+    }
+    uint32_t run = t > 0 ? sh[t - 1] : 0;
+    for (int i = 0; i < per; ++i) {
+        int idx = t * per + i;
+        if (idx < nb) {
+            uint32_t c = a.b.block_counts[idx];
+            a.b.block_offsets[idx] = run;
+            run += c;
+        }
+    }
+    if (t == 1023) {
+        uint64_t total = sh[1023];
+        a.b.state->link_count = (int64_t)total;
+        a.b.state->link_overflow = total > a.b.link_capacity ? 1u : 0u;
+    }
+}
+
+// Cut-link compaction: every persistent fluid cell appends its links (in
+// direction order) at the block offset plus the warp-ballot / shuffle prefix of
+// the preceding threads, so the list is ordered by box cell then direction.
+__global__ void __launch_bounds__(256) k_links_emit(const GeomArgs a, int geometry, int link_rule, int interpolated) {
+    __shared__ uint32_t wsum[8];
+    int x = 0, y = 0, z = 0;
+    int64_t bidx;
+    const Grid& g = a.g;
+    uint32_t mine = 0;
+    int64_t gid = 0;
+    bool valid = box_cell(a, x, y, z, bidx);
+    if (valid) {
+        gid = flat(g, x, y, z);
+        if (persistent_fluid(a.b.mask_next[gid], a.b.mask_prev[gid])) {
+            for (int q = 1; q < 19; ++q) {
+                int sx, sy, sz;
+                if (link_source(g, a.b.mask_next, x, y, z, q, sx, sy, sz) >= 0) ++mine;
+            }
+        } else {
+            valid = false;
+        }
+    }
+    // block-exclusive prefix of `mine`
+    const int t = linear_tid();
+    const int lane = t & 31, warp = t >> 5;
+    uint32_t incl = mine;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    uint32_t wbase = 0;
+    for (int w = 0; w < warp; ++w) wbase += wsum[w];
+    const int block = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    uint32_t pos = a.b.block_offsets[block] + wbase + incl - mine;
+    if (!valid || mine == 0) return;
+    for (int q = 1; q < 19; ++q) {
+        int sx, sy, sz;
+        int64_t s = link_source(g, a.b.mask_next, x, y, z, q, sx, sy, sz);
+        if (s < 0) continue;
+        float qf = 0.5f;
+        if (interpolated) {
+            if (geometry == BFX_GEOMETRY_ELLIPSOID) {
+                qf = ellipsoid_link_fraction(a, x, y, z, sx, sy, sz);
+            } else if (geometry == BFX_GEOMETRY_MESH) {
+                if (link_rule == BFX_LINK_RAY_ROOT) {
+                    qf = mesh_ray_root(a, x, y, z, sx, sy, sz);
+                } else {
+                    float sd = fminf(a.b.wall[s].w, 0.0f);
+                    float fd = fmaxf(a.b.wall[gid].w, 0.0f);
+                    qf = clampf(fd / fmaxf(fd - sd, 1.0e-6f), 1.0e-4f, 1.0f);
+                }
+            }
+        }
+        if (pos < a.b.link_capacity) {
+            a.b.link_cell[pos] = (uint32_t)gid;
+            a.b.link_meta[pos] = (uint32_t)q | ((uint32_t)(a.b.mask_next[s] & kPartMask) << 8);
+            a.b.link_q[pos] = qf;
+        }
+        ++pos;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Moving-wall bounce-back on the link list (BF.metal:2727-2873): reconstruct
+// the incoming population, write it where the fluid step will read it, and
+// accumulate the momentum-exchange load in FP64.
+// ---------------------------------------------------------------------------
+template <class S>
+__global__ void __launch_bounds__(256) k_links_apply(const GeomArgs a, int rep_s) {
+    __shared__ double sh[8][256];
+    using T = typename S::T;
+    using R = typename S::R;
+    const FluidParams& fp = a.fp;
+    const Grid& g = a.g;
+    const int sel = fp.interpolated;
+    const int mode = sel ? fp.force_mode : 6;
+    const int include_link = !sel || fp.load_component != 2;
+    T* A = (T*)a.pops;
+    const T* spill = (const T*)a.spill;
+    const double* body = a.b.state->body;
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int64_t count = a.b.state->link_count;
+    if (count > (int64_t)a.b.link_capacity) count = a.b.link_capacity;
+    const R cs2 = Lat<R>::cs2;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t gid = a.b.link_cell[i];
+        const uint32_t meta = a.b.link_meta[i];
+        const int q = (int)(meta & 0xFF);
+        const int part = (int)(meta >> 8);
+        int x, y, z;
+        unflat(g, gid, x, y, z);
+        int sx = x - cx(q), sy = y - cy(q), sz = z - cz(q);
+        wrap(g, sx, sy, sz);
+        const int64_t src = flat(g, sx, sy, sz);
+        R mwd = (R)fp.far[3];
+        if (fp.local_density) {
+            mwd = 0;
+            for (int k = 0; k < 19; ++k) mwd += canon_load<S>(A, g, a.sp, spill, rep_s, k, x, y, z);
+        }
+        const R reflected = canon_load<S>(A, g, a.sp, spill, rep_s, opp(q), x, y, z);
+        const R dx_ = (R)cx(q), dy_ = (R)cy(q), dz_ = (R)cz(q);
+        R qf = R(0.5);
+        const float4 ws = a.b.wall[src];
+        R wvx = ws.x, wvy = ws.y, wvz = ws.z;
+        int interp = sel;
+        int fx = 0, fy = 0, fz = 0;
+        if (interp) {
+            // clamp(q, 1e-4, 1) and the wall velocity at the intersection (BF.metal:2737-2775)
+            R ql = (R)a.b.link_q[i];
+            ql = ql < R(1.0e-4) ? R(1.0e-4) : ql;
+            qf = ql > R(1) ? R(1) : ql;
+            const float4 wx = a.b.wall[gid];
+            wvx = (R)wx.x + ((R)ws.x - (R)wx.x) * qf;
+            wvy = (R)wx.y + ((R)ws.y - (R)wx.y) * qf;
+            wvz = (R)wx.z + ((R)ws.z - (R)wx.z) * qf;
+            if (qf <= R(0.5)) {
+                fx = x + cx(q);
+                fy = y + cy(q);
+                fz = z + cz(q);
+                const bool fin = inside(g, fx, fy, fz);
+                if (!fin || (a.b.mask_next[flat(g, fx, fy, fz)] & kPartMask) != 0) {
+                    interp = 0;
+                    qf = R(0.5);
+                    wvx = ws.x;
+                    wvy = ws.y;
+                    wvz = ws.z;
+                }
+            }
+        }
+        const R wqv = q <= 6 ? Lat<R>::w1 : Lat<R>::w2;
+        const R wc = R(2) * wqv * mwd * (dx_ * wvx + dy_ * wvy + dz_ * wvz) / cs2;
+        R value = reflected + wc;
+        if (interp) {
+            if (qf <= R(0.5)) {
+                const R fo = canon_load<S>(A, g, a.sp, spill, rep_s, opp(q), fx, fy, fz);
+                value = R(2) * qf * reflected + (R(1) - R(2) * qf) * fo + wc;
+            } else {
+                const R pin = canon_load<S>(A, g, a.sp, spill, rep_s, q, x, y, z);
+                value = (reflected + wc) / (R(2) * qf) + (R(2) * qf - R(1)) * pin / (R(2) * qf);
+            }
+        }
+        int slot_dir = q;
+        T* slot = incoming_slot<S>(A, g, rep_s, q, x, y, z, slot_dir);
+        if (slot) S::st_rt(slot, slot_dir, value);
+        if (fp.accumulate && include_link && (fp.selected_part == 0 || fp.selected_part == part)) {
+            R lx, ly, lz;
+            switch (mode) {
+            case 0:
+                lx = -(value * (dx_ - wvx) - reflected * (-dx_ - wvx));
+                ly = -(value * (dy_ - wvy) - reflected * (-dy_ - wvy));
+                lz = -(value * (dz_ - wvz) - reflected * (-dz_ - wvz));
+                break;
+            case 1:
+            case 6:
+                lx = -(value + reflected) * dx_;
+                ly = -(value + reflected) * dy_;
+                lz = -(value + reflected) * dz_;
+                break;
+            case 2:
+                lx = R(-2) * reflected * dx_;
+                ly = R(-2) * reflected * dy_;
+                lz = R(-2) * reflected * dz_;
+                break;
+            case 3:
+                lx = -wc * dx_;
+                ly = -wc * dy_;
+                lz = -wc * dz_;
+                break;
+            case 4: {
+                R r = value - reflected - wc;
+                lx = -r * dx_;
+                ly = -r * dy_;
+                lz = -r * dz_;
+                break;
+            }
+            case 5:
+                lx = (value - reflected) * wvx;
+                ly = (value - reflected) * wvy;
+                lz = (value - reflected) * wvz;
+                break;
+            default: lx = ly = lz = 0; break;
+            }
+            const V3 world = cell_world(fp, x, y, z);
+            const R dxs = (R)fp.dx;
+            const R bpx = (R)world.x - qf * dx_ * dxs, bpy = (R)world.y - qf * dy_ * dxs, bpz = (R)world.z - qf * dz_ * dxs;
+            add_load<R>(acc, lx, ly, lz, bpx, bpy, bpz, body, fp.f2p);
+        }
+    }
+    block_sum<8>(acc, sh);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 8; ++k) a.b.link_partials[8 * blockIdx.x + k] = acc[k];
+}
+
+// Final fixed-order reduction of the topology and link partials.
+__global__ void k_reduce_loads(const GeomArgs a, int with_topology) {
+    __shared__ double sh[8][256];
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (with_topology)
+        for (int i = threadIdx.x; i < a.b.box_blocks; i += blockDim.x)
+            for (int k = 0; k < 8; ++k) acc[k] += a.b.topo_partials[8 * i + k];
+    double acc2[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int i = threadIdx.x; i < a.b.apply_blocks; i += blockDim.x)
+        for (int k = 0; k < 8; ++k) acc2[k] += a.b.link_partials[8 * i + k];
+    block_sum<8>(acc, sh);
+    __syncthreads();
+    block_sum<8>(acc2, sh);
+    if (threadIdx.x == 0) {
+        DeviceState* st = a.b.state;
+        for (int k = 0; k < 3; ++k) {
+            st->loads_lattice[k] = acc[k] + acc2[k];
+            st->loads_torque[k] = acc[3 + k] + acc2[3 + k];
+        }
+        if (with_topology) {
+            st->covered_count = (int64_t)acc[6];
+            st->uncovered_count = (int64_t)acc[7];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// End of step: FP64 6-DOF update (integrateBirdBody BF.metal:6574-6627 in
+// FP64), runtime safety ledger (monitorBirdRuntimeSafety BF.metal:6629-6707),
+// step counter.  One thread.
+// ---------------------------------------------------------------------------
+__device__ void qnormalize_d(double* q) {
+    double n2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+    if (n2 > 1.0e-40) {
+        double n = sqrt(n2);
+        for (int k = 0; k < 4; ++k) q[k] = q[k] / n;
+    } else {
+        q[0] = q[1] = q[2] = 0.0;
+        q[3] = 1.0;
+    }
+}
+
+__global__ void k_finish(const GeomArgs a, float gx, float gy, float gz, int substeps, int free_flight,
+                         const bfx_bird* bird_ptr) {
+    DeviceState* st = a.b.state;
+    const FluidParams& fp = a.fp;
+    if (free_flight) {
+        const bfx_bird& bird = *bird_ptr;
+        double force[3], torque[3];
+        for (int k = 0; k < 3; ++k) {
+            force[k] = st->loads_lattice[k] * (double)fp.f2p;
+            force[k] = force[k] + (double)st->wing_reaction[k] + (double)st->wing_reaction[8 + k];
+            torque[k] = st->loads_torque[k] + (double)st->wing_reaction[4 + k] + (double)st->wing_reaction[12 + k];
+        }
+        int n = substeps < 1 ? 1 : substeps;
+        double dt = (double)fp.dt / (double)n;
+        double mass = (double)bird.body_radii_mass.v[3];
+        double inertia[3] = {(double)bird.inertia.v[0], (double)bird.inertia.v[1], (double)bird.inertia.v[2]};
+        double grav[3] = {(double)gx, (double)gy, (double)gz};
+        double* b = st->body;
+        double v[3] = {b[7], b[8], b[9]}, x[3] = {b[0], b[1], b[2]}, o[4] = {b[3], b[4], b[5], b[6]},
+               w[3] = {b[10], b[11], b[12]};
+        qnormalize_d(o);
+        for (int s = 0; s < n; ++s) {
+            for (int k = 0; k < 3; ++k) v[k] += (force[k] / mass + grav[k]) * dt;
+            for (int k = 0; k < 3; ++k) x[k] += v[k] * dt;
+            // torque into the body frame: rotate by the conjugate
+            double cq[3] = {-o[0], -o[1], -o[2]};
+            double t1[3] = {cq[1] * torque[2] - cq[2] * torque[1], cq[2] * torque[0] - cq[0] * torque[2],
+                            cq[0] * torque[1] - cq[1] * torque[0]};
+            t1[0] *= 2.0;
+            t1[1] *= 2.0;
+            t1[2] *= 2.0;
+            double c2[3] = {cq[1] * t1[2] - cq[2] * t1[1], cq[2] * t1[0] - cq[0] * t1[2], cq[0] * t1[1] - cq[1] * t1[0]};
+            double tb[3];
+            for (int k = 0; k < 3; ++k) tb[k] = torque[k] + o[3] * t1[k] + c2[k];
+            double am[3] = {inertia[0] * w[0], inertia[1] * w[1], inertia[2] * w[2]};
+            double gyr[3] = {w[1] * am[2] - w[2] * am[1], w[2] * am[0] - w[0] * am[2], w[0] * am[1] - w[1] * am[0]};
+            for (int k = 0; k < 3; ++k) w[k] += ((tb[k] - gyr[k]) / inertia[k]) * dt;
+            double cr[3] = {o[1] * w[2] - o[2] * w[1], o[2] * w[0] - o[0] * w[2], o[0] * w[1] - o[1] * w[0]};
+            double d[4];
+            for (int k = 0; k < 3; ++k) d[k] = o[3] * w[k] + cr[k];
+            d[3] = -(o[0] * w[0] + o[1] * w[1] + o[2] * w[2]);
+            double nq[4];
+            for (int k = 0; k < 4; ++k) nq[k] = o[k] + 0.5 * dt * d[k];
+            qnormalize_d(nq);
+            for (int k = 0; k < 4; ++k) o[k] = nq[k];
+        }
+        b[0] = x[0]; b[1] = x[1]; b[2] = x[2];
+        b[3] = o[0]; b[4] = o[1]; b[5] = o[2]; b[6] = o[3];
+        b[7] = v[0]; b[8] = v[1]; b[9] = v[2];
+        b[10] = w[0]; b[11] = w[1]; b[12] = w[2];
+
+        // runtime safety on the FP32 view of the body
+        float4 of = qnormalize(make_float4((float)b[3], (float)b[4], (float)b[5], (float)b[6]));
+        const float* le = bird.safety_geometry.v;
+        V3 ea = qrotate(of, v3(le[0], 0, 0)), eb = qrotate(of, v3(0, le[1], 0)), ec = qrotate(of, v3(0, 0, le[2]));
+        V3 we = v3(fabsf(ea.x) + fabsf(eb.x) + fabsf(ec.x), fabsf(ea.y) + fabsf(eb.y) + fabsf(ec.y),
+                   fabsf(ea.z) + fabsf(eb.z) + fabsf(ec.z));
+        float dx = fp.dx;
+        float margin = (fp.sponge_width + 3.0f) * dx;
+        const int dims[3] = {a.g.nx, a.g.ny, a.g.nz};
+        float pos[3] = {(float)b[0], (float)b[1], (float)b[2]};
+        float wef[3] = {we.x, we.y, we.z};
+        float clearance = __int_as_float(0x7f800000);
+        for (int k = 0; k < 3; ++k) {
+            float mn = fp.origin[k] + margin;
+            float mx = fp.origin[k] + (float)dims[k] * dx - margin;
+            float lc = pos[k] - wef[k] - mn;
+            float uc = mx - pos[k] - wef[k];
+            clearance = fminf(clearance, fminf(lc, uc));
+        }
+        float v2l = fp.v2l;
+        V3 rv = v3((float)b[7] - fp.far[0] / v2l, (float)b[8] - fp.far[1] / v2l, (float)b[9] - fp.far[2] / v2l);
+        float rel = length(rv);
+        float rot = length(v3((float)b[10], (float)b[11], (float)b[12])) * bird.safety_geometry.v[3];
+        float surface = rel + rot + bird.safety_limits.v[0];
+        float mach = surface * v2l / sqrtf(1.0f / 3.0f);
+        bool finite = isfinite(mach) && isfinite(clearance);
+        for (int k = 0; k < 13; ++k) finite = finite && isfinite((float)b[k]);
+        if (isfinite(mach)) st->safety_metrics[0] = fmaxf(st->safety_metrics[0], mach);
+        if (isfinite(clearance)) st->safety_metrics[1] = fminf(st->safety_metrics[1], clearance);
+        uint32_t flags = 0;
+        if (!finite) flags |= 4u;
+        if (isfinite(mach) && mach > bird.safety_limits.v[1]) flags |= 1u;
+        if (isfinite(clearance) && clearance < 0.0f) flags |= 2u;
+        uint64_t absolute = st->step + 1;
+        if (flags != 0 && st->safety_event[2] == 0) {
+            st->safety_event[0] = (uint32_t)(absolute & 0xFFFFFFFFu);
+            st->safety_event[1] = (uint32_t)(absolute >> 32);
+            st->safety_event[2] = flags;
+            st->safety_event[3] = 0;
+            st->safety_metrics[2] = mach;
+            st->safety_metrics[3] = clearance;
+        }
+    }
+    st->step += 1;
+}
+
+__global__ void k_record_sample(const GeomArgs a, bfx_run_sample* samples, uint64_t index, float dt) {
+    const DeviceState* st = a.b.state;
+    bfx_run_sample& s = samples[index];
+    s.time = (double)(float)((double)st->step * (double)dt);
+    for (int k = 0; k < 3; ++k) s.position[k] = st->body[k];
+    for (int k = 0; k < 4; ++k) s.orientation[k] = st->body[3 + k];
+    for (int k = 0; k < 3; ++k) {
+        s.velocity[k] = st->body[7 + k];
+        s.omega_body[k] = st->body[10 + k];
+        s.force[k] = st->loads_lattice[k] * (double)a.fp.f2p;
+        s.torque[k] = st->loads_torque[k];
+        s.left_hinge_force[k] = st->wing_reaction[k];
+        s.left_hinge_torque[k] = st->wing_reaction[4 + k];
+        s.right_hinge_force[k] = st->wing_reaction[8 + k];
+        s.right_hinge_torque[k] = st->wing_reaction[12 + k];
+    }
+    s.step = st->step;
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers
+// ---------------------------------------------------------------------------
+static GeomArgs make_geom(const GridDesc& gd, const FluidParams& fp, const BoxDesc& box, const GeomBuffers& gb,
+                          void* pops, void* spill) {
+    GeomArgs a;
+    a.g.nx = gd.nx;
+    a.g.ny = gd.ny;
+    a.g.nz = gd.nz;
+    a.g.per_x = gd.per_x;
+    a.g.per_y = gd.per_y;
+    a.g.per_z = gd.per_z;
+    a.g.n = gd.n;
+    a.g.nxy = gd.nxy;
+    for (int f = 0; f < 6; ++f) a.sp.off[f] = gd.spill_off[f];
+    a.fp = fp;
+    a.bx = box.sx;
+    a.by = box.sy;
+    a.bz = box.sz;
+    a.box_cells = box.cells;
+    a.b = gb;
+    a.pops = pops;
+    a.spill = spill;
+    return a;
+}
+
+static void box_shape(const BoxDesc& box, dim3& grid, dim3& block) {
+    int bx = box.sx >= 64 ? 64 : ((box.sx + 31) / 32) * 32;
+    if (bx < 32) bx = 32;
+    int by = 256 / bx;
+    block = dim3(bx, by, 1);
+    grid = dim3((box.sx + bx - 1) / bx, (box.sy + by - 1) / by, box.sz);
+}
+
+int box_block_count(const BoxDesc& box) {
+    dim3 grid, block;
+    box_shape(box, grid, block);
+    return (int)(grid.x * grid.y * grid.z);
+}
+
+void launch_prepare(int geometry, float dt, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
+                    const GeomBuffers& gb, int init, cudaStream_t s) {
+    GeomArgs a = make_geom(g, fp, box, gb, nullptr, nullptr);
+    k_prepare<<<1, 1, 0, s>>>(a, init, dt, 0.0f);
+    (void)geometry;
+}
+
+void launch_classify(int geometry, int has_prev, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
+                     const GeomBuffers& gb, cudaStream_t s) {
+    GeomArgs a = make_geom(g, fp, box, gb, nullptr, nullptr);
+    dim3 grid, block;
+    box_shape(box, grid, block);
+    if (geometry == BFX_GEOMETRY_BIRD) {
+        k_classify_bird<<<grid, block, 0, s>>>(a, has_prev);
+    } else if (geometry == BFX_GEOMETRY_ELLIPSOID) {
+        k_classify_ellipsoid<<<grid, block, 0, s>>>(a, has_prev);
+    } else if (geometry == BFX_GEOMETRY_MESH) {
+        k_mesh_prepare<<<(gb.nverts + 255) / 256, 256, 0, s>>>(a);
+        k_mesh_clear<<<(unsigned)((box.cells + 255) / 256), 256, 0, s>>>(a);
+        k_mesh_raster<<<(gb.ntris + 127) / 128, 128, 0, s>>>(a);
+        k_mesh_resolve<<<grid, block, 0, s>>>(a, has_prev);
+    }
+}
+
+template <class S>
+static void scan_s(const GeomArgs& a, int rep_s, const BoxDesc& box, cudaStream_t s) {
+    dim3 grid, block;
+    box_shape(box, grid, block);
+    k_boundary_scan<S><<<grid, block, 0, s>>>(a, rep_s);
+}
+
+#define BFX_DISPATCH_STORAGE(storage, FN, ...)                             \
+    switch (storage) {                                                     \
+    case BFX_STORAGE_F16_DEVIATION: FN<StoreF16Dev>(__VA_ARGS__); break;   \
+    case BFX_STORAGE_BF16_DEVIATION: FN<StoreBF16Dev>(__VA_ARGS__); break; \
+    case BFX_STORAGE_F64: FN<StoreF64>(__VA_ARGS__); break;                \
+    default: FN<StoreF32>(__VA_ARGS__); break;                             \
+    }
+
+void launch_boundary_scan(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
+                          const GeomBuffers& gb, const FluidBuffers& fb, cudaStream_t s) {
+    GeomArgs a = make_geom(g, fp, box, gb, fb.pops, fb.spill);
+    BFX_DISPATCH_STORAGE(storage, scan_s, a, rep_s, box, s);
+}
+
+void launch_links_emit(int geometry, int link_rule, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
+                       const GeomBuffers& gb, cudaStream_t s) {
+    GeomArgs a = make_geom(g, fp, box, gb, nullptr, nullptr);
+    k_scan<<<1, 1024, 0, s>>>(a);
+    dim3 grid, block;
+    box_shape(box, grid, block);
+    k_links_emit<<<grid, block, 0, s>>>(a, geometry, link_rule, fp.interpolated);
+}
+
+template <class S>
+static void apply_s(const GeomArgs& a, int rep_s, cudaStream_t s) {
+    k_links_apply<S><<<a.b.apply_blocks, 256, 0, s>>>(a, rep_s);
+}
+
+void launch_links_apply(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const GeomBuffers& gb,
+                        const FluidBuffers& fb, cudaStream_t s) {
+    BoxDesc box = {1, 1, 1, 1};
+    GeomArgs a = make_geom(g, fp, box, gb, fb.pops, fb.spill);
+    BFX_DISPATCH_STORAGE(storage, apply_s, a, rep_s, s);
+}
+
+void launch_reduce_loads(const GeomBuffers& gb, int with_topology, cudaStream_t s) {
+    GridDesc g = {};
+    FluidParams fp = {};
+    BoxDesc box = {1, 1, 1, 1};
+    GeomArgs a = make_geom(g, fp, box, gb, nullptr, nullptr);
+    k_reduce_loads<<<1, 256, 0, s>>>(a, with_topology);
+}
+
+void launch_integrate(const GridDesc& g, const FluidParams& fp, const GeomBuffers& gb, float gravity_x,
+                      float gravity_y, float gravity_z, int substeps, int free_flight, cudaStream_t s) {
+    BoxDesc box = {1, 1, 1, 1};
+    GeomArgs a = make_geom(g, fp, box, gb, nullptr, nullptr);
+    k_finish<<<1, 1, 0, s>>>(a, gravity_x, gravity_y, gravity_z, substeps, free_flight, gb.bird);
+}
+
+void launch_record_sample(const GeomBuffers& gb, bfx_run_sample* samples, uint64_t index, float dt, cudaStream_t s) {
+    GridDesc g = {};
+    FluidParams fp = {};
+    BoxDesc box = {1, 1, 1, 1};
+    GeomArgs a = make_geom(g, fp, box, gb, nullptr, nullptr);
+    k_record_sample<<<1, 1, 0, s>>>(a, samples, index, dt);
+}
+
+void launch_fill_wall(float4* wall, int64_t n, float w, cudaStream_t s) {
+    k_fill_wall_w<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(wall, n, w);
+}
+
+}  // namespace bfx

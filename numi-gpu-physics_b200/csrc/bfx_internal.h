@@ -1,0 +1,107 @@
+// Host-side launcher interface between the runtime (bfx_api.cu) and the
+// kernel translation units.  Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "bfx_types.h"
+
+namespace bfx {
+
+struct GridDesc {
+    int nx, ny, nz;
+    int per_x, per_y, per_z;
+    int64_t n, nxy;
+    int64_t spill_off[6];   // element offsets of the six spill planes
+    int64_t ghost_off[6];   // element offsets of the six ghost planes
+    int64_t spill_total;
+};
+
+struct FluidBuffers {
+    void* pops;             // 19 * n elements of the storage type
+    void* spill;            // 5 * face cells per face
+    void* ghost;            // 5 * face cells per face (outflow faces)
+    uint8_t* mask;          // current occupancy (part id + topology flags); may be null
+    const float4* wall;     // wall velocity / distance; may be null without geometry
+    float* density;         // captured fields
+    float4* velocity;
+    DeviceState* state;
+};
+
+// Fused stream + collide over the whole lattice (one launch).
+void launch_bulk(int storage, int collision, int rep_s, const GridDesc& g, const FluidParams& fp,
+                 const FluidBuffers& b, int capture, cudaStream_t s);
+// Zero-gradient outflow ghost planes (before the step).
+void launch_ghost(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const FluidBuffers& b,
+                  cudaStream_t s);
+// Equilibrium initialisation into representation E.
+void launch_init(int storage, int init_kind, float amplitude, const GridDesc& g, const FluidParams& fp,
+                 const FluidBuffers& b, cudaStream_t s);
+// Canonical FP32 read-out / write-in of f*_q(x) ([19][n]).
+void launch_readout(int storage, int rep_s, const GridDesc& g, const FluidBuffers& b, float* out, cudaStream_t s);
+void launch_writein(int storage, int rep_s, const GridDesc& g, const FluidBuffers& b, const float* in,
+                    cudaStream_t s);
+// Macroscopic fields from the canonical populations.
+void launch_macroscopic(int storage, int rep_s, const GridDesc& g, const FluidBuffers& b, cudaStream_t s);
+// FP64 fluid mass / momentum (partials[blocks*4], result[4]).
+void launch_mass_momentum(int storage, int rep_s, const GridDesc& g, const FluidBuffers& b, double* partials,
+                          int blocks, double* result, cudaStream_t s);
+
+// ---- geometry, links, loads, body -------------------------------------
+struct BoxDesc {
+    int sx, sy, sz;         // extent of the geometry region (cells)
+    int64_t cells;
+};
+
+struct GeomBuffers {
+    const bfx_bird* bird;           // device copy
+    uint8_t* mask_prev;
+    uint8_t* mask_next;
+    float4* wall;
+    // mesh
+    const float* mesh_local;        // 3 per vertex
+    const uint8_t* mesh_segment;
+    const uint32_t* mesh_tris;
+    const uint8_t* mesh_tri_part;
+    float4* mesh_pos;
+    float4* mesh_vel;
+    unsigned long long* keys;       // box-local
+    uint32_t nverts, ntris;
+    float half_thickness;
+    // links
+    uint32_t* link_cell;
+    uint32_t* link_meta;            // direction | part << 8
+    float* link_q;
+    uint32_t link_capacity;
+    uint32_t* block_counts;         // per box block
+    uint32_t* block_offsets;
+    int box_blocks;
+    double* topo_partials;          // 8 per box block
+    double* link_partials;          // 8 per apply block
+    int apply_blocks;
+    DeviceState* state;
+};
+
+void launch_prepare(int geometry, float dt, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
+                    const GeomBuffers& gb, int init, cudaStream_t s);
+void launch_classify(int geometry, int has_prev, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
+                     const GeomBuffers& gb, cudaStream_t s);
+void launch_boundary_scan(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
+                          const GeomBuffers& gb, const FluidBuffers& fb, cudaStream_t s);
+void launch_links_emit(int geometry, int link_rule, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
+                       const GeomBuffers& gb, cudaStream_t s);
+void launch_links_apply(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const GeomBuffers& gb,
+                        const FluidBuffers& fb, cudaStream_t s);
+void launch_reduce_loads(const GeomBuffers& gb, int with_topology, cudaStream_t s);
+void launch_integrate(const GridDesc& g, const FluidParams& fp, const GeomBuffers& gb, float gravity_x,
+                      float gravity_y, float gravity_z, int substeps, int free_flight, cudaStream_t s);
+void launch_record_sample(const GeomBuffers& gb, bfx_run_sample* samples, uint64_t index, float dt, cudaStream_t s);
+void launch_step_counter(DeviceState* st, cudaStream_t s);
+
+}  // namespace bfx
+
+namespace bfx {
+int box_block_count(const BoxDesc& box);
+void launch_fill_wall(float4* wall, int64_t n, float w, cudaStream_t s);
+}  // namespace bfx

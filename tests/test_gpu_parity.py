@@ -1,0 +1,212 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle.
+
+Tolerances (from the reference's own gates and the task contract):
+  FP32 populations   <= 1e-6 relative per value (the FP32 path is built to be
+                     bit-identical; the tests also report exact equality)
+  body loads         <= 1e-5 relative (FP64 sums of identical contributions)
+  masks, cut links   bit-exact (set of (fluid cell, direction) pairs)
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import math
+
+import numpy as np
+import pytest
+
+import bfx._lib as L
+import bfx.cases as cases
+import oracle as O
+from bfx.simulation import Lattice, bird_struct
+from helpers import body_struct_from_tuple, oracle_twin, rel_diff
+
+pytestmark = pytest.mark.gpu
+
+POP_RTOL = 1e-6
+LOAD_RTOL = 1e-5
+
+
+def make_pair(cfg, rows=None, body=None, mesh=None):
+    lat = Lattice(cfg, bird_struct(rows) if rows is not None else None,
+                  body_struct_from_tuple(body) if body is not None else None, mesh)
+    osim = oracle_twin(cfg, rows, body, mesh)
+    return lat, osim
+
+
+def compare_pops(lat, osim, what=""):
+    g = lat.populations().ravel()
+    o = osim.pa
+    d = np.abs(g.astype(np.float64) - o.astype(np.float64))
+    rel = float(np.max(d / np.maximum(np.abs(o.astype(np.float64)), 1e-12)))
+    assert np.all(np.isfinite(g)), what
+    assert rel <= POP_RTOL, f"{what}: max relative population difference {rel:.3e}"
+    return rel, bool(np.array_equal(g, o))
+
+
+def compare_loads(lat, osim, what=""):
+    ld = lat.loads()
+    gf = np.array(ld.force)
+    gt = np.array(ld.torque)
+    of = np.array(osim.loads.f64_force)
+    ot = np.array(osim.loads.f64_torque)
+    fscale = max(np.max(np.abs(of)), 1e-30)
+    tscale = max(np.max(np.abs(ot)), 1e-30)
+    assert np.max(np.abs(gf - of)) <= LOAD_RTOL * fscale + 1e-300, f"{what}: force {gf} vs {of}"
+    assert np.max(np.abs(gt - ot)) <= LOAD_RTOL * tscale + 1e-300, f"{what}: torque {gt} vs {ot}"
+    return gf, of
+
+
+def oracle_links(osim):
+    n = osim.n
+    cap = 18 * n
+    cell = np.zeros(cap, np.uint32)
+    d = np.zeros(cap, np.uint8)
+    cnt = O.lib().or_enumerate_links(ct.byref(osim.p), O.u8ptr(osim.mnext), O.u8ptr(osim.mcur),
+                                     cell.ctypes.data_as(ct.POINTER(ct.c_uint32)), O.u8ptr(d), cap)
+    return cell[:cnt], d[:cnt]
+
+
+def link_set(cell, d):
+    key = cell.astype(np.uint64) * 32 + d.astype(np.uint64)
+    return np.sort(key)
+
+
+# --------------------------------------------------------------------------
+# Periodic shear wave (config 1 family): full-lattice pull + TRT
+# --------------------------------------------------------------------------
+def test_shear_wave_per_step_matches_oracle():
+    cfg, _, _, _ = cases.shear_wave(n=24, viscosity=0.03, magic=3.0 / 16.0, axis="y")
+    lat, osim = make_pair(cfg)
+    compare_pops(lat, osim, "initial")
+    exact = True
+    for step in range(8):
+        lat.advance(1)
+        osim.step()
+        rel, eq = compare_pops(lat, osim, f"step {step + 1}")
+        exact &= eq
+    # odd and even AA parities both covered; the FP32 build reproduces the oracle bit for bit
+    assert exact
+
+
+def test_shear_wave_64_analytic_decay_and_oracle():
+    """64^3, nu = 0.01, magic 1/4, u_x = 0.01 sin(2 pi z / 64), 2000 steps."""
+    cfg, _, _, _ = cases.shear_wave(n=64, viscosity=0.01, magic=0.25, amplitude=0.01, axis="z")
+    lat, osim = make_pair(cfg)
+    lat.advance(2000, batch_size=256, capture_fields=True)
+    rho, vel = lat.fields()
+    z = np.arange(64)
+    prof = vel[:, 0].reshape(64, 64, 64).mean(axis=(1, 2))
+    amp = 2.0 * np.dot(prof, np.sin(2 * np.pi * z / 64)) / 64
+    analytic = 0.01 * math.exp(-0.01 * (2 * math.pi / 64) ** 2 * 2000)
+    assert abs(amp - analytic) / analytic < 0.03
+    osim.advance(2000)
+    compare_pops(lat, osim, "2000 steps")
+    mm = lat.mass_momentum()
+    assert abs(mm[0] - 19 * 0 - 64 ** 3) / 64 ** 3 < 5e-6
+
+
+@pytest.mark.parametrize("collision", [L.COLLISION_TRT_LIMITER, L.COLLISION_REGULARIZED, L.COLLISION_RR3])
+def test_collision_operators_match_oracle(collision):
+    cfg, _, _, _ = cases.shear_wave(n=20, viscosity=0.02, magic=3.0 / 16.0, amplitude=0.05, axis="y",
+                                    collision=collision)
+    lat, osim = make_pair(cfg)
+    for step in range(6):
+        lat.advance(1)
+        osim.step()
+        compare_pops(lat, osim, f"collision {collision} step {step + 1}")
+
+
+# --------------------------------------------------------------------------
+# Ellipsoid in a channel (config 2 family): RR3, interpolated links,
+# velocity inlet, zero-gradient outflow, periodic y/z, static geometry
+# --------------------------------------------------------------------------
+@pytest.mark.parametrize("collision", [L.COLLISION_RR3, L.COLLISION_TRT])
+def test_ellipsoid_channel_matches_oracle(collision):
+    cfg, rows, body, _ = cases.ellipsoid_channel(nx=64, ny=32, nz=32, radii=(9.0, 5.0, 4.5), inflow=0.05,
+                                                 viscosity=0.02, collision=collision)
+    lat, osim = make_pair(cfg, rows, body)
+    assert np.array_equal(lat.mask(), osim.mcur)
+    for step in range(12):
+        lat.advance(1)
+        osim.step()
+        compare_pops(lat, osim, f"ellipsoid step {step + 1}")
+        compare_loads(lat, osim, f"ellipsoid step {step + 1}")
+    cell, d, q = lat.links()
+    oc, od = oracle_links(osim)
+    assert np.array_equal(link_set(cell, d), link_set(oc, od))
+    # link fractions against the oracle's bisection
+    nx, ny = cfg.nx, cfg.ny
+    for i in range(0, len(cell), max(1, len(cell) // 200)):
+        g = int(cell[i])
+        x, y, z = g % nx, (g // nx) % ny, g // (nx * ny)
+        qq = int(d[i])
+        c, _, _ = O.lattice()
+        sx, sy, sz = x - c[qq][0], y - c[qq][1], z - c[qq][2]
+        oq = O.lib().or_ellipsoid_link_fraction(ct.byref(osim.p), ct.byref(osim.bird), ct.byref(osim.prep),
+                                                x, y, z, sx, sy, sz)
+        assert q[i] == np.float32(oq)
+
+
+# --------------------------------------------------------------------------
+# Analytic bird (reference production path): moving halfway links
+# --------------------------------------------------------------------------
+def _compact_bird_lattice(free_flight=False):
+    from bfx.simulation import BirdFlowSimulation
+    config, bird, state = cases.compact_bird(free_flight=free_flight)
+    sim = BirdFlowSimulation(config, bird, state)
+    cfg = sim.lattice.config
+    rows = bird.packed()
+    body = (state.position_meters, state.orientation_body_to_world, state.linear_velocity_meters_per_second,
+            state.angular_velocity_body_radians_per_second)
+    osim = oracle_twin(cfg, rows, body)
+    return sim, osim
+
+
+def test_compact_bird_moving_boundary_matches_oracle():
+    sim, osim = _compact_bird_lattice(False)
+    lat = sim.lattice
+    assert np.array_equal(lat.mask(), osim.mcur)
+    for step in range(10):
+        lat.advance(1)
+        osim.step()
+        assert np.array_equal(lat.mask(), osim.mcur), f"mask step {step + 1}"
+        compare_pops(lat, osim, f"bird step {step + 1}")
+        compare_loads(lat, osim, f"bird step {step + 1}")
+        cell, d, _ = lat.links()
+        oc, od = oracle_links(osim)
+        assert np.array_equal(link_set(cell, d), link_set(oc, od)), f"links step {step + 1}"
+
+
+def test_compact_bird_free_flight_matches_oracle():
+    sim, osim = _compact_bird_lattice(True)
+    lat = sim.lattice
+    for step in range(10):
+        lat.advance(1)
+        osim.step()
+        compare_pops(lat, osim, f"free flight step {step + 1}")
+        compare_loads(lat, osim, f"free flight step {step + 1}")
+        b = lat.body()
+        assert rel_diff(list(b.position), list(osim.body64.position)) < 1e-12
+        assert np.allclose(list(b.velocity), list(osim.body64.velocity), rtol=1e-9, atol=1e-12)
+        assert np.allclose(list(b.orientation), list(osim.body64.orientation), rtol=1e-9, atol=1e-12)
+
+
+# --------------------------------------------------------------------------
+# Articulated triangle mesh (config 3 family): rasterise, resolve, cut links
+# --------------------------------------------------------------------------
+@pytest.mark.parametrize("link_rule", [L.LINK_LINEAR, L.LINK_RAY_ROOT])
+def test_flapping_plate_mesh_matches_oracle(link_rule):
+    cfg, rows, body, mesh = cases.flapping_plates(nx=96, ny=64, nz=64, span=16.0, chord=6.0, thickness=2.0,
+                                                  n_chord=6, n_span=16, period=120.0, viscosity=0.02,
+                                                  link_rule=link_rule, sponge_width=6.0)
+    lat, osim = make_pair(cfg, rows, body, mesh)
+    assert np.array_equal(lat.mask(), osim.mcur)
+    for step in range(8):
+        lat.advance(1)
+        osim.step()
+        assert np.array_equal(lat.mask(), osim.mcur), f"mask step {step + 1}"
+        compare_pops(lat, osim, f"mesh step {step + 1}")
+        compare_loads(lat, osim, f"mesh step {step + 1}")
+        cell, d, q = lat.links()
+        oc, od = oracle_links(osim)
+        assert np.array_equal(link_set(cell, d), link_set(oc, od)), f"links step {step + 1}"
