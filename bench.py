@@ -41,33 +41,55 @@ FALLBACK_HBM_GBS = 6650.0
 WORKLOAD_DEFAULT = "ellipsoid_channel"
 
 
-def build_case(name: str, storage: int):
+LATTICE_OVERRIDE = None  # (nx, ny, nz) for small profiling cases; geometry scales with it
+
+
+def build_case(name: str, storage: int, collision: str | None = None):
     import bfx._lib as L
     import bfx.cases as cases
+    coll_id = {"trt": L.COLLISION_TRT, "rr3": L.COLLISION_RR3, "reg": L.COLLISION_REGULARIZED,
+               "limiter": L.COLLISION_TRT_LIMITER}
     if name == "ellipsoid_channel":
-        cfg, rows, body, mesh = cases.ellipsoid_channel(storage=storage)
-        desc = ("ellipsoid_channel 256x128x128 semi-axes (24,12,12) at x=64, inflow u_x=0.05 velocity inlet, "
-                "zero-gradient outflow, periodic y/z, nu=0.005, RR3, interpolated bounce-back")
-        collision = "rr3"
+        kw = {}
+        if LATTICE_OVERRIDE:
+            nx, ny, nz = LATTICE_OVERRIDE
+            kw = dict(nx=nx, ny=ny, nz=nz, radii=(24.0 * nx / 256, 12.0 * ny / 128, 12.0 * nz / 128))
+        if collision:
+            kw["collision"] = coll_id[collision]
+        cfg, rows, body, mesh = cases.ellipsoid_channel(storage=storage, **kw)
+        desc = (f"ellipsoid_channel {cfg.nx}x{cfg.ny}x{cfg.nz} semi-axes {tuple(rows[0][:3])} at x={cfg.nx // 4}, "
+                f"inflow u_x=0.05 velocity inlet, zero-gradient outflow, periodic y/z, nu=0.005, "
+                f"{collision or 'rr3'}, interpolated bounce-back")
+        collision = collision or "rr3"
     elif name == "flapping_plates":
-        cfg, rows, body, mesh = cases.flapping_plates(storage=storage)
-        desc = ("flapping_plates 512x256x256 two 64x12x2 flat plates (2x8192 triangles), stroke 60deg sin, "
-                "pitch 45deg cos, T=4000, nu=0.004, TRT, ray-root links rebuilt each step")
-        collision = "trt"
+        kw = {}
+        if LATTICE_OVERRIDE:
+            kw = dict(zip(("nx", "ny", "nz"), LATTICE_OVERRIDE))
+        if collision:
+            kw["collision"] = coll_id[collision]
+        cfg, rows, body, mesh = cases.flapping_plates(storage=storage, **kw)
+        desc = (f"flapping_plates {cfg.nx}x{cfg.ny}x{cfg.nz} two 64x12x2 flat plates (2x8192 triangles), "
+                f"stroke 60deg sin, pitch 45deg cos, T=4000, nu=0.004, {collision or 'trt'}, ray-root links "
+                f"rebuilt each step")
+        collision = collision or "trt"
     elif name == "shear_wave":
-        cfg, rows, body, mesh = cases.shear_wave(n=64, viscosity=0.01, magic=0.25, axis="z", storage=storage)
-        desc = "shear_wave 64^3 periodic, u_x=0.01 sin(2 pi z/64), nu=0.01, magic 1/4, TRT (L2-resident)"
-        collision = "trt"
+        n = LATTICE_OVERRIDE[0] if LATTICE_OVERRIDE else 64
+        cfg, rows, body, mesh = cases.shear_wave(n=n, viscosity=0.01, magic=0.25, axis="z", storage=storage,
+                                                 collision=coll_id[collision] if collision else L.COLLISION_TRT)
+        desc = f"shear_wave {n}^3 periodic, u_x=0.01 sin(2 pi z/{n}), nu=0.01, magic 1/4, {collision or 'trt'}"
+        collision = collision or "trt"
     else:
         raise SystemExit(f"unknown workload {name}")
     return cfg, rows, body, mesh, desc, collision
 
 
+COLLISION_OVERRIDE = None
+
+
 def make_lattice(name, storage, device):
     import bfx._lib as L
     from bfx.simulation import Lattice, bird_struct
-    from bfx.simulation import default_config  # noqa: F401
-    cfg, rows, body, mesh, desc, coll = build_case(name, storage)
+    cfg, rows, body, mesh, desc, coll = build_case(name, storage, COLLISION_OVERRIDE)
     cfg.device = device
     bs = None
     if body is not None:
@@ -158,14 +180,18 @@ def profiled_traffic(workload: str, storage_name: str):
 
 
 def time_steps(lat, steps, warmup):
-    """Device time of `steps` steps (CUDA events on the library stream) plus kernel stats."""
+    """Device time of `steps` steps (CUDA events on the library stream), then the
+    fused interior kernel's own per-launch CUDA-event times over a second run of
+    the same steps (per-launch events disable the step graphs, so they are kept
+    out of the whole-step timing)."""
     lat.advance(warmup, batch_size=max(warmup, 1))
-    lat.set_kernel_timing(True)
     l0 = lat.launch_count()
     lat.timer_begin()
     lat.advance(steps, batch_size=steps)
     ms = lat.timer_end()
     l1 = lat.launch_count()
+    lat.set_kernel_timing(True)
+    lat.advance(min(steps, 400), batch_size=min(steps, 400))
     kms, klaunch = lat.kernel_timing()
     lat.set_kernel_timing(False)
     return ms, l1 - l0, kms, klaunch
@@ -212,7 +238,7 @@ def cpu_port_rate(name, seconds_budget=12.0, max_steps=64):
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle as O  # noqa: F401  (checker library, CPU baseline only)
     from helpers import oracle_twin
-    cfg, rows, body, mesh, desc, _ = build_case(name, 0)
+    cfg, rows, body, mesh, desc, _ = build_case(name, 0, COLLISION_OVERRIDE)
     osim = oracle_twin(cfg, rows, body, mesh)
     osim.step()
     t0 = time.perf_counter()
@@ -232,7 +258,7 @@ def run_reference_arm(args, rank, world):
     name = args.workload
     if rank != 0:
         return 0
-    cfg, rows, body, mesh, desc, coll = build_case(name, 0)
+    cfg, rows, body, mesh, desc, coll = build_case(name, 0, COLLISION_OVERRIDE)
     budget = 150.0
     per_step_budget = budget / max(args.steps + args.warmup, 1)
     rate, steps, cores, dt = cpu_port_rate(name, seconds_budget=min(60.0, per_step_budget * args.steps),
@@ -261,8 +287,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--lattice", type=int, nargs=3, default=None, help="profiling override of the lattice size")
+    ap.add_argument("--collision", default=None, choices=["trt", "rr3", "reg", "limiter"])
+    ap.add_argument("--storage", default="f32", choices=["f32", "f16dev", "bf16dev", "f64"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    global LATTICE_OVERRIDE, COLLISION_OVERRIDE
+    LATTICE_OVERRIDE = tuple(args.lattice) if args.lattice else None
+    COLLISION_OVERRIDE = args.collision
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -283,8 +315,10 @@ def main():
         return rc
 
     import bfx._lib as L
-    lat, cfg, desc, coll = make_lattice(args.workload, L.STORAGE_F32, local)
+    main_storage = {v: k for k, v in L.STORAGE_NAMES.items()}[args.storage]
+    lat, cfg, desc, coll = make_lattice(args.workload, main_storage, local)
     cells = cfg.nx * cfg.ny * cfg.nz
+    sbytes = L.STORAGE_BYTES[main_storage]
 
     def barrier():
         if dist is not None:
@@ -313,21 +347,24 @@ def main():
     lat.close()
 
     peak, peak_kind = measured_peak()
-    bytes_per_launch = cells * 38 * 4
+    interior = (cfg.nx - 2) * (cfg.ny - 2) * (cfg.nz - 2)
+    bytes_per_launch = interior * 38 * sbytes
     kernel_s = kms / max(klaunch, 1) / 1000.0
     achieved = bytes_per_launch / kernel_s / 1e9
-    traffic = profiled_traffic(args.workload, "f32")
+    traffic = profiled_traffic(args.workload, args.storage)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "peak_kind": f"of {peak_kind}", "kernel": "k_bulk (fused AA stream+collide)",
-                "bytes_per_launch": bytes_per_launch, "kernel_ms": kernel_s * 1000.0}
+                "traffic": traffic, "peak_kind": f"of {peak_kind}",
+                "kernel": "k_bulk_interior (fused AA stream+collide, interior cells)",
+                "bytes_per_launch": bytes_per_launch, "bytes_rule": "interior cells x 19 x 2 x storage bytes",
+                "kernel_ms": kernel_s * 1000.0}
 
     line = {
         "metric": "D3Q19 GLUPS", "value": value, "unit": "GLUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": desc, "lattice": [cfg.nx, cfg.ny, cfg.nz], "collision": coll, "storage": "f32",
-                   "l2": f"inputs larger than L2 ({19 * cells * 4 / 1e6:.1f} MB of populations)"
-                   if 19 * cells * 4 > 126e6 else "L2-resident working set",
+        "config": {"workload": desc, "lattice": [cfg.nx, cfg.ny, cfg.nz], "collision": coll, "storage": args.storage,
+                   "l2": f"inputs larger than L2 ({19 * cells * sbytes / 1e6:.1f} MB of populations)"
+                   if 19 * cells * sbytes > 126e6 else "L2-resident working set",
                    "parallelism": f"replicas{world}"},
         "e2e": {"value": e2e_value, "unit": "GLUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": e2e_n, "calls": "bfx_set_body + bfx_advance(1) + bfx_last_loads per step"},
@@ -349,7 +386,7 @@ def main():
                 vms, _, vkms, vkl = time_steps(vlat, args.steps, args.warmup)
                 vlat.close()
                 s = L.STORAGE_BYTES[st]
-                vach = cells * 38 * s / (vkms / max(vkl, 1) / 1000.0) / 1e9
+                vach = interior * 38 * s / (vkms / max(vkl, 1) / 1000.0) / 1e9
                 variants[nm] = {"value": cells * args.steps / (vms / 1000.0) / 1e9, "unit": "GLUPS",
                                 "roofline_frac": vach / peak, "achieved_gbs": vach,
                                 "speedup_vs_f32": (cells * args.steps / (vms / 1000.0) / 1e9) / value * world}

@@ -103,6 +103,11 @@ struct bfx_sim {
     uint64_t timing_launches = 0;
     std::vector<void*> allocations;
     cudaEvent_t region[2] = {nullptr, nullptr};
+    // CUDA graphs of two consecutive steps, keyed by the representation the
+    // pair starts from (the launch sequence repeats with period two).
+    cudaGraphExec_t pair_graph[2] = {nullptr, nullptr};
+    uint64_t pair_launches[2] = {0, 0};
+    bool graphs_enabled = true;
 
     bool geometry() const { return cfg.geometry != BFX_GEOMETRY_NONE; }
     bool moving() const { return geometry() && !cfg.static_geometry; }
@@ -247,20 +252,49 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
         launch_reduce_loads(gb, s->moving() ? 1 : 0, s->stream);
         s->launches += 2;
     }
+    const int box[3] = {s->box.sx, s->box.sy, s->box.sz};
     timing_begin(s);
-    launch_bulk(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, capture, s->stream);
+    launch_bulk(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, capture, 0, box, s->stream);
     timing_end(s);
-    s->launches += 1;
+    launch_bulk(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, capture, 1,
+                s->geometry() ? box : nullptr, s->stream);
+    s->launches += s->geometry() ? 3 : 2;
     GeomBuffers gb = geom_buffers(s, mprev, mnext);
     launch_integrate(s->g, s->fp, gb, s->cfg.gravity[0], s->cfg.gravity[1], s->cfg.gravity[2],
                      (int)s->cfg.body_substeps, s->cfg.free_flight && s->has_bird ? 1 : 0, s->stream);
     s->launches += 1;
     if (sample_slot_base) {
-        launch_record_sample(gb, sample_slot_base, sample_index, s->cfg.time_step, s->stream);
+        launch_record_sample(gb, s->fp, sample_slot_base, sample_index, s->cfg.time_step, s->stream);
         s->launches += 1;
     }
     s->rep_s ^= 1;
     if (s->moving()) s->cur ^= 1;
+}
+
+// Replays (capturing on first use) the two-step graph for the current parity.
+// Host-side state (representation, mask index) returns to its starting value
+// after two steps, so the captured launches stay valid for every later pair.
+int run_pair_graph(bfx_sim* s) {
+    const int key = s->rep_s;
+    if (!s->pair_graph[key]) {
+        cudaGraph_t graph = nullptr;
+        uint64_t before = s->launches;
+        cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return cuda_fail(s, e, "graph capture begin");
+        encode_step(s, 0, nullptr, 0);
+        encode_step(s, 0, nullptr, 0);
+        e = cudaStreamEndCapture(s->stream, &graph);
+        if (e != cudaSuccess) return cuda_fail(s, e, "graph capture end");
+        e = cudaGraphInstantiate(&s->pair_graph[key], graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return cuda_fail(s, e, "graph instantiate");
+        s->pair_launches[key] = s->launches - before;
+        s->launches = before;
+    }
+    cudaError_t e = cudaGraphLaunch(s->pair_graph[key], s->stream);
+    if (e != cudaSuccess) return cuda_fail(s, e, "graph launch");
+    s->launches += s->pair_launches[key];
+    return BFX_OK;
 }
 
 int sync_check(bfx_sim* s, const char* what) {
@@ -378,6 +412,8 @@ void bfx_destroy(bfx_sim* s) {
     for (auto e : s->ev_stop) cudaEventDestroy(e);
     for (auto e : s->region)
         if (e) cudaEventDestroy(e);
+    for (auto g : s->pair_graph)
+        if (g) cudaGraphExecDestroy(g);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -600,7 +636,17 @@ int bfx_advance(bfx_sim* s, uint64_t steps, uint32_t batch_size, uint32_t flags,
     uint64_t done = 0;
     while (done < steps) {
         uint64_t count = std::min<uint64_t>(batch_size, steps - done);
-        for (uint64_t k = 0; k < count; ++k) {
+        uint64_t k = 0;
+        // Pairs of plain steps replay a captured graph; steps that capture
+        // fields, record samples or are individually timed are encoded directly.
+        if (s->graphs_enabled && !record && !s->timing) {
+            uint64_t plain = capture && done + count == steps ? count - 1 : count;
+            for (; k + 1 < plain; k += 2) {
+                int rc = run_pair_graph(s);
+                if (rc != BFX_OK) return rc;
+            }
+        }
+        for (; k < count; ++k) {
             bool last = done + k + 1 == steps;
             encode_step(s, capture && last ? 1 : 0, record ? s->dsamples : nullptr, done + k);
         }

@@ -110,21 +110,25 @@ struct StoreF64 {
 };
 constexpr float kF16Scale = 4096.0f;
 constexpr float kF16InvScale = 1.0f / 4096.0f;
+// The 16-bit conversions use explicit fused multiply-adds: they are not part of
+// the FP32 parity contract, and one FMA per conversion keeps the 16-bit step
+// from becoming instruction-bound.
 struct StoreF16Dev {
     using T = __half;
     using R = float;
     template <int Q> __device__ __forceinline__ static R ld(const T* p) {
-        return __half2float(*p) * kF16InvScale + wq<float>(Q);
+        return __fmaf_rn(__half2float(*p), kF16InvScale, wq<float>(Q));
     }
     template <int Q> __device__ __forceinline__ static void st(T* p, R v) {
-        *p = __float2half_rn((v - wq<float>(Q)) * kF16Scale);
+        *p = __float2half_rn(__fmaf_rn(v, kF16Scale, -wq<float>(Q) * kF16Scale));
     }
     __device__ __forceinline__ static R ld_rt(const T* p, int q) {
-        return __half2float(*p) * kF16InvScale + (q == 0 ? Lat<float>::w0 : (q <= 6 ? Lat<float>::w1 : Lat<float>::w2));
+        return __fmaf_rn(__half2float(*p), kF16InvScale,
+                         q == 0 ? Lat<float>::w0 : (q <= 6 ? Lat<float>::w1 : Lat<float>::w2));
     }
     __device__ __forceinline__ static void st_rt(T* p, int q, R v) {
         float w = q == 0 ? Lat<float>::w0 : (q <= 6 ? Lat<float>::w1 : Lat<float>::w2);
-        *p = __float2half_rn((v - w) * kF16Scale);
+        *p = __float2half_rn(__fmaf_rn(v, kF16Scale, -w * kF16Scale));
     }
 };
 struct StoreBF16Dev {

@@ -14,6 +14,13 @@
 namespace bfx {
 
 struct BulkArgs {
+    void* plane[19];        // A + q*N: base of direction q's plane
+    int32_t doff[19];       // c_q . (1, nx, nx*ny): neighbour offset of direction q
+    float far_eq_f[19];     // equilibrium(q, far density, far velocity), FP32
+    double far_eq_d[19];    // same in FP64 (FP64 storage)
+    int64_t shell_cells;
+    int box[3];             // geometry box extent (origin in DeviceState)
+    int64_t box_cells;
     void* pops;
     void* spill;
     const void* ghost;
@@ -60,28 +67,49 @@ __device__ __forceinline__ typename S::R face_value(const BulkArgs& a, int f, in
     return feq_rt<R>(q, (R)fp.far[3], (R)ux, (R)uy, (R)uz);
 }
 
+// Collision (BF.metal:2907-3174).  Directions are processed in opposite pairs
+// (q odd, q+1 = opp(q)): the equilibrium, TRT and regularized terms of the pair
+// share their even parts and negate their odd parts, and in IEEE arithmetic
+// -(a-b) == b-a, (-a)*b == -(a*b), x-(-y) == x+y exactly.  Every value is
+// therefore bit-identical to evaluating the reference expression once per
+// direction, at about half the instruction count.
 template <class R, int COLL>
 __device__ __forceinline__ void collide(const R (&f)[19], R rho, R ux, R uy, R uz, R omega_p, R omega_m,
                                         R (&post)[19], float& activation, float& restriction) {
     const R cs2 = Lat<R>::cs2;
-    R u2 = ux * ux + uy * uy + uz * uz;
+    const R u2 = ux * ux + uy * uy + uz * uz;
+    const R t15 = R(1.5) * u2;
+    const R wr0 = Lat<R>::w0 * rho, wr1 = Lat<R>::w1 * rho, wr2 = Lat<R>::w2 * rho;
     R feqv[19];
+    feqv[0] = wr0 * (R(1) + R(3) * R(0) + R(4.5) * R(0) * R(0) - t15);
 #pragma unroll
-    for (int q = 0; q < 19; ++q) feqv[q] = feqq<R>(q, rho, ux, uy, uz, u2);
+    for (int q = 1; q < 19; q += 2) {
+        // equilibrium(q, rho, u) = W rho (1 + 3cu + 4.5cu^2 - 1.5u^2) for q and opp(q) (cu -> -cu)
+        const R cu = cdotq<R>(q, ux, uy, uz);
+        const R t3 = R(3) * cu;
+        const R t45 = R(4.5) * cu * cu;
+        const R wr = q <= 6 ? wr1 : wr2;
+        feqv[q] = wr * (R(1) + t3 + t45 - t15);
+        feqv[q + 1] = wr * (R(1) - t3 + t45 - t15);
+    }
 
     if (COLL == BFX_COLLISION_REGULARIZED || COLL == BFX_COLLISION_RR3) {
-        // BF.metal:2917-3062
+        // Projected second-order non-equilibrium stress; products with a zero
+        // lattice coefficient are dropped and +-1 products become sign flips
+        // (exact for finite values).
         R dsx = 0, dsy = 0, dsz = 0, odx = 0, ody = 0, odz = 0;
 #pragma unroll
         for (int q = 0; q < 19; ++q) {
-            const R dx = (R)cx(q), dy = (R)cy(q), dz = (R)cz(q);
             R ne = f[q] - feqv[q];
-            dsx += ne * (dx * dx - cs2);
-            dsy += ne * (dy * dy - cs2);
-            dsz += ne * (dz * dz - cs2);
-            odx += ne * (dx * dy);
-            ody += ne * (dx * dz);
-            odz += ne * (dy * dz);
+            dsx += ne * ((R)(cx(q) * cx(q)) - cs2);
+            dsy += ne * ((R)(cy(q) * cy(q)) - cs2);
+            dsz += ne * ((R)(cz(q) * cz(q)) - cs2);
+            if (cx(q) * cy(q) > 0) odx += ne;
+            if (cx(q) * cy(q) < 0) odx -= ne;
+            if (cx(q) * cz(q) > 0) ody += ne;
+            if (cx(q) * cz(q) < 0) ody -= ne;
+            if (cy(q) * cz(q) > 0) odz += ne;
+            if (cy(q) * cz(q) < 0) odz -= ne;
         }
         R aXxy = R(2) * ux * odx + uy * dsx;
         R aXxz = R(2) * ux * ody + uz * dsx;
@@ -89,48 +117,88 @@ __device__ __forceinline__ void collide(const R (&f)[19], R rho, R ux, R uy, R u
         R aXzz = ux * dsz + R(2) * uz * ody;
         R aYyz = R(2) * uy * odz + uz * dsy;
         R aYzz = uy * dsz + R(2) * uz * odz;
-        R unb[19];
+        const R one_minus = R(1) - omega_p;
         R scale = R(1);
-#pragma unroll
-        for (int q = 0; q < 19; ++q) {
-            const R dx = (R)cx(q), dy = (R)cy(q), dz = (R)cz(q);
-            R hx = dx * dx - cs2, hy = dy * dy - cs2, hz = dz * dz - cs2;
-            R contraction = (hx * dsx + hy * dsy + hz * dsz) + R(2) * ((dx * dy) * odx + (dx * dz) * ody + (dy * dz) * odz);
-            R third = 0;
-            if (COLL == BFX_COLLISION_RR3) {
-                third = dy * (dx * dx - cs2) * aXxy + dz * (dx * dx - cs2) * aXxz + dx * (dy * dy - cs2) * aXyy +
-                        dx * (dz * dz - cs2) * aXzz + dz * (dy * dy - cs2) * aYyz + dy * (dz * dz - cs2) * aYzz;
-            }
-            R rne = wq<R>(q) * R(4.5) * contraction;
-            if (COLL == BFX_COLLISION_RR3) rne += wq<R>(q) * R(13.5) * third;
-            R cand = feqv[q] + (R(1) - omega_p) * rne;
-            unb[q] = cand;
-            R fl = R(1.0e-6) * (feqv[q] > R(0) ? feqv[q] : R(0));
+        auto admit = [&](R fe, R cand) {
+            R fl = R(1.0e-6) * (fe > R(0) ? fe : R(0));
             R floor_ = R(1.0e-12) > fl ? R(1.0e-12) : fl;
             if (cand < floor_) {
-                R den = feqv[q] - cand;
+                R den = fe - cand;
                 den = den > R(1.0e-30) ? den : R(1.0e-30);
-                R adm = (feqv[q] - floor_) / den;
+                R adm = (fe - floor_) / den;
                 adm = adm < R(0) ? R(0) : (adm > R(1) ? R(1) : adm);
                 scale = scale < adm ? scale : adm;
             }
+        };
+        {
+            // rest direction: contraction = -cs2 (dsx + dsy + dsz), no third-order part
+            const R h = -cs2;
+            const R contraction = h * dsx + h * dsy + h * dsz;
+            const R rne = Lat<R>::w0 * R(4.5) * contraction;
+            post[0] = feqv[0] + one_minus * rne;
+            admit(feqv[0], post[0]);
+        }
+#pragma unroll
+        for (int q = 1; q < 19; q += 2) {
+            // the contraction is even in c (shared by q and opp q), the third-order sum is odd
+            const R hx = (R)(cx(q) * cx(q)) - cs2, hy = (R)(cy(q) * cy(q)) - cs2, hz = (R)(cz(q) * cz(q)) - cs2;
+            R contraction = hx * dsx + hy * dsy + hz * dsz;
+            {
+                const int xy = cx(q) * cy(q), xz = cx(q) * cz(q), yz = cy(q) * cz(q);
+                if (xy != 0) contraction = contraction + R(2) * (xy > 0 ? odx : -odx);
+                else if (xz != 0) contraction = contraction + R(2) * (xz > 0 ? ody : -ody);
+                else if (yz != 0) contraction = contraction + R(2) * (yz > 0 ? odz : -odz);
+            }
+            const R a = wq<R>(q) * R(4.5) * contraction;
+            R rq = a, ro = a;
+            if (COLL == BFX_COLLISION_RR3) {
+                R third = R(0);
+                bool any = false;
+                auto add = [&](int da, R hb, R amp) {
+                    if (da == 0) return;
+                    R t = ((R)da * hb) * amp;
+                    third = any ? third + t : t;
+                    any = true;
+                };
+                add(cy(q), hx, aXxy);
+                add(cz(q), hx, aXxz);
+                add(cx(q), hy, aXyy);
+                add(cx(q), hz, aXzz);
+                add(cz(q), hy, aYyz);
+                add(cy(q), hz, aYzz);
+                const R b = wq<R>(q) * R(13.5) * third;
+                rq = a + b;
+                ro = a - b;
+            }
+            post[q] = feqv[q] + one_minus * rq;
+            post[q + 1] = feqv[q + 1] + one_minus * ro;
+            admit(feqv[q], post[q]);
+            admit(feqv[q + 1], post[q + 1]);
         }
         if (scale < R(1)) {
             activation = 1.0f;
             restriction = (float)(R(1) - scale);
+#pragma unroll
+            for (int q = 0; q < 19; ++q) post[q] = feqv[q] + scale * (post[q] - feqv[q]);
+        } else {
+            // scale == 1: feq + 1 * (cand - feq) == cand only up to rounding, so keep
+            // the reference expression
+#pragma unroll
+            for (int q = 0; q < 19; ++q) post[q] = feqv[q] + scale * (post[q] - feqv[q]);
         }
-#pragma unroll
-        for (int q = 0; q < 19; ++q) post[q] = feqv[q] + scale * (unb[q] - feqv[q]);
     } else if (COLL == BFX_COLLISION_TRT) {
-        // BF.metal:3063-3093
+        // BF.metal:3063-3093, pairwise
+        post[0] = f[0] - omega_p * (f[0] - feqv[0]);
 #pragma unroll
-        for (int q = 0; q < 19; ++q) {
-            const int qo = opp(q);
-            R fp_ = R(0.5) * (f[q] + f[qo]);
-            R fm = R(0.5) * (f[q] - f[qo]);
-            R ep = R(0.5) * (feqv[q] + feqv[qo]);
-            R em = R(0.5) * (feqv[q] - feqv[qo]);
-            post[q] = f[q] - omega_p * (fp_ - ep) - omega_m * (fm - em);
+        for (int q = 1; q < 19; q += 2) {
+            const R fp_ = R(0.5) * (f[q] + f[q + 1]);
+            const R fm = R(0.5) * (f[q] - f[q + 1]);
+            const R ep = R(0.5) * (feqv[q] + feqv[q + 1]);
+            const R em = R(0.5) * (feqv[q] - feqv[q + 1]);
+            const R A = omega_p * (fp_ - ep);
+            const R B = omega_m * (fm - em);
+            post[q] = f[q] - A - B;
+            post[q + 1] = f[q + 1] - A + B;
         }
     } else {
         // symmetric positivity limiter: BF.metal:3094-3174
@@ -209,15 +277,63 @@ __device__ __forceinline__ void store_post(const BulkArgs& a, typename S::T* A, 
     }
 }
 
-template <class S, int REP_S, int COLL>
-__global__ void __launch_bounds__(256) k_bulk(const BulkArgs a) {
+// Cell of the domain shell (the six faces) with index t: both z faces, then
+// both y faces without their z edges, then both x faces without y/z edges.
+__device__ __forceinline__ bool shell_cell(const Grid& g, int64_t t, int& x, int& y, int& z) {
+    const int64_t fz = (int64_t)g.nx * g.ny;
+    if (t < 2 * fz) {
+        z = t < fz ? 0 : g.nz - 1;
+        const int64_t r = t < fz ? t : t - fz;
+        y = (int)(r / g.nx);
+        x = (int)(r - (int64_t)y * g.nx);
+        return true;
+    }
+    t -= 2 * fz;
+    const int64_t fy = (int64_t)g.nx * (g.nz - 2);
+    if (t < 2 * fy) {
+        y = t < fy ? 0 : g.ny - 1;
+        const int64_t r = t < fy ? t : t - fy;
+        z = 1 + (int)(r / g.nx);
+        x = (int)(r - (int64_t)(z - 1) * g.nx);
+        return true;
+    }
+    t -= 2 * fy;
+    const int64_t fx = (int64_t)(g.ny - 2) * (g.nz - 2);
+    if (t < 2 * fx) {
+        x = t < fx ? 0 : g.nx - 1;
+        const int64_t r = t < fx ? t : t - fx;
+        z = 1 + (int)(r / (g.ny - 2));
+        y = 1 + (int)(r - (int64_t)(z - 1) * (g.ny - 2));
+        return true;
+    }
+    return false;
+}
+
+// Generic cell update, used for the domain shell: periodic wrap, face rules,
+// spill planes, solid and uncovered cells.
+template <class S, int REP_S, int COLL, int MODE>
+__global__ void __launch_bounds__(128) k_bulk_generic(const BulkArgs a) {
     using T = typename S::T;
     using R = typename S::R;
     const Grid& g = a.g;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z;
-    if (x >= g.nx || y >= g.ny) return;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int x, y, z;
+    if (MODE == 0) {
+        if (t >= a.shell_cells) return;
+        if (!shell_cell(g, t, x, y, z)) return;
+    } else {
+        // interior cells of the geometry box that are solid or newly uncovered
+        if (t >= a.box_cells) return;
+        const int lz = (int)(t / ((int64_t)a.box[0] * a.box[1]));
+        const int64_t r = t - (int64_t)lz * a.box[0] * a.box[1];
+        const int ly = (int)(r / a.box[0]);
+        const int lx = (int)(r - (int64_t)ly * a.box[0]);
+        x = a.state->box_origin[0] + lx;
+        y = a.state->box_origin[1] + ly;
+        z = a.state->box_origin[2] + lz;
+        if (x < 1 || y < 1 || z < 1 || x >= g.nx - 1 || y >= g.ny - 1 || z >= g.nz - 1) return;
+        if (a.mask[(int64_t)x + (int64_t)g.nx * ((int64_t)y + (int64_t)g.ny * z)] == 0) return;
+    }
     const int64_t gid = (int64_t)x + (int64_t)g.nx * ((int64_t)y + (int64_t)g.ny * z);
     T* A = (T*)a.pops;
     const uint8_t m = a.mask ? a.mask[gid] : (uint8_t)0;
@@ -322,6 +438,96 @@ __global__ void __launch_bounds__(256) k_bulk(const BulkArgs a) {
         atomicAdd(&a.state->limiter_count, 1.0);
         atomicMax(&a.state->limiter_max_bits, __float_as_uint(restriction));
     }
+}
+
+// ---------------------------------------------------------------------------
+// Interior cells: one fluid path with no domain-face logic.  Directions are
+// addressed through per-direction plane pointers and 32-bit neighbour offsets
+// held in the kernel parameters; solid and newly uncovered cells (rare) take a
+// separate non-inlined path so the hot instruction stream stays short.
+// ---------------------------------------------------------------------------
+template <class S, int REP_S>
+__device__ __forceinline__ void store_interior(const BulkArgs& a, uint32_t gid, const typename S::R (&post)[19]) {
+    using T = typename S::T;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        if (REP_S) S::st_rt((T*)a.plane[opp(q)] + gid, opp(q), post[q]);
+        else S::st_rt((T*)a.plane[q] + (uint32_t)(gid + (uint32_t)a.doff[q]), q, post[q]);
+    }
+}
+
+template <class S, int COLL, int CAPTURE>
+__device__ __forceinline__ void finish_interior(const BulkArgs& a, uint32_t gid, int x, int y, int z,
+                                                typename S::R (&post)[19], float activation, float restriction) {
+    using R = typename S::R;
+    if (a.fp.has_sponge) {
+        const float sp = sponge_factor(a.g, a.fp, x, y, z);
+        if (sp > 0.0f) {
+#pragma unroll
+            for (int q = 0; q < 19; ++q) {
+                const R farv = sizeof(R) == 8 ? (R)a.far_eq_d[q] : (R)a.far_eq_f[q];
+                post[q] = post[q] + (farv - post[q]) * (R)sp;
+            }
+        }
+    }
+    if (CAPTURE) {
+        R cd = 0, cmx = 0, cmy = 0, cmz = 0;
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            cd += post[q];
+            if (cx(q) > 0) cmx += post[q];
+            if (cx(q) < 0) cmx -= post[q];
+            if (cy(q) > 0) cmy += post[q];
+            if (cy(q) < 0) cmy -= post[q];
+            if (cz(q) > 0) cmz += post[q];
+            if (cz(q) < 0) cmz -= post[q];
+        }
+        cd = cd > R(1.0e-8) ? cd : R(1.0e-8);
+        a.density[gid] = (float)cd;
+        a.velocity[gid] = make_float4((float)(cmx / cd), (float)(cmy / cd), (float)(cmz / cd), 0.0f);
+    }
+    if (COLL != BFX_COLLISION_TRT && activation != 0.0f) {
+        atomicAdd(&a.state->limiter_count, 1.0);
+        atomicMax(&a.state->limiter_max_bits, __float_as_uint(restriction));
+    }
+}
+
+template <class S, int REP_S, int COLL, int CAPTURE>
+__global__ void __launch_bounds__(256, sizeof(typename S::R) == 8 ? 1 : (COLL == BFX_COLLISION_TRT ? 4 : 2))
+    k_bulk_interior(const BulkArgs a) {
+    using T = typename S::T;
+    using R = typename S::R;
+    const int x = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = 1 + blockIdx.z;
+    if (x >= a.g.nx - 1 || y >= a.g.ny - 1) return;
+    const uint32_t gid = (uint32_t)x + (uint32_t)a.g.nx * ((uint32_t)y + (uint32_t)a.g.ny * (uint32_t)z);
+    // solid and newly uncovered cells are updated by k_bulk_generic over the geometry box
+    if (a.mask && a.mask[gid]) return;
+    R f[19];
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        if (REP_S) f[q] = S::ld_rt((const T*)a.plane[q] + gid, q);
+        else f[q] = S::ld_rt((const T*)a.plane[opp(q)] + (uint32_t)(gid - (uint32_t)a.doff[q]), opp(q));
+    }
+    R rho = 0, mx = 0, my = 0, mz = 0;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        rho += f[q];
+        if (cx(q) > 0) mx += f[q];
+        if (cx(q) < 0) mx -= f[q];
+        if (cy(q) > 0) my += f[q];
+        if (cy(q) < 0) my -= f[q];
+        if (cz(q) > 0) mz += f[q];
+        if (cz(q) < 0) mz -= f[q];
+    }
+    rho = rho > R(1.0e-8) ? rho : R(1.0e-8);
+    R post[19];
+    float activation = 0.0f, restriction = 0.0f;
+    collide<R, COLL>(f, rho, mx / rho, my / rho, mz / rho, (R)a.fp.omega_p, (R)a.fp.omega_m, post, activation,
+                     restriction);
+    finish_interior<S, COLL, CAPTURE>(a, gid, x, y, z, post, activation, restriction);
+    store_interior<S, REP_S>(a, gid, post);
 }
 
 // ---------------------------------------------------------------------------
@@ -506,8 +712,30 @@ __global__ void k_sum_partials4(const double* partials, int count, double* out) 
 // ---------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------
-static BulkArgs make_args(const GridDesc& gd, const FluidParams& fp, const FluidBuffers& b, int capture) {
+// Equilibrium with the reference's FP32 (or FP64) operation order, on the host
+// (compiled with -ffp-contract=off, so it matches the device values bit for bit).
+template <class R>
+static R host_feq(int q, R rho, R ux, R uy, R uz) {
+    R cu = (R)cx(q) * ux + (R)cy(q) * uy + (R)cz(q) * uz;
+    R u2 = ux * ux + uy * uy + uz * uz;
+    R w = q == 0 ? Lat<R>::w0 : (q <= 6 ? Lat<R>::w1 : Lat<R>::w2);
+    return w * rho * (R(1) + R(3) * cu + R(4.5) * cu * cu - R(1.5) * u2);
+}
+
+static size_t elem_bytes(int storage) {
+    return storage == BFX_STORAGE_F64 ? 8 : (storage == BFX_STORAGE_F32 ? 4 : 2);
+}
+
+static BulkArgs make_args(const GridDesc& gd, const FluidParams& fp, const FluidBuffers& b, int capture,
+                          int storage = BFX_STORAGE_F32) {
     BulkArgs a;
+    for (int q = 0; q < 19; ++q) {
+        a.plane[q] = (char*)b.pops + (size_t)q * (size_t)gd.n * elem_bytes(storage);
+        a.doff[q] = (int32_t)((int64_t)cx(q) + (int64_t)gd.nx * cy(q) + gd.nxy * cz(q));
+        a.far_eq_f[q] = host_feq<float>(q, fp.far[3], fp.far[0], fp.far[1], fp.far[2]);
+        a.far_eq_d[q] = host_feq<double>(q, (double)fp.far[3], (double)fp.far[0], (double)fp.far[1], (double)fp.far[2]);
+    }
+    a.shell_cells = 2 * (int64_t)gd.nx * gd.ny + 2 * (int64_t)gd.nx * (gd.nz - 2) + 2 * (int64_t)(gd.ny - 2) * (gd.nz - 2);
     a.pops = b.pops;
     a.spill = b.spill;
     a.ghost = b.ghost;
@@ -542,23 +770,37 @@ static void cell_launch_shape(const GridDesc& g, dim3& grid, dim3& block) {
 
 template <class S, int REP, int COLL>
 static void bulk_t(const BulkArgs& a, const GridDesc& g, cudaStream_t s) {
+    GridDesc in = g;
+    in.nx = g.nx - 2;
+    in.ny = g.ny - 2;
+    in.nz = g.nz - 2;
     dim3 grid, block;
-    cell_launch_shape(g, grid, block);
-    k_bulk<S, REP, COLL><<<grid, block, 0, s>>>(a);
+    cell_launch_shape(in, grid, block);
+    if (a.capture) k_bulk_interior<S, REP, COLL, 1><<<grid, block, 0, s>>>(a);
+    else k_bulk_interior<S, REP, COLL, 0><<<grid, block, 0, s>>>(a);
+}
+
+template <class S, int REP, int COLL>
+static void shell_t(const BulkArgs& a, cudaStream_t s) {
+    k_bulk_generic<S, REP, COLL, 0><<<(unsigned)((a.shell_cells + 127) / 128), 128, 0, s>>>(a);
+    if (a.mask && a.box_cells > 0)
+        k_bulk_generic<S, REP, COLL, 1><<<(unsigned)((a.box_cells + 127) / 128), 128, 0, s>>>(a);
 }
 
 template <class S>
-static void bulk_s(const BulkArgs& a, const GridDesc& g, int collision, int rep_s, cudaStream_t s) {
+static void bulk_s(const BulkArgs& a, const GridDesc& g, int collision, int rep_s, int part, cudaStream_t s) {
+#define BFX_PART(REP, COLL) (part == 0 ? bulk_t<S, REP, COLL>(a, g, s) : shell_t<S, REP, COLL>(a, s))
     switch (collision * 2 + rep_s) {
-    case 0: bulk_t<S, 0, BFX_COLLISION_TRT>(a, g, s); break;
-    case 1: bulk_t<S, 1, BFX_COLLISION_TRT>(a, g, s); break;
-    case 2: bulk_t<S, 0, BFX_COLLISION_TRT_LIMITER>(a, g, s); break;
-    case 3: bulk_t<S, 1, BFX_COLLISION_TRT_LIMITER>(a, g, s); break;
-    case 4: bulk_t<S, 0, BFX_COLLISION_REGULARIZED>(a, g, s); break;
-    case 5: bulk_t<S, 1, BFX_COLLISION_REGULARIZED>(a, g, s); break;
-    case 6: bulk_t<S, 0, BFX_COLLISION_RR3>(a, g, s); break;
-    default: bulk_t<S, 1, BFX_COLLISION_RR3>(a, g, s); break;
+    case 0: BFX_PART(0, BFX_COLLISION_TRT); break;
+    case 1: BFX_PART(1, BFX_COLLISION_TRT); break;
+    case 2: BFX_PART(0, BFX_COLLISION_TRT_LIMITER); break;
+    case 3: BFX_PART(1, BFX_COLLISION_TRT_LIMITER); break;
+    case 4: BFX_PART(0, BFX_COLLISION_REGULARIZED); break;
+    case 5: BFX_PART(1, BFX_COLLISION_REGULARIZED); break;
+    case 6: BFX_PART(0, BFX_COLLISION_RR3); break;
+    default: BFX_PART(1, BFX_COLLISION_RR3); break;
     }
+#undef BFX_PART
 }
 
 #define BFX_DISPATCH_STORAGE(storage, FN, ...)                 \
@@ -570,9 +812,13 @@ static void bulk_s(const BulkArgs& a, const GridDesc& g, int collision, int rep_
     }
 
 void launch_bulk(int storage, int collision, int rep_s, const GridDesc& g, const FluidParams& fp,
-                 const FluidBuffers& b, int capture, cudaStream_t s) {
-    BulkArgs a = make_args(g, fp, b, capture);
-    BFX_DISPATCH_STORAGE(storage, bulk_s, a, g, collision, rep_s, s);
+                 const FluidBuffers& b, int capture, int part, const int* box, cudaStream_t s) {
+    BulkArgs a = make_args(g, fp, b, capture, storage);
+    a.box[0] = box ? box[0] : 0;
+    a.box[1] = box ? box[1] : 0;
+    a.box[2] = box ? box[2] : 0;
+    a.box_cells = box ? (int64_t)box[0] * box[1] * box[2] : 0;
+    BFX_DISPATCH_STORAGE(storage, bulk_s, a, g, collision, rep_s, part, s);
 }
 
 template <class S>

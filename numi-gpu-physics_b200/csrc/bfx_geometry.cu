@@ -865,7 +865,7 @@ __global__ void __launch_bounds__(256) k_links_apply(const GeomArgs a, int rep_s
         int x, y, z;
         unflat(g, gid, x, y, z);
         int sx = x - cx(q), sy = y - cy(q), sz = z - cz(q);
-        wrap(g, sx, sy, sz);
+        if (!wrap(g, sx, sy, sz)) continue;  // cannot happen for an emitted link; keeps every index in range
         const int64_t src = flat(g, sx, sy, sz);
         R mwd = (R)fp.far[3];
         if (fp.local_density) {
@@ -1245,9 +1245,9 @@ void launch_integrate(const GridDesc& g, const FluidParams& fp, const GeomBuffer
     k_finish<<<1, 1, 0, s>>>(a, gravity_x, gravity_y, gravity_z, substeps, free_flight, gb.bird);
 }
 
-void launch_record_sample(const GeomBuffers& gb, bfx_run_sample* samples, uint64_t index, float dt, cudaStream_t s) {
+void launch_record_sample(const GeomBuffers& gb, const FluidParams& fp, bfx_run_sample* samples, uint64_t index,
+                          float dt, cudaStream_t s) {
     GridDesc g = {};
-    FluidParams fp = {};
     BoxDesc box = {1, 1, 1, 1};
     GeomArgs a = make_geom(g, fp, box, gb, nullptr, nullptr);
     k_record_sample<<<1, 1, 0, s>>>(a, samples, index, dt);

@@ -29,9 +29,12 @@ struct FluidBuffers {
     DeviceState* state;
 };
 
-// Fused stream + collide over the whole lattice (one launch).
+// Fused stream + collide: part 0 = fluid interior cells (the hot kernel);
+// part 1 = the six domain faces (wrap, face rules, spill planes) and the solid /
+// newly uncovered interior cells of the geometry box (box = extent or null).
+// One step launches both parts.
 void launch_bulk(int storage, int collision, int rep_s, const GridDesc& g, const FluidParams& fp,
-                 const FluidBuffers& b, int capture, cudaStream_t s);
+                 const FluidBuffers& b, int capture, int part, const int* box, cudaStream_t s);
 // Zero-gradient outflow ghost planes (before the step).
 void launch_ghost(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const FluidBuffers& b,
                   cudaStream_t s);
@@ -96,7 +99,8 @@ void launch_links_apply(int storage, int rep_s, const GridDesc& g, const FluidPa
 void launch_reduce_loads(const GeomBuffers& gb, int with_topology, cudaStream_t s);
 void launch_integrate(const GridDesc& g, const FluidParams& fp, const GeomBuffers& gb, float gravity_x,
                       float gravity_y, float gravity_z, int substeps, int free_flight, cudaStream_t s);
-void launch_record_sample(const GeomBuffers& gb, bfx_run_sample* samples, uint64_t index, float dt, cudaStream_t s);
+void launch_record_sample(const GeomBuffers& gb, const FluidParams& fp, bfx_run_sample* samples, uint64_t index,
+                          float dt, cudaStream_t s);
 void launch_step_counter(DeviceState* st, cudaStream_t s);
 
 }  // namespace bfx
