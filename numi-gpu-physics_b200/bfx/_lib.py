@@ -111,7 +111,7 @@ EXPORTED = (
     "bfx_copy_populations", "bfx_set_populations", "bfx_copy_mask", "bfx_copy_wall", "bfx_copy_links",
     "bfx_fluid_mass_momentum", "bfx_save_state", "bfx_restore_state", "bfx_get_body", "bfx_set_body",
     "bfx_step_index", "bfx_set_kernel_timing", "bfx_kernel_timing", "bfx_timer_begin", "bfx_timer_end",
-    "bfx_launch_count", "bfx_device_bytes", "bfx_last_error",
+    "bfx_launch_count", "bfx_device_bytes", "bfx_fluid_mass_momentum_noalloc", "bfx_last_error",
 )
 
 _lib = None
@@ -161,6 +161,7 @@ def load(path: str | None = None):
     L.bfx_timer_end.argtypes = [vp, P(ct.c_double)]
     L.bfx_launch_count.argtypes = [vp, P(ct.c_uint64)]
     L.bfx_device_bytes.argtypes = [vp, P(ct.c_uint64)]
+    L.bfx_fluid_mass_momentum_noalloc.argtypes = [vp, vp, ct.c_uint32, ct.c_uint32, ct.c_uint32, vp]
     L.bfx_last_error.argtypes = [vp, ct.c_char_p, ct.c_size_t]
     if path is None:
         _lib = L

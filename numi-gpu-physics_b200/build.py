@@ -16,7 +16,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libbfx.so")
-SOURCES = ["bfx_fluid.cu", "bfx_geometry.cu", "bfx_api.cu"]
+SOURCES = ["bfx_fluid.cu", "bfx_geometry.cu", "bfx_api.cu", "bfx_noalloc.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

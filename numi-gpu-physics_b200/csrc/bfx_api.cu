@@ -40,6 +40,11 @@ uint64_t fnv1a(const void* data, size_t n, uint64_t h = 1469598103934665603ull) 
 
 }  // namespace
 
+namespace bfx {
+// Message returned by bfx_last_error(NULL) (entry points without a handle).
+void set_global_error(const std::string& message) { g_create_error = message; }
+}  // namespace bfx
+
 struct bfx_sim {
     bfx_config cfg{};
     bfx_bird bird{};
