@@ -119,7 +119,8 @@ typedef struct bfx_config {
     float time_step;                /* timeStepSeconds (dt) */
     float velocity_to_lattice;      /* dt/dx */
     float force_to_physical;        /* rho dx^4 / dt^2 */
-    float _reserved0;
+    uint32_t fast_math;             /* SimulationConfiguration.fastMath: FP32 step with FMA contraction
+                                       (not bit-identical to the reference order; 16-bit storage always is) */
     float omega_plus, omega_minus;  /* 1/tau+, 1/tau- */
     float sponge_strength;
     float sponge_width;             /* cells */

@@ -39,7 +39,7 @@ class Config(ct.Structure):
         ("nx", ct.c_uint32), ("ny", ct.c_uint32), ("nz", ct.c_uint32), ("device", ct.c_int32),
         ("origin", ct.c_float * 3), ("cell_size", ct.c_float),
         ("time_step", ct.c_float), ("velocity_to_lattice", ct.c_float), ("force_to_physical", ct.c_float),
-        ("_reserved0", ct.c_float),
+        ("fast_math", ct.c_uint32),
         ("omega_plus", ct.c_float), ("omega_minus", ct.c_float),
         ("sponge_strength", ct.c_float), ("sponge_width", ct.c_float),
         ("far_field", ct.c_float * 4), ("gravity", ct.c_float * 3), ("body_substeps", ct.c_uint32),

@@ -16,7 +16,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libbfx.so")
-SOURCES = ["bfx_fluid.cu", "bfx_geometry.cu", "bfx_api.cu", "bfx_noalloc.cu"]
+SOURCES = ["bfx_fluid.cu", "bfx_fluid_fast.cu", "bfx_geometry.cu", "bfx_api.cu", "bfx_noalloc.cu"]
+# translation units built with FMA contraction (see csrc/bfx_bulk.cuh)
+CONTRACTED = {"bfx_fluid_fast.cu"}
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -29,6 +31,7 @@ FLAGS = [
 def build(verbose: bool = False, force: bool = False) -> str:
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
     deps = srcs + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".h", ".cuh"))]
+    deps.append(os.path.abspath(__file__))
     deps.append(os.path.join(HERE, "..", "include", "bfx.h"))
     if not force and os.path.exists(OUT):
         newest = max(os.path.getmtime(d) for d in deps)
@@ -40,7 +43,8 @@ def build(verbose: bool = False, force: bool = False) -> str:
     procs = []
     for src in srcs:
         obj = os.path.join(build_dir, os.path.basename(src) + ".o")
-        cmd = [NVCC, *FLAGS, "-c", src, "-o", obj]
+        flags = [("--fmad=true" if f == "--fmad=false" and os.path.basename(src) in CONTRACTED else f) for f in FLAGS]
+        cmd = [NVCC, *flags, "-c", src, "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
             print(" ".join(cmd), flush=True)

@@ -57,8 +57,6 @@ struct bfx_sim {
     BoxDesc box{};
     size_t elem = 4;
     void* pops = nullptr;
-    void* spill = nullptr;
-    void* ghost = nullptr;
     uint8_t* mask[2] = {nullptr, nullptr};
     int cur = 0;
     float4* wall = nullptr;
@@ -156,8 +154,6 @@ cudaError_t dalloc(bfx_sim* s, T** p, size_t bytes) {
 FluidBuffers fluid_buffers(bfx_sim* s, uint8_t* mask) {
     FluidBuffers b;
     b.pops = s->pops;
-    b.spill = s->spill;
-    b.ghost = s->ghost;
     b.mask = mask;
     b.wall = s->wall;
     b.density = s->density;
@@ -246,13 +242,13 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
         encode_geometry_build(s, 0, mprev, mnext);
     }
     FluidBuffers fb = fluid_buffers(s, s->geometry() ? mnext : nullptr);
-    if (s->fp.any_outflow) {
-        launch_ghost(s->cfg.storage, s->rep_s, s->g, s->fp, fb, s->stream);
-        s->launches += 1;
-    }
+    if (s->geometry() && s->moving()) encode_links(s, mprev, mnext);
+    // halo fill before the link writes: a link whose solid source is a periodic
+    // image writes into a halo slot and must win over the periodic copy
+    launch_halo(s->cfg.storage, s->rep_s, s->g, s->fp, fb, s->stream);
+    s->launches += 1;
     if (s->geometry()) {
         GeomBuffers gb = geom_buffers(s, mprev, mnext);
-        if (s->moving()) encode_links(s, mprev, mnext);
         launch_links_apply(s->cfg.storage, s->rep_s, s->g, s->fp, gb, fb, s->stream);
         launch_reduce_loads(gb, s->moving() ? 1 : 0, s->stream);
         s->launches += 2;
@@ -263,7 +259,7 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
     timing_end(s);
     launch_bulk(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, capture, 1,
                 s->geometry() ? box : nullptr, s->stream);
-    s->launches += s->geometry() ? 3 : 2;
+    s->launches += s->geometry() ? 2 : 1;
     GeomBuffers gb = geom_buffers(s, mprev, mnext);
     launch_integrate(s->g, s->fp, gb, s->cfg.gravity[0], s->cfg.gravity[1], s->cfg.gravity[2],
                      (int)s->cfg.body_substeps, s->cfg.free_flight && s->has_bird ? 1 : 0, s->stream);
@@ -460,15 +456,7 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
     g.per_z = c.face_bc[4] == BFX_BC_PERIODIC;
     g.n = (int64_t)g.nx * g.ny * g.nz;
     g.nxy = (int64_t)g.nx * g.ny;
-    int64_t face_cells[6] = {(int64_t)g.ny * g.nz, (int64_t)g.ny * g.nz, (int64_t)g.nx * g.nz,
-                             (int64_t)g.nx * g.nz, (int64_t)g.nx * g.ny, (int64_t)g.nx * g.ny};
-    int64_t off = 0;
-    for (int f = 0; f < 6; ++f) {
-        g.spill_off[f] = off;
-        g.ghost_off[f] = off;
-        off += 5 * face_cells[f];
-    }
-    g.spill_total = off;
+    g.padded = (int64_t)(g.nx + 2) * (g.ny + 2) * (g.nz + 2);
     // fluid parameters
     FluidParams& fp = s->fp;
     for (int k = 0; k < 3; ++k) fp.origin[k] = c.origin[k];
@@ -495,9 +483,10 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
     fp.local_density = c.moving_wall_local_density ? 1 : 0;
     fp.accumulate = c.accumulate_loads ? 1 : 0;
     fp.has_sponge = c.sponge_strength > 0.0f ? 1 : 0;
+    fp.fast_math = c.fast_math ? 1 : 0;
 
     s->elem = storage_bytes(c.storage);
-    size_t pop_bytes = (size_t)19 * (size_t)g.n * s->elem;
+    size_t pop_bytes = (size_t)19 * (size_t)g.padded * s->elem;
 #define BFX_ALLOC(ptr, bytes)                                   \
     do {                                                        \
         cudaError_t ee = dalloc(s, &(ptr), (bytes));            \
@@ -508,8 +497,6 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
         }                                                       \
     } while (0)
     BFX_ALLOC(s->pops, pop_bytes);
-    BFX_ALLOC(s->spill, (size_t)g.spill_total * s->elem);
-    if (fp.any_outflow) BFX_ALLOC(s->ghost, (size_t)g.spill_total * s->elem);
     BFX_ALLOC(s->density, (size_t)g.n * sizeof(float));
     BFX_ALLOC(s->velocity, (size_t)g.n * sizeof(float4));
     BFX_ALLOC(s->dstate, sizeof(DeviceState));
@@ -873,7 +860,7 @@ int bfx_fluid_mass_momentum(bfx_sim* s, double out[4]) {
     return BFX_OK;
 }
 
-// Restart state: header, device state, populations (storage format), spill
+// Restart state: header, device state, populations (storage format, with halo),
 // planes, both masks and the wall field, followed by an FNV-1a checksum.
 struct StateHeader {
     char magic[8];
@@ -886,8 +873,7 @@ struct StateHeader {
 };
 
 static size_t state_size(const bfx_sim* s) {
-    size_t n = sizeof(StateHeader) + sizeof(DeviceState) + (size_t)19 * s->g.n * s->elem +
-               (size_t)s->g.spill_total * s->elem;
+    size_t n = sizeof(StateHeader) + sizeof(DeviceState) + (size_t)19 * s->g.padded * s->elem;
     if (s->geometry()) n += 2 * (size_t)s->g.n + (size_t)s->g.n * sizeof(float4);
     return n + sizeof(uint64_t);
 }
@@ -917,10 +903,8 @@ int bfx_save_state(bfx_sim* s, void* buf, size_t capacity, size_t* size) {
     p += sizeof(h);
     cudaMemcpy(p, s->dstate, sizeof(DeviceState), cudaMemcpyDeviceToHost);
     p += sizeof(DeviceState);
-    cudaMemcpy(p, s->pops, (size_t)19 * s->g.n * s->elem, cudaMemcpyDeviceToHost);
-    p += (size_t)19 * s->g.n * s->elem;
-    cudaMemcpy(p, s->spill, (size_t)s->g.spill_total * s->elem, cudaMemcpyDeviceToHost);
-    p += (size_t)s->g.spill_total * s->elem;
+    cudaMemcpy(p, s->pops, (size_t)19 * s->g.padded * s->elem, cudaMemcpyDeviceToHost);
+    p += (size_t)19 * s->g.padded * s->elem;
     if (s->geometry()) {
         cudaMemcpy(p, s->mask[0], (size_t)s->g.n, cudaMemcpyDeviceToHost);
         p += s->g.n;
@@ -950,10 +934,8 @@ int bfx_restore_state(bfx_sim* s, const void* buf, size_t size) {
     const char* p = (const char*)buf + sizeof(h);
     cudaMemcpy(s->dstate, p, sizeof(DeviceState), cudaMemcpyHostToDevice);
     p += sizeof(DeviceState);
-    cudaMemcpy(s->pops, p, (size_t)19 * s->g.n * s->elem, cudaMemcpyHostToDevice);
-    p += (size_t)19 * s->g.n * s->elem;
-    cudaMemcpy(s->spill, p, (size_t)s->g.spill_total * s->elem, cudaMemcpyHostToDevice);
-    p += (size_t)s->g.spill_total * s->elem;
+    cudaMemcpy(s->pops, p, (size_t)19 * s->g.padded * s->elem, cudaMemcpyHostToDevice);
+    p += (size_t)19 * s->g.padded * s->elem;
     if (s->geometry()) {
         cudaMemcpy(s->mask[0], p, (size_t)s->g.n, cudaMemcpyHostToDevice);
         p += s->g.n;

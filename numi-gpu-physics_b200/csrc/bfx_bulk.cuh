@@ -1,0 +1,53 @@
+// Kernel templates of the fused stream + collide step, shared by two
+// translation units that differ only in floating-point contraction:
+//   bfx_fluid.cu       --fmad=false  FP32 and FP64 storage, bit-identical to the
+//                                    reference operation order (default)
+//   bfx_fluid_fast.cu  --fmad=true   the 16-bit deviation formats and the
+//                                    opt-in fast_math FP32 mode
+// The including file defines BFX_VARIANT, the namespace that keeps the two
+// sets of instantiations apart.
+#pragma once
+
+#include "bfx_device.cuh"
+#include "bfx_internal.h"
+
+namespace bfx {
+
+struct BulkArgs {
+    void* plane[19];        // A + q * padded cells: base of direction q's plane
+    int32_t doff[19];       // c_q . (1, px, px*py): padded neighbour offset of direction q
+    float far_eq_f[19];     // equilibrium(q, far density, far velocity), FP32
+    double far_eq_d[19];    // same in FP64 (FP64 storage)
+    int box[3];             // geometry box extent (origin in DeviceState)
+    int64_t box_cells;
+    void* pops;
+    const uint8_t* mask;
+    const float4* wall;
+    float* density;
+    float4* velocity;
+    DeviceState* state;
+    Grid g;
+    FluidParams fp;
+    int capture;
+};
+
+// Fused-step launch for the contracted variant (bfx_fluid_fast.cu).
+void launch_bulk_fast(int storage, int collision, int rep_s, const GridDesc& g, const BulkArgs& a, int part,
+                      cudaStream_t s);
+// Host-side construction of BulkArgs (bfx_fluid.cu).
+BulkArgs make_bulk_args(const GridDesc& gd, const FluidParams& fp, const FluidBuffers& b, int capture, int storage);
+void cell_launch_shape(const GridDesc& g, dim3& grid, dim3& block);
+
+// spongeFactor: BF.metal:2427-2446
+__device__ __forceinline__ float sponge_factor(const Grid& g, const FluidParams& fp, int x, int y, int z) {
+    unsigned dx = min((unsigned)x, (unsigned)(g.nx - 1 - x));
+    unsigned dy = min((unsigned)y, (unsigned)(g.ny - 1 - y));
+    unsigned dz = min((unsigned)z, (unsigned)(g.nz - 1 - z));
+    float distance = (float)min(dx, min(dy, dz));
+    float width = fp.sponge_width;
+    if (distance >= width) return 0.0f;
+    float nd = fminf(fmaxf((width - distance) / fmaxf(width, 1.0f), 0.0f), 1.0f);
+    return fp.sponge_strength * nd * nd;
+}
+
+}  // namespace bfx

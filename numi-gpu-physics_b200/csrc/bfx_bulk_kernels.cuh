@@ -1,0 +1,372 @@
+// Fused-step kernel templates (see bfx_bulk.cuh); included once per variant.
+#include "bfx_bulk.cuh"
+
+#ifndef BFX_VARIANT
+#error "define BFX_VARIANT before including bfx_bulk_kernels.cuh"
+#endif
+
+namespace bfx {
+namespace BFX_VARIANT {
+
+// Collision (BF.metal:2907-3174).  Directions are processed in opposite pairs
+// (q odd, q+1 = opp(q)): the equilibrium, TRT and regularized terms of the pair
+// share their even parts and negate their odd parts, and in IEEE arithmetic
+// -(a-b) == b-a, (-a)*b == -(a*b), x-(-y) == x+y exactly.  Every value is
+// therefore bit-identical to evaluating the reference expression once per
+// direction, at about half the instruction count.
+template <class R, int COLL>
+__device__ __forceinline__ void collide(const R (&f)[19], R rho, R ux, R uy, R uz, R omega_p, R omega_m,
+                                        R (&post)[19], float& activation, float& restriction) {
+    const R cs2 = Lat<R>::cs2;
+    const R u2 = ux * ux + uy * uy + uz * uz;
+    const R t15 = R(1.5) * u2;
+    const R wr0 = Lat<R>::w0 * rho, wr1 = Lat<R>::w1 * rho, wr2 = Lat<R>::w2 * rho;
+    R feqv[19];
+    feqv[0] = wr0 * (R(1) + R(3) * R(0) + R(4.5) * R(0) * R(0) - t15);
+#pragma unroll
+    for (int q = 1; q < 19; q += 2) {
+        // equilibrium(q, rho, u) = W rho (1 + 3cu + 4.5cu^2 - 1.5u^2) for q and opp(q) (cu -> -cu)
+        const R cu = cdotq<R>(q, ux, uy, uz);
+        const R t3 = R(3) * cu;
+        const R t45 = R(4.5) * cu * cu;
+        const R wr = q <= 6 ? wr1 : wr2;
+        feqv[q] = wr * (R(1) + t3 + t45 - t15);
+        feqv[q + 1] = wr * (R(1) - t3 + t45 - t15);
+    }
+
+    if (COLL == BFX_COLLISION_REGULARIZED || COLL == BFX_COLLISION_RR3) {
+        // Projected second-order non-equilibrium stress; products with a zero
+        // lattice coefficient are dropped and +-1 products become sign flips
+        // (exact for finite values).
+        R dsx = 0, dsy = 0, dsz = 0, odx = 0, ody = 0, odz = 0;
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            R ne = f[q] - feqv[q];
+            dsx += ne * ((R)(cx(q) * cx(q)) - cs2);
+            dsy += ne * ((R)(cy(q) * cy(q)) - cs2);
+            dsz += ne * ((R)(cz(q) * cz(q)) - cs2);
+            if (cx(q) * cy(q) > 0) odx += ne;
+            if (cx(q) * cy(q) < 0) odx -= ne;
+            if (cx(q) * cz(q) > 0) ody += ne;
+            if (cx(q) * cz(q) < 0) ody -= ne;
+            if (cy(q) * cz(q) > 0) odz += ne;
+            if (cy(q) * cz(q) < 0) odz -= ne;
+        }
+        R aXxy = R(2) * ux * odx + uy * dsx;
+        R aXxz = R(2) * ux * ody + uz * dsx;
+        R aXyy = ux * dsy + R(2) * uy * odx;
+        R aXzz = ux * dsz + R(2) * uz * ody;
+        R aYyz = R(2) * uy * odz + uz * dsy;
+        R aYzz = uy * dsz + R(2) * uz * odz;
+        const R one_minus = R(1) - omega_p;
+        R scale = R(1);
+        auto admit = [&](R fe, R cand) {
+            R fl = R(1.0e-6) * (fe > R(0) ? fe : R(0));
+            R floor_ = R(1.0e-12) > fl ? R(1.0e-12) : fl;
+            if (cand < floor_) {
+                R den = fe - cand;
+                den = den > R(1.0e-30) ? den : R(1.0e-30);
+                R adm = (fe - floor_) / den;
+                adm = adm < R(0) ? R(0) : (adm > R(1) ? R(1) : adm);
+                scale = scale < adm ? scale : adm;
+            }
+        };
+        {
+            // rest direction: contraction = -cs2 (dsx + dsy + dsz), no third-order part
+            const R h = -cs2;
+            const R contraction = h * dsx + h * dsy + h * dsz;
+            const R rne = Lat<R>::w0 * R(4.5) * contraction;
+            post[0] = feqv[0] + one_minus * rne;
+            admit(feqv[0], post[0]);
+        }
+#pragma unroll
+        for (int q = 1; q < 19; q += 2) {
+            // the contraction is even in c (shared by q and opp q), the third-order sum is odd
+            const R hx = (R)(cx(q) * cx(q)) - cs2, hy = (R)(cy(q) * cy(q)) - cs2, hz = (R)(cz(q) * cz(q)) - cs2;
+            R contraction = hx * dsx + hy * dsy + hz * dsz;
+            {
+                const int xy = cx(q) * cy(q), xz = cx(q) * cz(q), yz = cy(q) * cz(q);
+                if (xy != 0) contraction = contraction + R(2) * (xy > 0 ? odx : -odx);
+                else if (xz != 0) contraction = contraction + R(2) * (xz > 0 ? ody : -ody);
+                else if (yz != 0) contraction = contraction + R(2) * (yz > 0 ? odz : -odz);
+            }
+            const R a = wq<R>(q) * R(4.5) * contraction;
+            R rq = a, ro = a;
+            if (COLL == BFX_COLLISION_RR3) {
+                R third = R(0);
+                bool any = false;
+                auto add = [&](int da, R hb, R amp) {
+                    if (da == 0) return;
+                    R t = ((R)da * hb) * amp;
+                    third = any ? third + t : t;
+                    any = true;
+                };
+                add(cy(q), hx, aXxy);
+                add(cz(q), hx, aXxz);
+                add(cx(q), hy, aXyy);
+                add(cx(q), hz, aXzz);
+                add(cz(q), hy, aYyz);
+                add(cy(q), hz, aYzz);
+                const R b = wq<R>(q) * R(13.5) * third;
+                rq = a + b;
+                ro = a - b;
+            }
+            post[q] = feqv[q] + one_minus * rq;
+            post[q + 1] = feqv[q + 1] + one_minus * ro;
+            admit(feqv[q], post[q]);
+            admit(feqv[q + 1], post[q + 1]);
+        }
+        if (scale < R(1)) {
+            activation = 1.0f;
+            restriction = (float)(R(1) - scale);
+#pragma unroll
+            for (int q = 0; q < 19; ++q) post[q] = feqv[q] + scale * (post[q] - feqv[q]);
+        } else {
+            // scale == 1: feq + 1 * (cand - feq) == cand only up to rounding, so keep
+            // the reference expression
+#pragma unroll
+            for (int q = 0; q < 19; ++q) post[q] = feqv[q] + scale * (post[q] - feqv[q]);
+        }
+    } else if (COLL == BFX_COLLISION_TRT) {
+        // BF.metal:3063-3093, pairwise
+        post[0] = f[0] - omega_p * (f[0] - feqv[0]);
+#pragma unroll
+        for (int q = 1; q < 19; q += 2) {
+            const R fp_ = R(0.5) * (f[q] + f[q + 1]);
+            const R fm = R(0.5) * (f[q] - f[q + 1]);
+            const R ep = R(0.5) * (feqv[q] + feqv[q + 1]);
+            const R em = R(0.5) * (feqv[q] - feqv[q + 1]);
+            const R A = omega_p * (fp_ - ep);
+            const R B = omega_m * (fm - em);
+            post[q] = f[q] - A - B;
+            post[q + 1] = f[q + 1] - A + B;
+        }
+    } else {
+        // symmetric positivity limiter: BF.metal:3094-3174
+        R si[19], ai[19];
+        R sscale = R(1);
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            const int qo = opp(q);
+            R fp_ = R(0.5) * (f[q] + f[qo]);
+            R fm = R(0.5) * (f[q] - f[qo]);
+            R ep = R(0.5) * (feqv[q] + feqv[qo]);
+            R em = R(0.5) * (feqv[q] - feqv[qo]);
+            R sv = -omega_p * (fp_ - ep);
+            R av = -omega_m * (fm - em);
+            si[q] = sv;
+            ai[q] = av;
+            if (sv < R(0)) {
+                R base = f[q] + av;
+                R fl = R(1.0e-6) * (feqv[q] > R(0) ? feqv[q] : R(0));
+                R floor_ = R(1.0e-12) > fl ? R(1.0e-12) : fl;
+                if (base + sv < floor_) {
+                    R den = -sv > R(1.0e-30) ? -sv : R(1.0e-30);
+                    R cand = (base - floor_) / den;
+                    cand = cand < R(0) ? R(0) : (cand > R(1) ? R(1) : cand);
+                    sscale = sscale < cand ? sscale : cand;
+                }
+            }
+        }
+        if (sscale < R(1)) {
+            activation = 1.0f;
+            restriction = (float)(R(1) - sscale);
+        }
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            if (sscale < R(1)) {
+                post[q] = f[q] + sscale * si[q] + ai[q];
+            } else {
+                const int qo = opp(q);
+                R fp_ = R(0.5) * (f[q] + f[qo]);
+                R fm = R(0.5) * (f[q] - f[qo]);
+                R ep = R(0.5) * (feqv[q] + feqv[qo]);
+                R em = R(0.5) * (feqv[q] - feqv[qo]);
+                post[q] = f[q] - omega_p * (fp_ - ep) - omega_m * (fm - em);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Per-cell pieces shared by the fused kernel and the rare-cell kernel.
+// ---------------------------------------------------------------------------
+template <class S, int REP_S>
+__device__ __forceinline__ void load_cell(const BulkArgs& a, uint32_t pid, typename S::R (&f)[19]) {
+    using T = typename S::T;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        if (REP_S) f[q] = S::ld_rt((const T*)a.plane[q] + pid, q);
+        else f[q] = S::ld_rt((const T*)a.plane[opp(q)] + (uint32_t)(pid - (uint32_t)a.doff[q]), opp(q));
+    }
+}
+
+template <class S, int REP_S>
+__device__ __forceinline__ void store_cell(const BulkArgs& a, uint32_t pid, const typename S::R (&post)[19]) {
+    using T = typename S::T;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        if (REP_S) S::st_rt((T*)a.plane[opp(q)] + pid, opp(q), post[q]);
+        else S::st_rt((T*)a.plane[q] + (uint32_t)(pid + (uint32_t)a.doff[q]), q, post[q]);
+    }
+}
+
+// Moments in the reference order (rho over q = 0..18, momentum componentwise).
+template <class R>
+__device__ __forceinline__ void moments(const R (&f)[19], R& rho, R& ux, R& uy, R& uz) {
+    R r = 0, mx = 0, my = 0, mz = 0;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        r += f[q];
+        if (cx(q) > 0) mx += f[q];
+        if (cx(q) < 0) mx -= f[q];
+        if (cy(q) > 0) my += f[q];
+        if (cy(q) < 0) my -= f[q];
+        if (cz(q) > 0) mz += f[q];
+        if (cz(q) < 0) mz -= f[q];
+    }
+    r = r > R(1.0e-8) ? r : R(1.0e-8);
+    rho = r;
+    ux = mx / r;
+    uy = my / r;
+    uz = mz / r;
+}
+
+// Sponge relaxation toward the far field, captured fields, limiter statistics.
+template <class S, int COLL>
+__device__ __forceinline__ void finish_cell(const BulkArgs& a, uint32_t gid, int x, int y, int z, bool capture,
+                                            typename S::R (&post)[19], float activation, float restriction) {
+    using R = typename S::R;
+    if (a.fp.has_sponge) {
+        const float sp = sponge_factor(a.g, a.fp, x, y, z);
+        if (sp > 0.0f) {
+#pragma unroll
+            for (int q = 0; q < 19; ++q) {
+                const R farv = sizeof(R) == 8 ? (R)a.far_eq_d[q] : (R)a.far_eq_f[q];
+                post[q] = post[q] + (farv - post[q]) * (R)sp;
+            }
+        }
+    }
+    if (capture) {
+        R cd = 0, cmx = 0, cmy = 0, cmz = 0;
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            cd += post[q];
+            if (cx(q) > 0) cmx += post[q];
+            if (cx(q) < 0) cmx -= post[q];
+            if (cy(q) > 0) cmy += post[q];
+            if (cy(q) < 0) cmy -= post[q];
+            if (cz(q) > 0) cmz += post[q];
+            if (cz(q) < 0) cmz -= post[q];
+        }
+        cd = cd > R(1.0e-8) ? cd : R(1.0e-8);
+        a.density[gid] = (float)cd;
+        a.velocity[gid] = make_float4((float)(cmx / cd), (float)(cmy / cd), (float)(cmz / cd), 0.0f);
+    }
+    if (COLL != BFX_COLLISION_TRT && activation != 0.0f) {
+        atomicAdd(&a.state->limiter_count, 1.0);
+        atomicMax(&a.state->limiter_max_bits, __float_as_uint(restriction));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The fused kernel: every fluid cell of the lattice.  Solid and newly
+// uncovered cells (flagged in the mask) are left to k_bulk_rare.
+// ---------------------------------------------------------------------------
+template <class S, int REP_S, int COLL, int CAPTURE>
+__global__ void __launch_bounds__(256, sizeof(typename S::R) == 8 ? 1 : (COLL == BFX_COLLISION_TRT ? 4 : 2))
+    k_bulk(const BulkArgs a) {
+    using R = typename S::R;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= a.g.nx || y >= a.g.ny) return;
+    const uint32_t gid = (uint32_t)x + (uint32_t)a.g.nx * ((uint32_t)y + (uint32_t)a.g.ny * (uint32_t)z);
+    if (a.mask && a.mask[gid]) return;
+    const uint32_t pid =
+        (uint32_t)(x + 1) + (uint32_t)a.g.px * ((uint32_t)(y + 1) + (uint32_t)a.g.py * (uint32_t)(z + 1));
+    R f[19];
+    load_cell<S, REP_S>(a, pid, f);
+    R rho, ux, uy, uz;
+    moments<R>(f, rho, ux, uy, uz);
+    R post[19];
+    float activation = 0.0f, restriction = 0.0f;
+    collide<R, COLL>(f, rho, ux, uy, uz, (R)a.fp.omega_p, (R)a.fp.omega_m, post, activation, restriction);
+    finish_cell<S, COLL>(a, gid, x, y, z, CAPTURE != 0, post, activation, restriction);
+    store_cell<S, REP_S>(a, pid, post);
+}
+
+// Solid cells write the moving-wall equilibrium eq(1, u_wall)
+// (BF.metal:2557-2570); newly uncovered cells refill from it and collide
+// (BF.metal:2610-2625).  Both lie inside the geometry box.
+template <class S, int REP_S, int COLL>
+__global__ void __launch_bounds__(128) k_bulk_rare(const BulkArgs a) {
+    using R = typename S::R;
+    const Grid& g = a.g;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.box_cells) return;
+    const int lz = (int)(t / ((int64_t)a.box[0] * a.box[1]));
+    const int64_t r = t - (int64_t)lz * a.box[0] * a.box[1];
+    const int ly = (int)(r / a.box[0]);
+    const int lx = (int)(r - (int64_t)ly * a.box[0]);
+    const int x = a.state->box_origin[0] + lx;
+    const int y = a.state->box_origin[1] + ly;
+    const int z = a.state->box_origin[2] + lz;
+    if (!inside(g, x, y, z)) return;
+    const uint32_t gid = (uint32_t)flat(g, x, y, z);
+    const uint8_t m = a.mask[gid];
+    if (m == 0) return;
+    const uint32_t pid = (uint32_t)pflat(g, x, y, z);
+    const float4 w = a.wall[gid];
+    const R ux = w.x, uy = w.y, uz = w.z;
+    const R u2 = ux * ux + uy * uy + uz * uz;
+    R post[19];
+    if (m & kPartMask) {
+#pragma unroll
+        for (int q = 0; q < 19; ++q) post[q] = feqq<R>(q, R(1), ux, uy, uz, u2);
+        store_cell<S, REP_S>(a, pid, post);
+        if (a.capture) {
+            a.density[gid] = 1.0f;
+            a.velocity[gid] = make_float4(w.x, w.y, w.z, 0.0f);
+        }
+        return;
+    }
+    R f[19];
+#pragma unroll
+    for (int q = 0; q < 19; ++q) f[q] = feqq<R>(q, R(1), ux, uy, uz, u2);
+    R rho, vx, vy, vz;
+    moments<R>(f, rho, vx, vy, vz);
+    float activation = 0.0f, restriction = 0.0f;
+    collide<R, COLL>(f, rho, vx, vy, vz, (R)a.fp.omega_p, (R)a.fp.omega_m, post, activation, restriction);
+    finish_cell<S, COLL>(a, gid, x, y, z, a.capture != 0, post, activation, restriction);
+    store_cell<S, REP_S>(a, pid, post);
+}
+
+template <class S, int REP, int COLL>
+static void bulk_t(const BulkArgs& a, const GridDesc& g, int part, cudaStream_t s) {
+    if (part == 0) {
+        dim3 grid, block;
+        cell_launch_shape(g, grid, block);
+        if (a.capture) k_bulk<S, REP, COLL, 1><<<grid, block, 0, s>>>(a);
+        else k_bulk<S, REP, COLL, 0><<<grid, block, 0, s>>>(a);
+    } else if (a.mask && a.box_cells > 0) {
+        k_bulk_rare<S, REP, COLL><<<(unsigned)((a.box_cells + 127) / 128), 128, 0, s>>>(a);
+    }
+}
+
+template <class S>
+static void bulk_s(const BulkArgs& a, const GridDesc& g, int collision, int rep_s, int part, cudaStream_t s) {
+    switch (collision * 2 + rep_s) {
+    case 0: bulk_t<S, 0, BFX_COLLISION_TRT>(a, g, part, s); break;
+    case 1: bulk_t<S, 1, BFX_COLLISION_TRT>(a, g, part, s); break;
+    case 2: bulk_t<S, 0, BFX_COLLISION_TRT_LIMITER>(a, g, part, s); break;
+    case 3: bulk_t<S, 1, BFX_COLLISION_TRT_LIMITER>(a, g, part, s); break;
+    case 4: bulk_t<S, 0, BFX_COLLISION_REGULARIZED>(a, g, part, s); break;
+    case 5: bulk_t<S, 1, BFX_COLLISION_REGULARIZED>(a, g, part, s); break;
+    case 6: bulk_t<S, 0, BFX_COLLISION_RR3>(a, g, part, s); break;
+    default: bulk_t<S, 1, BFX_COLLISION_RR3>(a, g, part, s); break;
+    }
+}
+
+}  // namespace BFX_VARIANT
+}  // namespace bfx

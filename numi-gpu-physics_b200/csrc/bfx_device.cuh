@@ -159,14 +159,22 @@ struct StoreBF16Dev {
 // A step that starts from rep E pulls f_q(x) = A[opp q][x - c_q] and pushes
 // its result to A[q][x + c_q]; a step from rep S reads A[q][x] and writes
 // A[opp q][x].  Each cell reads and writes the same 19 slots, so the update is
-// race-free in place.  Values pushed across a non-periodic face (rep S) are
-// kept in per-face spill planes so the canonical field stays complete.
+// race-free in place.
+//
+// The population array carries a one-cell halo around the lattice (padded
+// extent (nx+2, ny+2, nz+2)).  Values pushed across a face land in the halo,
+// and a small fill kernel writes the values the boundary cells will pull
+// (periodic copies, face rules) before each step, so the fused kernel uses the
+// same uniform addressing for every real cell.  Masks, wall velocities and
+// captured fields stay unpadded.
 // ---------------------------------------------------------------------------
 struct Grid {
     int nx, ny, nz;
     int per_x, per_y, per_z;  // periodic axes
-    int64_t n;                // cells
+    int64_t n;                // real cells
     int64_t nxy;
+    int px, py, pz;           // padded extent
+    int64_t pxy, pn;          // padded plane and total
 };
 
 // Cell counts are limited to 2^32 - 1 (GridSize, SimulationConfiguration.swift:32-44),
@@ -183,6 +191,10 @@ __device__ __forceinline__ void unflat(const Grid& g, int64_t gid, int& x, int& 
 }
 __device__ __forceinline__ int64_t flat(const Grid& g, int x, int y, int z) {
     return (int64_t)x + (int64_t)g.nx * ((int64_t)y + (int64_t)g.ny * z);
+}
+// Padded index of (x, y, z), valid for -1 <= x <= nx (and likewise y, z).
+__device__ __forceinline__ int64_t pflat(const Grid& g, int x, int y, int z) {
+    return (int64_t)(x + 1) + (int64_t)g.px * ((int64_t)(y + 1) + (int64_t)g.py * (z + 1));
 }
 __device__ __forceinline__ bool inside(const Grid& g, int x, int y, int z) {
     return x >= 0 && y >= 0 && z >= 0 && x < g.nx && y < g.ny && z < g.nz;
@@ -203,73 +215,31 @@ __device__ __forceinline__ int exit_face(const Grid& g, int x, int y, int z) {
     if (y >= g.ny) return 3;
     return z < 0 ? 4 : 5;
 }
-// Slot of direction q among the five directions leaving through face f.
-__device__ __forceinline__ int face_slot(int f, int q) {
-    int a = f >> 1;
-    int s = (f & 1) ? 1 : -1;
-    int k = 0;
-    for (int j = 1; j < 19; ++j) {
-        int c = a == 0 ? cx(j) : (a == 1 ? cy(j) : cz(j));
-        if (c == s) {
-            if (j == q) return k;
-            ++k;
-        }
-    }
-    return 0;
-}
-// Plane index of an in-range cell (x,y,z) on face f.
-__device__ __forceinline__ int64_t face_index(const Grid& g, int f, int x, int y, int z) {
-    int a = f >> 1;
-    if (a == 0) return (int64_t)y + (int64_t)g.ny * z;
-    if (a == 1) return (int64_t)x + (int64_t)g.nx * z;
-    return (int64_t)x + (int64_t)g.nx * y;
-}
 
-// Spill planes: face f holds 5 * plane_cells(f) values at offset spill_off[f].
-struct Spill {
-    int64_t off[6];
-};
-
-// Canonical accessor f*_q(x) for the current representation (sparse kernels).
+// Canonical accessor f*_q(x) of a real cell in the current representation.
 template <class S>
-__device__ __forceinline__ typename S::R canon_load(const typename S::T* A, const Grid& g, const Spill& sp,
-                                                    const typename S::T* spill, int rep_s, int q, int x, int y,
-                                                    int z) {
-    if (!rep_s) return S::ld_rt(A + (int64_t)opp(q) * g.n + flat(g, x, y, z), opp(q));
-    int tx = x + cx(q), ty = y + cy(q), tz = z + cz(q);
-    if (wrap(g, tx, ty, tz)) return S::ld_rt(A + (int64_t)q * g.n + flat(g, tx, ty, tz), q);
-    int f = exit_face(g, tx, ty, tz);
-    return S::ld_rt(spill + sp.off[f] + face_index(g, f, x, y, z) * 5 + face_slot(f, q), q);
+__device__ __forceinline__ typename S::R canon_load(const typename S::T* A, const Grid& g, int rep_s, int q, int x,
+                                                    int y, int z) {
+    if (!rep_s) return S::ld_rt(A + (int64_t)opp(q) * g.pn + pflat(g, x, y, z), opp(q));
+    return S::ld_rt(A + (int64_t)q * g.pn + pflat(g, x + cx(q), y + cy(q), z + cz(q)), q);
 }
 template <class S>
-__device__ __forceinline__ void canon_store(typename S::T* A, const Grid& g, const Spill& sp, typename S::T* spill,
-                                            int rep_s, int q, int x, int y, int z, typename S::R v) {
-    if (!rep_s) {
-        S::st_rt(A + (int64_t)opp(q) * g.n + flat(g, x, y, z), opp(q), v);
-        return;
-    }
-    int tx = x + cx(q), ty = y + cy(q), tz = z + cz(q);
-    if (wrap(g, tx, ty, tz)) {
-        S::st_rt(A + (int64_t)q * g.n + flat(g, tx, ty, tz), q, v);
-        return;
-    }
-    int f = exit_face(g, tx, ty, tz);
-    S::st_rt(spill + sp.off[f] + face_index(g, f, x, y, z) * 5 + face_slot(f, q), q, v);
+__device__ __forceinline__ void canon_store(typename S::T* A, const Grid& g, int rep_s, int q, int x, int y, int z,
+                                            typename S::R v) {
+    if (!rep_s) S::st_rt(A + (int64_t)opp(q) * g.pn + pflat(g, x, y, z), opp(q), v);
+    else S::st_rt(A + (int64_t)q * g.pn + pflat(g, x + cx(q), y + cy(q), z + cz(q)), q, v);
 }
-// Address of the slot cell (x,y,z) reads for incoming direction q in the NEXT
-// step (rep E -> pulls A[opp q][x - c_q]; rep S -> reads A[q][x]); null when
-// the source lies outside a non-periodic face (the step applies the face rule).
+// Slot that real cell (x,y,z) reads as its incoming direction q in the NEXT
+// step: rep E pulls A[opp q][x - c_q] (possibly a halo cell), rep S reads A[q][x].
 template <class S>
 __device__ __forceinline__ typename S::T* incoming_slot(typename S::T* A, const Grid& g, int rep_s, int q, int x,
                                                         int y, int z, int& slot_dir) {
     if (rep_s) {
         slot_dir = q;
-        return A + (int64_t)q * g.n + flat(g, x, y, z);
+        return A + (int64_t)q * g.pn + pflat(g, x, y, z);
     }
-    int sx = x - cx(q), sy = y - cy(q), sz = z - cz(q);
-    if (!wrap(g, sx, sy, sz)) return nullptr;
     slot_dir = opp(q);
-    return A + (int64_t)opp(q) * g.n + flat(g, sx, sy, sz);
+    return A + (int64_t)opp(q) * g.pn + pflat(g, x - cx(q), y - cy(q), z - cz(q));
 }
 
 // Mask byte: bits 0-5 part id (0 = fluid), bit 6 newly uncovered, bit 7 newly covered.

@@ -1,0 +1,19 @@
+// Fused-step kernels compiled with FMA contraction (--fmad=true): the 16-bit
+// deviation storage formats, whose collision arithmetic is FP32 but which are
+// not part of the bit-exact FP32 parity contract, and the opt-in fast_math FP32
+// mode (the reference's SimulationConfiguration.fastMath).
+#define BFX_VARIANT fast
+#include "bfx_bulk_kernels.cuh"
+
+namespace bfx {
+
+void launch_bulk_fast(int storage, int collision, int rep_s, const GridDesc& g, const BulkArgs& a, int part,
+                      cudaStream_t s) {
+    switch (storage) {
+    case BFX_STORAGE_F16_DEVIATION: fast::bulk_s<StoreF16Dev>(a, g, collision, rep_s, part, s); break;
+    case BFX_STORAGE_BF16_DEVIATION: fast::bulk_s<StoreBF16Dev>(a, g, collision, rep_s, part, s); break;
+    default: fast::bulk_s<StoreF32>(a, g, collision, rep_s, part, s); break;
+    }
+}
+
+}  // namespace bfx

@@ -16,13 +16,11 @@ namespace bfx {
 
 struct GeomArgs {
     Grid g;
-    Spill sp;
     FluidParams fp;
     int bx, by, bz;          // box extent
     int64_t box_cells;
     GeomBuffers b;
     void* pops;
-    void* spill;
 };
 
 // ---------------------------------------------------------------------------
@@ -665,14 +663,13 @@ __global__ void __launch_bounds__(256) k_boundary_scan(const GeomArgs a, int rep
         const uint8_t m1 = a.b.mask_next[gid];
         const uint8_t m0 = a.b.mask_prev[gid];
         const typename S::T* A = (const typename S::T*)a.pops;
-        const typename S::T* spill = (const typename S::T*)a.spill;
         const double* body = a.b.state->body;
         const V3 world = cell_world(fp, x, y, z);
         if ((m1 & kCovered) && fp.accumulate && include_topo) {
             // newly covered: previous fluid momentum (minus the wall-moving density for estimators 0-5)
             R pd = 0, pmx = 0, pmy = 0, pmz = 0;
             for (int q = 0; q < 19; ++q) {
-                R prev = canon_load<S>(A, g, a.sp, spill, rep_s, q, x, y, z);
+                R prev = canon_load<S>(A, g, rep_s, q, x, y, z);
                 pd += prev;
                 pmx += prev * (R)cx(q);
                 pmy += prev * (R)cy(q);
@@ -703,8 +700,8 @@ __global__ void __launch_bounds__(256) k_boundary_scan(const GeomArgs a, int rep
                 if (!inside(g, bx, by, bz)) continue;
                 int64_t nb = flat(g, bx, by, bz);
                 if (!((a.b.mask_prev[nb] & kPartMask) == 0 && (a.b.mask_next[nb] & kPartMask) == 0)) continue;
-                R old_out = canon_load<S>(A, g, a.sp, spill, rep_s, q, x, y, z);
-                R sup_in = canon_load<S>(A, g, a.sp, spill, rep_s, opp(q), bx, by, bz);
+                R old_out = canon_load<S>(A, g, rep_s, q, x, y, z);
+                R sup_in = canon_load<S>(A, g, rep_s, opp(q), bx, by, bz);
                 R sum = old_out + sup_in;
                 tx -= sum * (R)cx(q);
                 ty -= sum * (R)cy(q);
@@ -851,7 +848,6 @@ __global__ void __launch_bounds__(256) k_links_apply(const GeomArgs a, int rep_s
     const int mode = sel ? fp.force_mode : 6;
     const int include_link = !sel || fp.load_component != 2;
     T* A = (T*)a.pops;
-    const T* spill = (const T*)a.spill;
     const double* body = a.b.state->body;
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int64_t count = a.b.state->link_count;
@@ -870,9 +866,9 @@ __global__ void __launch_bounds__(256) k_links_apply(const GeomArgs a, int rep_s
         R mwd = (R)fp.far[3];
         if (fp.local_density) {
             mwd = 0;
-            for (int k = 0; k < 19; ++k) mwd += canon_load<S>(A, g, a.sp, spill, rep_s, k, x, y, z);
+            for (int k = 0; k < 19; ++k) mwd += canon_load<S>(A, g, rep_s, k, x, y, z);
         }
-        const R reflected = canon_load<S>(A, g, a.sp, spill, rep_s, opp(q), x, y, z);
+        const R reflected = canon_load<S>(A, g, rep_s, opp(q), x, y, z);
         const R dx_ = (R)cx(q), dy_ = (R)cy(q), dz_ = (R)cz(q);
         R qf = R(0.5);
         const float4 ws = a.b.wall[src];
@@ -907,10 +903,10 @@ __global__ void __launch_bounds__(256) k_links_apply(const GeomArgs a, int rep_s
         R value = reflected + wc;
         if (interp) {
             if (qf <= R(0.5)) {
-                const R fo = canon_load<S>(A, g, a.sp, spill, rep_s, opp(q), fx, fy, fz);
+                const R fo = canon_load<S>(A, g, rep_s, opp(q), fx, fy, fz);
                 value = R(2) * qf * reflected + (R(1) - R(2) * qf) * fo + wc;
             } else {
-                const R pin = canon_load<S>(A, g, a.sp, spill, rep_s, q, x, y, z);
+                const R pin = canon_load<S>(A, g, rep_s, q, x, y, z);
                 value = (reflected + wc) / (R(2) * qf) + (R(2) * qf - R(1)) * pin / (R(2) * qf);
             }
         }
@@ -1128,17 +1124,9 @@ __global__ void k_record_sample(const GeomArgs a, bfx_run_sample* samples, uint6
 // Host launchers
 // ---------------------------------------------------------------------------
 static GeomArgs make_geom(const GridDesc& gd, const FluidParams& fp, const BoxDesc& box, const GeomBuffers& gb,
-                          void* pops, void* spill) {
+                          void* pops) {
     GeomArgs a;
-    a.g.nx = gd.nx;
-    a.g.ny = gd.ny;
-    a.g.nz = gd.nz;
-    a.g.per_x = gd.per_x;
-    a.g.per_y = gd.per_y;
-    a.g.per_z = gd.per_z;
-    a.g.n = gd.n;
-    a.g.nxy = gd.nxy;
-    for (int f = 0; f < 6; ++f) a.sp.off[f] = gd.spill_off[f];
+    a.g = device_grid(gd);
     a.fp = fp;
     a.bx = box.sx;
     a.by = box.sy;
@@ -1146,7 +1134,6 @@ static GeomArgs make_geom(const GridDesc& gd, const FluidParams& fp, const BoxDe
     a.box_cells = box.cells;
     a.b = gb;
     a.pops = pops;
-    a.spill = spill;
     return a;
 }
 
@@ -1166,14 +1153,14 @@ int box_block_count(const BoxDesc& box) {
 
 void launch_prepare(int geometry, float dt, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
                     const GeomBuffers& gb, int init, cudaStream_t s) {
-    GeomArgs a = make_geom(g, fp, box, gb, nullptr, nullptr);
+    GeomArgs a = make_geom(g, fp, box, gb, nullptr);
     k_prepare<<<1, 1, 0, s>>>(a, init, dt, 0.0f);
     (void)geometry;
 }
 
 void launch_classify(int geometry, int has_prev, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
                      const GeomBuffers& gb, cudaStream_t s) {
-    GeomArgs a = make_geom(g, fp, box, gb, nullptr, nullptr);
+    GeomArgs a = make_geom(g, fp, box, gb, nullptr);
     dim3 grid, block;
     box_shape(box, grid, block);
     if (geometry == BFX_GEOMETRY_BIRD) {
@@ -1205,13 +1192,13 @@ static void scan_s(const GeomArgs& a, int rep_s, const BoxDesc& box, cudaStream_
 
 void launch_boundary_scan(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
                           const GeomBuffers& gb, const FluidBuffers& fb, cudaStream_t s) {
-    GeomArgs a = make_geom(g, fp, box, gb, fb.pops, fb.spill);
+    GeomArgs a = make_geom(g, fp, box, gb, fb.pops);
     BFX_DISPATCH_STORAGE(storage, scan_s, a, rep_s, box, s);
 }
 
 void launch_links_emit(int geometry, int link_rule, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
                        const GeomBuffers& gb, cudaStream_t s) {
-    GeomArgs a = make_geom(g, fp, box, gb, nullptr, nullptr);
+    GeomArgs a = make_geom(g, fp, box, gb, nullptr);
     k_scan<<<1, 1024, 0, s>>>(a);
     dim3 grid, block;
     box_shape(box, grid, block);
@@ -1226,7 +1213,7 @@ static void apply_s(const GeomArgs& a, int rep_s, cudaStream_t s) {
 void launch_links_apply(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const GeomBuffers& gb,
                         const FluidBuffers& fb, cudaStream_t s) {
     BoxDesc box = {1, 1, 1, 1};
-    GeomArgs a = make_geom(g, fp, box, gb, fb.pops, fb.spill);
+    GeomArgs a = make_geom(g, fp, box, gb, fb.pops);
     BFX_DISPATCH_STORAGE(storage, apply_s, a, rep_s, s);
 }
 
@@ -1234,14 +1221,14 @@ void launch_reduce_loads(const GeomBuffers& gb, int with_topology, cudaStream_t 
     GridDesc g = {};
     FluidParams fp = {};
     BoxDesc box = {1, 1, 1, 1};
-    GeomArgs a = make_geom(g, fp, box, gb, nullptr, nullptr);
+    GeomArgs a = make_geom(g, fp, box, gb, nullptr);
     k_reduce_loads<<<1, 256, 0, s>>>(a, with_topology);
 }
 
 void launch_integrate(const GridDesc& g, const FluidParams& fp, const GeomBuffers& gb, float gravity_x,
                       float gravity_y, float gravity_z, int substeps, int free_flight, cudaStream_t s) {
     BoxDesc box = {1, 1, 1, 1};
-    GeomArgs a = make_geom(g, fp, box, gb, nullptr, nullptr);
+    GeomArgs a = make_geom(g, fp, box, gb, nullptr);
     k_finish<<<1, 1, 0, s>>>(a, gravity_x, gravity_y, gravity_z, substeps, free_flight, gb.bird);
 }
 
@@ -1249,7 +1236,7 @@ void launch_record_sample(const GeomBuffers& gb, const FluidParams& fp, bfx_run_
                           float dt, cudaStream_t s) {
     GridDesc g = {};
     BoxDesc box = {1, 1, 1, 1};
-    GeomArgs a = make_geom(g, fp, box, gb, nullptr, nullptr);
+    GeomArgs a = make_geom(g, fp, box, gb, nullptr);
     k_record_sample<<<1, 1, 0, s>>>(a, samples, index, dt);
 }
 

@@ -13,15 +13,11 @@ struct GridDesc {
     int nx, ny, nz;
     int per_x, per_y, per_z;
     int64_t n, nxy;
-    int64_t spill_off[6];   // element offsets of the six spill planes
-    int64_t ghost_off[6];   // element offsets of the six ghost planes
-    int64_t spill_total;
+    int64_t padded;         // (nx+2)(ny+2)(nz+2): cells of the population array with its halo
 };
 
 struct FluidBuffers {
-    void* pops;             // 19 * n elements of the storage type
-    void* spill;            // 5 * face cells per face
-    void* ghost;            // 5 * face cells per face (outflow faces)
+    void* pops;             // 19 * padded elements of the storage type
     uint8_t* mask;          // current occupancy (part id + topology flags); may be null
     const float4* wall;     // wall velocity / distance; may be null without geometry
     float* density;         // captured fields
@@ -35,9 +31,9 @@ struct FluidBuffers {
 // One step launches both parts.
 void launch_bulk(int storage, int collision, int rep_s, const GridDesc& g, const FluidParams& fp,
                  const FluidBuffers& b, int capture, int part, const int* box, cudaStream_t s);
-// Zero-gradient outflow ghost planes (before the step).
-void launch_ghost(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const FluidBuffers& b,
-                  cudaStream_t s);
+// Halo fill: the values boundary cells pull from outside the lattice (before the step).
+void launch_halo(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const FluidBuffers& b,
+                 cudaStream_t s);
 // Equilibrium initialisation into representation E.
 void launch_init(int storage, int init_kind, float amplitude, const GridDesc& g, const FluidParams& fp,
                  const FluidBuffers& b, cudaStream_t s);
@@ -106,6 +102,8 @@ void launch_step_counter(DeviceState* st, cudaStream_t s);
 }  // namespace bfx
 
 namespace bfx {
+struct Grid;
+Grid device_grid(const GridDesc& gd);
 int box_block_count(const BoxDesc& box);
 void launch_fill_wall(float4* wall, int64_t n, float w, cudaStream_t s);
 }  // namespace bfx

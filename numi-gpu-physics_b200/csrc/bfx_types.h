@@ -29,6 +29,7 @@ struct FluidParams {
     int accumulate;
     int has_sponge;
     int any_outflow;
+    int fast_math;
 };
 
 // Prepared articulated geometry (GPUPreparedBirdGeometry, BF.metal:112-127).

@@ -1,0 +1,190 @@
+"""GPU feature tests modelled on the reference's own test strategy
+(Tests/BirdFlowMetalTests): batch-partition invariance (MetalExecutionTests.swift:473-592),
+checkpoint round trip and continuation (ObservationAndCheckpointTests.swift:116-161),
+runtime-safety failure (MetalExecutionTests.swift:690-736), field capture,
+determinism, meshes beyond the reference's 4,096-triangle cap, and the
+16-bit storage formats.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import math
+
+import numpy as np
+import pytest
+
+import bfx._lib as L
+import bfx.cases as cases
+import oracle as O
+from bfx.simulation import BirdFlowError, Lattice, bird_struct
+from helpers import body_struct_from_tuple, oracle_twin
+
+pytestmark = pytest.mark.gpu
+
+
+def lattice(cfg, rows=None, body=None, mesh=None):
+    return Lattice(cfg, bird_struct(rows) if rows is not None else None,
+                   body_struct_from_tuple(body) if body is not None else None, mesh)
+
+
+def small_mesh_case(**kw):
+    # period 1000: tip speed ~0.1 cells/step (Mach ~0.17 at the tip), still
+    # covering and uncovering cells every step
+    args = dict(nx=96, ny=64, nz=64, span=16.0, chord=6.0, thickness=2.0, n_chord=6, n_span=16, period=1000.0,
+                viscosity=0.02, sponge_width=6.0)
+    args.update(kw)
+    return cases.flapping_plates(**args)
+
+
+def test_batch_partition_invariance_is_bit_exact():
+    """16 steps as 16x1, 4x4 and 1x16 give identical populations and loads."""
+    cfg, rows, body, mesh = small_mesh_case()
+    results = []
+    for batches in ((1,) * 16, (4,) * 4, (16,)):
+        lat = lattice(cfg, rows, body, mesh)
+        for b in batches:
+            lat.advance(b, batch_size=b)
+        results.append((lat.populations(), np.array(lat.loads().force)))
+        lat.close()
+    assert np.all(np.isfinite(results[0][0]))
+    for pops, force in results[1:]:
+        assert np.array_equal(pops, results[0][0])
+        assert np.array_equal(force, results[0][1])
+
+
+def test_two_runs_are_bit_identical():
+    cfg, rows, body, _ = cases.ellipsoid_channel(nx=64, ny=32, nz=32, radii=(9.0, 5.0, 4.5), viscosity=0.02)
+    out = []
+    for _ in range(2):
+        lat = lattice(cfg, rows, body)
+        lat.advance(25, batch_size=7)
+        out.append((lat.populations(), np.array(lat.loads().force), np.array(lat.loads().torque)))
+        lat.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[0][2], out[1][2])
+
+
+def test_checkpoint_round_trip_and_continuation():
+    cfg, rows, body, mesh = small_mesh_case()
+    lat = lattice(cfg, rows, body, mesh)
+    lat.advance(5)
+    state = lat.save_state()
+    pops_saved = lat.populations()
+    lat.advance(7)
+    cont = lat.populations()
+    assert np.all(np.isfinite(cont))
+    force = np.array(lat.loads().force)
+    lat.restore_state(state)
+    assert np.array_equal(lat.populations(), pops_saved)
+    assert lat.step_index()[0] == 5
+    lat.advance(7)
+    assert np.array_equal(lat.populations(), cont)
+    assert np.array_equal(np.array(lat.loads().force), force)
+    # restoring into a fresh handle continues identically
+    fresh = lattice(cfg, rows, body, mesh)
+    fresh.restore_state(state)
+    fresh.advance(7)
+    assert np.array_equal(fresh.populations(), cont)
+
+
+def test_corrupted_checkpoint_fails_cleanly():
+    cfg, _, _, _ = cases.shear_wave(n=16, viscosity=0.03, magic=3.0 / 16.0, axis="y")
+    lat = lattice(cfg)
+    lat.advance(2)
+    state = bytearray(lat.save_state())
+    state[len(state) // 2] ^= 0xFF
+    with pytest.raises(BirdFlowError) as e:
+        lat.restore_state(bytes(state))
+    assert e.value.status == 8
+    lat.advance(1)  # the handle stays usable
+
+
+def test_field_capture_matches_oracle():
+    cfg, rows, body, _ = cases.ellipsoid_channel(nx=48, ny=24, nz=24, radii=(7.0, 4.0, 4.0), viscosity=0.02)
+    lat = lattice(cfg, rows, body)
+    osim = oracle_twin(cfg, rows, body)
+    lat.advance(5, capture_fields=True)
+    osim.advance(4)
+    osim.step(capture_fields=True)
+    rho, vel = lat.fields()
+    assert np.array_equal(rho, osim.density)
+    assert np.array_equal(vel, osim.velocity.reshape(-1, 4)[:, :3])
+
+
+def test_mesh_beyond_4096_triangles_matches_oracle():
+    """16,384 triangles: the reference's 12-bit key would cap this at 4,096."""
+    cfg, rows, body, mesh = small_mesh_case(nx=80, ny=64, nz=64, span=20.0, chord=8.0, n_chord=32, n_span=128,
+                                            link_rule=L.LINK_RAY_ROOT)
+    assert mesh["tris"].shape[0] == 16384
+    lat = lattice(cfg, rows, body, mesh)
+    osim = oracle_twin(cfg, rows, body, mesh)
+    assert np.array_equal(lat.mask(), osim.mcur)
+    for step in range(3):
+        lat.advance(1)
+        osim.step()
+        assert np.array_equal(lat.mask(), osim.mcur)
+        g = lat.populations().ravel()
+        rel = np.max(np.abs(g.astype(np.float64) - osim.pa) / np.maximum(np.abs(osim.pa), 1e-12))
+        assert rel <= 1e-6
+
+
+def test_runtime_safety_violation_invalidates_the_handle():
+    """A free-flying body launched far above Mach 0.15 trips the safety ledger
+    on the first step (host-side check after the batch, as the reference's
+    advance does); the handle is then terminally invalid."""
+    from bfx.simulation import BirdFlowSimulation
+    config, bird, state = cases.compact_bird(free_flight=True)
+    state.linear_velocity_meters_per_second = (60.0, 0.0, 0.0)
+    sim = BirdFlowSimulation(config, bird, state)
+    with pytest.raises(BirdFlowError) as e:
+        sim.advance(3, batch_size=1)
+    assert e.value.status == 5
+    with pytest.raises(BirdFlowError) as e2:
+        sim.advance(1)
+    assert e2.value.status == 6
+
+
+def test_invalid_advance_request():
+    cfg, _, _, _ = cases.shear_wave(n=16, axis="y")
+    lat = lattice(cfg)
+    rc = lat.lib.bfx_advance(lat.handle, 1, 0, 0, None, 0, None)
+    assert rc == 3
+
+
+def test_bird_simulation_run_samples_and_snapshot():
+    from bfx.simulation import BirdFlowSimulation
+    config, bird, state = cases.compact_bird(free_flight=True)
+    sim = BirdFlowSimulation(config, bird, state)
+    res = sim.advance(6, batch_size=4, record_run_samples=True)
+    assert len(res.run_samples) == 6
+    assert [s.step for s in res.run_samples] == [1, 2, 3, 4, 5, 6]
+    snap = sim.snapshot()
+    assert snap.step == 6
+    assert res.runtime_safety["passed"]
+    last = res.run_samples[-1]
+    assert np.allclose(list(last.position), list(snap.body.position))
+    rho, vel = sim.copy_macroscopic_fields()
+    assert np.all(np.isfinite(rho)) and np.all(rho > 0.5)
+    p = sim.copy_gauge_pressure_field_pascals()
+    assert p.shape == rho.shape
+
+
+# Measured on B200: FP64 differs from FP32 by ~1e-5 (FP32 round-off), the FP16
+# deviation format by ~3e-3.  BF16 keeps only 8 significant bits of f - w_q,
+# which cannot resolve this small-amplitude wave: its amplitude is off by ~35%,
+# so BF16 storage is only checked for staying finite and bounded.
+@pytest.mark.parametrize("storage,tol", [(L.STORAGE_F16_DEVIATION, 6e-3), (L.STORAGE_BF16_DEVIATION, 0.6),
+                                         (L.STORAGE_F64, 1e-4)])
+def test_storage_formats_track_f32(storage, tol):
+    """Shear-wave amplitude after 400 steps in each storage format vs FP32."""
+    amps = {}
+    for st in (L.STORAGE_F32, storage):
+        cfg, _, _, _ = cases.shear_wave(n=32, viscosity=0.02, magic=0.25, amplitude=0.02, axis="z", storage=st)
+        lat = lattice(cfg)
+        lat.advance(400, capture_fields=True)
+        _, vel = lat.fields()
+        prof = vel[:, 0].reshape(32, 32, 32).mean(axis=(1, 2))
+        amps[st] = 2.0 * np.dot(prof, np.sin(2 * np.pi * np.arange(32) / 32)) / 32
+        lat.close()
+    assert abs(amps[storage] - amps[L.STORAGE_F32]) / abs(amps[L.STORAGE_F32]) < tol

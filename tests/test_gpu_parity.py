@@ -204,7 +204,7 @@ def test_compact_bird_free_flight_matches_oracle():
 @pytest.mark.parametrize("link_rule", [L.LINK_LINEAR, L.LINK_RAY_ROOT])
 def test_flapping_plate_mesh_matches_oracle(link_rule):
     cfg, rows, body, mesh = cases.flapping_plates(nx=96, ny=64, nz=64, span=16.0, chord=6.0, thickness=2.0,
-                                                  n_chord=6, n_span=16, period=120.0, viscosity=0.02,
+                                                  n_chord=6, n_span=16, period=1000.0, viscosity=0.02,
                                                   link_rule=link_rule, sponge_width=6.0)
     lat, osim = make_pair(cfg, rows, body, mesh)
     assert np.array_equal(lat.mask(), osim.mcur)
@@ -217,3 +217,6 @@ def test_flapping_plate_mesh_matches_oracle(link_rule):
         cell, d, q = lat.links()
         oc, od = oracle_links(osim)
         assert np.array_equal(link_set(cell, d), link_set(oc, od)), f"links step {step + 1}"
+        ld = lat.loads()
+        assert ld.covered_count == osim.loads.covered_count and ld.uncovered_count == osim.loads.uncovered_count
+    assert osim.loads.covered_count + osim.loads.uncovered_count > 0
