@@ -227,9 +227,17 @@ __device__ __forceinline__ void moments(const R (&f)[19], R& rho, R& ux, R& uy, 
     }
     r = r > R(1.0e-8) ? r : R(1.0e-8);
     rho = r;
+#ifdef BFX_CONTRACTED
+    // contracted variant: one reciprocal instead of three correctly rounded divisions
+    const R inv = R(1) / r;
+    ux = mx * inv;
+    uy = my * inv;
+    uz = mz * inv;
+#else
     ux = mx / r;
     uy = my / r;
     uz = mz / r;
+#endif
 }
 
 // Sponge relaxation toward the far field, captured fields, limiter statistics.

@@ -3,6 +3,7 @@
 // not part of the bit-exact FP32 parity contract, and the opt-in fast_math FP32
 // mode (the reference's SimulationConfiguration.fastMath).
 #define BFX_VARIANT fast
+#define BFX_CONTRACTED 1
 #include "bfx_bulk_kernels.cuh"
 
 namespace bfx {
