@@ -52,7 +52,8 @@ typedef enum bfx_status {
     BFX_ERR_INVALIDATED = 6,        /* simulationStateInvalidated */
     BFX_ERR_INVALID_CONFIG = 7,     /* BirdFlowConfigurationError */
     BFX_ERR_INVALID_ARGUMENT = 8,
-    BFX_ERR_CAPACITY = 9            /* caller buffer or link list too small */
+    BFX_ERR_CAPACITY = 9,           /* caller buffer or link list too small */
+    BFX_ERR_UNSUPPORTED = 10        /* configuration outside the adjoint's scope */
 } bfx_status;
 
 /* Collision operator.  The reference selects these through caseParameters.w
@@ -157,7 +158,10 @@ typedef struct bfx_bird {
     bfx_float4 wing_geometry1;      /* sweep, root offset xyz */
     bfx_float4 tail_geometry;       /* length, half width, thickness, - */
     bfx_float4 wing_kinematics0;    /* frequency Hz, stroke amplitude, stroke bias, pitch mean */
-    bfx_float4 wing_kinematics1;    /* pitch amplitude, pitch phase, -, - */
+    bfx_float4 wing_kinematics1;    /* pitch amplitude, pitch phase, deviation amplitude, measured-keyframe flag
+                                       (must be 0).  Deviation about the stroke-plane normal is
+                                       amplitude * sin(2 * phase); the reference uses this slot for the
+                                       keyframe count of measured kinematics, which bfx does not support. */
     bfx_float4 safety_geometry;     /* conservative local half extent xyz, bounding radius */
     bfx_float4 safety_limits;       /* max prescribed wing speed, Mach limit */
     bfx_float4 left_wing_mass_com;  /* mass, centre of mass from hinge (chord, span, normal) */
@@ -318,6 +322,49 @@ BFX_API int bfx_device_bytes(bfx_sim* sim, uint64_t* bytes);
  * scratch: calls that overlap on the GPU race and must be serialised. */
 BFX_API int bfx_fluid_mass_momentum_noalloc(const float* populations, const uint8_t* mask, uint32_t nx, uint32_t ny,
                                             uint32_t nz, double* out);
+/* ---- discrete adjoint ------------------------------------------------------
+ * No reference counterpart (the reference has no adjoint).  Gradient of a
+ * time-averaged load objective with respect to the four prescribed wing
+ * kinematic parameters theta = (wing_kinematics0.y stroke amplitude,
+ * wing_kinematics1.x pitch amplitude, wing_kinematics1.y pitch phase,
+ * wing_kinematics1.z deviation amplitude), all in radians:
+ *   J = mean over steps k in [window_first, window_last] of
+ *       force_weight . F_k + power_weight * P_k,
+ * F_k the momentum-exchange body force (N) of step k and
+ * P_k = -sum over cut links of F_link . u_wall the aerodynamic power (W) the
+ * wings deliver to the fluid.  Step indices count from 1 at the call.
+ * The call advances the simulation by `steps` (the final state equals that of
+ * bfx_advance(steps)), then runs the discrete adjoint backward with two-level
+ * checkpointing: a population snapshot every `checkpoint_interval` steps
+ * (0 = ceil(sqrt(steps))), each interval recomputed once with its adjoint
+ * tape.  Scope: TRT collision, F32 or F64 storage, mesh geometry with moving
+ * wings and no free flight, far-field / velocity / periodic faces, force
+ * estimator 6, all parts, link and topology loads; anything else returns
+ * BFX_ERR_UNSUPPORTED.  The topology of every step (solid cells, links,
+ * bounce-back case) is held fixed, so the gradient is that of the smooth piece
+ * of J the parameters lie on. */
+typedef struct bfx_adjoint_objective {
+    double force_weight[3];
+    double power_weight;
+    uint64_t window_first;          /* 0 and 0: every step of the call */
+    uint64_t window_last;
+} bfx_adjoint_objective;
+
+typedef struct bfx_adjoint_result {
+    double objective;               /* J */
+    double gradient[4];             /* dJ/dtheta */
+    uint64_t steps;
+    uint32_t checkpoint_interval;
+    uint32_t snapshots;
+    double forward_ms;              /* device time of the forward pass with its snapshots */
+    double reverse_ms;              /* device time of the recomputation and the reverse sweep */
+    uint64_t max_links;             /* largest cut-link count of the run */
+    uint64_t work_bytes;            /* device memory of snapshots, tape and adjoint fields */
+} bfx_adjoint_result;
+
+BFX_API int bfx_adjoint(bfx_sim* sim, uint64_t steps, const bfx_adjoint_objective* objective,
+                        uint32_t checkpoint_interval, bfx_adjoint_result* result);
+
 /* Message of the last failure on this handle (or of the last failed create when sim is NULL). */
 BFX_API int bfx_last_error(bfx_sim* sim, char* buf, size_t capacity);
 

@@ -105,13 +105,24 @@ class AdvanceResult(ct.Structure):
                 ("safety_passed", ct.c_uint32), ("safety", SafetyRecord)]
 
 
+class AdjointObjective(ct.Structure):
+    _fields_ = [("force_weight", ct.c_double * 3), ("power_weight", ct.c_double),
+                ("window_first", ct.c_uint64), ("window_last", ct.c_uint64)]
+
+
+class AdjointResult(ct.Structure):
+    _fields_ = [("objective", ct.c_double), ("gradient", ct.c_double * 4), ("steps", ct.c_uint64),
+                ("checkpoint_interval", ct.c_uint32), ("snapshots", ct.c_uint32), ("forward_ms", ct.c_double),
+                ("reverse_ms", ct.c_double), ("max_links", ct.c_uint64), ("work_bytes", ct.c_uint64)]
+
+
 EXPORTED = (
     "bfx_version", "bfx_abi_version", "bfx_device_count", "bfx_create", "bfx_destroy", "bfx_advance",
     "bfx_snapshot", "bfx_copy_fields", "bfx_copy_gauge_pressure", "bfx_runtime_safety", "bfx_last_loads",
     "bfx_copy_populations", "bfx_set_populations", "bfx_copy_mask", "bfx_copy_wall", "bfx_copy_links",
     "bfx_fluid_mass_momentum", "bfx_save_state", "bfx_restore_state", "bfx_get_body", "bfx_set_body",
     "bfx_step_index", "bfx_set_kernel_timing", "bfx_kernel_timing", "bfx_timer_begin", "bfx_timer_end",
-    "bfx_launch_count", "bfx_device_bytes", "bfx_fluid_mass_momentum_noalloc", "bfx_last_error",
+    "bfx_launch_count", "bfx_device_bytes", "bfx_fluid_mass_momentum_noalloc", "bfx_adjoint", "bfx_last_error",
 )
 
 _lib = None
@@ -162,6 +173,7 @@ def load(path: str | None = None):
     L.bfx_launch_count.argtypes = [vp, P(ct.c_uint64)]
     L.bfx_device_bytes.argtypes = [vp, P(ct.c_uint64)]
     L.bfx_fluid_mass_momentum_noalloc.argtypes = [vp, vp, ct.c_uint32, ct.c_uint32, ct.c_uint32, vp]
+    L.bfx_adjoint.argtypes = [vp, ct.c_uint64, P(AdjointObjective), ct.c_uint32, P(AdjointResult)]
     L.bfx_last_error.argtypes = [vp, ct.c_char_p, ct.c_size_t]
     if path is None:
         _lib = L

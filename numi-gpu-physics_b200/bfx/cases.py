@@ -90,7 +90,8 @@ def plate_mesh(span=64.0, chord=12.0, n_chord=32, n_span=128, chord_offset=-3.0,
 def flapping_plates(nx=512, ny=256, nz=256, span=64.0, chord=12.0, thickness=2.0, n_chord=32, n_span=128,
                     period=4000.0, stroke_deg=60.0, pitch_deg=45.0, viscosity=0.004, magic=3.0 / 16.0,
                     storage=L.STORAGE_F32, collision=L.COLLISION_TRT, link_rule=L.LINK_RAY_ROOT,
-                    wall_rule=L.WALL_INTERPOLATED, sponge_width=16.0, sponge_strength=0.05):
+                    wall_rule=L.WALL_INTERPOLATED, sponge_width=16.0, sponge_strength=0.05, deviation_deg=0.0,
+                    pitch_phase_offset_deg=0.0):
     op, om = _trt_rates(viscosity, magic)
     rows = zero_bird_rows()
     rows[0] = (4.0, 4.0, 4.0, 1.0)
@@ -99,7 +100,8 @@ def flapping_plates(nx=512, ny=256, nz=256, span=64.0, chord=12.0, thickness=2.0
     rows[3] = (0.0, 0.0, 0.0, 0.0)
     freq = 1.0 / period
     rows[5] = (freq, float(f32(math.radians(stroke_deg))), 0.0, 0.0)
-    rows[6] = (float(f32(math.radians(pitch_deg))), float(f32(math.pi / 2.0)), 0.0, 0.0)
+    rows[6] = (float(f32(math.radians(pitch_deg))), float(f32(math.pi / 2.0 + math.radians(pitch_phase_offset_deg))),
+               float(f32(math.radians(deviation_deg))), 0.0)
     rows[8] = (0.0, 0.15, 0.0, 0.0)
     cfg = default_config(nx, ny, nz, omega_plus=op, omega_minus=om, face_bc=[L.BC_FARFIELD] * 6,
                          geometry=L.GEOMETRY_MESH, wall_rule=wall_rule, collision=collision, storage=storage,
@@ -129,3 +131,34 @@ def compact_bird(free_flight=False, storage=L.STORAGE_F32, n=48):
     state = BirdBodyState(position_meters=half,
                           linear_velocity_meters_per_second=(1.0, 0.0, 0.0) if free_flight else (0.0, 0.0, 0.0))
     return config, bird, state
+
+
+# Kinematic parameters the adjoint differentiates, as (row, column) of the bird rows.
+KINEMATIC_PARAMETERS = (("stroke amplitude", 5, 1), ("pitch amplitude", 6, 0), ("pitch phase", 6, 1),
+                        ("deviation amplitude", 6, 2))
+
+
+def kinematic_parameters(rows) -> tuple:
+    """theta = (stroke amplitude, pitch amplitude, pitch phase, deviation amplitude) of bird rows."""
+    return tuple(float(rows[r][c]) for _, r, c in KINEMATIC_PARAMETERS)
+
+
+def with_kinematic_parameters(rows, theta):
+    """Copy of the bird rows with theta written into the kinematic slots."""
+    out = [tuple(r) for r in rows]
+    for (name, r, c), v in zip(KINEMATIC_PARAMETERS, theta):
+        row = list(out[r])
+        row[c] = float(f32(v))
+        out[r] = tuple(row)
+    return out
+
+
+def adjoint_plates(nx=96, ny=64, nz=64, span=20.0, chord=6.0, thickness=2.0, period=600.0, stroke_deg=60.0,
+                   pitch_deg=45.0, deviation_deg=5.0, viscosity=0.02, storage=L.STORAGE_F32,
+                   link_rule=L.LINK_LINEAR, n_chord=8, n_span=24):
+    """Flapping plate pair for the adjoint: TRT, prescribed stroke / pitch /
+    deviation, far-field faces."""
+    return flapping_plates(nx=nx, ny=ny, nz=nz, span=span, chord=chord, thickness=thickness, n_chord=n_chord,
+                           n_span=n_span, period=period, stroke_deg=stroke_deg, pitch_deg=pitch_deg,
+                           viscosity=viscosity, storage=storage, link_rule=link_rule, sponge_width=6.0,
+                           deviation_deg=deviation_deg)

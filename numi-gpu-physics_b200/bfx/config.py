@@ -117,6 +117,8 @@ class WingKinematics:
     pitch_mean_radians: float = 0.0
     pitch_amplitude_radians: float = 0.0
     pitch_phase_radians: float = 0.0
+    # bfx extension: deviation about the stroke-plane normal, amplitude * sin(2 * phase)
+    deviation_amplitude_radians: float = 0.0
 
 
 @dataclass
@@ -202,7 +204,7 @@ class BirdParameters:
             (self.wing_sweep_meters, *self.wing_root_offset_meters),
             (self.tail_length_meters, self.tail_half_width_meters, self.tail_thickness_meters, 0.0),
             (k.frequency_hz, k.stroke_amplitude_radians, k.stroke_bias_radians, k.pitch_mean_radians),
-            (k.pitch_amplitude_radians, k.pitch_phase_radians, 0.0, 0.0),
+            (k.pitch_amplitude_radians, k.pitch_phase_radians, k.deviation_amplitude_radians, 0.0),
             (*ext, self.conservative_bounding_radius()),
             (self.maximum_prescribed_wing_speed(), 0.15, 0.0, 0.0),
         ]

@@ -231,6 +231,24 @@ class Lattice:
         buf = ct.create_string_buffer(data, len(data))
         _check(self.lib.bfx_restore_state(self.handle, buf, len(data)), self.handle)
 
+    def adjoint(self, steps: int, force_weight=(0.0, 0.0, 0.0), power_weight: float = 0.0, window=None,
+                checkpoint_interval: int = 0) -> L.AdjointResult:
+        """Advances `steps` steps and runs the discrete adjoint backward
+        (bfx_adjoint).  The result holds J (the window mean of
+        force_weight . F + power_weight * P) and dJ/dtheta for
+        theta = (stroke amplitude, pitch amplitude, pitch phase, deviation
+        amplitude)."""
+        obj = L.AdjointObjective()
+        for k in range(3):
+            obj.force_weight[k] = float(force_weight[k])
+        obj.power_weight = float(power_weight)
+        if window is not None:
+            obj.window_first, obj.window_last = int(window[0]), int(window[1])
+        res = L.AdjointResult()
+        _check(self.lib.bfx_adjoint(self.handle, int(steps), ct.byref(obj), int(checkpoint_interval), ct.byref(res)),
+               self.handle)
+        return res
+
     def set_kernel_timing(self, enabled: bool):
         _check(self.lib.bfx_set_kernel_timing(self.handle, int(enabled)), self.handle)
 

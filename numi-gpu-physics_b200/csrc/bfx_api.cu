@@ -63,6 +63,7 @@ struct bfx_sim {
     float* density = nullptr;
     float4* velocity = nullptr;
     DeviceState* dstate = nullptr;
+    Objective* dobjective = nullptr;
     bfx_bird* dbird = nullptr;
     // mesh
     float* mesh_local = nullptr;
@@ -159,6 +160,7 @@ FluidBuffers fluid_buffers(bfx_sim* s, uint8_t* mask) {
     b.density = s->density;
     b.velocity = s->velocity;
     b.state = s->dstate;
+    b.tape = nullptr;
     return b;
 }
 
@@ -189,8 +191,24 @@ GeomBuffers geom_buffers(bfx_sim* s, uint8_t* mprev, uint8_t* mnext) {
     b.link_partials = s->link_partials;
     b.apply_blocks = s->apply_blocks;
     b.state = s->dstate;
+    b.objective = s->dobjective;
+    b.link_tape = nullptr;
+    b.link_tangent = nullptr;
+    b.frames = nullptr;
     return b;
 }
+
+// Device pointers of one taped step (discrete adjoint recomputation).
+struct TapeSlot {
+    void* moments;
+    uint8_t* mask_next;
+    uint8_t* mask_prev;
+    unsigned long long* keys;
+    DeviceState* state;
+    FrameTangent* frames;
+    void* links;
+    float* link_tangent;    // per-link tangent scratch shared by all slots
+};
 
 // Classification + link build for the geometry at the current state.
 void encode_geometry_build(bfx_sim* s, int init, uint8_t* mprev, uint8_t* mnext) {
@@ -235,23 +253,50 @@ void timing_collect(bfx_sim* s) {
 }
 
 // One time step (BirdFlowSimulation.encodeBatch body, BirdFlowSimulation.swift:1374-1437).
-void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint64_t sample_index) {
+// With a tape slot the step also records what its adjoint needs: the wing-frame
+// and link tangents, the link values, masks, keys, state and pre-collision moments.
+void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint64_t sample_index,
+                 const TapeSlot* tape = nullptr) {
     uint8_t* mprev = s->mask[s->cur];
     uint8_t* mnext = s->moving() ? s->mask[s->cur ^ 1] : s->mask[s->cur];
     if (s->moving()) {
         encode_geometry_build(s, 0, mprev, mnext);
     }
+    if (tape) {
+        launch_frame_tangent(geom_buffers(s, mprev, mnext), s->cfg.time_step, tape->frames, s->stream);
+        s->launches += 1;
+    }
     FluidBuffers fb = fluid_buffers(s, s->geometry() ? mnext : nullptr);
     if (s->geometry() && s->moving()) encode_links(s, mprev, mnext);
+    if (tape) {
+        GeomBuffers gb = geom_buffers(s, mprev, mnext);
+        gb.frames = tape->frames;
+        launch_link_tangent(s->cfg.link_rule, s->fp.interpolated, s->g, s->fp, s->box, gb, tape->link_tangent,
+                            s->stream);
+        s->launches += 1;
+    }
     // halo fill before the link writes: a link whose solid source is a periodic
     // image writes into a halo slot and must win over the periodic copy
     launch_halo(s->cfg.storage, s->rep_s, s->g, s->fp, fb, s->stream);
     s->launches += 1;
     if (s->geometry()) {
         GeomBuffers gb = geom_buffers(s, mprev, mnext);
+        if (tape) {
+            gb.link_tape = tape->links;
+            gb.link_tangent = tape->link_tangent;
+        }
         launch_links_apply(s->cfg.storage, s->rep_s, s->g, s->fp, gb, fb, s->stream);
         launch_reduce_loads(gb, s->moving() ? 1 : 0, s->stream);
         s->launches += 2;
+    }
+    if (tape) {
+        cudaMemcpyAsync(tape->state, s->dstate, sizeof(DeviceState), cudaMemcpyDeviceToDevice, s->stream);
+        cudaMemcpyAsync(tape->mask_next, mnext, (size_t)s->g.n, cudaMemcpyDeviceToDevice, s->stream);
+        cudaMemcpyAsync(tape->mask_prev, mprev, (size_t)s->g.n, cudaMemcpyDeviceToDevice, s->stream);
+        cudaMemcpyAsync(tape->keys, s->keys, (size_t)s->box.cells * sizeof(unsigned long long),
+                        cudaMemcpyDeviceToDevice, s->stream);
+        fb.tape = tape->moments;
+        capture = 2;
     }
     const int box[3] = {s->box.sx, s->box.sy, s->box.sz};
     timing_begin(s);
@@ -346,6 +391,8 @@ int validate_config(const bfx_config* c, const bfx_bird* bird, const bfx_mesh* m
     if (c->geometry == BFX_GEOMETRY_MESH && !(c->mesh_half_thickness > 0.0f))
         return fail(nullptr, BFX_ERR_INVALID_CONFIG, "mesh half thickness must be positive");
     if (c->free_flight && bird == nullptr) return fail(nullptr, BFX_ERR_INVALID_CONFIG, "free flight needs bird parameters");
+    if (bird && bird->wing_kinematics1.v[3] > 0.5f)
+        return fail(nullptr, BFX_ERR_INVALID_CONFIG, "measured keyframe kinematics are not supported");
     if (c->free_flight && c->static_geometry)
         return fail(nullptr, BFX_ERR_INVALID_CONFIG, "a free-flying body cannot be static geometry");
     if (mesh && mesh->triangles) {
@@ -500,6 +547,7 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
     BFX_ALLOC(s->density, (size_t)g.n * sizeof(float));
     BFX_ALLOC(s->velocity, (size_t)g.n * sizeof(float4));
     BFX_ALLOC(s->dstate, sizeof(DeviceState));
+    BFX_ALLOC(s->dobjective, sizeof(Objective));
     s->mm_blocks = 4 * s->sm_count;
     BFX_ALLOC(s->mm_partials, (size_t)s->mm_blocks * 4 * sizeof(double));
     BFX_ALLOC(s->mm_result, 4 * sizeof(double));
@@ -1045,6 +1093,256 @@ int bfx_launch_count(bfx_sim* s, uint64_t* launches) {
 int bfx_device_bytes(bfx_sim* s, uint64_t* bytes) {
     if (!s || !bytes) return BFX_ERR_INVALID_ARGUMENT;
     *bytes = s->device_bytes;
+    return BFX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Discrete adjoint driver (kernels in bfx_adjoint.cu).
+//
+// Pass 1 runs the steps forward with the load objective enabled and keeps a
+// snapshot (populations, current mask, device state) at the start of every
+// checkpoint interval plus one of the final state.  The reverse pass walks the
+// intervals backward: it restores the interval's snapshot, recomputes the
+// interval once while recording a tape per step (moments, masks, keys, state,
+// frame and link tangents, link values), then runs the adjoint steps of the
+// interval in reverse.  Every step is recomputed exactly once; memory is
+// (steps / interval) snapshots plus interval tapes.
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+namespace {
+
+struct AdjointAllocs {
+    std::vector<void*> ptrs;
+    uint64_t bytes = 0;
+    ~AdjointAllocs() {
+        for (void* p : ptrs) cudaFree(p);
+    }
+    template <class T>
+    cudaError_t get(T** p, size_t n) {
+        if (n == 0) n = 16;
+        cudaError_t e = cudaMalloc((void**)p, n);
+        if (e == cudaSuccess) {
+            ptrs.push_back((void*)*p);
+            bytes += n;
+        }
+        return e;
+    }
+};
+
+int adjoint_scope(bfx_sim* s) {
+    const bfx_config& c = s->cfg;
+    if (c.geometry != BFX_GEOMETRY_MESH || c.static_geometry)
+        return fail(s, BFX_ERR_UNSUPPORTED, "the adjoint needs moving mesh geometry");
+    if (c.free_flight) return fail(s, BFX_ERR_UNSUPPORTED, "the adjoint needs prescribed motion (no free flight)");
+    if (c.collision != BFX_COLLISION_TRT) return fail(s, BFX_ERR_UNSUPPORTED, "the adjoint supports the TRT collision");
+    if (c.storage != BFX_STORAGE_F32 && c.storage != BFX_STORAGE_F64)
+        return fail(s, BFX_ERR_UNSUPPORTED, "the adjoint supports F32 and F64 storage");
+    if (c.fast_math) return fail(s, BFX_ERR_UNSUPPORTED, "the adjoint differentiates the non-contracted step");
+    for (int f = 0; f < 6; ++f)
+        if (c.face_bc[f] == BFX_BC_OUTFLOW)
+            return fail(s, BFX_ERR_UNSUPPORTED, "the adjoint does not support zero-gradient outflow faces");
+    if (c.force_estimator != 6 || c.load_component != 0 || c.selected_part != 0 || !c.accumulate_loads ||
+        c.moving_wall_local_density)
+        return fail(s, BFX_ERR_UNSUPPORTED,
+                    "the adjoint needs estimator 6, all parts, both load components and the far-field wall density");
+    return BFX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bfx_adjoint(bfx_sim* s, uint64_t steps, const bfx_adjoint_objective* objective, uint32_t checkpoint_interval,
+                bfx_adjoint_result* result) {
+    BFX_GUARD(s);
+    if (!objective || steps == 0) return fail(s, BFX_ERR_INVALID_ARGUMENT, "objective and a positive step count are required");
+    int rc = adjoint_scope(s);
+    if (rc != BFX_OK) return rc;
+    uint64_t first = objective->window_first, last = objective->window_last;
+    if (first == 0 && last == 0) {
+        first = 1;
+        last = steps;
+    }
+    if (first < 1 || last < first || last > steps)
+        return fail(s, BFX_ERR_INVALID_ARGUMENT, "objective window must satisfy 1 <= first <= last <= steps");
+    uint64_t K = checkpoint_interval ? checkpoint_interval : (uint64_t)std::ceil(std::sqrt((double)steps));
+    K = std::max<uint64_t>(1, std::min<uint64_t>(K, steps));
+    const uint64_t nseg = (steps + K - 1) / K;
+    rc = sync_check(s, "adjoint start");
+    if (rc != BFX_OK) return rc;
+
+    const size_t pop_bytes = (size_t)19 * (size_t)s->g.padded * s->elem;
+    const size_t n = (size_t)s->g.n;
+    AdjointAllocs mem;
+#define BFX_ADJ_ALLOC(ptr, bytes)                                                   \
+    do {                                                                            \
+        cudaError_t ee = mem.get(&(ptr), (bytes));                                  \
+        if (ee != cudaSuccess) return fail(s, BFX_ERR_ALLOCATION, "adjoint work memory allocation failed"); \
+    } while (0)
+    // snapshots: nseg interval starts + the final state
+    char* snap_pops = nullptr;
+    uint8_t* snap_mask = nullptr;
+    DeviceState* snap_state = nullptr;
+    BFX_ADJ_ALLOC(snap_pops, (nseg + 1) * pop_bytes);
+    BFX_ADJ_ALLOC(snap_mask, (nseg + 1) * n);
+    BFX_ADJ_ALLOC(snap_state, (nseg + 1) * sizeof(DeviceState));
+    std::vector<int> snap_rep(nseg + 1), snap_cur(nseg + 1);
+    auto snapshot = [&](uint64_t i) {
+        cudaMemcpyAsync(snap_pops + i * pop_bytes, s->pops, pop_bytes, cudaMemcpyDeviceToDevice, s->stream);
+        cudaMemcpyAsync(snap_mask + i * n, s->mask[s->cur], n, cudaMemcpyDeviceToDevice, s->stream);
+        cudaMemcpyAsync(snap_state + i, s->dstate, sizeof(DeviceState), cudaMemcpyDeviceToDevice, s->stream);
+        snap_rep[i] = s->rep_s;
+        snap_cur[i] = s->cur;
+    };
+    auto restore = [&](uint64_t i) {
+        cudaMemcpyAsync(s->pops, snap_pops + i * pop_bytes, pop_bytes, cudaMemcpyDeviceToDevice, s->stream);
+        cudaMemcpyAsync(s->mask[snap_cur[i]], snap_mask + i * n, n, cudaMemcpyDeviceToDevice, s->stream);
+        cudaMemcpyAsync(s->dstate, snap_state + i, sizeof(DeviceState), cudaMemcpyDeviceToDevice, s->stream);
+        s->rep_s = snap_rep[i];
+        s->cur = snap_cur[i];
+    };
+
+    // objective on, accumulators cleared
+    Objective ob;
+    std::memset(&ob, 0, sizeof(ob));
+    ob.enabled = 1;
+    ob.start = s->step;
+    ob.first = first;
+    ob.last = last;
+    for (int k = 0; k < 3; ++k) ob.force_weight[k] = objective->force_weight[k];
+    ob.power_weight = objective->power_weight;
+    cudaMemcpyAsync(s->dobjective, &ob, sizeof(ob), cudaMemcpyHostToDevice, s->stream);
+
+    cudaEvent_t ev[3];
+    for (auto& e : ev) cudaEventCreate(&e);
+    cudaEventRecord(ev[0], s->stream);
+    // pass 1: forward with snapshots
+    for (uint64_t seg = 0; seg < nseg; ++seg) {
+        snapshot(seg);
+        const uint64_t len = std::min<uint64_t>(K, steps - seg * K);
+        uint64_t k = 0;
+        if (s->graphs_enabled && !s->timing)
+            for (; k + 1 < len; k += 2) {
+                rc = run_pair_graph(s);
+                if (rc != BFX_OK) return rc;
+            }
+        for (; k < len; ++k) encode_step(s, 0, nullptr, 0);
+    }
+    snapshot(nseg);
+    cudaEventRecord(ev[1], s->stream);
+    rc = sync_check(s, "adjoint forward pass");
+    if (rc != BFX_OK) return rc;
+    DeviceState st_end;
+    cudaMemcpy(&st_end, s->dstate, sizeof(st_end), cudaMemcpyDeviceToHost);
+    cudaMemcpy(&ob, s->dobjective, sizeof(ob), cudaMemcpyDeviceToHost);
+    if (st_end.link_overflow) return fail(s, BFX_ERR_KERNEL, "the cut-link list exceeded its capacity; raise link_capacity");
+    const uint64_t link_slots = (uint64_t)std::max<int64_t>(1, std::min<int64_t>(ob.max_links, s->link_capacity));
+
+    // tape of one interval and the adjoint work arrays
+    const size_t R = s->elem;
+    const size_t link_rec = R == 8 ? sizeof(LinkTape<double>) : sizeof(LinkTape<float>);
+    char* t_moments = nullptr;
+    uint8_t *t_mnext = nullptr, *t_mprev = nullptr;
+    unsigned long long* t_keys = nullptr;
+    DeviceState* t_state = nullptr;
+    FrameTangent* t_frames = nullptr;
+    char* t_links = nullptr;
+    float* link_tangent = nullptr;
+    void* lam = nullptr;
+    void* nu = nullptr;
+    double *p_rare = nullptr, *p_links = nullptr;
+    BFX_ADJ_ALLOC(t_moments, K * n * 4 * R);
+    BFX_ADJ_ALLOC(t_mnext, K * n);
+    BFX_ADJ_ALLOC(t_mprev, K * n);
+    BFX_ADJ_ALLOC(t_keys, K * (size_t)s->box.cells * sizeof(unsigned long long));
+    BFX_ADJ_ALLOC(t_state, K * sizeof(DeviceState));
+    BFX_ADJ_ALLOC(t_frames, K * sizeof(FrameTangent));
+    BFX_ADJ_ALLOC(t_links, K * link_slots * link_rec);
+    BFX_ADJ_ALLOC(link_tangent, (size_t)s->link_capacity * kLinkTangentWords * sizeof(float));
+    BFX_ADJ_ALLOC(lam, pop_bytes);
+    BFX_ADJ_ALLOC(nu, (size_t)s->link_capacity * R);
+    BFX_ADJ_ALLOC(p_rare, (size_t)s->box_blocks * 4 * sizeof(double));
+    BFX_ADJ_ALLOC(p_links, (size_t)s->apply_blocks * 4 * sizeof(double));
+#undef BFX_ADJ_ALLOC
+    cudaMemsetAsync(lam, 0, pop_bytes, s->stream);
+    const int32_t off = 0;
+    cudaMemcpyAsync(&s->dobjective->enabled, &off, sizeof(off), cudaMemcpyHostToDevice, s->stream);
+    auto slot = [&](uint64_t j) {
+        TapeSlot t;
+        t.moments = t_moments + j * n * 4 * R;
+        t.mask_next = t_mnext + j * n;
+        t.mask_prev = t_mprev + j * n;
+        t.keys = t_keys + j * (size_t)s->box.cells;
+        t.state = t_state + j;
+        t.frames = t_frames + j;
+        t.links = t_links + j * link_slots * link_rec;
+        t.link_tangent = link_tangent;
+        return t;
+    };
+    AdjointWork w;
+    w.lam = lam;
+    w.nu = nu;
+    w.partials_rare = p_rare;
+    w.partials_links = p_links;
+    w.objective = s->dobjective;
+    const uint32_t saved_capacity = s->link_capacity;
+    std::vector<int> reps(K);
+    const double inv_window = 1.0 / (double)(last - first + 1);
+    for (uint64_t seg = nseg; seg-- > 0;) {
+        restore(seg);
+        const uint64_t len = std::min<uint64_t>(K, steps - seg * K);
+        // the tape holds link_slots links per step: cap the link list there (the
+        // recomputation reproduces the forward pass, whose largest count it is)
+        s->link_capacity = (uint32_t)link_slots;
+        for (uint64_t j = 0; j < len; ++j) {
+            reps[j] = s->rep_s;
+            TapeSlot t = slot(j);
+            encode_step(s, 0, nullptr, 0, &t);
+        }
+        s->link_capacity = saved_capacity;
+        for (uint64_t j = len; j-- > 0;) {
+            const uint64_t rel = seg * K + j + 1;
+            const double weight = rel >= first && rel <= last ? inv_window : 0.0;
+            TapeSlot t = slot(j);
+            StepTape tape;
+            tape.moments = t.moments;
+            tape.mask_next = t.mask_next;
+            tape.mask_prev = t.mask_prev;
+            tape.keys = t.keys;
+            tape.state = t.state;
+            tape.frames = t.frames;
+            tape.links = t.links;
+            GeomBuffers gb = geom_buffers(s, s->mask[0], s->mask[1]);
+            gb.link_capacity = (uint32_t)link_slots;  // the tape slot's size
+            launch_adjoint_step(s->cfg.storage, reps[j], s->g, s->fp, s->box, gb, tape, w, weight, s->stream);
+            s->launches += 9;
+        }
+        cudaError_t le = cudaGetLastError();
+        if (le != cudaSuccess) return cuda_fail(s, le, "adjoint launch");
+    }
+    cudaEventRecord(ev[2], s->stream);
+    restore(nseg);
+    rc = sync_check(s, "adjoint reverse pass");
+    if (rc != BFX_OK) return rc;
+    cudaMemcpy(&ob, s->dobjective, sizeof(ob), cudaMemcpyDeviceToHost);
+    s->step = st_end.step;
+    float f_ms = 0.0f, r_ms = 0.0f;
+    cudaEventElapsedTime(&f_ms, ev[0], ev[1]);
+    cudaEventElapsedTime(&r_ms, ev[1], ev[2]);
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (result) {
+        std::memset(result, 0, sizeof(*result));
+        result->objective = ob.value;
+        for (int k = 0; k < 4; ++k) result->gradient[k] = ob.grad[k];
+        result->steps = steps;
+        result->checkpoint_interval = (uint32_t)K;
+        result->snapshots = (uint32_t)(nseg + 1);
+        result->forward_ms = f_ms;
+        result->reverse_ms = r_ms;
+        result->max_links = (uint64_t)ob.max_links;
+        result->work_bytes = mem.bytes;
+    }
     return BFX_OK;
 }
 

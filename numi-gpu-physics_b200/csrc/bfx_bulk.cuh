@@ -26,9 +26,10 @@ struct BulkArgs {
     float* density;
     float4* velocity;
     DeviceState* state;
+    void* tape;             // pre-collision (rho, u) per cell (capture == 2)
     Grid g;
     FluidParams fp;
-    int capture;
+    int capture;            // 0 none, 1 macroscopic fields, 2 adjoint tape
 };
 
 // Fused-step launch for the contracted variant (bfx_fluid_fast.cu).

@@ -297,10 +297,18 @@ __global__ void __launch_bounds__(256, sizeof(typename S::R) == 8 ? 1 : (COLL ==
     load_cell<S, REP_S>(a, pid, f);
     R rho, ux, uy, uz;
     moments<R>(f, rho, ux, uy, uz);
+    if (CAPTURE == 2) {
+        // adjoint tape: the collision Jacobian depends on the pre-collision moments only
+        R* t = (R*)a.tape + 4 * (size_t)gid;
+        t[0] = rho;
+        t[1] = ux;
+        t[2] = uy;
+        t[3] = uz;
+    }
     R post[19];
     float activation = 0.0f, restriction = 0.0f;
     collide<R, COLL>(f, rho, ux, uy, uz, (R)a.fp.omega_p, (R)a.fp.omega_m, post, activation, restriction);
-    finish_cell<S, COLL>(a, gid, x, y, z, CAPTURE != 0, post, activation, restriction);
+    finish_cell<S, COLL>(a, gid, x, y, z, CAPTURE == 1, post, activation, restriction);
     store_cell<S, REP_S>(a, pid, post);
 }
 
@@ -333,7 +341,7 @@ __global__ void __launch_bounds__(128) k_bulk_rare(const BulkArgs a) {
 #pragma unroll
         for (int q = 0; q < 19; ++q) post[q] = feqq<R>(q, R(1), ux, uy, uz, u2);
         store_cell<S, REP_S>(a, pid, post);
-        if (a.capture) {
+        if (a.capture == 1) {
             a.density[gid] = 1.0f;
             a.velocity[gid] = make_float4(w.x, w.y, w.z, 0.0f);
         }
@@ -346,7 +354,7 @@ __global__ void __launch_bounds__(128) k_bulk_rare(const BulkArgs a) {
     moments<R>(f, rho, vx, vy, vz);
     float activation = 0.0f, restriction = 0.0f;
     collide<R, COLL>(f, rho, vx, vy, vz, (R)a.fp.omega_p, (R)a.fp.omega_m, post, activation, restriction);
-    finish_cell<S, COLL>(a, gid, x, y, z, a.capture != 0, post, activation, restriction);
+    finish_cell<S, COLL>(a, gid, x, y, z, a.capture == 1, post, activation, restriction);
     store_cell<S, REP_S>(a, pid, post);
 }
 
@@ -355,7 +363,10 @@ static void bulk_t(const BulkArgs& a, const GridDesc& g, int part, cudaStream_t 
     if (part == 0) {
         dim3 grid, block;
         cell_launch_shape(g, grid, block);
-        if (a.capture) k_bulk<S, REP, COLL, 1><<<grid, block, 0, s>>>(a);
+        if (a.capture == 1) k_bulk<S, REP, COLL, 1><<<grid, block, 0, s>>>(a);
+#ifndef BFX_CONTRACTED
+        else if (a.capture == 2 && COLL == BFX_COLLISION_TRT) k_bulk<S, REP, BFX_COLLISION_TRT, 2><<<grid, block, 0, s>>>(a);
+#endif
         else k_bulk<S, REP, COLL, 0><<<grid, block, 0, s>>>(a);
     } else if (a.mask && a.box_cells > 0) {
         k_bulk_rare<S, REP, COLL><<<(unsigned)((a.box_cells + 127) / 128), 128, 0, s>>>(a);

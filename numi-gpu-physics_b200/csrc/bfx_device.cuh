@@ -242,6 +242,38 @@ __device__ __forceinline__ typename S::T* incoming_slot(typename S::T* A, const 
     return A + (int64_t)opp(q) * g.pn + pflat(g, x - cx(q), y - cy(q), z - cz(q));
 }
 
+// Cell t of the halo shell of the padded array (the -z / +z planes, then the
+// -y / +y rows, then the -x / +x columns), in padded coordinates.
+__device__ __forceinline__ bool padded_shell_cell(const Grid& g, int64_t t, int& x, int& y, int& z) {
+    const int64_t fz = (int64_t)g.px * g.py;
+    if (t < 2 * fz) {
+        z = t < fz ? 0 : g.pz - 1;
+        const int64_t r = t < fz ? t : t - fz;
+        y = (int)(r / g.px);
+        x = (int)(r - (int64_t)y * g.px);
+        return true;
+    }
+    t -= 2 * fz;
+    const int64_t fy = (int64_t)g.px * (g.pz - 2);
+    if (t < 2 * fy) {
+        y = t < fy ? 0 : g.py - 1;
+        const int64_t r = t < fy ? t : t - fy;
+        z = 1 + (int)(r / g.px);
+        x = (int)(r - (int64_t)(z - 1) * g.px);
+        return true;
+    }
+    t -= 2 * fy;
+    const int64_t fx = (int64_t)(g.py - 2) * (g.pz - 2);
+    if (t < 2 * fx) {
+        x = t < fx ? 0 : g.px - 1;
+        const int64_t r = t < fx ? t : t - fx;
+        z = 1 + (int)(r / (g.py - 2));
+        y = 1 + (int)(r - (int64_t)(z - 1) * (g.py - 2));
+        return true;
+    }
+    return false;
+}
+
 // Mask byte: bits 0-5 part id (0 = fluid), bit 6 newly uncovered, bit 7 newly covered.
 constexpr uint8_t kPartMask = 0x3F;
 constexpr uint8_t kUncovered = 0x40;

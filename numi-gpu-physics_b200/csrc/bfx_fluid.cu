@@ -30,35 +30,6 @@ namespace bfx {
 // The reference has only the far-field rule and an all-axes periodic flag
 // (BF.metal:2696-2725).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ bool padded_shell_cell(const Grid& g, int64_t t, int& x, int& y, int& z) {
-    const int64_t fz = (int64_t)g.px * g.py;
-    if (t < 2 * fz) {
-        z = t < fz ? 0 : g.pz - 1;
-        const int64_t r = t < fz ? t : t - fz;
-        y = (int)(r / g.px);
-        x = (int)(r - (int64_t)y * g.px);
-        return true;
-    }
-    t -= 2 * fz;
-    const int64_t fy = (int64_t)g.px * (g.pz - 2);
-    if (t < 2 * fy) {
-        y = t < fy ? 0 : g.py - 1;
-        const int64_t r = t < fy ? t : t - fy;
-        z = 1 + (int)(r / g.px);
-        x = (int)(r - (int64_t)(z - 1) * g.px);
-        return true;
-    }
-    t -= 2 * fy;
-    const int64_t fx = (int64_t)(g.py - 2) * (g.pz - 2);
-    if (t < 2 * fx) {
-        x = t < fx ? 0 : g.px - 1;
-        const int64_t r = t < fx ? t : t - fx;
-        z = 1 + (int)(r / (g.py - 2));
-        y = 1 + (int)(r - (int64_t)(z - 1) * (g.py - 2));
-        return true;
-    }
-    return false;
-}
 
 template <class S>
 __global__ void __launch_bounds__(128) k_halo(const BulkArgs a, int rep_s, int64_t halo_cells) {
@@ -297,6 +268,7 @@ BulkArgs make_bulk_args(const GridDesc& gd, const FluidParams& fp, const FluidBu
     a.density = b.density;
     a.velocity = b.velocity;
     a.state = b.state;
+    a.tape = b.tape;
     a.fp = fp;
     a.capture = capture;
     return a;

@@ -9,75 +9,10 @@
 // fixed at creation from the conservative body radius plus a 4-cell margin,
 // its origin is recomputed on the device every step), so a step costs
 // O(box) here and O(lattice) only in the fused fluid kernel.
-#include "bfx_device.cuh"
-#include "bfx_internal.h"
+#include "bfx_geom_common.cuh"
 
 namespace bfx {
 
-struct GeomArgs {
-    Grid g;
-    FluidParams fp;
-    int bx, by, bz;          // box extent
-    int64_t box_cells;
-    GeomBuffers b;
-    void* pops;
-};
-
-// ---------------------------------------------------------------------------
-// float3 helpers with the reference's operation order.
-// ---------------------------------------------------------------------------
-struct V3 {
-    float x, y, z;
-};
-__device__ __forceinline__ V3 v3(float x, float y, float z) { return V3{x, y, z}; }
-__device__ __forceinline__ V3 v3(const float4& a) { return V3{a.x, a.y, a.z}; }
-__device__ __forceinline__ V3 operator+(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
-__device__ __forceinline__ V3 operator-(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
-__device__ __forceinline__ V3 operator*(V3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
-__device__ __forceinline__ float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-__device__ __forceinline__ V3 cross(V3 a, V3 b) {
-    return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
-}
-__device__ __forceinline__ float length(V3 a) { return sqrtf(dot(a, a)); }
-__device__ __forceinline__ float mixf(float a, float b, float t) { return a + (b - a) * t; }
-__device__ __forceinline__ float clampf(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); }
-__device__ __forceinline__ float4 f4(V3 a, float w) { return make_float4(a.x, a.y, a.z, w); }
-
-__device__ __forceinline__ V3 cell_world(const FluidParams& fp, int x, int y, int z) {
-    return v3(fp.origin[0] + ((float)x + 0.5f) * fp.dx, fp.origin[1] + ((float)y + 0.5f) * fp.dx,
-              fp.origin[2] + ((float)z + 0.5f) * fp.dx);
-}
-
-// Quaternions (x, y, z, w).  Normalisation divides by the correctly rounded
-// norm so host and device agree bit for bit.
-__device__ __forceinline__ float4 qnormalize(float4 q) {
-    float n2 = q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w;
-    if (n2 > 1.0e-20f) {
-        float n = sqrtf(n2);
-        return make_float4(q.x / n, q.y / n, q.z / n, q.w / n);
-    }
-    return make_float4(0.0f, 0.0f, 0.0f, 1.0f);
-}
-__device__ __forceinline__ V3 qrotate(float4 q, V3 v) {
-    V3 qv = v3(q.x, q.y, q.z);
-    V3 t = cross(qv, v);
-    t = v3(t.x * 2.0f, t.y * 2.0f, t.z * 2.0f);
-    V3 c2 = cross(qv, t);
-    return v3(v.x + q.w * t.x + c2.x, v.y + q.w * t.y + c2.y, v.z + q.w * t.z + c2.z);
-}
-__device__ __forceinline__ V3 qunrotate(float4 q, V3 v) { return qrotate(make_float4(-q.x, -q.y, -q.z, q.w), v); }
-// rotateAroundAxis: BF.metal:466-473
-__device__ __forceinline__ V3 rotate_axis(V3 v, V3 axis, float angle) {
-    float s = bfx_sinf(angle), c = bfx_cosf(angle);
-    V3 cr = cross(axis, v);
-    float d = dot(axis, v);
-    return v3(v.x * c + cr.x * s + axis.x * d * (1.0f - c), v.y * c + cr.y * s + axis.y * d * (1.0f - c),
-              v.z * c + cr.z * s + axis.z * d * (1.0f - c));
-}
-__device__ __forceinline__ V3 normalize3(V3 v) {
-    float l = length(v);
-    return v3(v.x / l, v.y / l, v.z / l);
-}
 
 struct WingFrame {
     V3 root, chord, span, normal, rel;
@@ -85,8 +20,9 @@ struct WingFrame {
 };
 
 // makeWingFrame: BF.metal:611-684
-__device__ void make_wing_frame(float side, float stroke, float stroke_rate, float pitch, float pitch_rate,
-                                const bfx_bird& bird, V3 pos, float4 orient, WingFrame& fr) {
+__device__ void make_wing_frame(float side, float stroke, float stroke_rate, float deviation, float deviation_rate,
+                                float pitch, float pitch_rate, const bfx_bird& bird, V3 pos, float4 orient,
+                                WingFrame& fr) {
     float4 o = qnormalize(orient);
     V3 bx = qrotate(o, v3(1, 0, 0)), by = qrotate(o, v3(0, 1, 0)), bz = qrotate(o, v3(0, 0, 1));
     V3 root_local = v3(bird.wing_geometry1.v[1], side * bird.wing_geometry1.v[2], bird.wing_geometry1.v[3]);
@@ -95,8 +31,8 @@ __device__ void make_wing_frame(float side, float stroke, float stroke_rate, flo
     float signed_stroke = side * stroke;
     V3 span_after = rotate_axis(v3(side * by.x, side * by.y, side * by.z), bx, signed_stroke);
     V3 normal_after = rotate_axis(v3(side * bz.x, side * bz.y, side * bz.z), bx, signed_stroke);
-    V3 span = rotate_axis(span_after, normal_after, 0.0f);
-    V3 chord_before = rotate_axis(bx, normal_after, 0.0f);
+    V3 span = rotate_axis(span_after, normal_after, deviation);
+    V3 chord_before = rotate_axis(bx, normal_after, deviation);
     float signed_pitch = side * pitch;
     V3 chord = rotate_axis(chord_before, span, signed_pitch);
     V3 normal = rotate_axis(normal_after, span, signed_pitch);
@@ -105,8 +41,9 @@ __device__ void make_wing_frame(float side, float stroke, float stroke_rate, flo
     fr.span = normalize3(span);
     fr.normal = normalize3(normal);
     float sr = side * stroke_rate, pr = side * pitch_rate;
-    fr.rel = v3(bx.x * sr + normal_after.x * 0.0f + fr.span.x * pr, bx.y * sr + normal_after.y * 0.0f + fr.span.y * pr,
-                bx.z * sr + normal_after.z * 0.0f + fr.span.z * pr);
+    fr.rel = v3(bx.x * sr + normal_after.x * deviation_rate + fr.span.x * pr,
+                bx.y * sr + normal_after.y * deviation_rate + fr.span.y * pr,
+                bx.z * sr + normal_after.z * deviation_rate + fr.span.z * pr);
     fr.tip_twist = side * 0.0f;
     fr.tip_rate = side * 0.0f;
 }
@@ -144,9 +81,13 @@ __global__ void k_prepare(const GeomArgs a, int init, float dt, float box_radius
     float stroke_rate = af * bird.wing_kinematics0.v[1] * bfx_cosf(phase);
     float pitch = bird.wing_kinematics0.v[3] + bird.wing_kinematics1.v[0] * bfx_sinf(phase + bird.wing_kinematics1.v[1]);
     float pitch_rate = af * bird.wing_kinematics1.v[0] * bfx_cosf(phase + bird.wing_kinematics1.v[1]);
+    // stroke-plane deviation at twice the flapping frequency (figure-of-eight
+    // tip path); the reference feeds deviation only from measured keyframes
+    float deviation = bird.wing_kinematics1.v[2] * bfx_sinf(2.0f * phase);
+    float deviation_rate = 2.0f * af * bird.wing_kinematics1.v[2] * bfx_cosf(2.0f * phase);
     WingFrame l, r;
-    make_wing_frame(1.0f, stroke, stroke_rate, pitch, pitch_rate, bird, pos, orient, l);
-    make_wing_frame(-1.0f, stroke, stroke_rate, pitch, pitch_rate, bird, pos, orient, r);
+    make_wing_frame(1.0f, stroke, stroke_rate, deviation, deviation_rate, pitch, pitch_rate, bird, pos, orient, l);
+    make_wing_frame(-1.0f, stroke, stroke_rate, deviation, deviation_rate, pitch, pitch_rate, bird, pos, orient, r);
     float4 o = qnormalize(orient);
     Prepared& p = st->prep;
     p.body_position = f4(pos, 0.0f);
@@ -251,26 +192,6 @@ __device__ __forceinline__ float sd_tail(V3 bl, V3 br, const float* tg) {
     return sd_box_tail(dx, dy, dz);
 }
 
-__device__ __forceinline__ bool box_cell(const GeomArgs& a, int& x, int& y, int& z, int64_t& bidx) {
-    int lx = blockIdx.x * blockDim.x + threadIdx.x;
-    int ly = blockIdx.y * blockDim.y + threadIdx.y;
-    int lz = blockIdx.z;
-    if (lx >= a.bx || ly >= a.by || lz >= a.bz) return false;
-    const int32_t* o = a.b.state->box_origin;
-    x = o[0] + lx;
-    y = o[1] + ly;
-    z = o[2] + lz;
-    bidx = (int64_t)lx + (int64_t)a.bx * ((int64_t)ly + (int64_t)a.by * lz);
-    return x < a.g.nx && y < a.g.ny && z < a.g.nz;
-}
-
-__device__ __forceinline__ uint8_t topo_flags(uint8_t part, uint8_t prev_part, int has_prev) {
-    if (!has_prev) return part;
-    if (part && !prev_part) return (uint8_t)(part | kCovered);
-    if (!part && prev_part) return kUncovered;
-    return part;
-}
-
 // buildBirdGeometry: BF.metal:816-938
 __global__ void k_classify_bird(const GeomArgs a, int has_prev) {
     int x, y, z;
@@ -362,57 +283,6 @@ __global__ void k_classify_ellipsoid(const GeomArgs a, int has_prev) {
                                 (p.linear_velocity.z + cr.z) * a.fp.v2l, imp);
 }
 
-// ---------------------------------------------------------------------------
-// Triangle mesh (BF.metal:1529-1583 closest point, 1638-1686 raster,
-// 1697-1738 / 1978-2039 resolve).  Keys are 64-bit: quantised distance
-// (1/65536 cell) in the high word, triangle id in the low word, so meshes are
-// not limited to the reference's 4,096 triangles and ties stay deterministic.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ V3 closest_point(V3 p, V3 a, V3 b, V3 c, V3& bary) {
-    V3 ab = b - a, ac = c - a, ap = p - a;
-    float d1 = dot(ab, ap), d2 = dot(ac, ap);
-    if (d1 <= 0.0f && d2 <= 0.0f) {
-        bary = v3(1, 0, 0);
-        return a;
-    }
-    V3 bp = p - b;
-    float d3 = dot(ab, bp), d4 = dot(ac, bp);
-    if (d3 >= 0.0f && d4 <= d3) {
-        bary = v3(0, 1, 0);
-        return b;
-    }
-    float vc = d1 * d4 - d3 * d2;
-    if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
-        float v = d1 / (d1 - d3);
-        bary = v3(1.0f - v, v, 0);
-        return v3(a.x + v * ab.x, a.y + v * ab.y, a.z + v * ab.z);
-    }
-    V3 cp = p - c;
-    float d5 = dot(ab, cp), d6 = dot(ac, cp);
-    if (d6 >= 0.0f && d5 <= d6) {
-        bary = v3(0, 0, 1);
-        return c;
-    }
-    float vb = d5 * d2 - d1 * d6;
-    if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
-        float w = d2 / (d2 - d6);
-        bary = v3(1.0f - w, 0, w);
-        return v3(a.x + w * ac.x, a.y + w * ac.y, a.z + w * ac.z);
-    }
-    float va = d3 * d6 - d5 * d4;
-    if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f) {
-        float w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
-        bary = v3(0, 1.0f - w, w);
-        return v3(b.x + w * (c.x - b.x), b.y + w * (c.y - b.y), b.z + w * (c.z - b.z));
-    }
-    float inv = 1.0f / fmaxf(va + vb + vc, 1.0e-20f);
-    float v = vb * inv, w = vc * inv;
-    bary = v3(1.0f - v - w, v, w);
-    return v3(a.x + ab.x * v + ac.x * w, a.y + ab.y * v + ac.y * w, a.z + ab.z * v + ac.z * w);
-}
-
-// Articulated vertex placement: segment 0 rides the body frame, 1 / 2 the left
-// / right wing frames (the indexed surface preparation of BF.metal:1589-1622,
 // driven by the rigid frames instead of keyframes).
 __global__ void k_mesh_prepare(const GeomArgs a) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -445,12 +315,6 @@ __global__ void k_mesh_prepare(const GeomArgs a) {
 __global__ void k_mesh_clear(const GeomArgs a) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < a.box_cells) a.b.keys[i] = 0xFFFFFFFFFFFFFFFFull;
-}
-
-__device__ __forceinline__ void tri_vertices(const GeomArgs& a, uint32_t t, V3& A, V3& B, V3& C) {
-    A = v3(a.b.mesh_pos[a.b.mesh_tris[3 * t]]);
-    B = v3(a.b.mesh_pos[a.b.mesh_tris[3 * t + 1]]);
-    C = v3(a.b.mesh_pos[a.b.mesh_tris[3 * t + 2]]);
 }
 
 __global__ void k_mesh_raster(const GeomArgs a) {
@@ -521,24 +385,6 @@ __global__ void k_fill_wall_w(float4* wall, int64_t n, float w) {
     if (i < n) wall[i] = make_float4(0.0f, 0.0f, 0.0f, w);
 }
 
-// ---------------------------------------------------------------------------
-// Link predicate and link fractions.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ bool persistent_fluid(uint8_t m_next, uint8_t m_prev) {
-    return (m_next & (kPartMask | kUncovered)) == 0 && (m_prev & kPartMask) == 0;
-}
-// Solid source of link (x, q) or -1.
-__device__ __forceinline__ int64_t link_source(const Grid& g, const uint8_t* mask_next, int x, int y, int z, int q,
-                                               int& sx, int& sy, int& sz) {
-    sx = x - cx(q);
-    sy = y - cy(q);
-    sz = z - cz(q);
-    if (!wrap(g, sx, sy, sz)) return -1;
-    int64_t s = flat(g, sx, sy, sz);
-    return (mask_next[s] & kPartMask) ? s : -1;
-}
-
-// Ten-iteration bisection from the fluid node toward the solid node on the
 // ellipsoid implicit (the prescribedWingLinkFraction rule, BF.metal:1144-1175).
 __device__ float ellipsoid_link_fraction(const GeomArgs& a, int fx, int fy, int fz, int sx, int sy, int sz) {
     const Prepared& p = a.b.state->prep;
@@ -554,21 +400,6 @@ __device__ float ellipsoid_link_fraction(const GeomArgs& a, int fx, int fy, int 
     return clampf(0.5f * (lo + hi), 1.0e-4f, 1.0f);
 }
 
-__device__ __forceinline__ float tri_distance(const GeomArgs& a, uint32_t t, V3 w) {
-    V3 A, B, C, bary;
-    tri_vertices(a, t, A, B, C);
-    V3 cp = closest_point(w, A, B, C, bary);
-    return length(w - cp);
-}
-
-__device__ __forceinline__ unsigned long long box_key(const GeomArgs& a, int x, int y, int z) {
-    const int32_t* o = a.b.state->box_origin;
-    int lx = x - o[0], ly = y - o[1], lz = z - o[2];
-    if (lx < 0 || ly < 0 || lz < 0 || lx >= a.bx || ly >= a.by || lz >= a.bz) return 0xFFFFFFFFFFFFFFFFull;
-    return a.b.keys[(int64_t)lx + (int64_t)a.bx * ((int64_t)ly + (int64_t)a.by * lz)];
-}
-
-// Wall position along the link as the bracketed root of
 // min(d_A, d_B) - h, A and B the winning triangles of the two end cells.
 __device__ float mesh_ray_root(const GeomArgs& a, int fx, int fy, int fz, int sx, int sy, int sz) {
     V3 fw = cell_world(a.fp, fx, fy, fz), sw = cell_world(a.fp, sx, sy, sz);
@@ -602,44 +433,6 @@ __device__ float mesh_ray_root(const GeomArgs& a, int fx, int fy, int fz, int sx
     return clampf(0.5f * (lo + hi), 1.0e-4f, 1.0f);
 }
 
-// ---------------------------------------------------------------------------
-// Block reductions in a fixed order (deterministic).
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ int linear_tid() { return threadIdx.x + blockDim.x * threadIdx.y; }
-
-// Fixed-order tree over the (up to 256) threads of a block; every thread
-// receives the block total.
-template <int K>
-__device__ __forceinline__ void block_sum(double (&v)[K], double (*sh)[256]) {
-    const int t = linear_tid();
-    const int nt = blockDim.x * blockDim.y;
-    for (int k = 0; k < K; ++k) sh[k][t] = v[k];
-    for (int k = 0; k < K; ++k)
-        if (t + nt < 256) sh[k][t + nt] = 0.0;
-    __syncthreads();
-    for (int s = 128; s > 0; s >>= 1) {
-        if (t < s)
-            for (int k = 0; k < K; ++k) sh[k][t] += sh[k][t + s];
-        __syncthreads();
-    }
-    for (int k = 0; k < K; ++k) v[k] = sh[k][0];
-    __syncthreads();
-}
-
-// FP64 load contribution: lattice force fl applied at point pt (both in the
-// precision the step computes in), torque about the FP64 body position.
-template <class R>
-__device__ __forceinline__ void add_load(double (&acc)[8], R flx, R fly, R flz, R ptx, R pty, R ptz,
-                                         const double* body, float f2p) {
-    double fp[3] = {(double)flx * (double)f2p, (double)fly * (double)f2p, (double)flz * (double)f2p};
-    double r[3] = {(double)ptx - body[0], (double)pty - body[1], (double)ptz - body[2]};
-    acc[0] += (double)flx;
-    acc[1] += (double)fly;
-    acc[2] += (double)flz;
-    acc[3] += r[1] * fp[2] - r[2] * fp[1];
-    acc[4] += r[2] * fp[0] - r[0] * fp[2];
-    acc[5] += r[0] * fp[1] - r[1] * fp[0];
-}
 
 // ---------------------------------------------------------------------------
 // Topology impulses (BF.metal:2557-2609 covered, 2616-2666 uncovered) and the
@@ -955,6 +748,37 @@ __global__ void __launch_bounds__(256) k_links_apply(const GeomArgs a, int rep_s
             const R dxs = (R)fp.dx;
             const R bpx = (R)world.x - qf * dx_ * dxs, bpy = (R)world.y - qf * dy_ * dxs, bpz = (R)world.z - qf * dz_ * dxs;
             add_load<R>(acc, lx, ly, lz, bpx, bpy, bpz, body, fp.f2p);
+            acc[6] += (double)lx * (double)wvx + (double)ly * (double)wvy + (double)lz * (double)wvz;
+        }
+        if (a.b.link_tape) {
+            // record the link for the adjoint: values, the bounce-back case and
+            // the tangents of q and of the wall velocity at the link
+            LinkTape<R>& t = ((LinkTape<R>*)a.b.link_tape)[i];
+            const float* tg = a.b.link_tangent + (size_t)kLinkTangentWords * i;
+            t.cell = (uint32_t)gid;
+            t.dir = (uint32_t)q;
+            t.kase = interp ? (qf <= R(0.5) ? 1u : 2u) : 0u;
+            t._pad = 0;
+            t.value = value;
+            t.reflected = reflected;
+            t.other = R(0);
+            if (t.kase == 1) t.other = canon_load<S>(A, g, rep_s, opp(q), fx, fy, fz);
+            if (t.kase == 2) t.other = canon_load<S>(A, g, rep_s, q, x, y, z);
+            t.q = qf;
+            t.wv[0] = wvx;
+            t.wv[1] = wvy;
+            t.wv[2] = wvz;
+            const float4 wxf = a.b.wall[gid];
+            const float ud[3] = {ws.x - wxf.x, ws.y - wxf.y, ws.z - wxf.z};
+            for (int k = 0; k < kKinematicParams; ++k) {
+                const float dqk = t.kase ? tg[k] : 0.0f;
+                t.dq[k] = dqk;
+                for (int c = 0; c < 3; ++c) {
+                    const float duf = tg[4 + 3 * k + c], dus = tg[16 + 3 * k + c];
+                    const float qv = (float)qf;
+                    t.dwv[k][c] = t.kase ? (1.0f - qv) * duf + qv * dus + ud[c] * dqk : dus;
+                }
+            }
         }
     }
     block_sum<8>(acc, sh);
@@ -981,6 +805,7 @@ __global__ void k_reduce_loads(const GeomArgs a, int with_topology) {
             st->loads_lattice[k] = acc[k] + acc2[k];
             st->loads_torque[k] = acc[3 + k] + acc2[3 + k];
         }
+        st->power_lattice = acc2[6];
         if (with_topology) {
             st->covered_count = (int64_t)acc[6];
             st->uncovered_count = (int64_t)acc[7];
@@ -1098,6 +923,19 @@ __global__ void k_finish(const GeomArgs a, float gx, float gy, float gz, int sub
             st->safety_metrics[3] = clearance;
         }
     }
+    Objective* ob = a.b.objective;
+    if (ob && ob->enabled) {
+        if (st->link_count > ob->max_links) ob->max_links = st->link_count;
+        // time-averaged load objective: this step completes relative step k
+        const uint64_t k = st->step + 1 - ob->start;
+        if (k >= ob->first && k <= ob->last) {
+            const double inv = 1.0 / (double)(ob->last - ob->first + 1);
+            double j = 0.0;
+            for (int c = 0; c < 3; ++c) j += ob->force_weight[c] * (st->loads_lattice[c] * (double)fp.f2p);
+            j += ob->power_weight * (-st->power_lattice * (double)fp.f2p / (double)fp.v2l);
+            ob->value += j * inv;
+        }
+    }
     st->step += 1;
 }
 
@@ -1123,27 +961,6 @@ __global__ void k_record_sample(const GeomArgs a, bfx_run_sample* samples, uint6
 // ---------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------
-static GeomArgs make_geom(const GridDesc& gd, const FluidParams& fp, const BoxDesc& box, const GeomBuffers& gb,
-                          void* pops) {
-    GeomArgs a;
-    a.g = device_grid(gd);
-    a.fp = fp;
-    a.bx = box.sx;
-    a.by = box.sy;
-    a.bz = box.sz;
-    a.box_cells = box.cells;
-    a.b = gb;
-    a.pops = pops;
-    return a;
-}
-
-static void box_shape(const BoxDesc& box, dim3& grid, dim3& block) {
-    int bx = box.sx >= 64 ? 64 : ((box.sx + 31) / 32) * 32;
-    if (bx < 32) bx = 32;
-    int by = 256 / bx;
-    block = dim3(bx, by, 1);
-    grid = dim3((box.sx + bx - 1) / bx, (box.sy + by - 1) / by, box.sz);
-}
 
 int box_block_count(const BoxDesc& box) {
     dim3 grid, block;

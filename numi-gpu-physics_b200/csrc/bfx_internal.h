@@ -23,6 +23,7 @@ struct FluidBuffers {
     float* density;         // captured fields
     float4* velocity;
     DeviceState* state;
+    void* tape;             // pre-collision (rho, u) per cell when the step is taped (capture == 2)
 };
 
 // Fused stream + collide: part 0 = fluid interior cells (the hot kernel);
@@ -80,6 +81,10 @@ struct GeomBuffers {
     double* link_partials;          // 8 per apply block
     int apply_blocks;
     DeviceState* state;
+    Objective* objective;           // load objective accumulated by the step end (may be null)
+    void* link_tape;                // LinkTape<R> per link when the step is taped (else null)
+    const float* link_tangent;      // per link: dq[4], du_fluid[4][3], du_solid[4][3]
+    const FrameTangent* frames;     // wing-frame tangent of the taped step
 };
 
 void launch_prepare(int geometry, float dt, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
@@ -98,6 +103,41 @@ void launch_integrate(const GridDesc& g, const FluidParams& fp, const GeomBuffer
 void launch_record_sample(const GeomBuffers& gb, const FluidParams& fp, bfx_run_sample* samples, uint64_t index,
                           float dt, cudaStream_t s);
 void launch_step_counter(DeviceState* st, cudaStream_t s);
+
+// ---- discrete adjoint (bfx_adjoint.cu) ----------------------------------
+constexpr int kLinkTangentWords = 28;   // dq[4] + du_fluid[4][3] + du_solid[4][3]
+
+// Wing-frame tangent of the step the state is about to take.
+void launch_frame_tangent(const GeomBuffers& gb, float dt, FrameTangent* out, cudaStream_t s);
+// Per-link tangents dq/dtheta and du_wall/dtheta at both link ends (mesh geometry).
+void launch_link_tangent(int link_rule, int interpolated, const GridDesc& g, const FluidParams& fp,
+                         const BoxDesc& box, const GeomBuffers& gb, float* out, cudaStream_t s);
+
+// Taped data of one forward step, as the adjoint step reads it.
+struct StepTape {
+    const void* moments;            // R4 per real cell: pre-collision rho, u
+    const uint8_t* mask_next;       // occupancy after the step (with topology flags)
+    const uint8_t* mask_prev;       // occupancy before the step
+    const unsigned long long* keys; // box-local mesh keys of the step
+    const DeviceState* state;       // box origin, link count, step index
+    const FrameTangent* frames;
+    const void* links;              // LinkTape<R>[link count]
+};
+
+struct AdjointWork {
+    void* lam;                      // adjoint populations, same layout as the populations
+    void* nu;                       // R per link: adjoint of the bounce-back value
+    double* partials_rare;          // 4 per box block
+    double* partials_links;         // 4 per apply block
+    Objective* objective;
+};
+
+// One reverse step: the adjoint of the forward step that took the populations
+// from representation rep_s (before) to the taped state.  weight is the
+// objective weight of that step (0 outside the averaging window).
+void launch_adjoint_step(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
+                         const GeomBuffers& gb, const StepTape& tape, const AdjointWork& w, double weight,
+                         cudaStream_t s);
 
 }  // namespace bfx
 

@@ -59,6 +59,48 @@ struct DeviceState {
     int64_t covered_count;
     int64_t uncovered_count;
     uint64_t launches_device;
+    double power_lattice;          // last step: sum over cut links of F_link . u_wall (lattice units)
+};
+
+// Time-averaged load objective of the adjoint (one per simulation; disabled
+// outside bfx_adjoint).  J = mean over the window of
+// force_weight . F + power_weight * P, with F the body force (N) and
+// P = -sum_links F_link . u_wall the aerodynamic power (W) the wings deliver.
+struct Objective {
+    int32_t enabled;
+    int32_t _pad;
+    uint64_t start;                // completed steps when the window count starts
+    uint64_t first, last;          // window of relative step indices (1-based, inclusive)
+    double force_weight[3];
+    double power_weight;
+    double value;                  // accumulated J
+    double grad[4];                // accumulated dJ/dtheta
+    int64_t max_links;             // largest cut-link count while enabled
+};
+
+// Number of kinematic parameters the adjoint differentiates: stroke
+// amplitude, pitch amplitude, pitch phase, deviation amplitude (radians).
+constexpr int kKinematicParams = 4;
+
+// Forward-mode tangent of the wing frames with respect to the kinematic
+// parameters, one step: value and the four partials of each component of
+// chord, span, normal and the relative angular velocity, per side.
+struct FrameTangent {
+    float v[2][4][3];
+    float d[2][4][3][kKinematicParams];
+};
+
+// Everything the adjoint of one cut link needs from its forward step.
+template <class R>
+struct LinkTape {
+    uint32_t cell;                 // fluid cell (flat index)
+    uint32_t dir;                  // direction q (the solid source is cell - c_q)
+    uint32_t kase;                 // 0 halfway / fallback, 1 interpolated q <= 1/2, 2 interpolated q > 1/2
+    uint32_t _pad;
+    R value, reflected, other, q;  // other: f*_opp(q)(x + c_q) (kase 1) or f*_q(x) (kase 2)
+    R wv[3];                       // wall velocity at the link (lattice)
+    float dq[kKinematicParams];
+    float dwv[kKinematicParams][3];
 };
 
 }  // namespace bfx

@@ -788,11 +788,16 @@ void or_prepare_bird(const or_bird* bird, const or_body_f32* body, float time, f
     float stroke_rate = af * bird->wing_kinematics0.v[1] * bfx_cosf(phase);
     float pitch = bird->wing_kinematics0.v[3] + bird->wing_kinematics1.v[0] * bfx_sinf(phase + bird->wing_kinematics1.v[1]);
     float pitch_rate = af * bird->wing_kinematics1.v[0] * bfx_cosf(phase + bird->wing_kinematics1.v[1]);
+    /* Stroke-plane deviation at twice the flapping frequency, amplitude in
+     * wing_kinematics1.z (the library's extension: the reference feeds
+     * deviation only from measured keyframes). */
+    float deviation = bird->wing_kinematics1.v[2] * bfx_sinf(2.0f * phase);
+    float deviation_rate = 2.0f * af * bird->wing_kinematics1.v[2] * bfx_cosf(2.0f * phase);
     wing_frame l, r;
-    make_wing_frame(1.0f, stroke, stroke_rate, 0.0f, 0.0f, pitch, pitch_rate, 0.0f, 0.0f, bird, body->position,
-                    body->orientation, &l);
-    make_wing_frame(-1.0f, stroke, stroke_rate, 0.0f, 0.0f, pitch, pitch_rate, 0.0f, 0.0f, bird, body->position,
-                    body->orientation, &r);
+    make_wing_frame(1.0f, stroke, stroke_rate, deviation, deviation_rate, pitch, pitch_rate, 0.0f, 0.0f, bird,
+                    body->position, body->orientation, &l);
+    make_wing_frame(-1.0f, stroke, stroke_rate, deviation, deviation_rate, pitch, pitch_rate, 0.0f, 0.0f, bird,
+                    body->position, body->orientation, &r);
     float o[4];
     quat_normalize(body->orientation, o);
     set4(&out->body_position, body->position, 0.0f);

@@ -1,0 +1,119 @@
+"""Discrete adjoint (bfx_adjoint) on the flapping plate pair: gradient of the
+window-mean lift and aerodynamic power with respect to the four wing-kinematic
+parameters, checked against central finite differences of the forward step
+(FP64 populations), the FP32 gradient against the FP64 one, checkpoint-interval
+invariance, the final state, and the torch.autograd bridge."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import bfx._lib as L
+import bfx.cases as cases
+from bfx.simulation import BirdFlowError, Lattice, bird_struct
+from helpers import body_struct_from_tuple
+
+pytestmark = pytest.mark.gpu
+
+STEPS = 40
+
+
+def build(theta=None, storage=L.STORAGE_F64, link_rule=L.LINK_LINEAR):
+    cfg, rows, body, mesh = cases.adjoint_plates(storage=storage, link_rule=link_rule)
+    if theta is not None:
+        rows = cases.with_kinematic_parameters(rows, theta)
+    return Lattice(cfg, bird_struct(rows), body_struct_from_tuple(body), mesh)
+
+
+def theta0(link_rule=L.LINK_LINEAR):
+    _, rows, _, _ = cases.adjoint_plates(link_rule=link_rule)
+    return np.array(cases.kinematic_parameters(rows), dtype=np.float64)
+
+
+def adjoint(theta, storage, link_rule, force_weight, power_weight, steps=STEPS, interval=0):
+    lat = build(theta, storage, link_rule)
+    try:
+        return lat.adjoint(steps, force_weight, power_weight, checkpoint_interval=interval)
+    finally:
+        lat.close()
+
+
+def central_difference(storage, link_rule, force_weight, power_weight, h):
+    t0 = theta0(link_rule)
+    fd = np.zeros(4)
+    for k in range(4):
+        tp, tm = t0.copy(), t0.copy()
+        tp[k] += h
+        tm[k] -= h
+        jp = adjoint(tp, storage, link_rule, force_weight, power_weight).objective
+        jm = adjoint(tm, storage, link_rule, force_weight, power_weight).objective
+        fd[k] = (jp - jm) / (2 * h)
+    return fd
+
+
+# FD step 1e-4 rad: small enough that no cell changes occupancy between the
+# two runs, large enough that the FP32 geometry's round-off stays below 1e-3.
+@pytest.mark.parametrize("link_rule", [L.LINK_LINEAR, L.LINK_RAY_ROOT])
+@pytest.mark.parametrize("objective", ["lift", "power"])
+def test_fp64_gradient_matches_central_differences(link_rule, objective):
+    fw, pw = ((0.0, 0.0, 1.0), 0.0) if objective == "lift" else ((0.0, 0.0, 0.0), 1.0)
+    res = adjoint(theta0(link_rule), L.STORAGE_F64, link_rule, fw, pw)
+    g = np.array(list(res.gradient))
+    fd = central_difference(L.STORAGE_F64, link_rule, fw, pw, 1e-4)
+    scale = np.max(np.abs(fd))
+    assert scale > 0
+    assert np.max(np.abs(g - fd)) <= 1e-2 * scale, f"adjoint {g} vs central differences {fd}"
+
+
+def test_fp32_gradient_tracks_fp64():
+    fw, pw = (0.0, 0.0, 1.0), 0.0
+    g64 = np.array(list(adjoint(theta0(), L.STORAGE_F64, L.LINK_LINEAR, fw, pw).gradient))
+    g32 = np.array(list(adjoint(theta0(), L.STORAGE_F32, L.LINK_LINEAR, fw, pw).gradient))
+    assert np.max(np.abs(g32 - g64)) <= 1e-2 * np.max(np.abs(g64)), f"{g32} vs {g64}"
+
+
+def test_checkpoint_interval_does_not_change_the_gradient():
+    fw, pw = (0.0, 0.0, 1.0), 0.5
+    a = adjoint(theta0(), L.STORAGE_F32, L.LINK_LINEAR, fw, pw, interval=0)
+    b = adjoint(theta0(), L.STORAGE_F32, L.LINK_LINEAR, fw, pw, interval=3)
+    c = adjoint(theta0(), L.STORAGE_F32, L.LINK_LINEAR, fw, pw, interval=STEPS)
+    assert a.objective == b.objective == c.objective
+    assert list(a.gradient) == list(b.gradient) == list(c.gradient)
+
+
+def test_adjoint_leaves_the_forward_state_and_objective():
+    """After bfx_adjoint the handle holds the state bfx_advance would reach, and
+    J is the window mean of the per-step lift."""
+    ref = build(storage=L.STORAGE_F32)
+    forces = []
+    for _ in range(STEPS):
+        ref.advance(1)
+        forces.append(ref.loads().force[2])
+    lat = build(storage=L.STORAGE_F32)
+    res = lat.adjoint(STEPS, (0.0, 0.0, 1.0), 0.0, window=(11, STEPS))
+    assert np.array_equal(lat.populations(), ref.populations())
+    assert lat.step_index()[0] == STEPS
+    assert abs(res.objective - np.mean(forces[10:])) <= 1e-12 * max(1.0, abs(res.objective))
+    lat.advance(3)   # the handle keeps stepping
+    ref.advance(3)
+    assert np.array_equal(lat.populations(), ref.populations())
+
+
+def test_torch_autograd_bridge():
+    torch = pytest.importorskip("torch")
+    from bfx.autograd import kinematic_objective
+    direct = adjoint(theta0(), L.STORAGE_F32, L.LINK_LINEAR, (0.0, 0.0, 1.0), 0.0)
+    theta = torch.tensor(theta0(), dtype=torch.float64, requires_grad=True)
+    J = kinematic_objective(theta, lambda t: build(t, L.STORAGE_F32), STEPS, force_weight=(0.0, 0.0, 1.0))
+    (2.0 * J).backward()
+    assert J.item() == direct.objective
+    assert np.allclose(theta.grad.numpy(), 2.0 * np.array(list(direct.gradient)), rtol=0, atol=0)
+
+
+def test_out_of_scope_configuration_is_rejected():
+    cfg, rows, body, _ = cases.ellipsoid_channel(nx=48, ny=24, nz=24, radii=(7.0, 4.0, 4.0))
+    lat = Lattice(cfg, bird_struct(rows), body_struct_from_tuple(body))
+    with pytest.raises(BirdFlowError) as e:
+        lat.adjoint(4, (1.0, 0.0, 0.0), 0.0)
+    assert e.value.status == 10
+    lat.advance(1)   # still usable
