@@ -200,6 +200,7 @@ typedef struct bfx_loads {
     int64_t link_count;
     int64_t covered_count;
     int64_t uncovered_count;
+    double power;                   /* W: aerodynamic power -sum over cut links of F_link . u_wall */
 } bfx_loads;
 
 /* RunSample (Sources/BirdFlowMetal/GPUFieldObservation.swift; GPURunSample GPUData.swift:457-501). */

@@ -81,7 +81,8 @@ class Mesh(ct.Structure):
 class Loads(ct.Structure):
     _fields_ = [("force", ct.c_double * 3), ("torque", ct.c_double * 3), ("force_lattice", ct.c_double * 3),
                 ("limiter_activations", ct.c_double), ("max_restriction", ct.c_double),
-                ("link_count", ct.c_int64), ("covered_count", ct.c_int64), ("uncovered_count", ct.c_int64)]
+                ("link_count", ct.c_int64), ("covered_count", ct.c_int64), ("uncovered_count", ct.c_int64),
+                ("power", ct.c_double)]
 
 
 class RunSample(ct.Structure):

@@ -503,7 +503,8 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
     g.per_z = c.face_bc[4] == BFX_BC_PERIODIC;
     g.n = (int64_t)g.nx * g.ny * g.nz;
     g.nxy = (int64_t)g.nx * g.ny;
-    g.padded = (int64_t)(g.nx + 2) * (g.ny + 2) * (g.nz + 2);
+    g.px = ((g.nx + 2 + 7) / 8) * 8;
+    g.padded = (int64_t)g.px * (g.ny + 2) * (g.nz + 2);
     // fluid parameters
     FluidParams& fp = s->fp;
     for (int k = 0; k < 3; ++k) fp.origin[k] = c.origin[k];
@@ -750,6 +751,7 @@ static void loads_from_state(const bfx_sim* s, const DeviceState& st, bfx_loads*
     out->link_count = st.link_count;
     out->covered_count = st.covered_count;
     out->uncovered_count = st.uncovered_count;
+    out->power = -st.power_lattice * (double)s->fp.f2p / (double)s->fp.v2l;
 }
 
 int bfx_last_loads(bfx_sim* s, bfx_loads* out) {

@@ -162,7 +162,8 @@ struct StoreBF16Dev {
 // race-free in place.
 //
 // The population array carries a one-cell halo around the lattice (padded
-// extent (nx+2, ny+2, nz+2)).  Values pushed across a face land in the halo,
+// extent (px, ny+2, nz+2), the row pitch px = nx + 2 rounded up to 8 cells so
+// every row starts on a 16-byte boundary; columns past nx + 1 are unused).  Values pushed across a face land in the halo,
 // and a small fill kernel writes the values the boundary cells will pull
 // (periodic copies, face rules) before each step, so the fused kernel uses the
 // same uniform addressing for every real cell.  Masks, wall velocities and
@@ -173,7 +174,7 @@ struct Grid {
     int per_x, per_y, per_z;  // periodic axes
     int64_t n;                // real cells
     int64_t nxy;
-    int px, py, pz;           // padded extent
+    int px, py, pz;           // padded extent (px: row pitch, at least nx + 2)
     int64_t pxy, pn;          // padded plane and total
 };
 
@@ -265,7 +266,7 @@ __device__ __forceinline__ bool padded_shell_cell(const Grid& g, int64_t t, int&
     t -= 2 * fy;
     const int64_t fx = (int64_t)(g.py - 2) * (g.pz - 2);
     if (t < 2 * fx) {
-        x = t < fx ? 0 : g.px - 1;
+        x = t < fx ? 0 : g.nx + 1;
         const int64_t r = t < fx ? t : t - fx;
         z = 1 + (int)(r / (g.py - 2));
         y = 1 + (int)(r - (int64_t)(z - 1) * (g.py - 2));

@@ -242,7 +242,7 @@ Grid device_grid(const GridDesc& gd) {
     g.per_z = gd.per_z;
     g.n = gd.n;
     g.nxy = gd.nxy;
-    g.px = gd.nx + 2;
+    g.px = gd.px;
     g.py = gd.ny + 2;
     g.pz = gd.nz + 2;
     g.pxy = (int64_t)g.px * g.py;

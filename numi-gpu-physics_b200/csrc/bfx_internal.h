@@ -13,7 +13,8 @@ struct GridDesc {
     int nx, ny, nz;
     int per_x, per_y, per_z;
     int64_t n, nxy;
-    int64_t padded;         // (nx+2)(ny+2)(nz+2): cells of the population array with its halo
+    int px;                 // padded row pitch: nx + 2 rounded up to 8 cells (16-byte rows for TMA)
+    int64_t padded;         // px (ny+2)(nz+2): cells of the population array with its halo
 };
 
 struct FluidBuffers {
