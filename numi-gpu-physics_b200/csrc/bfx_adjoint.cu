@@ -156,9 +156,9 @@ __device__ DV dnormalize(const DV& v) {
 // ---------------------------------------------------------------------------
 // Wing-frame tangent: k_prepare's kinematics and makeWingFrame on duals.
 // ---------------------------------------------------------------------------
-__global__ void k_frame_tangent(const bfx_bird* birdp, const DeviceState* st, float dt, FrameTangent* out) {
+__global__ void k_frame_tangent(const bfx_bird* birdp, const DeviceState* st, float dt, int init, FrameTangent* out) {
     const bfx_bird& bird = *birdp;
-    const uint64_t absolute = st->step + 1;
+    const uint64_t absolute = init ? 0 : st->step + 1;
     const float time = (float)((double)absolute * (double)dt);
     const V3 pos = v3((float)st->body[0], (float)st->body[1], (float)st->body[2]);
     const float4 orient = make_float4((float)st->body[3], (float)st->body[4], (float)st->body[5], (float)st->body[6]);
@@ -774,6 +774,34 @@ __global__ void __launch_bounds__(256) k_adj_topology(const AdjArgs a, int rep_s
     }
 }
 
+// Initial state: k_init writes equilibrium(1, u_wall(t = 0)) into the cells
+// that are solid at t = 0, so lambda^0 of those cells feeds dJ/dtheta through
+// the initial wall velocity.
+template <class R>
+__global__ void __launch_bounds__(256) k_adj_init(const AdjArgs a, int rep_s) {
+    const GeomArgs& ga = a.ga;
+    const Grid& g = ga.g;
+    double grad[NP] = {0.0, 0.0, 0.0, 0.0};
+    int x, y, z;
+    int64_t bidx;
+    if (box_cell(ga, x, y, z, bidx)) {
+        const int64_t gid = flat(g, x, y, z);
+        if (ga.b.mask_next[gid] & kPartMask) {
+            R lam[19];
+#pragma unroll
+            for (int q = 0; q < 19; ++q) lam[q] = *canon_slot((const R*)a.lam, g, rep_s, q, x, y, z);
+            const V3 world = cell_world(ga.fp, x, y, z);
+            const CellDual cd = cell_dual(ga, *ga.b.frames, key_triangle(ga.b.keys[bidx]), world);
+            R G[3];
+            feq_velocity_adjoint<R>(lam, (R)cd.u.x.v, (R)cd.u.y.v, (R)cd.u.z.v, G);
+            const Du* du[3] = {&cd.u.x, &cd.u.y, &cd.u.z};
+            for (int k = 0; k < NP; ++k)
+                for (int c = 0; c < 3; ++c) grad[k] += (double)G[c] * (double)du[c]->d[k];
+        }
+    }
+    write_partials<NP>(grad, a.part_rare);
+}
+
 __global__ void k_adj_reduce(const double* rare, int nrare, const double* links, int nlinks, Objective* obj) {
     __shared__ double sh[NP][256];
     double acc[NP] = {0.0, 0.0, 0.0, 0.0};
@@ -791,8 +819,8 @@ __global__ void k_adj_reduce(const double* rare, int nrare, const double* links,
 // ---------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------
-void launch_frame_tangent(const GeomBuffers& gb, float dt, FrameTangent* out, cudaStream_t s) {
-    k_frame_tangent<<<1, 1, 0, s>>>(gb.bird, gb.state, dt, out);
+void launch_frame_tangent(const GeomBuffers& gb, float dt, int init, FrameTangent* out, cudaStream_t s) {
+    k_frame_tangent<<<1, 1, 0, s>>>(gb.bird, gb.state, dt, init, out);
 }
 
 void launch_link_tangent(int link_rule, int interpolated, const GridDesc& g, const FluidParams& fp,
@@ -825,9 +853,8 @@ static void adjoint_step_t(int rep_s, const GridDesc& gd, const BoxDesc& box, Ad
     k_adj_reduce<<<1, 256, 0, s>>>(a.part_rare, (int)(bgrid.x * bgrid.y * bgrid.z), a.part_links, apply_blocks, a.obj);
 }
 
-void launch_adjoint_step(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
-                         const GeomBuffers& gb, const StepTape& tape, const AdjointWork& w, double weight,
-                         cudaStream_t s) {
+static AdjArgs adjoint_args(int storage, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
+                            const GeomBuffers& gb, const StepTape& tape, const AdjointWork& w, double weight) {
     GeomBuffers tb = gb;
     tb.mask_next = (uint8_t*)tape.mask_next;
     tb.mask_prev = (uint8_t*)tape.mask_prev;
@@ -849,8 +876,25 @@ void launch_adjoint_step(int storage, int rep_s, const GridDesc& g, const FluidP
     a.part_links = w.partials_links;
     a.obj = w.objective;
     a.weight = weight;
+    return a;
+}
+
+void launch_adjoint_step(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
+                         const GeomBuffers& gb, const StepTape& tape, const AdjointWork& w, double weight,
+                         cudaStream_t s) {
+    AdjArgs a = adjoint_args(storage, g, fp, box, gb, tape, w, weight);
     if (storage == BFX_STORAGE_F64) adjoint_step_t<double>(rep_s, g, box, a, gb.apply_blocks, s);
     else adjoint_step_t<float>(rep_s, g, box, a, gb.apply_blocks, s);
+}
+
+void launch_adjoint_init(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
+                         const GeomBuffers& gb, const StepTape& init, const AdjointWork& w, cudaStream_t s) {
+    AdjArgs a = adjoint_args(storage, g, fp, box, gb, init, w, 0.0);
+    dim3 bgrid, bblock;
+    box_shape(box, bgrid, bblock);
+    if (storage == BFX_STORAGE_F64) k_adj_init<double><<<bgrid, bblock, 0, s>>>(a, rep_s);
+    else k_adj_init<float><<<bgrid, bblock, 0, s>>>(a, rep_s);
+    k_adj_reduce<<<1, 256, 0, s>>>(a.part_rare, (int)(bgrid.x * bgrid.y * bgrid.z), a.part_links, 0, a.obj);
 }
 
 }  // namespace bfx

@@ -263,7 +263,7 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
         encode_geometry_build(s, 0, mprev, mnext);
     }
     if (tape) {
-        launch_frame_tangent(geom_buffers(s, mprev, mnext), s->cfg.time_step, tape->frames, s->stream);
+        launch_frame_tangent(geom_buffers(s, mprev, mnext), s->cfg.time_step, 0, tape->frames, s->stream);
         s->launches += 1;
     }
     FluidBuffers fb = fluid_buffers(s, s->geometry() ? mnext : nullptr);
@@ -1216,6 +1216,23 @@ int bfx_adjoint(bfx_sim* s, uint64_t steps, const bfx_adjoint_objective* objecti
     ob.power_weight = objective->power_weight;
     cudaMemcpyAsync(s->dobjective, &ob, sizeof(ob), cudaMemcpyHostToDevice, s->stream);
 
+    // From a fresh simulation the initial populations depend on theta (the
+    // wall equilibria of the cells solid at t = 0): keep the t = 0 geometry.
+    const bool from_start = s->step == 0;
+    unsigned long long* init_keys = nullptr;
+    DeviceState* init_state = nullptr;
+    FrameTangent* init_frames = nullptr;
+    if (from_start) {
+        BFX_ADJ_ALLOC(init_keys, (size_t)s->box.cells * sizeof(unsigned long long));
+        BFX_ADJ_ALLOC(init_state, sizeof(DeviceState));
+        BFX_ADJ_ALLOC(init_frames, sizeof(FrameTangent));
+        cudaMemcpyAsync(init_keys, s->keys, (size_t)s->box.cells * sizeof(unsigned long long),
+                        cudaMemcpyDeviceToDevice, s->stream);
+        cudaMemcpyAsync(init_state, s->dstate, sizeof(DeviceState), cudaMemcpyDeviceToDevice, s->stream);
+        launch_frame_tangent(geom_buffers(s, s->mask[s->cur], s->mask[s->cur]), s->cfg.time_step, 1, init_frames,
+                             s->stream);
+    }
+
     cudaEvent_t ev[3];
     for (auto& e : ev) cudaEventCreate(&e);
     cudaEventRecord(ev[0], s->stream);
@@ -1322,6 +1339,18 @@ int bfx_adjoint(bfx_sim* s, uint64_t steps, const bfx_adjoint_objective* objecti
         }
         cudaError_t le = cudaGetLastError();
         if (le != cudaSuccess) return cuda_fail(s, le, "adjoint launch");
+    }
+    if (from_start) {
+        StepTape init;
+        init.moments = nullptr;
+        init.mask_next = snap_mask;   // the t = 0 occupancy
+        init.mask_prev = snap_mask;
+        init.keys = init_keys;
+        init.state = init_state;
+        init.frames = init_frames;
+        init.links = nullptr;
+        GeomBuffers gb = geom_buffers(s, s->mask[0], s->mask[1]);
+        launch_adjoint_init(s->cfg.storage, snap_rep[0], s->g, s->fp, s->box, gb, init, w, s->stream);
     }
     cudaEventRecord(ev[2], s->stream);
     restore(nseg);

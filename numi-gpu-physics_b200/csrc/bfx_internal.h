@@ -108,8 +108,8 @@ void launch_step_counter(DeviceState* st, cudaStream_t s);
 // ---- discrete adjoint (bfx_adjoint.cu) ----------------------------------
 constexpr int kLinkTangentWords = 28;   // dq[4] + du_fluid[4][3] + du_solid[4][3]
 
-// Wing-frame tangent of the step the state is about to take.
-void launch_frame_tangent(const GeomBuffers& gb, float dt, FrameTangent* out, cudaStream_t s);
+// Wing-frame tangent of the step the state is about to take (init: of t = 0).
+void launch_frame_tangent(const GeomBuffers& gb, float dt, int init, FrameTangent* out, cudaStream_t s);
 // Per-link tangents dq/dtheta and du_wall/dtheta at both link ends (mesh geometry).
 void launch_link_tangent(int link_rule, int interpolated, const GridDesc& g, const FluidParams& fp,
                          const BoxDesc& box, const GeomBuffers& gb, float* out, cudaStream_t s);
@@ -139,6 +139,11 @@ struct AdjointWork {
 void launch_adjoint_step(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
                          const GeomBuffers& gb, const StepTape& tape, const AdjointWork& w, double weight,
                          cudaStream_t s);
+// dJ/dtheta through the initial state (the wall equilibria k_init writes into
+// cells solid at t = 0); init holds the t = 0 mask (mask_next), keys, state and
+// frame tangent, rep_s the representation of the initial populations.
+void launch_adjoint_init(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
+                         const GeomBuffers& gb, const StepTape& init, const AdjointWork& w, cudaStream_t s);
 
 }  // namespace bfx
 

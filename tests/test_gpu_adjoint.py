@@ -39,7 +39,10 @@ def adjoint(theta, storage, link_rule, force_weight, power_weight, steps=STEPS, 
         lat.close()
 
 
-def trajectory(theta, storage, link_rule, coarse, steps=STEPS):
+FD_STEPS = 12
+
+
+def trajectory(theta, storage, link_rule, coarse, steps=FD_STEPS):
     """Per-step topology (links, covered, uncovered), lift F_z and power."""
     lat = build(theta, storage, link_rule, coarse)
     topo, lift, power = [], [], []
@@ -71,20 +74,22 @@ def central_differences(storage, link_rule, coarse, h):
     return lift, power
 
 
-# FP64 populations and h = 1e-5 rad: small enough that no cell changes
-# occupancy between the two runs of a pair (checked), large enough that the
-# FP32 geometry's round-off stays far below the difference.  The ray-root
+# FP64 populations, h = 1e-4 rad over 12 steps: no cell changes occupancy
+# between the two runs of a pair (checked step by step), while the FP32 wing
+# frames' round-off (about one ulp of the rotation angle, ~1e-7 rad, coherent
+# over the whole wing) stays a ~0.1 % error of the difference.  The ray-root
 # case uses one quad per wing: the root search looks at the two triangles that
 # own the link's end cells, so a finer mesh makes its q jump where ownership
 # changes, which no derivative describes.
 @pytest.mark.parametrize("link_rule,coarse", [(L.LINK_LINEAR, False), (L.LINK_RAY_ROOT, True)])
 def test_fp64_gradient_matches_central_differences(link_rule, coarse):
-    fd_lift, fd_power = central_differences(L.STORAGE_F64, link_rule, coarse, 1e-5)
+    fd_lift, fd_power = central_differences(L.STORAGE_F64, link_rule, coarse, 1e-4)
     for (fw, pw), fd in ((((0.0, 0.0, 1.0), 0.0), fd_lift), (((0.0, 0.0, 0.0), 1.0), fd_power)):
-        g = np.array(list(adjoint(theta0(link_rule), L.STORAGE_F64, link_rule, fw, pw, coarse=coarse).gradient))
+        g = np.array(list(adjoint(theta0(link_rule), L.STORAGE_F64, link_rule, fw, pw, steps=FD_STEPS,
+                                  coarse=coarse).gradient))
         scale = np.max(np.abs(fd))
         assert scale > 0
-        assert np.max(np.abs(g - fd)) <= 2e-2 * scale, f"adjoint {g} vs central differences {fd}"
+        assert np.max(np.abs(g - fd)) <= 1e-2 * scale, f"adjoint {g} vs central differences {fd}"
 
 
 def test_fp32_gradient_tracks_fp64():
