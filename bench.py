@@ -21,6 +21,16 @@ Workloads (lattice units):
   shear_wave         64^3 periodic, nu 0.01, magic 1/4 (L2-resident)
 Multi-GPU: the step does not shard here (one GPU per lattice), so N GPUs run N
 independent replicas; ``value`` is the aggregate and ``scaling`` is weak.
+
+On one GPU the line also carries
+  ``variants``  FP32 / FP16-deviation / BF16-deviation storage on the flapping
+                plates (512x256x256, TRT): GLUPS, roofline fraction, and the
+                force averaged over the first stroke period against FP64;
+  ``adjoint``   the discrete adjoint on the plates at 256x128x128 over one
+                period: lift and power gradients, cost against a forward pass,
+                central differences (h = 1e-3 rad) and FP32 vs FP64 gradients
+                at 96x48x48.
+(--no-variants / --no-adjoint / --no-cpu skip the extras.)
 """
 from __future__ import annotations
 
@@ -232,6 +242,127 @@ def force_history(name, storage, steps, device):
     return f
 
 
+def storage_forms(device, steps=200, warmup=5):
+    """FP32 / FP16-deviation / BF16-deviation on the flapping-plate workload
+    (512x256x256, TRT, links rebuilt every step): throughput, fraction of the
+    HBM roofline of the fused kernel, and the force averaged over the first
+    stroke period (4000 steps) against an FP64 run of the same kernels."""
+    import bfx._lib as L
+    peak, _ = measured_peak()
+    period = 4000
+    ref = force_history("flapping_plates", L.STORAGE_F64, period, device).mean(axis=0)
+    out = {"workload": "flapping_plates 512x256x256 TRT, stroke 60 deg, pitch 45 deg, T=4000",
+           "force_window_steps": [1, period], "force_reference": "FP64 storage, same kernels"}
+    base = None
+    for st in (L.STORAGE_F32, L.STORAGE_F16_DEVIATION, L.STORAGE_BF16_DEVIATION):
+        nm = L.STORAGE_NAMES[st]
+        vlat, cfg, _, _ = make_lattice("flapping_plates", st, device)
+        cells = cfg.nx * cfg.ny * cfg.nz
+        vms, _, vkms, vkl = time_steps(vlat, steps, warmup)
+        fluid = cells - int(np.count_nonzero(vlat.mask()))
+        vlat.close()
+        rate = cells * steps / (vms / 1000.0) / 1e9
+        kernel_s = vkms / max(vkl, 1) / 1000.0
+        ach = fluid * 38 * L.STORAGE_BYTES[st] / kernel_s / 1e9
+        f = force_history("flapping_plates", st, period, device).mean(axis=0)
+        err = float(np.linalg.norm(f - ref) / max(np.linalg.norm(ref), 1e-30))
+        base = rate if base is None else base
+        out[nm] = {"value": rate, "unit": "GLUPS", "kernel_ms": kernel_s * 1000.0, "achieved_gbs": ach,
+                   "roofline_frac": ach / peak, "speedup_vs_f32": rate / base,
+                   "cycle_mean_force_error_vs_f64": err}
+    return out
+
+
+def adjoint_measure(device):
+    """Discrete adjoint on the flapping-plate pair at 256x128x128 (span 40,
+    chord 8, T = 2000, one period, FP32, TRT, linear links): gradient of the
+    cycle-mean lift and aerodynamic power with respect to (stroke amplitude,
+    pitch amplitude, pitch phase, deviation amplitude); cost against a plain
+    forward pass; central differences with h = 1e-3 rad; FP32 against FP64
+    gradients at 96x48x48."""
+    import bfx._lib as L
+    import bfx.cases as cases
+    from bfx.simulation import Lattice, bird_struct
+
+    def plates(storage, theta=None, n=(256, 128, 128), span=40.0, chord=8.0):
+        cfg, rows, body, mesh = cases.flapping_plates(
+            nx=n[0], ny=n[1], nz=n[2], span=span, chord=chord, thickness=2.0, n_chord=16, n_span=64, period=2000.0,
+            stroke_deg=60.0, pitch_deg=45.0, deviation_deg=5.0, viscosity=0.004, storage=storage,
+            link_rule=L.LINK_LINEAR, sponge_width=12.0)
+        if theta is not None:
+            rows = cases.with_kinematic_parameters(rows, theta)
+        cfg.device = device
+        bs = L.BodyState()
+        bs.position[:] = list(body[0])
+        bs.orientation[:] = list(body[1])
+        return Lattice(cfg, bird_struct(rows), bs, mesh), rows
+
+    steps = 2000
+    lat, rows = plates(L.STORAGE_F32)
+    theta0 = np.array(cases.kinematic_parameters(rows), dtype=np.float64)
+    lat.advance(1)  # warm the code paths, then time a plain forward pass on a fresh handle
+    lat.close()
+    lat, _ = plates(L.STORAGE_F32)
+    lat.timer_begin()
+    lat.advance(steps, batch_size=steps)
+    fwd_ms = lat.timer_end()
+    lat.close()
+    out = {"case": "flapping_plates 256x128x128, span 40, chord 8, 2x2048 triangles, T=2000, nu=0.004, TRT, "
+                   "linear links, FP32", "steps": steps,
+           "parameters": ["stroke amplitude", "pitch amplitude", "pitch phase", "deviation amplitude"],
+           "theta": theta0.tolist(), "forward_ms": fwd_ms}
+    for name, fw, pw in (("lift", (0.0, 0.0, 1.0), 0.0), ("power", (0.0, 0.0, 0.0), 1.0)):
+        lat, _ = plates(L.STORAGE_F32)
+        r = lat.adjoint(steps, fw, pw)
+        lat.close()
+        out[name] = {"objective": r.objective, "gradient": list(r.gradient), "adjoint_forward_ms": r.forward_ms,
+                     "adjoint_reverse_ms": r.reverse_ms, "checkpoint_interval": r.checkpoint_interval,
+                     "snapshots": r.snapshots, "work_bytes": r.work_bytes,
+                     "cost_vs_forward": (r.forward_ms + r.reverse_ms) / fwd_ms}
+    # central differences of both objectives with h = 1e-3 rad.  Over a full
+    # period some cells change occupancy between the two runs of a pair; those
+    # cover / uncover jumps are in the differences but not in the derivative
+    # of the smooth piece the adjoint computes.
+    h = 1e-3
+
+    def objectives(theta):
+        lat, _ = plates(L.STORAGE_F32, theta)
+        lift, power = [], []
+        for _ in range(steps):
+            lat.advance(1)
+            ld = lat.loads()
+            lift.append(ld.force[2])
+            power.append(ld.power)
+        lat.close()
+        return float(np.mean(lift)), float(np.mean(power))
+
+    fd_lift, fd_power = [], []
+    for k in range(4):
+        tp, tm = theta0.copy(), theta0.copy()
+        tp[k] += h
+        tm[k] -= h
+        (lp, pp), (lm, pm) = objectives(tp), objectives(tm)
+        fd_lift.append((lp - lm) / (2 * h))
+        fd_power.append((pp - pm) / (2 * h))
+    for name, fd in (("lift", fd_lift), ("power", fd_power)):
+        g = np.array(out[name]["gradient"])
+        out[name]["central_difference"] = fd
+        out[name]["relative_difference_vs_fd"] = float(np.max(np.abs(g - np.array(fd))) / max(np.max(np.abs(fd)), 1e-30))
+    out["central_difference_h"] = h
+    # FP64 reference gradient on a 96x48x48 lattice (the same case scaled)
+    small = dict(n=(96, 48, 48), span=15.0, chord=4.0)
+    grads = {}
+    for st in (L.STORAGE_F32, L.STORAGE_F64):
+        lat, _ = plates(st, **small)
+        grads[st] = np.array(list(lat.adjoint(steps, (0.0, 0.0, 1.0), 0.0).gradient))
+        lat.close()
+    out["fp64_reference_96x48x48"] = {
+        "gradient_fp64": grads[L.STORAGE_F64].tolist(), "gradient_fp32": grads[L.STORAGE_F32].tolist(),
+        "relative_difference": float(np.max(np.abs(grads[L.STORAGE_F32] - grads[L.STORAGE_F64])) /
+                                     max(np.max(np.abs(grads[L.STORAGE_F64])), 1e-30))}
+    return out
+
+
 def cpu_port_rate(name, seconds_budget=12.0, max_steps=64):
     """The oracle (CPU restatement of the reference path) on the same workload."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -287,6 +418,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--lattice", type=int, nargs=3, default=None, help="profiling override of the lattice size")
     ap.add_argument("--collision", default=None, choices=["trt", "rr3", "reg", "limiter"])
     ap.add_argument("--storage", default="f32", choices=["f32", "f16dev", "bf16dev", "f64"])
@@ -355,7 +487,9 @@ def main():
     traffic = profiled_traffic(args.workload, args.storage)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "peak_kind": f"of {peak_kind}",
-                "kernel": "k_bulk (fused AA stream+collide over every fluid cell)",
+                "kernel": ("k_stream (TMA-staged fused AA stream+collide, 16-bit TRT)"
+                           if coll == "trt" and args.storage in ("f16dev", "bf16dev")
+                           else "k_bulk (fused AA stream+collide over every fluid cell)"),
                 "bytes_per_launch": bytes_per_launch, "bytes_rule": "fluid cells x 19 x 2 x storage bytes",
                 "kernel_ms": kernel_s * 1000.0}
 
@@ -374,31 +508,10 @@ def main():
         "clocks": clocks.summary(),
     }
 
-    if rank == 0 and not args.no_variants:
-        variants = {}
-        hist_steps = 400 if args.workload != "flapping_plates" else 4000
-        ref = force_history(args.workload, L.STORAGE_F64, hist_steps, local)
-        half = hist_steps // 2
-        ref_mean = ref[half:].mean(axis=0)
-        for st in (L.STORAGE_F32, L.STORAGE_F16_DEVIATION, L.STORAGE_BF16_DEVIATION):
-            nm = L.STORAGE_NAMES[st]
-            if st != L.STORAGE_F32:
-                vlat, _, _, _ = make_lattice(args.workload, st, local)
-                vms, _, vkms, vkl = time_steps(vlat, args.steps, args.warmup)
-                vlat.close()
-                s = L.STORAGE_BYTES[st]
-                vach = fluid * 38 * s / (vkms / max(vkl, 1) / 1000.0) / 1e9
-                variants[nm] = {"value": cells * args.steps / (vms / 1000.0) / 1e9, "unit": "GLUPS",
-                                "roofline_frac": vach / peak, "achieved_gbs": vach,
-                                "speedup_vs_f32": (cells * args.steps / (vms / 1000.0) / 1e9) / value * world}
-            else:
-                variants[nm] = {"value": value / world, "unit": "GLUPS", "roofline_frac": roofline["frac"]}
-            f = force_history(args.workload, st, hist_steps, local)
-            mean = f[half:].mean(axis=0)
-            scale = max(np.linalg.norm(ref_mean), 1e-30)
-            variants[nm]["force_error_vs_f64"] = float(np.linalg.norm(mean - ref_mean) / scale)
-            variants[nm]["force_window_steps"] = [half, hist_steps]
-        line["variants"] = variants
+    if rank == 0 and world == 1 and not args.no_variants:
+        line["variants"] = storage_forms(local)
+    if rank == 0 and world == 1 and not args.no_adjoint:
+        line["adjoint"] = adjoint_measure(local)
 
     if rank == 0 and world == 1 and not args.no_cpu:
         rate, steps, cores, dt = cpu_port_rate(args.workload)

@@ -2,6 +2,7 @@
 // simulation, encodes the per-step kernel sequence on one CUDA stream, and
 // implements the BirdFlowSimulation surface (Sources/BirdFlowMetal/
 // BirdFlowSimulation.swift) behind plain-C entry points (include/bfx.h).
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -57,6 +58,8 @@ struct bfx_sim {
     BoxDesc box{};
     size_t elem = 4;
     void* pops = nullptr;
+    alignas(64) CUtensorMap tmap;   // population array for the staged fused kernel
+    bool tma_ok = false;
     uint8_t* mask[2] = {nullptr, nullptr};
     int cur = 0;
     float4* wall = nullptr;
@@ -161,6 +164,8 @@ FluidBuffers fluid_buffers(bfx_sim* s, uint8_t* mask) {
     b.velocity = s->velocity;
     b.state = s->dstate;
     b.tape = nullptr;
+    b.tmap = s->tma_ok ? &s->tmap : nullptr;
+    b.sm_count = s->sm_count;
     return b;
 }
 
@@ -545,6 +550,11 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
         }                                                       \
     } while (0)
     BFX_ALLOC(s->pops, pop_bytes);
+    std::memset(&s->tmap, 0, sizeof(s->tmap));
+    s->tma_ok = (c.storage == BFX_STORAGE_F16_DEVIATION || c.storage == BFX_STORAGE_BF16_DEVIATION) &&
+                c.collision == BFX_COLLISION_TRT &&
+                encode_population_map(&s->tmap, s->pops, c.storage, g.px, g.ny + 2, g.nz + 2);
+    if (s->tma_ok) prepare_stream(c.storage);
     BFX_ALLOC(s->density, (size_t)g.n * sizeof(float));
     BFX_ALLOC(s->velocity, (size_t)g.n * sizeof(float4));
     BFX_ALLOC(s->dstate, sizeof(DeviceState));
@@ -701,6 +711,7 @@ int bfx_advance(bfx_sim* s, uint64_t steps, uint32_t batch_size, uint32_t flags,
             cudaMemcpy(&st, s->dstate, sizeof(st), cudaMemcpyDeviceToHost);
             s->step = st.step;
             if (st.link_overflow) return fail(s, BFX_ERR_KERNEL, "the cut-link list exceeded its capacity; raise link_capacity");
+            if (st.stream_error) return fail(s, BFX_ERR_KERNEL, "a fused-kernel pipeline wait timed out");
             if (s->cfg.free_flight && st.safety_event[2] != 0) {
                 if (result) {
                     result->steps_done = done;

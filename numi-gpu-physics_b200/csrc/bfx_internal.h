@@ -2,6 +2,7 @@
 // kernel translation units.  Not part of the public ABI.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -25,6 +26,8 @@ struct FluidBuffers {
     float4* velocity;
     DeviceState* state;
     void* tape;             // pre-collision (rho, u) per cell when the step is taped (capture == 2)
+    const void* tmap;       // CUtensorMap of the population array for the staged kernel (null: k_bulk)
+    int sm_count;
 };
 
 // Fused stream + collide: part 0 = fluid interior cells (the hot kernel);
@@ -152,4 +155,11 @@ struct Grid;
 Grid device_grid(const GridDesc& gd);
 int box_block_count(const BoxDesc& box);
 void launch_fill_wall(float4* wall, int64_t n, float w, cudaStream_t s);
+// Tensor map (px, py, pz, 19) of a 16-bit population array for the staged
+// fused kernel; false when the driver entry point is missing or the format is
+// not 16-bit.
+bool encode_population_map(CUtensorMap* map, void* pops, int storage, int64_t px, int64_t py, int64_t pz);
+// Raises the staged kernel's shared-memory limit for a 16-bit storage format
+// (call before any graph capture).
+void prepare_stream(int storage);
 }  // namespace bfx

@@ -60,6 +60,8 @@ struct DeviceState {
     int64_t uncovered_count;
     uint64_t launches_device;
     double power_lattice;          // last step: sum over cut links of F_link . u_wall (lattice units)
+    uint32_t stream_error;         // nonzero: a staged-kernel pipeline wait timed out (1 producer, 2 consumer)
+    uint32_t _pad1;
 };
 
 // Time-averaged load objective of the adjoint (one per simulation; disabled
