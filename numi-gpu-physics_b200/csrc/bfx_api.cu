@@ -227,7 +227,7 @@ void encode_links(bfx_sim* s, uint8_t* mprev, uint8_t* mnext) {
     GeomBuffers gb = geom_buffers(s, mprev, mnext);
     launch_boundary_scan(s->cfg.storage, s->rep_s, s->g, s->fp, s->box, gb, fluid_buffers(s, mnext), s->stream);
     launch_links_emit(s->cfg.geometry, s->cfg.link_rule, s->g, s->fp, s->box, gb, s->stream);
-    s->launches += 3;
+    s->launches += 4;
 }
 
 void timing_begin(bfx_sim* s) {

@@ -73,7 +73,11 @@ __global__ void __launch_bounds__(128) k_halo(const BulkArgs a, int rep_s, int64
                 uy = fp.face_u[f][1];
                 uz = fp.face_u[f][2];
             }
-            if (!done) val = feq_rt<R>(q, (R)fp.far[3], (R)ux, (R)uy, (R)uz);
+            if (!done) {
+                // far-field faces take the precomputed equilibrium (same expression, evaluated on the host)
+                if (bc == BFX_BC_VELOCITY) val = feq_rt<R>(q, (R)fp.far[3], (R)ux, (R)uy, (R)uz);
+                else val = sizeof(R) == 8 ? (R)a.far_eq_d[q] : (R)a.far_eq_f[q];
+            }
         }
         if (rep_s) S::st_rt(A + (int64_t)q * g.pn + pflat(g, bx, by, bz), q, val);
         else S::st_rt(A + (int64_t)opp(q) * g.pn + pflat(g, hx, hy, hz), opp(q), val);

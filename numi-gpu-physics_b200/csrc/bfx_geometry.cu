@@ -9,6 +9,8 @@
 // fixed at creation from the conservative body radius plus a 4-cell margin,
 // its origin is recomputed on the device every step), so a step costs
 // O(box) here and O(lattice) only in the fused fluid kernel.
+#include <algorithm>
+
 #include "bfx_geom_common.cuh"
 
 namespace bfx {
@@ -317,8 +319,13 @@ __global__ void k_mesh_clear(const GeomArgs a) {
     if (i < a.box_cells) a.b.keys[i] = 0xFFFFFFFFFFFFFFFFull;
 }
 
-__global__ void k_mesh_raster(const GeomArgs a) {
-    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+// One warp per triangle: the lanes share the triangle's voxel box (its AABB
+// grown by the half thickness plus two cells, clamped to the lattice and the
+// geometry box) and each keeps the atomic minimum of (quantised distance,
+// triangle id) per voxel.
+__global__ void __launch_bounds__(128) k_mesh_raster(const GeomArgs a) {
+    const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if (t >= a.b.ntris) return;
     V3 A, B, C;
     tri_vertices(a, t, A, B, C);
@@ -339,18 +346,22 @@ __global__ void k_mesh_raster(const GeomArgs a) {
         lo[k] = lo[k] < o[k] ? o[k] : lo[k];
         hi[k] = hi[k] > o[k] + ext[k] - 1 ? o[k] + ext[k] - 1 : hi[k];
     }
-    for (int z = lo[2]; z <= hi[2]; ++z)
-        for (int y = lo[1]; y <= hi[1]; ++y)
-            for (int x = lo[0]; x <= hi[0]; ++x) {
-                V3 w = cell_world(a.fp, x, y, z), bary;
-                V3 cp = closest_point(w, A, B, C, bary);
-                float dc = length(w - cp) / cs;
-                float bin = roundf(dc * 65536.0f);
-                unsigned long long ub = bin >= 4294967295.0f ? 0xFFFFFFFFull : (unsigned long long)bin;
-                unsigned long long key = (ub << 32) | (unsigned long long)t;
-                int64_t bi = (int64_t)(x - o[0]) + (int64_t)a.bx * ((int64_t)(y - o[1]) + (int64_t)a.by * (z - o[2]));
-                atomicMin(&a.b.keys[bi], key);
-            }
+    const int ex = hi[0] - lo[0] + 1, ey = hi[1] - lo[1] + 1, ez = hi[2] - lo[2] + 1;
+    if (ex <= 0 || ey <= 0 || ez <= 0) return;
+    const int total = ex * ey * ez;
+    for (int i = lane; i < total; i += 32) {
+        const int xi = i % ex;
+        const int r = i / ex;
+        const int x = lo[0] + xi, y = lo[1] + r % ey, z = lo[2] + r / ey;
+        V3 w = cell_world(a.fp, x, y, z), bary;
+        V3 cp = closest_point(w, A, B, C, bary);
+        float dc = length(w - cp) / cs;
+        float bin = roundf(dc * 65536.0f);
+        unsigned long long ub = bin >= 4294967295.0f ? 0xFFFFFFFFull : (unsigned long long)bin;
+        unsigned long long key = (ub << 32) | (unsigned long long)t;
+        int64_t bi = (int64_t)(x - o[0]) + (int64_t)a.bx * ((int64_t)(y - o[1]) + (int64_t)a.by * (z - o[2]));
+        atomicMin(&a.b.keys[bi], key);
+    }
 }
 
 __global__ void k_mesh_resolve(const GeomArgs a, int has_prev) {
@@ -434,6 +445,15 @@ __device__ float mesh_ray_root(const GeomArgs& a, int fx, int fy, int fz, int sx
 }
 
 
+// Persistent fluid cell that may border a solid one.  With a mesh, a cell
+// next to a solid cell lies within h + sqrt(3) dx of its triangle, inside the
+// raster's h + 2 dx guard, so it owns a key: keyless cells are skipped without
+// reading their 18 neighbours.  Link counting and emission use this same test.
+__device__ __forceinline__ bool may_have_links(const GeomArgs& a, int64_t bidx, uint8_t m_next, uint8_t m_prev) {
+    if (!persistent_fluid(m_next, m_prev)) return false;
+    return a.b.keys == nullptr || a.b.keys[bidx] != 0xFFFFFFFFFFFFFFFFull;
+}
+
 // ---------------------------------------------------------------------------
 // Topology impulses (BF.metal:2557-2609 covered, 2616-2666 uncovered) and the
 // per-block cut-link count.  Reads populations only; runs before any link write.
@@ -503,14 +523,18 @@ __global__ void __launch_bounds__(256) k_boundary_scan(const GeomArgs a, int rep
             add_load<R>(acc, tx, ty, tz, (R)world.x, (R)world.y, (R)world.z, body, fp.f2p);
             acc[7] += 1.0;
         }
-        if (persistent_fluid(m1, m0)) {
+        if (may_have_links(a, bidx, m1, m0)) {
             for (int q = 1; q < 19; ++q) {
                 int sx, sy, sz;
                 if (link_source(g, a.b.mask_next, x, y, z, q, sx, sy, sz) >= 0) ++links;
             }
         }
     }
-    block_sum<8>(acc, sh);
+    // most blocks hold no covered / uncovered cell: skip their FP64 tree
+    bool nonzero = false;
+    for (int k = 0; k < 8; ++k) nonzero = nonzero || acc[k] != 0.0;
+    const bool block_nonzero = __syncthreads_or(nonzero) != 0;
+    if (block_nonzero) block_sum<8>(acc, sh);
     __shared__ uint32_t wcount[8];
     uint32_t wl = links;
     for (int o = 16; o > 0; o >>= 1) wl += __shfl_down_sync(0xffffffffu, wl, o);
@@ -522,7 +546,7 @@ __global__ void __launch_bounds__(256) k_boundary_scan(const GeomArgs a, int rep
         uint32_t tot = 0;
         for (int w = 0; w < 8; ++w) tot += wcount[w];
         a.b.block_counts[block] = tot;
-        for (int k = 0; k < 8; ++k) a.b.topo_partials[8 * block + k] = acc[k];
+        for (int k = 0; k < 8; ++k) a.b.topo_partials[8 * block + k] = block_nonzero ? acc[k] : 0.0;
     }
 }
 
@@ -574,7 +598,7 @@ __global__ void __launch_bounds__(256) k_links_emit(const GeomArgs a, int geomet
     bool valid = box_cell(a, x, y, z, bidx);
     if (valid) {
         gid = flat(g, x, y, z);
-        if (persistent_fluid(a.b.mask_next[gid], a.b.mask_prev[gid])) {
+        if (may_have_links(a, bidx, a.b.mask_next[gid], a.b.mask_prev[gid])) {
             for (int q = 1; q < 19; ++q) {
                 int sx, sy, sz;
                 if (link_source(g, a.b.mask_next, x, y, z, q, sx, sy, sz) >= 0) ++mine;
@@ -602,8 +626,33 @@ __global__ void __launch_bounds__(256) k_links_emit(const GeomArgs a, int geomet
         int sx, sy, sz;
         int64_t s = link_source(g, a.b.mask_next, x, y, z, q, sx, sy, sz);
         if (s < 0) continue;
+        if (pos < a.b.link_capacity) {
+            a.b.link_cell[pos] = (uint32_t)gid;
+            a.b.link_meta[pos] = (uint32_t)q | ((uint32_t)(a.b.mask_next[s] & kPartMask) << 8);
+        }
+        ++pos;
+    }
+    (void)geometry;
+    (void)link_rule;
+    (void)interpolated;
+}
+
+// Link fractions, one thread per emitted link (the bisections and ray roots
+// are long and occur only at the surface: a thread per box cell would leave
+// most lanes idle while a few run them).
+__global__ void __launch_bounds__(128) k_links_fraction(const GeomArgs a, int geometry, int link_rule, int interpolated) {
+    const Grid& g = a.g;
+    int64_t count = a.b.state->link_count;
+    if (count > (int64_t)a.b.link_capacity) count = a.b.link_capacity;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t gid = a.b.link_cell[i];
+        const int q = (int)(a.b.link_meta[i] & 0xFF);
+        int x, y, z;
+        unflat(g, gid, x, y, z);
+        int sx = x - cx(q), sy = y - cy(q), sz = z - cz(q);
         float qf = 0.5f;
-        if (interpolated) {
+        if (interpolated && wrap(g, sx, sy, sz)) {
+            const int64_t s = flat(g, sx, sy, sz);
             if (geometry == BFX_GEOMETRY_ELLIPSOID) {
                 qf = ellipsoid_link_fraction(a, x, y, z, sx, sy, sz);
             } else if (geometry == BFX_GEOMETRY_MESH) {
@@ -616,12 +665,7 @@ __global__ void __launch_bounds__(256) k_links_emit(const GeomArgs a, int geomet
                 }
             }
         }
-        if (pos < a.b.link_capacity) {
-            a.b.link_cell[pos] = (uint32_t)gid;
-            a.b.link_meta[pos] = (uint32_t)q | ((uint32_t)(a.b.mask_next[s] & kPartMask) << 8);
-            a.b.link_q[pos] = qf;
-        }
-        ++pos;
+        a.b.link_q[i] = qf;
     }
 }
 
@@ -786,9 +830,28 @@ __global__ void __launch_bounds__(256) k_links_apply(const GeomArgs a, int rep_s
         for (int k = 0; k < 8; ++k) a.b.link_partials[8 * blockIdx.x + k] = acc[k];
 }
 
-// Final fixed-order reduction of the topology and link partials.
-__global__ void k_reduce_loads(const GeomArgs a, int with_topology) {
-    __shared__ double sh[8][256];
+// Fixed-order sum over a 1024-thread block: shuffle tree inside each warp,
+// then the 32 warp totals in order by thread 0 (the result is valid there).
+template <int K>
+__device__ __forceinline__ void block_sum_1024(double (&v)[K], double (*sh)[32]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = 0; k < K; ++k)
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    if (lane == 0)
+        for (int k = 0; k < K; ++k) sh[k][warp] = v[k];
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int k = 0; k < K; ++k) {
+            double t = 0.0;
+            for (int w = 0; w < 32; ++w) t += sh[k][w];
+            v[k] = t;
+        }
+    __syncthreads();
+}
+
+// Final fixed-order reduction of the topology and link partials (1024 threads).
+__global__ void __launch_bounds__(1024) k_reduce_loads(const GeomArgs a, int with_topology) {
+    __shared__ double sh[8][32];
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     if (with_topology)
         for (int i = threadIdx.x; i < a.b.box_blocks; i += blockDim.x)
@@ -796,9 +859,8 @@ __global__ void k_reduce_loads(const GeomArgs a, int with_topology) {
     double acc2[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (int i = threadIdx.x; i < a.b.apply_blocks; i += blockDim.x)
         for (int k = 0; k < 8; ++k) acc2[k] += a.b.link_partials[8 * i + k];
-    block_sum<8>(acc, sh);
-    __syncthreads();
-    block_sum<8>(acc2, sh);
+    block_sum_1024<8>(acc, sh);
+    block_sum_1024<8>(acc2, sh);
     if (threadIdx.x == 0) {
         DeviceState* st = a.b.state;
         for (int k = 0; k < 3; ++k) {
@@ -987,7 +1049,7 @@ void launch_classify(int geometry, int has_prev, const GridDesc& g, const FluidP
     } else if (geometry == BFX_GEOMETRY_MESH) {
         k_mesh_prepare<<<(gb.nverts + 255) / 256, 256, 0, s>>>(a);
         k_mesh_clear<<<(unsigned)((box.cells + 255) / 256), 256, 0, s>>>(a);
-        k_mesh_raster<<<(gb.ntris + 127) / 128, 128, 0, s>>>(a);
+        k_mesh_raster<<<(unsigned)(((int64_t)gb.ntris * 32 + 127) / 128), 128, 0, s>>>(a);
         k_mesh_resolve<<<grid, block, 0, s>>>(a, has_prev);
     }
 }
@@ -1020,6 +1082,8 @@ void launch_links_emit(int geometry, int link_rule, const GridDesc& g, const Flu
     dim3 grid, block;
     box_shape(box, grid, block);
     k_links_emit<<<grid, block, 0, s>>>(a, geometry, link_rule, fp.interpolated);
+    const unsigned fblocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(4096, ((int64_t)gb.link_capacity + 127) / 128));
+    k_links_fraction<<<fblocks, 128, 0, s>>>(a, geometry, link_rule, fp.interpolated);
 }
 
 template <class S>
@@ -1039,7 +1103,7 @@ void launch_reduce_loads(const GeomBuffers& gb, int with_topology, cudaStream_t 
     FluidParams fp = {};
     BoxDesc box = {1, 1, 1, 1};
     GeomArgs a = make_geom(g, fp, box, gb, nullptr);
-    k_reduce_loads<<<1, 256, 0, s>>>(a, with_topology);
+    k_reduce_loads<<<1, 1024, 0, s>>>(a, with_topology);
 }
 
 void launch_integrate(const GridDesc& g, const FluidParams& fp, const GeomBuffers& gb, float gravity_x,
