@@ -178,9 +178,27 @@ typedef struct bfx_body_state {
     double omega_body[3];
 } bfx_body_state;
 
+/* Hinge of an articulated wing segment: the child segment's frame is its
+ * parent's frame rotated about `axis` by
+ *   angle(t) = side * (bias + amplitude * sin(2 pi f t + phase))
+ * and moved to `origin` (f the wing-beat frequency, side +1 left / -1 right).
+ * Origin and axis are in the parent's (chord, span, normal) frame; the axis
+ * must be a unit vector.  On the right wing the axis's normal component is
+ * negated too (its normal is the mirror image of the left's, negated), so the
+ * two wings stay mirror images. */
+typedef struct bfx_joint {
+    float origin[3];
+    float axis[3];
+    float bias, amplitude, phase;
+    float _reserved;
+} bfx_joint;
+
 /* Articulated triangle mesh: vertex coordinates in the frame of their segment
- * (0 = body frame, relative to the body origin; 1 = left wing frame and
- * 2 = right wing frame, as (chord, span, normal) offsets from the wing root). */
+ * (0 = body frame, relative to the body origin; 1 / 2 = left / right wing
+ * frame, as (chord, span, normal) offsets from the wing root; with joints,
+ * 3 / 4 = left / right middle segment after joints[0] (the elbow) and 5 / 6 =
+ * left / right outer segment after joints[1] (the wrist), as offsets from the
+ * joint in the segment's frame). */
 typedef struct bfx_mesh {
     const float* local_vertices;    /* 3 * vertex_count */
     const uint8_t* vertex_segment;  /* vertex_count */
@@ -188,6 +206,8 @@ typedef struct bfx_mesh {
     const uint32_t* triangles;      /* 3 * triangle_count vertex indices */
     const uint8_t* triangle_part;   /* part id 1..63 per triangle */
     uint32_t triangle_count;
+    uint32_t joint_count;           /* 0, 1 (elbow) or 2 (elbow, wrist) */
+    const bfx_joint* joints;
 } bfx_mesh;
 
 /* ForceTorque (Sources/BirdFlowCore/Diagnostics.swift) plus step diagnostics. */

@@ -72,10 +72,16 @@ class BodyState(ct.Structure):
                 ("velocity", ct.c_double * 3), ("omega_body", ct.c_double * 3)]
 
 
+class Joint(ct.Structure):
+    _fields_ = [("origin", ct.c_float * 3), ("axis", ct.c_float * 3), ("bias", ct.c_float),
+                ("amplitude", ct.c_float), ("phase", ct.c_float), ("_reserved", ct.c_float)]
+
+
 class Mesh(ct.Structure):
     _fields_ = [("local_vertices", ct.POINTER(ct.c_float)), ("vertex_segment", ct.POINTER(ct.c_uint8)),
                 ("vertex_count", ct.c_uint32), ("triangles", ct.POINTER(ct.c_uint32)),
-                ("triangle_part", ct.POINTER(ct.c_uint8)), ("triangle_count", ct.c_uint32)]
+                ("triangle_part", ct.POINTER(ct.c_uint8)), ("triangle_count", ct.c_uint32),
+                ("joint_count", ct.c_uint32), ("joints", ct.POINTER(Joint))]
 
 
 class Loads(ct.Structure):

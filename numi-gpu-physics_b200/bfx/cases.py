@@ -162,3 +162,154 @@ def adjoint_plates(nx=96, ny=64, nz=64, span=20.0, chord=6.0, thickness=2.0, per
                            n_span=n_span, period=period, stroke_deg=stroke_deg, pitch_deg=pitch_deg,
                            viscosity=viscosity, storage=storage, link_rule=link_rule, sponge_width=6.0,
                            deviation_deg=deviation_deg)
+
+
+def _quad_strip(c0, c1, span, n_chord, n_span, chord_offset):
+    """Triangulated trapezoid in a segment frame: chord c0 at span 0 tapering
+    to c1 at `span`, leading edge at chord_offset * chord."""
+    verts, tris = [], []
+    for j in range(n_span + 1):
+        s = span * j / n_span
+        c = c0 + (c1 - c0) * j / n_span
+        for i in range(n_chord + 1):
+            verts.append((chord_offset * c + c * i / n_chord, s, 0.0))
+    w = n_chord + 1
+    for j in range(n_span):
+        for i in range(n_chord):
+            a = j * w + i
+            tris.append((a, a + 1, a + w))
+            tris.append((a + w + 1, a + w, a + 1))
+    return np.asarray(verts, np.float32), np.asarray(tris, np.uint32)
+
+
+def jointed_wing_mesh(spans=(24.0, 24.0, 24.0), chords=(12.0, 10.0, 8.0, 6.0), n_chord=6, n_span=8,
+                      elbow=(0.0, 20.0, 0.5), wrist=(0.0, 20.0, 1.0), axis=(0.0, 0.0, 1.0)):
+    """Two 3-segment flat wings (inner, middle, outer) hinged at the elbow and
+    the wrist, as jointed mesh segments 1-6.  spans: segment spans; chords:
+    chord at the root, elbow, wrist and tip; elbow / wrist: (bias deg,
+    amplitude deg, phase rad) of the hinge angle about `axis` (segment frame;
+    the default folds the wing in its own plane)."""
+    verts, tris, segs, parts = [], [], [], []
+    base = 0
+    for side in (0, 1):
+        for k in range(3):
+            v, t = _quad_strip(chords[k], chords[k + 1], spans[k], n_chord, n_span, -0.25)
+            verts.append(v)
+            tris.append(t + base)
+            seg = (1 + side) if k == 0 else (3 + 2 * (k - 1) + side)
+            segs.append(np.full(v.shape[0], seg, np.uint8))
+            parts.append(np.full(t.shape[0], 2 + side, np.uint8))
+            base += v.shape[0]
+    joints = []
+    for k, (bias_deg, amp_deg, phase) in enumerate((elbow, wrist)):
+        joints.append({"origin": (0.0, spans[k], 0.0), "axis": axis, "bias": math.radians(bias_deg),
+                       "amplitude": math.radians(amp_deg), "phase": phase})
+    return {"local": np.concatenate(verts), "segment": np.concatenate(segs), "tris": np.concatenate(tris),
+            "tri_part": np.concatenate(parts), "joints": joints}
+
+
+def jointed_plates(nx=96, ny=96, nz=64, spans=(10.0, 9.0, 8.0), chords=(8.0, 7.0, 6.0, 5.0), thickness=2.0,
+                   period=800.0, stroke_deg=50.0, pitch_deg=30.0, viscosity=0.02, storage=L.STORAGE_F32,
+                   collision=L.COLLISION_TRT, link_rule=L.LINK_LINEAR, n_chord=4, n_span=6):
+    """Flapping 3-segment plate wings (elbow and wrist folding in the wing
+    plane) about a fixed body point: the jointed-mesh parity case."""
+    op, om = _trt_rates(viscosity, 3.0 / 16.0)
+    rows = zero_bird_rows()
+    rows[0] = (4.0, 4.0, 4.0, 1.0)
+    rows[1] = (1.0, 1.0, 1.0, 0.0)
+    rows[2] = (sum(spans), chords[0], chords[-1], thickness)
+    rows[5] = (1.0 / period, float(f32(math.radians(stroke_deg))), 0.0, 0.0)
+    rows[6] = (float(f32(math.radians(pitch_deg))), float(f32(math.pi / 2.0)), 0.0, 0.0)
+    rows[8] = (0.0, 0.15, 0.0, 0.0)
+    mesh = jointed_wing_mesh(spans, chords, n_chord, n_span, elbow=(0.0, 20.0, 0.5), wrist=(0.0, 25.0, 1.0))
+    cfg = default_config(nx, ny, nz, omega_plus=op, omega_minus=om, face_bc=[L.BC_FARFIELD] * 6,
+                         geometry=L.GEOMETRY_MESH, wall_rule=L.WALL_INTERPOLATED, collision=collision,
+                         storage=storage, link_rule=link_rule, mesh_half_thickness=0.5 * thickness,
+                         sponge_width=6.0, sponge_strength=0.05)
+    body = ((nx / 2.0, ny / 2.0, nz / 2.0), (0.0, 0.0, 0.0, 1.0), (0.0, 0.0, 0.0), (0.0, 0.0, 0.0))
+    return cfg, rows, body, mesh
+
+
+def _ellipsoid_surface(radii, n_theta, n_phi):
+    """Latitude-longitude triangulation of an ellipsoid surface (body frame)."""
+    verts = [(0.0, 0.0, radii[2])]
+    for i in range(1, n_theta):
+        th = math.pi * i / n_theta
+        for j in range(n_phi):
+            ph = 2.0 * math.pi * j / n_phi
+            verts.append((radii[0] * math.sin(th) * math.cos(ph), radii[1] * math.sin(th) * math.sin(ph),
+                          radii[2] * math.cos(th)))
+    verts.append((0.0, 0.0, -radii[2]))
+    tris = []
+    for j in range(n_phi):
+        tris.append((0, 1 + j, 1 + (j + 1) % n_phi))
+    for i in range(n_theta - 2):
+        r0, r1 = 1 + i * n_phi, 1 + (i + 1) * n_phi
+        for j in range(n_phi):
+            a, b = r0 + j, r0 + (j + 1) % n_phi
+            c, d = r1 + j, r1 + (j + 1) % n_phi
+            tris.append((a, c, b))
+            tris.append((b, c, d))
+    south = len(verts) - 1
+    r0 = 1 + (n_theta - 2) * n_phi
+    for j in range(n_phi):
+        tris.append((r0 + j, south, r0 + (j + 1) % n_phi))
+    return np.asarray(verts, np.float32), np.asarray(tris, np.uint32)
+
+
+def articulated_bird(nx=768, ny=384, nz=384, storage=L.STORAGE_F16_DEVIATION, collision=L.COLLISION_RR3,
+                     inflow=0.04, viscosity=0.002, sponge_width=32.0, mass_ratio=50.0, seed=5,
+                     body_radii=(60.0, 18.0, 18.0), wing_spans=(50.0, 48.0, 42.0), chords=(36.0, 28.0, 20.0, 12.0),
+                     resolution=1.0, free_flight=True, period=16000.0, mach_limit=0.25):
+    """Synthetic articulated bird: ellipsoid body (semi-axes 60, 18, 18 cells),
+    two 3-segment wings (span 140, chord 36 -> 12) hinged at shoulder / elbow /
+    wrist with seeded sinusoidal joint angles, a tapered tail plate, about 150k
+    triangles; inflow u_x = 0.04, nu = 0.002, RR3, sponge 32, free 6-DOF body
+    with mass ratio 50 (mass = 50 x the displaced fluid mass of the body).
+    The wing-beat period (16000 steps) keeps the wing tip near lattice Mach
+    0.15 over the inflow (tip speed 2 pi A span / T); the safety ledger's Mach
+    limit is raised to 0.25 to leave room for the joint motion."""
+    rng = np.random.default_rng(seed)
+    op, om = _trt_rates(viscosity, 3.0 / 16.0)
+    n_th, n_ph = int(round(96 * resolution)), int(round(192 * resolution))
+    bv, bt = _ellipsoid_surface(body_radii, n_th, n_ph)
+    # tail: tapered plate behind the body (body frame), 2 cells thick
+    tv, tt = _quad_strip(30.0, 12.0, 40.0, int(24 * resolution), int(32 * resolution), -0.5)
+    tv = np.stack([-(tv[:, 1] + body_radii[0] - 6.0), tv[:, 0], np.zeros(len(tv))], axis=1).astype(np.float32)
+    ang = lambda lo, hi: float(rng.uniform(lo, hi))
+    wing = jointed_wing_mesh(wing_spans, chords, int(64 * resolution), int(140 * resolution),
+                             elbow=(ang(-5, 5), ang(15, 30), ang(0.3, 0.9)),
+                             wrist=(ang(-5, 5), ang(20, 35), ang(0.6, 1.4)))
+    verts = np.concatenate([bv, tv, wing["local"]])
+    nb, nt = len(bv), len(tv)
+    tris = np.concatenate([bt, tt + nb, wing["tris"] + nb + nt])
+    segs = np.concatenate([np.zeros(nb + nt, np.uint8), wing["segment"]])
+    parts = np.concatenate([np.full(len(bt), 1, np.uint8), np.full(len(tt), 4, np.uint8), wing["tri_part"]])
+    mesh = {"local": verts, "segment": segs, "tris": tris, "tri_part": parts, "joints": wing["joints"]}
+    volume = 4.0 / 3.0 * math.pi * body_radii[0] * body_radii[1] * body_radii[2]
+    mass = mass_ratio * volume
+    a, b, c = body_radii
+    inertia = (mass * (b * b + c * c) / 5.0, mass * (a * a + c * c) / 5.0, mass * (a * a + b * b) / 5.0)
+    rows = zero_bird_rows()
+    rows[0] = (float(a), float(b), float(c), float(mass))
+    rows[1] = inertia + (0.0,)
+    span = float(sum(wing_spans))
+    rows[2] = (span, chords[0], chords[-1], 2.0)
+    rows[3] = (0.0, 0.0, float(b * 0.6), 0.0)
+    rows[4] = (40.0, 15.0, 2.0, 0.0)
+    stroke = math.radians(ang(50, 65))
+    rows[5] = (1.0 / period, float(f32(stroke)), 0.0, 0.0)
+    rows[6] = (float(f32(math.radians(ang(20, 35)))), float(f32(math.pi / 2.0)), 0.0, 0.0)
+    half = (a + 40.0, span + b, span)
+    rows[7] = half + (float(math.sqrt(sum(h * h for h in half))),)
+    rows[8] = (float(2.0 * math.pi / period * stroke * span), float(mach_limit), 0.0, 0.0)
+    cfg = default_config(nx, ny, nz, omega_plus=op, omega_minus=om,
+                         face_bc=[L.BC_VELOCITY, L.BC_FARFIELD, L.BC_FARFIELD, L.BC_FARFIELD, L.BC_FARFIELD,
+                                  L.BC_FARFIELD],
+                         face_velocity=[(inflow, 0.0, 0.0)] + [(0.0, 0.0, 0.0)] * 5,
+                         far_field=[inflow, 0.0, 0.0, 1.0], geometry=L.GEOMETRY_MESH,
+                         wall_rule=L.WALL_INTERPOLATED, collision=collision, storage=storage,
+                         link_rule=L.LINK_LINEAR, mesh_half_thickness=1.0, sponge_width=sponge_width,
+                         sponge_strength=0.05, free_flight=1 if free_flight else 0)
+    body = ((nx * 0.4, ny / 2.0, nz / 2.0), (0.0, 0.0, 0.0, 1.0), (0.0, 0.0, 0.0), (0.0, 0.0, 0.0))
+    return cfg, rows, body, mesh

@@ -113,6 +113,16 @@ class Lattice:
             m.triangles = tris.ctypes.data_as(ct.POINTER(ct.c_uint32))
             m.triangle_part = parts.ctypes.data_as(ct.POINTER(ct.c_uint8))
             m.triangle_count = tris.shape[0]
+            joints = mesh.get("joints") or []
+            if joints:
+                arr = (L.Joint * len(joints))()
+                for j, d in enumerate(joints):
+                    arr[j].origin[:] = [float(v) for v in d["origin"]]
+                    arr[j].axis[:] = [float(v) for v in d["axis"]]
+                    arr[j].bias, arr[j].amplitude, arr[j].phase = d["bias"], d["amplitude"], d["phase"]
+                m.joint_count = len(joints)
+                m.joints = arr
+                self._mesh_joints = arr
             mesh_ptr = ct.byref(m)
             self._mesh_struct = m
         handle = ct.c_void_p()

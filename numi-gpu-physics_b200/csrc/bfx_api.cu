@@ -71,6 +71,8 @@ struct bfx_sim {
     // mesh
     float* mesh_local = nullptr;
     uint8_t* mesh_segment = nullptr;
+    bfx_joint* joints = nullptr;
+    int joint_count = 0;
     uint32_t* mesh_tris = nullptr;
     uint8_t* mesh_tri_part = nullptr;
     float4* mesh_pos = nullptr;
@@ -177,6 +179,8 @@ GeomBuffers geom_buffers(bfx_sim* s, uint8_t* mprev, uint8_t* mnext) {
     b.wall = s->wall;
     b.mesh_local = s->mesh_local;
     b.mesh_segment = s->mesh_segment;
+    b.joints = s->joints;
+    b.joint_count = s->joint_count;
     b.mesh_tris = s->mesh_tris;
     b.mesh_tri_part = s->mesh_tri_part;
     b.mesh_pos = s->mesh_pos;
@@ -404,8 +408,18 @@ int validate_config(const bfx_config* c, const bfx_bird* bird, const bfx_mesh* m
         for (uint32_t i = 0; i < 3 * mesh->triangle_count; ++i)
             if (mesh->triangles[i] >= mesh->vertex_count)
                 return fail(nullptr, BFX_ERR_INVALID_CONFIG, "triangle index out of range");
+        if (mesh->joint_count > 2 || (mesh->joint_count > 0 && mesh->joints == nullptr))
+            return fail(nullptr, BFX_ERR_INVALID_CONFIG, "a mesh has at most two joints (elbow, wrist)");
+        const uint32_t max_segment = 2 + 2 * mesh->joint_count;
         for (uint32_t i = 0; i < mesh->vertex_count; ++i)
-            if (mesh->vertex_segment[i] > 2) return fail(nullptr, BFX_ERR_INVALID_CONFIG, "vertex segment must be 0, 1 or 2");
+            if (mesh->vertex_segment[i] > max_segment)
+                return fail(nullptr, BFX_ERR_INVALID_CONFIG, "vertex segment exceeds the mesh's joint chain");
+        for (uint32_t j = 0; j < mesh->joint_count; ++j) {
+            const float* ax = mesh->joints[j].axis;
+            const float n2 = ax[0] * ax[0] + ax[1] * ax[1] + ax[2] * ax[2];
+            if (!(std::fabs(n2 - 1.0f) < 1.0e-4f))
+                return fail(nullptr, BFX_ERR_INVALID_CONFIG, "joint axis must be a unit vector");
+        }
         for (uint32_t i = 0; i < mesh->triangle_count; ++i)
             if (mesh->triangle_part[i] == 0 || mesh->triangle_part[i] > 63)
                 return fail(nullptr, BFX_ERR_INVALID_CONFIG, "triangle part must be 1...63");
@@ -429,11 +443,19 @@ float geometry_radius(const bfx_config* c, const bfx_bird* b, const bfx_mesh* m)
         float wing = root + w0[0] + std::fabs(w1[0]) + 0.5f * std::max(w0[1], w0[2]) + 0.5f * w0[3];
         return std::max(body, std::max(tail, wing)) + 2.0f * c->cell_size;
     }
+    // joint chain: a segment's vertices lie within the sum of the joint offsets
+    // before it plus their own offset from the joint
+    float chain[3] = {0.0f, 0.0f, 0.0f};
+    for (uint32_t j = 0; j < m->joint_count && j < 2; ++j) {
+        const float* o = m->joints[j].origin;
+        chain[j + 1] = chain[j] + std::sqrt(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
+    }
     float r = 0.0f;
     for (uint32_t i = 0; i < m->vertex_count; ++i) {
         const float* l = m->local_vertices + 3 * i;
         float d = std::sqrt(l[0] * l[0] + l[1] * l[1] + l[2] * l[2]);
-        if (m->vertex_segment[i] != 0) d += root;
+        const int seg = m->vertex_segment[i];
+        if (seg != 0) d += root + chain[(seg - 1) / 2];
         r = std::max(r, d);
     }
     return r + c->mesh_half_thickness + 2.0f * c->cell_size;
@@ -618,6 +640,12 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
             cudaMemcpyAsync(s->mesh_tris, mesh->triangles, (size_t)s->ntris * 3 * sizeof(uint32_t),
                             cudaMemcpyHostToDevice, s->stream);
             cudaMemcpyAsync(s->mesh_tri_part, mesh->triangle_part, s->ntris, cudaMemcpyHostToDevice, s->stream);
+            if (mesh->joint_count > 0) {
+                s->joint_count = (int)mesh->joint_count;
+                BFX_ALLOC(s->joints, (size_t)s->joint_count * sizeof(bfx_joint));
+                cudaMemcpyAsync(s->joints, mesh->joints, (size_t)s->joint_count * sizeof(bfx_joint),
+                                cudaMemcpyHostToDevice, s->stream);
+            }
         }
     }
 #undef BFX_ALLOC
@@ -1148,6 +1176,7 @@ int adjoint_scope(bfx_sim* s) {
     if (c.geometry != BFX_GEOMETRY_MESH || c.static_geometry)
         return fail(s, BFX_ERR_UNSUPPORTED, "the adjoint needs moving mesh geometry");
     if (c.free_flight) return fail(s, BFX_ERR_UNSUPPORTED, "the adjoint needs prescribed motion (no free flight)");
+    if (s->joint_count > 0) return fail(s, BFX_ERR_UNSUPPORTED, "the adjoint supports unjointed wing meshes");
     if (c.collision != BFX_COLLISION_TRT) return fail(s, BFX_ERR_UNSUPPORTED, "the adjoint supports the TRT collision");
     if (c.storage != BFX_STORAGE_F32 && c.storage != BFX_STORAGE_F64)
         return fail(s, BFX_ERR_UNSUPPORTED, "the adjoint supports F32 and F64 storage");

@@ -90,6 +90,44 @@ __global__ void k_prepare(const GeomArgs a, int init, float dt, float box_radius
     WingFrame l, r;
     make_wing_frame(1.0f, stroke, stroke_rate, deviation, deviation_rate, pitch, pitch_rate, bird, pos, orient, l);
     make_wing_frame(-1.0f, stroke, stroke_rate, deviation, deviation_rate, pitch, pitch_rate, bird, pos, orient, r);
+    // articulated segments: each joint rotates its parent's frame about the
+    // hinge axis and moves it to the joint (angles mirrored on the right wing)
+    for (int side = 0; side < 2 && a.b.joint_count > 0; ++side) {
+        const WingFrame& wf = side == 0 ? l : r;
+        const float sgn = side == 0 ? 1.0f : -1.0f;
+        V3 po = wf.root, pc = wf.chord, ps = wf.span, pn = wf.normal, pw = wf.rel, pu = v3(0.0f, 0.0f, 0.0f);
+        for (int j = 0; j < a.b.joint_count; ++j) {
+            const bfx_joint& jt = a.b.joints[j];
+            const V3 o = v3(po.x + pc.x * jt.origin[0] + ps.x * jt.origin[1] + pn.x * jt.origin[2],
+                            po.y + pc.y * jt.origin[0] + ps.y * jt.origin[1] + pn.y * jt.origin[2],
+                            po.z + pc.z * jt.origin[0] + ps.z * jt.origin[1] + pn.z * jt.origin[2]);
+            // the right frame's normal is the mirror image of the left's negated: its
+            // hinge takes the axis with the normal component negated (and the angle
+            // negated) so the two wings stay mirror images
+            const float a2 = sgn * jt.axis[2];
+            const V3 ax = v3(pc.x * jt.axis[0] + ps.x * jt.axis[1] + pn.x * a2,
+                             pc.y * jt.axis[0] + ps.y * jt.axis[1] + pn.y * a2,
+                             pc.z * jt.axis[0] + ps.z * jt.axis[1] + pn.z * a2);
+            const float ang = sgn * (jt.bias + jt.amplitude * bfx_sinf(phase + jt.phase));
+            const float rate = sgn * (af * jt.amplitude * bfx_cosf(phase + jt.phase));
+            const V3 cc = rotate_axis(pc, ax, ang), cs = rotate_axis(ps, ax, ang), cn = rotate_axis(pn, ax, ang);
+            const V3 om = v3(pw.x + ax.x * rate, pw.y + ax.y * rate, pw.z + ax.z * rate);
+            const V3 uu = pu + cross(pw, o - po);
+            SegmentFrame& f = st->seg[2 * j + side];
+            f.origin = f4(o, 0.0f);
+            f.chord = f4(cc, 0.0f);
+            f.span = f4(cs, 0.0f);
+            f.normal = f4(cn, 0.0f);
+            f.omega = f4(om, 0.0f);
+            f.uvel = f4(uu, 0.0f);
+            po = o;
+            pc = cc;
+            ps = cs;
+            pn = cn;
+            pw = om;
+            pu = uu;
+        }
+    }
     float4 o = qnormalize(orient);
     Prepared& p = st->prep;
     p.body_position = f4(pos, 0.0f);
@@ -298,6 +336,18 @@ __global__ void k_mesh_prepare(const GeomArgs a) {
         w = v3(p.body_position.x + r.x, p.body_position.y + r.y, p.body_position.z + r.z);
         V3 cr = cross(v3(p.omega_body_world), r);
         v = v3(p.linear_velocity.x + cr.x, p.linear_velocity.y + cr.y, p.linear_velocity.z + cr.z);
+    } else if (seg >= 3) {
+        // articulated segment: rigid motion of its own frame on top of the chain
+        const SegmentFrame& f = a.b.state->seg[seg - 3];
+        w = v3(f.origin.x + f.chord.x * l.x + f.span.x * l.y + f.normal.x * l.z,
+               f.origin.y + f.chord.y * l.x + f.span.y * l.y + f.normal.y * l.z,
+               f.origin.z + f.chord.z * l.x + f.span.z * l.y + f.normal.z * l.z);
+        V3 rb = v3(w.x - p.body_position.x, w.y - p.body_position.y, w.z - p.body_position.z);
+        V3 cr = cross(v3(p.omega_body_world), rb);
+        V3 rr = v3(w.x - f.origin.x, w.y - f.origin.y, w.z - f.origin.z);
+        V3 cw = cross(v3(f.omega), rr);
+        v = v3(p.linear_velocity.x + cr.x + cw.x + f.uvel.x, p.linear_velocity.y + cr.y + cw.y + f.uvel.y,
+               p.linear_velocity.z + cr.z + cw.z + f.uvel.z);
     } else {
         const float4* fr = seg == 1 ? &p.left_root : &p.right_root;
         w = v3(fr[0].x + fr[1].x * l.x + fr[2].x * l.y + fr[3].x * l.z,

@@ -66,6 +66,8 @@ struct GeomBuffers {
     // mesh
     const float* mesh_local;        // 3 per vertex
     const uint8_t* mesh_segment;
+    const bfx_joint* joints;        // elbow, wrist (device copy)
+    int joint_count;
     const uint32_t* mesh_tris;
     const uint8_t* mesh_tri_part;
     float4* mesh_pos;

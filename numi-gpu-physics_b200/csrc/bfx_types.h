@@ -39,6 +39,13 @@ struct Prepared {
     float4 right_root, right_chord, right_span, right_normal, right_angular_velocity;
 };
 
+// Frame of an articulated wing segment after the elbow / wrist joints:
+// origin, axes, angular velocity relative to the body (world) and the velocity
+// of the origin relative to the body.
+struct SegmentFrame {
+    float4 origin, chord, span, normal, omega, uvel;
+};
+
 // Device-resident per-simulation state updated by the single-thread kernels.
 struct DeviceState {
     uint64_t step;                 // completed steps
@@ -62,6 +69,7 @@ struct DeviceState {
     double power_lattice;          // last step: sum over cut links of F_link . u_wall (lattice units)
     uint32_t stream_error;         // nonzero: a staged-kernel pipeline wait timed out (1 producer, 2 consumer)
     uint32_t _pad1;
+    SegmentFrame seg[4];           // mesh segments 3..6: left / right middle, left / right outer
 };
 
 // Time-averaged load objective of the adjoint (one per simulation; disabled

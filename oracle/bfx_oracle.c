@@ -1084,6 +1084,86 @@ void or_mesh_prepare_articulated(const or_prepared* prep, const float* local, co
     }
 }
 
+void or_prepare_segments(const or_bird* bird, const or_prepared* prep, const or_joint* joints, int njoints,
+                         float time, or_segment* out) {
+    float af = 2.0f * 3.14159265358979323846f * bird->wing_kinematics0.v[0];
+    float phase = af * time;
+    for (int side = 0; side < 2 && njoints > 0; ++side) {
+        const or_f4* fr = side == 0 ? &prep->left_root : &prep->right_root;
+        float sgn = side == 0 ? 1.0f : -1.0f;
+        float po[3], pc[3], ps[3], pn[3], pw[3], pu[3] = {0.0f, 0.0f, 0.0f};
+        for (int k = 0; k < 3; ++k) {
+            po[k] = fr[0].v[k];
+            pc[k] = fr[1].v[k];
+            ps[k] = fr[2].v[k];
+            pn[k] = fr[3].v[k];
+            pw[k] = fr[4].v[k];
+        }
+        for (int j = 0; j < njoints; ++j) {
+            const or_joint* jt = &joints[j];
+            float o[3], ax[3], cc[3], cs[3], cn[3], om[3], d[3], cr[3], uu[3];
+            /* the right frame's normal is the mirror of the left's negated: negate
+             * the axis's normal component there (with the angle) to keep the mirror */
+            float a2 = sgn * jt->axis[2];
+            for (int k = 0; k < 3; ++k) {
+                o[k] = po[k] + pc[k] * jt->origin[0] + ps[k] * jt->origin[1] + pn[k] * jt->origin[2];
+                ax[k] = pc[k] * jt->axis[0] + ps[k] * jt->axis[1] + pn[k] * a2;
+            }
+            float ang = sgn * (jt->bias + jt->amplitude * bfx_sinf(phase + jt->phase));
+            float rate = sgn * (af * jt->amplitude * bfx_cosf(phase + jt->phase));
+            rotate_axis(pc, ax, ang, cc);
+            rotate_axis(ps, ax, ang, cs);
+            rotate_axis(pn, ax, ang, cn);
+            for (int k = 0; k < 3; ++k) {
+                om[k] = pw[k] + ax[k] * rate;
+                d[k] = o[k] - po[k];
+            }
+            cross3(pw, d, cr);
+            for (int k = 0; k < 3; ++k) uu[k] = pu[k] + cr[k];
+            or_segment* f = &out[2 * j + side];
+            for (int k = 0; k < 3; ++k) {
+                f->origin[k] = o[k];
+                f->chord[k] = cc[k];
+                f->span[k] = cs[k];
+                f->normal[k] = cn[k];
+                f->omega[k] = om[k];
+                f->uvel[k] = uu[k];
+            }
+            f->origin[3] = f->chord[3] = f->span[3] = f->normal[3] = f->omega[3] = f->uvel[3] = 0.0f;
+            memcpy(po, o, sizeof(o));
+            memcpy(pc, cc, sizeof(cc));
+            memcpy(ps, cs, sizeof(cs));
+            memcpy(pn, cn, sizeof(cn));
+            memcpy(pw, om, sizeof(om));
+            memcpy(pu, uu, sizeof(uu));
+        }
+    }
+}
+
+void or_mesh_prepare_segments(const or_prepared* prep, const or_segment* segs, const float* local,
+                              const uint8_t* segment, uint32_t nverts, float v2l, float* pos, float* vel) {
+    or_mesh_prepare_articulated(prep, local, segment, nverts, v2l, pos, vel);
+    for (uint32_t i = 0; i < nverts; ++i) {
+        if (segment[i] < 3) continue;
+        const or_segment* f = &segs[segment[i] - 3];
+        const float* l = local + 3 * i;
+        float w[3], rb[3], rr[3], cr[3], cw[3];
+        for (int k = 0; k < 3; ++k) w[k] = f->origin[k] + f->chord[k] * l[0] + f->span[k] * l[1] + f->normal[k] * l[2];
+        for (int k = 0; k < 3; ++k) {
+            rb[k] = w[k] - prep->body_position.v[k];
+            rr[k] = w[k] - f->origin[k];
+        }
+        cross3(prep->omega_body_world.v, rb, cr);
+        cross3(f->omega, rr, cw);
+        for (int k = 0; k < 3; ++k) {
+            pos[4 * i + k] = w[k];
+            vel[4 * i + k] = (prep->linear_velocity.v[k] + cr[k] + cw[k] + f->uvel[k]) * v2l;
+        }
+        pos[4 * i + 3] = 0.0f;
+        vel[4 * i + 3] = 0.0f;
+    }
+}
+
 static void tri_vertices(const float* pos, const uint32_t* tris, uint32_t t, float a[3], float b[3], float c[3]) {
     uint32_t ia = tris[3 * t], ib = tris[3 * t + 1], ic = tris[3 * t + 2];
     memcpy(a, pos + 4 * ia, 12);

@@ -137,6 +137,18 @@ int64_t or_enumerate_links(const or_params* p, const uint8_t* mprev, const uint8
 /* ---- triangle mesh -------------------------------------------------- */
 /* Articulated rigid-segment vertices: local (chord, span, normal) coords per
  * vertex and segment 0 = body frame, 1 = left wing, 2 = right wing. */
+/* Wing joints (bfx_joint) and the frames of the jointed segments 3..6:
+ * the elbow / wrist hinge rotates its parent's frame about the hinge axis by
+ * side * (bias + amplitude sin(phase_t + phase)) and moves it to the joint.
+ * This is the library's extension for the multi-segment wings of the north
+ * star's articulated bird; the reference drives its wings as one rigid frame
+ * each (makeWingFrame, BF.metal:611-684). */
+typedef struct or_joint { float origin[3], axis[3], bias, amplitude, phase, reserved; } or_joint;
+typedef struct or_segment { float origin[4], chord[4], span[4], normal[4], omega[4], uvel[4]; } or_segment;
+void or_prepare_segments(const or_bird* bird, const or_prepared* prep, const or_joint* joints, int njoints,
+                         float time, or_segment* out /* 4: left / right middle, left / right outer */);
+void or_mesh_prepare_segments(const or_prepared* prep, const or_segment* segs, const float* local,
+                              const uint8_t* segment, uint32_t nverts, float v2l, float* pos, float* vel);
 void or_mesh_prepare_articulated(const or_prepared* prep, const float* local /*3 per vertex*/,
                                  const uint8_t* segment, uint32_t nverts, float v2l,
                                  float* pos /*4 per vertex*/, float* vel /*4 per vertex*/);

@@ -115,6 +115,8 @@ def lib():
         L.or_enumerate_links.restype = ct.c_int64
         L.or_enumerate_links.argtypes = [P(Params), u8p, u8p, P(ct.c_uint32), u8p, ct.c_int64]
         L.or_mesh_prepare_articulated.argtypes = [P(Prepared), fp, u8p, ct.c_uint32, ct.c_float, fp, fp]
+        L.or_prepare_segments.argtypes = [P(Bird), P(Prepared), fp, ct.c_int, ct.c_float, fp]
+        L.or_mesh_prepare_segments.argtypes = [P(Prepared), fp, fp, u8p, ct.c_uint32, ct.c_float, fp, fp]
         L.or_mesh_rasterize.argtypes = [P(Params), fp, P(ct.c_uint32), ct.c_uint32, ct.c_float, P(ct.c_uint64)]
         L.or_mesh_resolve.argtypes = [P(Params), fp, fp, P(ct.c_uint32), u8p, ct.c_uint32, ct.c_float,
                                       P(ct.c_uint64), u8p, fp]
@@ -298,8 +300,19 @@ class OracleSim:
             nv = m["local"].shape[0]
             self.mesh_pos = np.zeros(4 * nv, np.float32)
             self.mesh_vel = np.zeros(4 * nv, np.float32)
-            L.or_mesh_prepare_articulated(ct.byref(self.prep), fptr(m["local"]), u8ptr(m["segment"]), nv,
-                                          self.p.v2l, fptr(self.mesh_pos), fptr(self.mesh_vel))
+            joints = m.get("joints") or []
+            if joints:
+                # or_joint: origin[3], axis[3], bias, amplitude, phase, reserved
+                jarr = np.array([list(j["origin"]) + list(j["axis"]) + [j["bias"], j["amplitude"], j["phase"], 0.0]
+                                 for j in joints], dtype=np.float32).ravel()
+                segs = np.zeros(4 * 24, np.float32)
+                L.or_prepare_segments(ct.byref(self.bird), ct.byref(self.prep), fptr(jarr), len(joints), time,
+                                      fptr(segs))
+                L.or_mesh_prepare_segments(ct.byref(self.prep), fptr(segs), fptr(m["local"]), u8ptr(m["segment"]),
+                                           nv, self.p.v2l, fptr(self.mesh_pos), fptr(self.mesh_vel))
+            else:
+                L.or_mesh_prepare_articulated(ct.byref(self.prep), fptr(m["local"]), u8ptr(m["segment"]), nv,
+                                              self.p.v2l, fptr(self.mesh_pos), fptr(self.mesh_vel))
             self.keys = np.full(self.n, np.iinfo(np.uint64).max, np.uint64)
             ntri = m["tris"].shape[0]
             tris = m["tris"].astype(np.uint32).ravel()

@@ -228,6 +228,47 @@ def test_flapping_plate_mesh_matches_oracle(link_rule):
     assert osim.loads.covered_count + osim.loads.uncovered_count > 0
 
 
+@pytest.mark.parametrize("link_rule", [L.LINK_LINEAR, L.LINK_RAY_ROOT])
+def test_jointed_wing_mesh_matches_oracle(link_rule):
+    """3-segment wings hinged at elbow and wrist (mesh segments 1-6): masks,
+    cut links and covered / uncovered counts bit-exact, populations and loads
+    within tolerance, every step."""
+    cfg, rows, body, mesh = cases.jointed_plates(link_rule=link_rule)
+    assert set(mesh["segment"].tolist()) == {1, 2, 3, 4, 5, 6}
+    lat, osim = make_pair(cfg, rows, body, mesh)
+    assert np.array_equal(lat.mask(), osim.mcur)
+    for step in range(8):
+        lat.advance(1)
+        osim.step()
+        assert np.array_equal(lat.mask(), osim.mcur), f"mask step {step + 1}"
+        compare_pops(lat, osim, f"jointed step {step + 1}")
+        compare_loads(lat, osim, f"jointed step {step + 1}")
+        cell, d, q = lat.links()
+        oc, od = oracle_links(osim)
+        assert np.array_equal(link_set(cell, d), link_set(oc, od)), f"links step {step + 1}"
+    assert osim.loads.covered_count + osim.loads.uncovered_count > 0
+
+
+def test_articulated_bird_free_flight_matches_oracle():
+    """Config-5 family at reduced size: ellipsoid body, tail plate and two
+    jointed wings as one mesh, free 6-DOF body, RR3, velocity inlet."""
+    cfg, rows, body, mesh = cases.articulated_bird(nx=160, ny=128, nz=96, storage=L.STORAGE_F32,
+                                                   body_radii=(16.0, 5.0, 5.0), wing_spans=(12.0, 11.0, 10.0),
+                                                   chords=(10.0, 8.0, 6.0, 4.0), resolution=0.25,
+                                                   sponge_width=8.0, viscosity=0.01)
+    assert set(mesh["segment"].tolist()) == {0, 1, 2, 3, 4, 5, 6}
+    lat, osim = make_pair(cfg, rows, body, mesh)
+    for step in range(3):
+        lat.advance(1)
+        osim.step()
+        assert np.array_equal(lat.mask(), osim.mcur), f"mask step {step + 1}"
+        compare_pops(lat, osim, f"bird step {step + 1}")
+        compare_loads(lat, osim, f"bird step {step + 1}")
+    lat.advance(20)
+    assert np.all(np.isfinite(lat.populations()))
+    assert lat.safety().event[2] == 0
+
+
 def test_fast_math_fp32_stays_within_tolerance_of_oracle():
     """fast_math (the reference's SimulationConfiguration.fastMath) contracts
     a*b+c into FMA and uses one reciprocal for the velocity: no longer

@@ -206,3 +206,34 @@ def test_oracle_twins_of_every_case_step():
         osim.advance(2)
         assert np.all(np.isfinite(osim.pa))
         assert osim.mcur.any()
+
+
+def test_jointed_wing_chain_stays_connected_at_the_joints():
+    """Elbow and wrist frames (or_prepare_segments): the joint point of each
+    segment coincides with the matching point of its parent at every phase, and
+    the chain mirrors between the wings."""
+    import bfx.cases as cases
+    from helpers import oracle_twin
+    spans, chords = (10.0, 9.0, 8.0), (8.0, 7.0, 6.0, 5.0)
+    cfg, rows, body, mesh = cases.jointed_plates(nx=96, ny=96, nz=64, spans=spans, chords=chords, n_chord=4,
+                                                 n_span=6)
+    osim = oracle_twin(cfg, rows, body, mesh)
+    local, seg = mesh["local"], mesh["segment"]
+    for steps in (0, 37, 150):
+        osim.advance(steps)
+        pos = osim.mesh_pos.reshape(-1, 4)[:, :3]
+        for side in (0, 1):
+            chain = [1 + side, 3 + side, 5 + side]
+            for k in range(2):
+                parent, child = chain[k], chain[k + 1]
+                tip = np.where((seg == parent) & np.isclose(local[:, 1], spans[k]) & np.isclose(local[:, 0], 0.0))[0]
+                root = np.where((seg == child) & np.isclose(local[:, 1], 0.0) & np.isclose(local[:, 0], 0.0))[0]
+                assert len(tip) == 1 and len(root) == 1
+                assert np.max(np.abs(pos[tip[0]] - pos[root[0]])) < 1e-4
+        # mirror symmetry of the two wings about the body's x-z plane (y -> 2 y_c - y)
+        yc = body[0][1]
+        left = pos[seg == 5]
+        right = pos[seg == 6]
+        mirrored = right.copy()
+        mirrored[:, 1] = 2.0 * yc - mirrored[:, 1]
+        assert np.max(np.abs(left - mirrored)) < 1e-3
