@@ -18,6 +18,8 @@ Workloads (lattice units):
                      zero-gradient outlet / periodic y,z (default)
   flapping_plates    512x256x256, two 64x12x2 plates as 2x8192 triangles,
                      stroke 60 sin, pitch 45 cos, T = 4000, nu 0.004, TRT
+  articulated_bird   768x384x384, ellipsoid body + tail + two 3-segment wings
+                     (~145k triangles), free flight, RR3
   shear_wave         64^3 periodic, nu 0.01, magic 1/4 (L2-resident)
 Multi-GPU: the step does not shard here (one GPU per lattice), so N GPUs run N
 independent replicas; ``value`` is the aggregate and ``scaling`` is weak.
@@ -26,6 +28,8 @@ On one GPU the line also carries
   ``variants``  FP32 / FP16-deviation / BF16-deviation storage on the flapping
                 plates (512x256x256, TRT): GLUPS, roofline fraction, and the
                 force averaged over the first stroke period against FP64;
+  ``articulated``  the articulated bird at 768x384x384 in FP16-deviation
+                storage: GLUPS and the share of the step outside the fused kernel;
   ``adjoint``   the discrete adjoint on the plates at 256x128x128 over one
                 period: lift and power gradients, cost against a forward pass,
                 central differences (h = 1e-3 rad) and FP32 vs FP64 gradients
@@ -82,6 +86,21 @@ def build_case(name: str, storage: int, collision: str | None = None):
                 f"stroke 60deg sin, pitch 45deg cos, T=4000, nu=0.004, {collision or 'trt'}, ray-root links "
                 f"rebuilt each step")
         collision = collision or "trt"
+    elif name == "articulated_bird":
+        kw = {}
+        if LATTICE_OVERRIDE:
+            nx, ny, nz = LATTICE_OVERRIDE
+            f = nx / 768.0
+            kw = dict(nx=nx, ny=ny, nz=nz, body_radii=(60.0 * f, 18.0 * f, 18.0 * f),
+                      wing_spans=(50.0 * f, 48.0 * f, 42.0 * f), chords=(36.0 * f, 28.0 * f, 20.0 * f, 12.0 * f),
+                      resolution=max(f, 0.25), sponge_width=32.0 * f)
+        if collision:
+            kw["collision"] = coll_id[collision]
+        cfg, rows, body, mesh = cases.articulated_bird(storage=storage, **kw)
+        desc = (f"articulated_bird {cfg.nx}x{cfg.ny}x{cfg.nz} ellipsoid body + tail + two 3-segment wings "
+                f"(shoulder/elbow/wrist, {mesh['tris'].shape[0]} triangles), free 6-DOF flight, inflow 0.04, "
+                f"nu=0.002, {collision or 'rr3'}, sponge 32, linear links rebuilt each step")
+        collision = collision or "rr3"
     elif name == "shear_wave":
         n = LATTICE_OVERRIDE[0] if LATTICE_OVERRIDE else 64
         cfg, rows, body, mesh = cases.shear_wave(n=n, viscosity=0.01, magic=0.25, axis="z", storage=storage,
@@ -271,6 +290,29 @@ def storage_forms(device, steps=200, warmup=5):
                    "roofline_frac": ach / peak, "speedup_vs_f32": rate / base,
                    "cycle_mean_force_error_vs_f64": err}
     return out
+
+
+def articulated_measure(device, steps=100, warmup=5):
+    """The articulated bird (768x384x384, RR3, FP16-deviation storage, free
+    6-DOF flight, ~145k triangles on shoulder / elbow / wrist segments):
+    whole-step GLUPS, the fused kernel's roofline fraction and the share of the
+    step spent outside it (geometry, links, loads, body)."""
+    import bfx._lib as L
+    peak, _ = measured_peak()
+    st = L.STORAGE_F16_DEVIATION
+    lat, cfg, desc, _ = make_lattice("articulated_bird", st, device)
+    cells = cfg.nx * cfg.ny * cfg.nz
+    ms, launches, kms, kl = time_steps(lat, steps, warmup)
+    fluid = cells - int(np.count_nonzero(lat.mask()))
+    body = lat.body()
+    lat.close()
+    kernel_s = kms / max(kl, 1) / 1000.0
+    ach = fluid * 38 * L.STORAGE_BYTES[st] / kernel_s / 1e9
+    step_ms = ms / steps
+    return {"workload": desc, "storage": L.STORAGE_NAMES[st], "steps": steps, "value": cells * steps / (ms / 1e3) / 1e9,
+            "unit": "GLUPS", "ms_per_step": step_ms, "kernel_ms": kernel_s * 1e3, "achieved_gbs": ach,
+            "roofline_frac": ach / peak, "outside_kernel_share": max(0.0, 1.0 - kernel_s * 1e3 / step_ms),
+            "gpu_launches": launches, "body_position_after": [float(x) for x in body.position]}
 
 
 def adjoint_measure(device):
@@ -510,6 +552,8 @@ def main():
 
     if rank == 0 and world == 1 and not args.no_variants:
         line["variants"] = storage_forms(local)
+    if rank == 0 and world == 1 and not args.no_variants:
+        line["articulated"] = articulated_measure(local)
     if rank == 0 and world == 1 and not args.no_adjoint:
         line["adjoint"] = adjoint_measure(local)
 

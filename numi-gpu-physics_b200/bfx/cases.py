@@ -271,11 +271,16 @@ def articulated_bird(nx=768, ny=384, nz=384, storage=L.STORAGE_F16_DEVIATION, co
     limit is raised to 0.25 to leave room for the joint motion."""
     rng = np.random.default_rng(seed)
     op, om = _trt_rates(viscosity, 3.0 / 16.0)
+    stroke = math.radians(float(rng.uniform(50, 65)))
     n_th, n_ph = int(round(96 * resolution)), int(round(192 * resolution))
     bv, bt = _ellipsoid_surface(body_radii, n_th, n_ph)
-    # tail: tapered plate behind the body (body frame), 2 cells thick
-    tv, tt = _quad_strip(30.0, 12.0, 40.0, int(24 * resolution), int(32 * resolution), -0.5)
-    tv = np.stack([-(tv[:, 1] + body_radii[0] - 6.0), tv[:, 0], np.zeros(len(tv))], axis=1).astype(np.float32)
+    # tail: tapered plate behind the body (body frame), 2 cells thick, scaled
+    # with the body (length 2/3 of the semi-axis, width 1/2 -> 1/5 of it)
+    a0 = body_radii[0]
+    tail_len = 2.0 * a0 / 3.0
+    tv, tt = _quad_strip(0.5 * a0, 0.2 * a0, tail_len, max(2, int(24 * resolution)), max(2, int(32 * resolution)),
+                         -0.5)
+    tv = np.stack([-(tv[:, 1] + a0 - 0.1 * a0), tv[:, 0], np.zeros(len(tv))], axis=1).astype(np.float32)
     ang = lambda lo, hi: float(rng.uniform(lo, hi))
     wing = jointed_wing_mesh(wing_spans, chords, int(64 * resolution), int(140 * resolution),
                              elbow=(ang(-5, 5), ang(15, 30), ang(0.3, 0.9)),
@@ -295,12 +300,12 @@ def articulated_bird(nx=768, ny=384, nz=384, storage=L.STORAGE_F16_DEVIATION, co
     rows[1] = inertia + (0.0,)
     span = float(sum(wing_spans))
     rows[2] = (span, chords[0], chords[-1], 2.0)
-    rows[3] = (0.0, 0.0, float(b * 0.6), 0.0)
-    rows[4] = (40.0, 15.0, 2.0, 0.0)
-    stroke = math.radians(ang(50, 65))
+    rows[3] = (0.0, 0.0, float(0.6 * b), 0.0)
+    rows[4] = (float(tail_len), float(0.25 * a0), 2.0, 0.0)
     rows[5] = (1.0 / period, float(f32(stroke)), 0.0, 0.0)
     rows[6] = (float(f32(math.radians(ang(20, 35)))), float(f32(math.pi / 2.0)), 0.0, 0.0)
-    half = (a + 40.0, span + b, span)
+    root_y = 0.6 * b
+    half = (a + tail_len, span + root_y + 1.0, span * math.sin(stroke) + b)
     rows[7] = half + (float(math.sqrt(sum(h * h for h in half))),)
     rows[8] = (float(2.0 * math.pi / period * stroke * span), float(mach_limit), 0.0, 0.0)
     cfg = default_config(nx, ny, nz, omega_plus=op, omega_minus=om,
