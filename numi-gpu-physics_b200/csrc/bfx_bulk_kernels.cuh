@@ -8,6 +8,10 @@
 namespace bfx {
 namespace BFX_VARIANT {
 
+#ifdef BFX_CONTRACTED
+#include "bfx_pair_math.cuh"
+#endif
+
 // Collision (BF.metal:2907-3174).  Directions are processed in opposite pairs
 // (q odd, q+1 = opp(q)): the equilibrium, TRT and regularized terms of the pair
 // share their even parts and negate their odd parts, and in IEEE arithmetic
@@ -60,6 +64,16 @@ __device__ __forceinline__ void collide(const R (&f)[19], R rho, R ux, R uy, R u
         R aYzz = uy * dsz + R(2) * uz * odz;
         const R one_minus = R(1) - omega_p;
         R scale = R(1);
+        // Positivity admission (BF.metal:3035-3052).  The floor test runs on
+        // every population; the admissible scale, which only a population below
+        // its floor changes, is evaluated afterwards in the same direction order
+        // for the rare cell that has one.
+        bool need = false;
+        auto below = [&](R fe, R cand) {
+            R fl = R(1.0e-6) * (fe > R(0) ? fe : R(0));
+            R floor_ = R(1.0e-12) > fl ? R(1.0e-12) : fl;
+            need = need || cand < floor_;
+        };
         auto admit = [&](R fe, R cand) {
             R fl = R(1.0e-6) * (fe > R(0) ? fe : R(0));
             R floor_ = R(1.0e-12) > fl ? R(1.0e-12) : fl;
@@ -77,7 +91,7 @@ __device__ __forceinline__ void collide(const R (&f)[19], R rho, R ux, R uy, R u
             const R contraction = h * dsx + h * dsy + h * dsz;
             const R rne = Lat<R>::w0 * R(4.5) * contraction;
             post[0] = feqv[0] + one_minus * rne;
-            admit(feqv[0], post[0]);
+            below(feqv[0], post[0]);
         }
 #pragma unroll
         for (int q = 1; q < 19; q += 2) {
@@ -113,17 +127,25 @@ __device__ __forceinline__ void collide(const R (&f)[19], R rho, R ux, R uy, R u
             }
             post[q] = feqv[q] + one_minus * rq;
             post[q + 1] = feqv[q + 1] + one_minus * ro;
-            admit(feqv[q], post[q]);
-            admit(feqv[q + 1], post[q + 1]);
+            below(feqv[q], post[q]);
+            below(feqv[q + 1], post[q + 1]);
+        }
+        if (need) {
+#pragma unroll
+            for (int q = 0; q < 19; ++q) admit(feqv[q], post[q]);
         }
         if (scale < R(1)) {
             activation = 1.0f;
             restriction = (float)(R(1) - scale);
 #pragma unroll
             for (int q = 0; q < 19; ++q) post[q] = feqv[q] + scale * (post[q] - feqv[q]);
+        } else if (scale == R(1)) {
+            // 1 * d == d exactly, but feq + (cand - feq) equals cand only up to
+            // rounding, so the rest of the reference expression stays
+#pragma unroll
+            for (int q = 0; q < 19; ++q) post[q] = feqv[q] + (post[q] - feqv[q]);
         } else {
-            // scale == 1: feq + 1 * (cand - feq) == cand only up to rounding, so keep
-            // the reference expression
+            // NaN scale (a non-finite equilibrium): the reference expression as is
 #pragma unroll
             for (int q = 0; q < 19; ++q) post[q] = feqv[q] + scale * (post[q] - feqv[q]);
         }
@@ -282,7 +304,7 @@ __device__ __forceinline__ void finish_cell(const BulkArgs& a, uint32_t gid, int
 // uncovered cells (flagged in the mask) are left to k_bulk_rare.
 // ---------------------------------------------------------------------------
 template <class S, int REP_S, int COLL, int CAPTURE>
-__global__ void __launch_bounds__(256, sizeof(typename S::R) == 8 ? 1 : (COLL == BFX_COLLISION_TRT ? 4 : 2))
+__global__ void __launch_bounds__(256, sizeof(typename S::R) == 8 ? 1 : (COLL == BFX_COLLISION_TRT_LIMITER ? 2 : 4))
     k_bulk(const BulkArgs a) {
     using R = typename S::R;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -295,19 +317,29 @@ __global__ void __launch_bounds__(256, sizeof(typename S::R) == 8 ? 1 : (COLL ==
         (uint32_t)(x + 1) + (uint32_t)a.g.px * ((uint32_t)(y + 1) + (uint32_t)a.g.py * (uint32_t)(z + 1));
     R f[19];
     load_cell<S, REP_S>(a, pid, f);
-    R rho, ux, uy, uz;
-    moments<R>(f, rho, ux, uy, uz);
-    if (CAPTURE == 2) {
-        // adjoint tape: the collision Jacobian depends on the pre-collision moments only
-        R* t = (R*)a.tape + 4 * (size_t)gid;
-        t[0] = rho;
-        t[1] = ux;
-        t[2] = uy;
-        t[3] = uz;
-    }
     R post[19];
     float activation = 0.0f, restriction = 0.0f;
-    collide<R, COLL>(f, rho, ux, uy, uz, (R)a.fp.omega_p, (R)a.fp.omega_m, post, activation, restriction);
+#ifdef BFX_CONTRACTED
+    if constexpr (COLL == BFX_COLLISION_RR3 || COLL == BFX_COLLISION_REGULARIZED) {
+        float act[1] = {0.0f}, res[1] = {0.0f};
+        collide_pairs<R, COLL>(f, a.fp.omega_p, post, act, res);
+        activation = act[0];
+        restriction = res[0];
+    } else
+#endif
+    {
+        R rho, ux, uy, uz;
+        moments<R>(f, rho, ux, uy, uz);
+        if (CAPTURE == 2) {
+            // adjoint tape: the collision Jacobian depends on the pre-collision moments only
+            R* t = (R*)a.tape + 4 * (size_t)gid;
+            t[0] = rho;
+            t[1] = ux;
+            t[2] = uy;
+            t[3] = uz;
+        }
+        collide<R, COLL>(f, rho, ux, uy, uz, (R)a.fp.omega_p, (R)a.fp.omega_m, post, activation, restriction);
+    }
     finish_cell<S, COLL>(a, gid, x, y, z, CAPTURE == 1, post, activation, restriction);
     store_cell<S, REP_S>(a, pid, post);
 }

@@ -330,9 +330,14 @@ bool encode_population_map(CUtensorMap* map, void* pops, int storage, int64_t px
            CUDA_SUCCESS;
 }
 
-void prepare_stream(int storage) {
+bool staged_collision(int collision) {
+    return collision == BFX_COLLISION_TRT || collision == BFX_COLLISION_RR3 ||
+           collision == BFX_COLLISION_REGULARIZED;
+}
+
+void prepare_stream(int storage, int collision) {
     const GridDesc g = {};
-    for (int rep = 0; rep < 2; ++rep) launch_stream_fast(storage, rep, g, nullptr, nullptr, 0, nullptr);
+    for (int rep = 0; rep < 2; ++rep) launch_stream_fast(storage, collision, rep, g, nullptr, nullptr, 0, nullptr);
 }
 
 void launch_bulk(int storage, int collision, int rep_s, const GridDesc& g, const FluidParams& fp,
@@ -351,8 +356,8 @@ void launch_bulk(int storage, int collision, int rep_s, const GridDesc& g, const
     // FP64 and the regularized operators k_bulk was measured as fast or faster:
     // their collision issue time, not load latency, bounds the step.
     const bool staged = storage == BFX_STORAGE_F16_DEVIATION || storage == BFX_STORAGE_BF16_DEVIATION;
-    if (part == 0 && b.tmap && staged && collision == BFX_COLLISION_TRT && capture != 2) {
-        launch_stream_fast(storage, rep_s, g, &a, (const CUtensorMap*)b.tmap, b.sm_count, s);
+    if (part == 0 && b.tmap && staged && staged_collision(collision) && capture != 2) {
+        launch_stream_fast(storage, collision, rep_s, g, &a, (const CUtensorMap*)b.tmap, b.sm_count, s);
         return;
     }
     if (contracted) {

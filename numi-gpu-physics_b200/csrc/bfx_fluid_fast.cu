@@ -9,10 +9,10 @@
 
 namespace bfx {
 
-void launch_stream_fast(int storage, int rep_s, const GridDesc& g, const BulkArgs* a, const CUtensorMap* map,
-                        int sm_count, cudaStream_t s) {
-    if (storage == BFX_STORAGE_BF16_DEVIATION) fast::stream_s<StoreBF16Dev>(rep_s, g, a, map, sm_count, s);
-    else fast::stream_s<StoreF16Dev>(rep_s, g, a, map, sm_count, s);
+void launch_stream_fast(int storage, int collision, int rep_s, const GridDesc& g, const BulkArgs* a,
+                        const CUtensorMap* map, int sm_count, cudaStream_t s) {
+    if (storage == BFX_STORAGE_BF16_DEVIATION) fast::stream_s<StoreBF16Dev>(collision, rep_s, g, a, map, sm_count, s);
+    else fast::stream_s<StoreF16Dev>(collision, rep_s, g, a, map, sm_count, s);
 }
 
 void launch_bulk_fast(int storage, int collision, int rep_s, const GridDesc& g, const BulkArgs& a, int part,

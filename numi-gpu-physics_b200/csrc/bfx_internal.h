@@ -161,7 +161,9 @@ void launch_fill_wall(float4* wall, int64_t n, float w, cudaStream_t s);
 // fused kernel; false when the driver entry point is missing or the format is
 // not 16-bit.
 bool encode_population_map(CUtensorMap* map, void* pops, int storage, int64_t px, int64_t py, int64_t pz);
+// Collision operators whose 16-bit fluid step runs the staged kernel.
+bool staged_collision(int collision);
 // Raises the staged kernel's shared-memory limit for a 16-bit storage format
-// (call before any graph capture).
-void prepare_stream(int storage);
+// and collision operator (call before any graph capture).
+void prepare_stream(int storage, int collision);
 }  // namespace bfx

@@ -86,9 +86,10 @@ __device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map
         : "memory");
 }
 
-// Launch of the staged TRT kernel for a 16-bit format (bfx_fluid_fast.cu); a
-// null BulkArgs only prepares the instantiations (shared-memory limit, occupancy).
-void launch_stream_fast(int storage, int rep_s, const GridDesc& g, const BulkArgs* a, const CUtensorMap* map,
-                        int sm_count, cudaStream_t s);
+// Launch of the staged kernel for a 16-bit format and a collision operator
+// that staged_collision accepts (bfx_fluid_fast.cu); a null BulkArgs only
+// prepares the instantiations (shared-memory limit, occupancy).
+void launch_stream_fast(int storage, int collision, int rep_s, const GridDesc& g, const BulkArgs* a,
+                        const CUtensorMap* map, int sm_count, cudaStream_t s);
 
 }  // namespace bfx

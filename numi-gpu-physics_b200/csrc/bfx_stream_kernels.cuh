@@ -18,31 +18,6 @@
 namespace bfx {
 namespace BFX_VARIANT {
 
-// ---------------------------------------------------------------------------
-// Packed pair arithmetic.
-// ---------------------------------------------------------------------------
-using P2 = float2;
-__device__ __forceinline__ P2 pv(float s) { return make_float2(s, s); }
-#define BFX_F32X2_OP(NAME, INSTR)                                                                   \
-    __device__ __forceinline__ P2 NAME(P2 a, P2 b) {                                               \
-        P2 r;                                                                                      \
-        asm("{\n .reg .b64 a, b, d;\n mov.b64 a, {%2, %3};\n mov.b64 b, {%4, %5};\n " INSTR     \
-            " d, a, b;\n mov.b64 {%0, %1}, d;\n}"                                                  \
-            : "=f"(r.x), "=f"(r.y)                                                                 \
-            : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));                                             \
-        return r;                                                                                  \
-    }
-BFX_F32X2_OP(padd, "add.rn.f32x2")
-BFX_F32X2_OP(psub, "sub.rn.f32x2")
-BFX_F32X2_OP(pmul, "mul.rn.f32x2")
-#undef BFX_F32X2_OP
-__device__ __forceinline__ P2 operator+(P2 a, P2 b) { return padd(a, b); }
-__device__ __forceinline__ P2 operator-(P2 a) { return make_float2(-a.x, -a.y); }
-__device__ __forceinline__ P2 operator-(P2 a, P2 b) { return psub(a, b); }
-__device__ __forceinline__ P2 operator*(P2 a, P2 b) { return pmul(a, b); }
-__device__ __forceinline__ P2 operator*(float s, P2 a) { return pmul(make_float2(s, s), a); }
-__device__ __forceinline__ P2 operator*(P2 a, float s) { return pmul(a, make_float2(s, s)); }
-
 // c_q . u with the zero products dropped (cdotq on pairs)
 __device__ __forceinline__ P2 cdot2(int q, P2 ux, P2 uy, P2 uz) {
     P2 r = pv(0.0f);
@@ -75,25 +50,11 @@ __device__ __forceinline__ void moments2(const P2 (&f)[19], P2& rho, P2& ux, P2&
     uz = mz * inv;
 }
 
-// Positivity admission of one lane (the admit step of collide<R, RR3>).
-__device__ __forceinline__ void admit1(float fe, float cand, float& scale) {
-    float fl = 1.0e-6f * (fe > 0.0f ? fe : 0.0f);
-    float floor_ = 1.0e-12f > fl ? 1.0e-12f : fl;
-    if (cand < floor_) {
-        float den = fe - cand;
-        den = den > 1.0e-30f ? den : 1.0e-30f;
-        float adm = (fe - floor_) / den;
-        adm = adm < 0.0f ? 0.0f : (adm > 1.0f ? 1.0f : adm);
-        scale = scale < adm ? scale : adm;
-    }
-}
-
 // collide<float, COLL> on two cells; the limiter runs lane by lane through
 // the scalar operator.
 template <int COLL>
 __device__ __forceinline__ void collide2(const P2 (&f)[19], P2 rho, P2 ux, P2 uy, P2 uz, float omega_p, float omega_m,
                                          P2 (&post)[19], float (&activation)[2], float (&restriction)[2]) {
-    const float cs2 = Lat<float>::cs2;
     if (COLL == BFX_COLLISION_TRT_LIMITER) {
 #pragma unroll
         for (int l = 0; l < 2; ++l) {
@@ -125,7 +86,8 @@ __device__ __forceinline__ void collide2(const P2 (&f)[19], P2 rho, P2 ux, P2 uy
         feqv[q] = wr * (((pv(1.0f) + t3) + t45) - t15);
         feqv[q + 1] = wr * (((pv(1.0f) - t3) + t45) - t15);
     }
-    if (COLL == BFX_COLLISION_TRT) {
+    {
+        // TRT; the regularized operators run through collide_pairs
         post[0] = f[0] - omega_p * (f[0] - feqv[0]);
 #pragma unroll
         for (int q = 1; q < 19; q += 2) {
@@ -138,87 +100,7 @@ __device__ __forceinline__ void collide2(const P2 (&f)[19], P2 rho, P2 ux, P2 uy
             post[q] = (f[q] - A) - B;
             post[q + 1] = (f[q + 1] - A) + B;
         }
-        return;
     }
-    // regularized / RR3
-    P2 dsx = pv(0.0f), dsy = pv(0.0f), dsz = pv(0.0f), odx = pv(0.0f), ody = pv(0.0f), odz = pv(0.0f);
-#pragma unroll
-    for (int q = 0; q < 19; ++q) {
-        const P2 ne = f[q] - feqv[q];
-        dsx = dsx + ne * ((float)(cx(q) * cx(q)) - cs2);
-        dsy = dsy + ne * ((float)(cy(q) * cy(q)) - cs2);
-        dsz = dsz + ne * ((float)(cz(q) * cz(q)) - cs2);
-        if (cx(q) * cy(q) > 0) odx = odx + ne;
-        if (cx(q) * cy(q) < 0) odx = odx - ne;
-        if (cx(q) * cz(q) > 0) ody = ody + ne;
-        if (cx(q) * cz(q) < 0) ody = ody - ne;
-        if (cy(q) * cz(q) > 0) odz = odz + ne;
-        if (cy(q) * cz(q) < 0) odz = odz - ne;
-    }
-    const P2 aXxy = (2.0f * ux) * odx + uy * dsx;
-    const P2 aXxz = (2.0f * ux) * ody + uz * dsx;
-    const P2 aXyy = ux * dsy + (2.0f * uy) * odx;
-    const P2 aXzz = ux * dsz + (2.0f * uz) * ody;
-    const P2 aYyz = (2.0f * uy) * odz + uz * dsy;
-    const P2 aYzz = uy * dsz + (2.0f * uz) * odz;
-    const float one_minus = 1.0f - omega_p;
-    float scale[2] = {1.0f, 1.0f};
-    {
-        const float h = -cs2;
-        const P2 contraction = (h * dsx + h * dsy) + h * dsz;
-        const P2 rne = (Lat<float>::w0 * 4.5f) * contraction;
-        post[0] = feqv[0] + one_minus * rne;
-        admit1(feqv[0].x, post[0].x, scale[0]);
-        admit1(feqv[0].y, post[0].y, scale[1]);
-    }
-#pragma unroll
-    for (int q = 1; q < 19; q += 2) {
-        const float hx = (float)(cx(q) * cx(q)) - cs2, hy = (float)(cy(q) * cy(q)) - cs2,
-                    hz = (float)(cz(q) * cz(q)) - cs2;
-        P2 contraction = (hx * dsx + hy * dsy) + hz * dsz;
-        {
-            const int xy = cx(q) * cy(q), xz = cx(q) * cz(q), yz = cy(q) * cz(q);
-            if (xy != 0) contraction = contraction + 2.0f * (xy > 0 ? odx : -odx);
-            else if (xz != 0) contraction = contraction + 2.0f * (xz > 0 ? ody : -ody);
-            else if (yz != 0) contraction = contraction + 2.0f * (yz > 0 ? odz : -odz);
-        }
-        const P2 a = (wq<float>(q) * 4.5f) * contraction;
-        P2 rq = a, ro = a;
-        if (COLL == BFX_COLLISION_RR3) {
-            P2 third = pv(0.0f);
-            bool any = false;
-            auto add = [&](int da, float hb, P2 amp) {
-                if (da == 0) return;
-                const P2 t = ((float)da * hb) * amp;
-                third = any ? third + t : t;
-                any = true;
-            };
-            add(cy(q), hx, aXxy);
-            add(cz(q), hx, aXxz);
-            add(cx(q), hy, aXyy);
-            add(cx(q), hz, aXzz);
-            add(cz(q), hy, aYyz);
-            add(cy(q), hz, aYzz);
-            const P2 b = (wq<float>(q) * 13.5f) * third;
-            rq = a + b;
-            ro = a - b;
-        }
-        post[q] = feqv[q] + one_minus * rq;
-        post[q + 1] = feqv[q + 1] + one_minus * ro;
-        admit1(feqv[q].x, post[q].x, scale[0]);
-        admit1(feqv[q].y, post[q].y, scale[1]);
-        admit1(feqv[q + 1].x, post[q + 1].x, scale[0]);
-        admit1(feqv[q + 1].y, post[q + 1].y, scale[1]);
-    }
-    for (int l = 0; l < 2; ++l)
-        if (scale[l] < 1.0f) {
-            activation[l] = 1.0f;
-            restriction[l] = 1.0f - scale[l];
-        }
-    // feq + 1 * (cand - feq) is not cand in general: keep the reference expression
-    const P2 sc = make_float2(scale[0], scale[1]);
-#pragma unroll
-    for (int q = 0; q < 19; ++q) post[q] = feqv[q] + sc * (post[q] - feqv[q]);
 }
 
 // Storage conversions of one population (ld_rt / st_rt on pairs).
@@ -233,7 +115,7 @@ __device__ __forceinline__ float ld1(const typename S::T* p, int q) {
 // Four CTAs per SM (16 consumer warps) for TRT; the heavier operators keep
 // their registers at three.
 template <class S, int REP_S, int COLL, int CAPTURE>
-__global__ void __launch_bounds__(kStreamThreads, COLL == BFX_COLLISION_TRT ? 4 : 3)
+__global__ void __launch_bounds__(kStreamThreads, 4)
     k_stream(const __grid_constant__ CUtensorMap map, const BulkArgs a, const StreamTiles tl) {
     using T = typename S::T;
     using G = StreamGeom<T>;
@@ -349,11 +231,15 @@ __global__ void __launch_bounds__(kStreamThreads, COLL == BFX_COLLISION_TRT ? 4 
         va = va && ma == 0;
         vb = vb && mb == 0;
         if (!__any_sync(0xffffffffu, va || vb)) continue;
-        P2 rho, ux, uy, uz;
-        moments2(f, rho, ux, uy, uz);
         P2 post[19];
         float activation[2] = {0.0f, 0.0f}, restriction[2] = {0.0f, 0.0f};
-        collide2<COLL>(f, rho, ux, uy, uz, fp.omega_p, fp.omega_m, post, activation, restriction);
+        if constexpr (COLL == BFX_COLLISION_RR3 || COLL == BFX_COLLISION_REGULARIZED) {
+            collide_pairs<P2, COLL>(f, fp.omega_p, post, activation, restriction);
+        } else {
+            P2 rho, ux, uy, uz;
+            moments2(f, rho, ux, uy, uz);
+            collide2<COLL>(f, rho, ux, uy, uz, fp.omega_p, fp.omega_m, post, activation, restriction);
+        }
         if (fp.has_sponge) {
             const float spa = va ? sponge_factor(g, fp, xa, y, z) : 0.0f;
             const float spb = vb ? sponge_factor(g, fp, xb, y, z) : 0.0f;
@@ -451,12 +337,19 @@ static void stream_t(const GridDesc& gd, const BulkArgs* a, const CUtensorMap* m
     else stream_launch<S, REP, COLL, 0>(gd, *a, *map, sm_count, s);
 }
 
-// Launch (a non-null) or prepare (a null) the staged TRT kernel of one storage type.
+// Launch (a non-null) or prepare (a null) the staged kernel of one storage
+// type and collision operator (TRT, regularized or RR3).
 template <class S>
-static void stream_s(int rep_s, const GridDesc& g, const BulkArgs* a, const CUtensorMap* map, int sm_count,
-                     cudaStream_t s) {
-    if (rep_s) stream_t<S, 1, BFX_COLLISION_TRT>(g, a, map, sm_count, s);
-    else stream_t<S, 0, BFX_COLLISION_TRT>(g, a, map, sm_count, s);
+static void stream_s(int collision, int rep_s, const GridDesc& g, const BulkArgs* a, const CUtensorMap* map,
+                     int sm_count, cudaStream_t s) {
+    switch (collision * 2 + rep_s) {
+    case 1: stream_t<S, 1, BFX_COLLISION_TRT>(g, a, map, sm_count, s); break;
+    case 4: stream_t<S, 0, BFX_COLLISION_REGULARIZED>(g, a, map, sm_count, s); break;
+    case 5: stream_t<S, 1, BFX_COLLISION_REGULARIZED>(g, a, map, sm_count, s); break;
+    case 6: stream_t<S, 0, BFX_COLLISION_RR3>(g, a, map, sm_count, s); break;
+    case 7: stream_t<S, 1, BFX_COLLISION_RR3>(g, a, map, sm_count, s); break;
+    default: stream_t<S, 0, BFX_COLLISION_TRT>(g, a, map, sm_count, s); break;
+    }
 }
 
 }  // namespace BFX_VARIANT
