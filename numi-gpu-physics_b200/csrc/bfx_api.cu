@@ -288,15 +288,21 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
     // image writes into a halo slot and must win over the periodic copy
     launch_halo(s->cfg.storage, s->rep_s, s->g, s->fp, fb, s->stream);
     s->launches += 1;
+    // The end-of-step body update needs only the reduced loads: it runs in the
+    // link kernel's last block, except while taping (the tape records the
+    // state between the loads and the body update).
+    const FinishParams fin = {{s->cfg.gravity[0], s->cfg.gravity[1], s->cfg.gravity[2]}, (int)s->cfg.body_substeps,
+                              s->cfg.free_flight && s->has_bird ? 1 : 0};
+    const bool finish_fused = s->geometry() && !tape;
     if (s->geometry()) {
         GeomBuffers gb = geom_buffers(s, mprev, mnext);
         if (tape) {
             gb.link_tape = tape->links;
             gb.link_tangent = tape->link_tangent;
         }
-        launch_links_apply(s->cfg.storage, s->rep_s, s->g, s->fp, gb, fb, s->stream);
-        launch_reduce_loads(gb, s->moving() ? 1 : 0, s->stream);
-        s->launches += 2;
+        launch_links_apply(s->cfg.storage, s->rep_s, s->g, s->fp, gb, fb, s->moving() ? 1 : 0,
+                           finish_fused ? &fin : nullptr, s->stream);
+        s->launches += 1;
     }
     if (tape) {
         cudaMemcpyAsync(tape->state, s->dstate, sizeof(DeviceState), cudaMemcpyDeviceToDevice, s->stream);
@@ -309,15 +315,16 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
     }
     const int box[3] = {s->box.sx, s->box.sy, s->box.sz};
     timing_begin(s);
-    launch_bulk(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, capture, 0, box, s->stream);
+    launch_bulk(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, capture, s->geometry() ? box : nullptr,
+                s->stream);
     timing_end(s);
-    launch_bulk(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, capture, 1,
-                s->geometry() ? box : nullptr, s->stream);
-    s->launches += s->geometry() ? 2 : 1;
+    s->launches += launch_bulk_count(s->cfg.storage, s->cfg.collision, capture, s->tma_ok, s->geometry());
     GeomBuffers gb = geom_buffers(s, mprev, mnext);
-    launch_integrate(s->g, s->fp, gb, s->cfg.gravity[0], s->cfg.gravity[1], s->cfg.gravity[2],
-                     (int)s->cfg.body_substeps, s->cfg.free_flight && s->has_bird ? 1 : 0, s->stream);
-    s->launches += 1;
+    if (!finish_fused) {
+        launch_integrate(s->g, s->fp, gb, fin.gravity[0], fin.gravity[1], fin.gravity[2], fin.substeps,
+                         fin.free_flight, s->stream);
+        s->launches += 1;
+    }
     if (sample_slot_base) {
         launch_record_sample(gb, s->fp, sample_slot_base, sample_index, s->cfg.time_step, s->stream);
         s->launches += 1;
@@ -617,7 +624,7 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
         BFX_ALLOC(s->block_offsets, (size_t)s->box_blocks * sizeof(uint32_t));
         BFX_ALLOC(s->topo_partials, (size_t)s->box_blocks * 8 * sizeof(double));
         s->apply_blocks = 4 * s->sm_count;
-        BFX_ALLOC(s->link_partials, (size_t)s->apply_blocks * 8 * sizeof(double));
+        BFX_ALLOC(s->link_partials, (size_t)s->apply_blocks * 16 * sizeof(double));
         uint64_t cap = c.link_capacity ? c.link_capacity
                                        : std::max<uint64_t>(1u << 18, std::min<uint64_t>((uint64_t)s->box.cells, 1u << 24));
         s->link_capacity = (uint32_t)cap;

@@ -18,8 +18,7 @@ struct BulkArgs {
     int32_t doff[19];       // c_q . (1, px, px*py): padded neighbour offset of direction q
     float far_eq_f[19];     // equilibrium(q, far density, far velocity), FP32
     double far_eq_d[19];    // same in FP64 (FP64 storage)
-    int box[3];             // geometry box extent (origin in DeviceState)
-    int64_t box_cells;
+    int box[3];             // geometry box extent (origin in DeviceState); rare-cell launch
     void* pops;
     const uint8_t* mask;
     const float4* wall;
@@ -33,8 +32,9 @@ struct BulkArgs {
 };
 
 // Fused-step launch for the contracted variant (bfx_fluid_fast.cu).
-void launch_bulk_fast(int storage, int collision, int rep_s, const GridDesc& g, const BulkArgs& a, int part,
-                      cudaStream_t s);
+void launch_bulk_fast(int storage, int collision, int rep_s, const GridDesc& g, const BulkArgs& a, cudaStream_t s);
+// Solid / newly uncovered cells of the geometry box for the staged kernel (contracted variant).
+void launch_rare_fast(int storage, int collision, int rep_s, const BulkArgs& a, cudaStream_t s);
 // Host-side construction of BulkArgs (bfx_fluid.cu).
 BulkArgs make_bulk_args(const GridDesc& gd, const FluidParams& fp, const FluidBuffers& b, int capture, int storage);
 void cell_launch_shape(const GridDesc& g, dim3& grid, dim3& block);

@@ -299,9 +299,42 @@ __device__ __forceinline__ void finish_cell(const BulkArgs& a, uint32_t gid, int
     }
 }
 
+// Solid cells write the moving-wall equilibrium eq(1, u_wall)
+// (BF.metal:2557-2570); newly uncovered cells refill from it and collide
+// (BF.metal:2610-2625).  Called for a cell whose mask byte is nonzero (only
+// cells of the geometry box have one) by the fused kernels.
+template <class S, int REP_S, int COLL>
+__device__ __forceinline__ void rare_cell(const BulkArgs& a, uint32_t gid, int x, int y, int z, uint32_t pid,
+                                       uint8_t m) {
+    using R = typename S::R;
+    const float4 w = a.wall[gid];
+    const R ux = w.x, uy = w.y, uz = w.z;
+    const R u2 = ux * ux + uy * uy + uz * uz;
+    R post[19];
+    if (m & kPartMask) {
+#pragma unroll
+        for (int q = 0; q < 19; ++q) post[q] = feqq<R>(q, R(1), ux, uy, uz, u2);
+        store_cell<S, REP_S>(a, pid, post);
+        if (a.capture == 1) {
+            a.density[gid] = 1.0f;
+            a.velocity[gid] = make_float4(w.x, w.y, w.z, 0.0f);
+        }
+        return;
+    }
+    R f[19];
+#pragma unroll
+    for (int q = 0; q < 19; ++q) f[q] = feqq<R>(q, R(1), ux, uy, uz, u2);
+    R rho, vx, vy, vz;
+    moments<R>(f, rho, vx, vy, vz);
+    float activation = 0.0f, restriction = 0.0f;
+    collide<R, COLL>(f, rho, vx, vy, vz, (R)a.fp.omega_p, (R)a.fp.omega_m, post, activation, restriction);
+    finish_cell<S, COLL>(a, gid, x, y, z, a.capture == 1, post, activation, restriction);
+    store_cell<S, REP_S>(a, pid, post);
+}
+
 // ---------------------------------------------------------------------------
-// The fused kernel: every fluid cell of the lattice.  Solid and newly
-// uncovered cells (flagged in the mask) are left to k_bulk_rare.
+// The fused kernel: every cell of the lattice; solid and newly uncovered
+// cells (flagged in the mask) take rare_cell.
 // ---------------------------------------------------------------------------
 template <class S, int REP_S, int COLL, int CAPTURE>
 __global__ void __launch_bounds__(256, sizeof(typename S::R) == 8 ? 1 : (COLL == BFX_COLLISION_TRT_LIMITER ? 2 : 4))
@@ -312,9 +345,15 @@ __global__ void __launch_bounds__(256, sizeof(typename S::R) == 8 ? 1 : (COLL ==
     const int z = blockIdx.z;
     if (x >= a.g.nx || y >= a.g.ny) return;
     const uint32_t gid = (uint32_t)x + (uint32_t)a.g.nx * ((uint32_t)y + (uint32_t)a.g.ny * (uint32_t)z);
-    if (a.mask && a.mask[gid]) return;
     const uint32_t pid =
         (uint32_t)(x + 1) + (uint32_t)a.g.px * ((uint32_t)(y + 1) + (uint32_t)a.g.py * (uint32_t)(z + 1));
+    if (a.mask) {
+        const uint8_t m = a.mask[gid];
+        if (m) {
+            rare_cell<S, REP_S, COLL>(a, gid, x, y, z, pid, m);
+            return;
+        }
+    }
     R f[19];
     load_cell<S, REP_S>(a, pid, f);
     R post[19];
@@ -344,78 +383,77 @@ __global__ void __launch_bounds__(256, sizeof(typename S::R) == 8 ? 1 : (COLL ==
     store_cell<S, REP_S>(a, pid, post);
 }
 
-// Solid cells write the moving-wall equilibrium eq(1, u_wall)
-// (BF.metal:2557-2570); newly uncovered cells refill from it and collide
-// (BF.metal:2610-2625).  Both lie inside the geometry box.
+// Solid / newly uncovered cells of the geometry box in a launch of their own
+// (the staged kernel skips them).  A thread scans kRareZ cells along z of one
+// (x, y) column of the box, all mask bytes loaded before the first is used.
+constexpr int kRareZ = 8;
 template <class S, int REP_S, int COLL>
-__global__ void __launch_bounds__(128) k_bulk_rare(const BulkArgs a) {
-    using R = typename S::R;
-    const Grid& g = a.g;
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= a.box_cells) return;
-    const int lz = (int)(t / ((int64_t)a.box[0] * a.box[1]));
-    const int64_t r = t - (int64_t)lz * a.box[0] * a.box[1];
-    const int ly = (int)(r / a.box[0]);
-    const int lx = (int)(r - (int64_t)ly * a.box[0]);
+__global__ void __launch_bounds__(128) k_rare(const BulkArgs a) {
+    const int lx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (lx >= a.box[0]) return;
     const int x = a.state->box_origin[0] + lx;
-    const int y = a.state->box_origin[1] + ly;
-    const int z = a.state->box_origin[2] + lz;
-    if (!inside(g, x, y, z)) return;
-    const uint32_t gid = (uint32_t)flat(g, x, y, z);
-    const uint8_t m = a.mask[gid];
-    if (m == 0) return;
-    const uint32_t pid = (uint32_t)pflat(g, x, y, z);
-    const float4 w = a.wall[gid];
-    const R ux = w.x, uy = w.y, uz = w.z;
-    const R u2 = ux * ux + uy * uy + uz * uz;
-    R post[19];
-    if (m & kPartMask) {
+    const int y = a.state->box_origin[1] + (int)blockIdx.y;
+    const int z0 = a.state->box_origin[2] + (int)blockIdx.z * kRareZ;
+    if (x < 0 || x >= a.g.nx || y < 0 || y >= a.g.ny) return;
+    const int lz_end = a.box[2] - (int)blockIdx.z * kRareZ;
+    const uint32_t plane = (uint32_t)a.g.nx * (uint32_t)a.g.ny;
+    uint8_t m[kRareZ];
 #pragma unroll
-        for (int q = 0; q < 19; ++q) post[q] = feqq<R>(q, R(1), ux, uy, uz, u2);
-        store_cell<S, REP_S>(a, pid, post);
-        if (a.capture == 1) {
-            a.density[gid] = 1.0f;
-            a.velocity[gid] = make_float4(w.x, w.y, w.z, 0.0f);
-        }
-        return;
+    for (int k = 0; k < kRareZ; ++k) {
+        const int z = z0 + k;
+        m[k] = (k < lz_end && z >= 0 && z < a.g.nz)
+                   ? a.mask[(uint32_t)x + (uint32_t)a.g.nx * (uint32_t)y + plane * (uint32_t)z]
+                   : (uint8_t)0;
     }
-    R f[19];
-#pragma unroll
-    for (int q = 0; q < 19; ++q) f[q] = feqq<R>(q, R(1), ux, uy, uz, u2);
-    R rho, vx, vy, vz;
-    moments<R>(f, rho, vx, vy, vz);
-    float activation = 0.0f, restriction = 0.0f;
-    collide<R, COLL>(f, rho, vx, vy, vz, (R)a.fp.omega_p, (R)a.fp.omega_m, post, activation, restriction);
-    finish_cell<S, COLL>(a, gid, x, y, z, a.capture == 1, post, activation, restriction);
-    store_cell<S, REP_S>(a, pid, post);
-}
-
-template <class S, int REP, int COLL>
-static void bulk_t(const BulkArgs& a, const GridDesc& g, int part, cudaStream_t s) {
-    if (part == 0) {
-        dim3 grid, block;
-        cell_launch_shape(g, grid, block);
-        if (a.capture == 1) k_bulk<S, REP, COLL, 1><<<grid, block, 0, s>>>(a);
-#ifndef BFX_CONTRACTED
-        else if (a.capture == 2 && COLL == BFX_COLLISION_TRT) k_bulk<S, REP, BFX_COLLISION_TRT, 2><<<grid, block, 0, s>>>(a);
-#endif
-        else k_bulk<S, REP, COLL, 0><<<grid, block, 0, s>>>(a);
-    } else if (a.mask && a.box_cells > 0) {
-        k_bulk_rare<S, REP, COLL><<<(unsigned)((a.box_cells + 127) / 128), 128, 0, s>>>(a);
+#pragma unroll 1
+    for (int k = 0; k < kRareZ; ++k) {
+        if (m[k] == 0) continue;
+        const int z = z0 + k;
+        const uint32_t gid = (uint32_t)x + (uint32_t)a.g.nx * (uint32_t)y + plane * (uint32_t)z;
+        const uint32_t pid =
+            (uint32_t)(x + 1) + (uint32_t)a.g.px * ((uint32_t)(y + 1) + (uint32_t)a.g.py * (uint32_t)(z + 1));
+        rare_cell<S, REP_S, COLL>(a, gid, x, y, z, pid, m[k]);
     }
 }
 
 template <class S>
-static void bulk_s(const BulkArgs& a, const GridDesc& g, int collision, int rep_s, int part, cudaStream_t s) {
+static void rare_s(const BulkArgs& a, int collision, int rep_s, cudaStream_t s) {
+    const dim3 grid((unsigned)((a.box[0] + 127) / 128), (unsigned)a.box[1],
+                    (unsigned)((a.box[2] + kRareZ - 1) / kRareZ));
     switch (collision * 2 + rep_s) {
-    case 0: bulk_t<S, 0, BFX_COLLISION_TRT>(a, g, part, s); break;
-    case 1: bulk_t<S, 1, BFX_COLLISION_TRT>(a, g, part, s); break;
-    case 2: bulk_t<S, 0, BFX_COLLISION_TRT_LIMITER>(a, g, part, s); break;
-    case 3: bulk_t<S, 1, BFX_COLLISION_TRT_LIMITER>(a, g, part, s); break;
-    case 4: bulk_t<S, 0, BFX_COLLISION_REGULARIZED>(a, g, part, s); break;
-    case 5: bulk_t<S, 1, BFX_COLLISION_REGULARIZED>(a, g, part, s); break;
-    case 6: bulk_t<S, 0, BFX_COLLISION_RR3>(a, g, part, s); break;
-    default: bulk_t<S, 1, BFX_COLLISION_RR3>(a, g, part, s); break;
+    case 0: k_rare<S, 0, BFX_COLLISION_TRT><<<grid, 128, 0, s>>>(a); break;
+    case 1: k_rare<S, 1, BFX_COLLISION_TRT><<<grid, 128, 0, s>>>(a); break;
+    case 2: k_rare<S, 0, BFX_COLLISION_TRT_LIMITER><<<grid, 128, 0, s>>>(a); break;
+    case 3: k_rare<S, 1, BFX_COLLISION_TRT_LIMITER><<<grid, 128, 0, s>>>(a); break;
+    case 4: k_rare<S, 0, BFX_COLLISION_REGULARIZED><<<grid, 128, 0, s>>>(a); break;
+    case 5: k_rare<S, 1, BFX_COLLISION_REGULARIZED><<<grid, 128, 0, s>>>(a); break;
+    case 6: k_rare<S, 0, BFX_COLLISION_RR3><<<grid, 128, 0, s>>>(a); break;
+    default: k_rare<S, 1, BFX_COLLISION_RR3><<<grid, 128, 0, s>>>(a); break;
+    }
+}
+
+template <class S, int REP, int COLL>
+static void bulk_t(const BulkArgs& a, const GridDesc& g, cudaStream_t s) {
+    dim3 grid, block;
+    cell_launch_shape(g, grid, block);
+    if (a.capture == 1) k_bulk<S, REP, COLL, 1><<<grid, block, 0, s>>>(a);
+#ifndef BFX_CONTRACTED
+    else if (a.capture == 2 && COLL == BFX_COLLISION_TRT) k_bulk<S, REP, BFX_COLLISION_TRT, 2><<<grid, block, 0, s>>>(a);
+#endif
+    else k_bulk<S, REP, COLL, 0><<<grid, block, 0, s>>>(a);
+}
+
+template <class S>
+static void bulk_s(const BulkArgs& a, const GridDesc& g, int collision, int rep_s, cudaStream_t s) {
+    switch (collision * 2 + rep_s) {
+    case 0: bulk_t<S, 0, BFX_COLLISION_TRT>(a, g, s); break;
+    case 1: bulk_t<S, 1, BFX_COLLISION_TRT>(a, g, s); break;
+    case 2: bulk_t<S, 0, BFX_COLLISION_TRT_LIMITER>(a, g, s); break;
+    case 3: bulk_t<S, 1, BFX_COLLISION_TRT_LIMITER>(a, g, s); break;
+    case 4: bulk_t<S, 0, BFX_COLLISION_REGULARIZED>(a, g, s); break;
+    case 5: bulk_t<S, 1, BFX_COLLISION_REGULARIZED>(a, g, s); break;
+    case 6: bulk_t<S, 0, BFX_COLLISION_RR3>(a, g, s); break;
+    default: bulk_t<S, 1, BFX_COLLISION_RR3>(a, g, s); break;
     }
 }
 

@@ -46,9 +46,17 @@ __global__ void __launch_bounds__(128) k_halo(const BulkArgs a, int rep_s, int64
     hz -= 1;
     T* A = (T*)a.pops;
     const FluidParams& fp = a.fp;
+    // Two passes: every value is loaded before any is stored, so the loads of
+    // one cell overlap.  No load of this launch reads a stored slot: rep E
+    // loads A[opp q][w] and stores A[opp q][h], rep S loads A[q][w + c_q] and
+    // stores A[q][h + c_q], with w always a real cell and h a halo cell.
+    R vals[19];
+    uint32_t live = 0;
+#pragma unroll
     for (int q = 1; q < 19; ++q) {
         const int bx = hx + cx(q), by = hy + cy(q), bz = hz + cz(q);
         if (!inside(g, bx, by, bz)) continue;
+        live |= 1u << q;
         int wx = hx, wy = hy, wz = hz;
         R val;
         if (wrap(g, wx, wy, wz)) {
@@ -79,8 +87,13 @@ __global__ void __launch_bounds__(128) k_halo(const BulkArgs a, int rep_s, int64
                 else val = sizeof(R) == 8 ? (R)a.far_eq_d[q] : (R)a.far_eq_f[q];
             }
         }
-        if (rep_s) S::st_rt(A + (int64_t)q * g.pn + pflat(g, bx, by, bz), q, val);
-        else S::st_rt(A + (int64_t)opp(q) * g.pn + pflat(g, hx, hy, hz), opp(q), val);
+        vals[q] = val;
+    }
+#pragma unroll
+    for (int q = 1; q < 19; ++q) {
+        if (!(live & (1u << q))) continue;
+        if (rep_s) S::st_rt(A + (int64_t)q * g.pn + pflat(g, hx + cx(q), hy + cy(q), hz + cz(q)), q, vals[q]);
+        else S::st_rt(A + (int64_t)opp(q) * g.pn + pflat(g, hx, hy, hz), opp(q), vals[q]);
     }
 }
 
@@ -258,6 +271,7 @@ Grid device_grid(const GridDesc& gd) {
 BulkArgs make_bulk_args(const GridDesc& gd, const FluidParams& fp, const FluidBuffers& b, int capture,
                         int storage) {
     BulkArgs a;
+    a.box[0] = a.box[1] = a.box[2] = 0;
     a.g = device_grid(gd);
     for (int q = 0; q < 19; ++q) {
         a.plane[q] = (char*)b.pops + (size_t)q * (size_t)a.g.pn * elem_bytes(storage);
@@ -265,8 +279,6 @@ BulkArgs make_bulk_args(const GridDesc& gd, const FluidParams& fp, const FluidBu
         a.far_eq_f[q] = host_feq<float>(q, fp.far[3], fp.far[0], fp.far[1], fp.far[2]);
         a.far_eq_d[q] = host_feq<double>(q, (double)fp.far[3], (double)fp.far[0], (double)fp.far[1], (double)fp.far[2]);
     }
-    a.box[0] = a.box[1] = a.box[2] = 0;
-    a.box_cells = 0;
     a.pops = b.pops;
     a.mask = b.mask;
     a.wall = b.wall;
@@ -340,32 +352,42 @@ void prepare_stream(int storage, int collision) {
     for (int rep = 0; rep < 2; ++rep) launch_stream_fast(storage, collision, rep, g, nullptr, nullptr, 0, nullptr);
 }
 
+static bool use_staged(int storage, int collision, int capture, bool tma_ok) {
+    const bool sixteen = storage == BFX_STORAGE_F16_DEVIATION || storage == BFX_STORAGE_BF16_DEVIATION;
+    return tma_ok && sixteen && staged_collision(collision) && capture != 2;
+}
+
+int launch_bulk_count(int storage, int collision, int capture, bool tma_ok, bool geometry) {
+    return use_staged(storage, collision, capture, tma_ok) && geometry ? 2 : 1;
+}
+
 void launch_bulk(int storage, int collision, int rep_s, const GridDesc& g, const FluidParams& fp,
-                 const FluidBuffers& b, int capture, int part, const int* box, cudaStream_t s) {
+                 const FluidBuffers& b, int capture, const int* box, cudaStream_t s) {
     BulkArgs a = make_bulk_args(g, fp, b, capture, storage);
     if (box) {
         a.box[0] = box[0];
         a.box[1] = box[1];
         a.box[2] = box[2];
-        a.box_cells = (int64_t)box[0] * box[1] * box[2];
     }
     const bool contracted = storage == BFX_STORAGE_F16_DEVIATION || storage == BFX_STORAGE_BF16_DEVIATION ||
                             (storage == BFX_STORAGE_F32 && fp.fast_math);
-    // Fluid cells of the 16-bit TRT step: the TMA-staged kernel, measured
-    // 1.2x faster there (16-bit loads leave k_bulk latency-bound).  For FP32,
-    // FP64 and the regularized operators k_bulk was measured as fast or faster:
-    // their collision issue time, not load latency, bounds the step.
-    const bool staged = storage == BFX_STORAGE_F16_DEVIATION || storage == BFX_STORAGE_BF16_DEVIATION;
-    if (part == 0 && b.tmap && staged && staged_collision(collision) && capture != 2) {
+    // 16-bit TRT / regularized / RR3: the TMA-staged kernel, measured faster
+    // there (16-bit loads leave k_bulk latency-bound; the packed pair
+    // arithmetic halves the regularized operators' issue time), with the
+    // geometry box's solid and uncovered cells in a second launch (inlined,
+    // their path cost the staged kernel registers).  FP32 and FP64 keep k_bulk
+    // (bit-identical scalar arithmetic), which takes those cells inline.
+    if (use_staged(storage, collision, capture, b.tmap != nullptr)) {
         launch_stream_fast(storage, collision, rep_s, g, &a, (const CUtensorMap*)b.tmap, b.sm_count, s);
+        if (box && a.mask) launch_rare_fast(storage, collision, rep_s, a, s);
         return;
     }
     if (contracted) {
-        launch_bulk_fast(storage, collision, rep_s, g, a, part, s);
+        launch_bulk_fast(storage, collision, rep_s, g, a, s);
     } else if (storage == BFX_STORAGE_F64) {
-        exact::bulk_s<StoreF64>(a, g, collision, rep_s, part, s);
+        exact::bulk_s<StoreF64>(a, g, collision, rep_s, s);
     } else {
-        exact::bulk_s<StoreF32>(a, g, collision, rep_s, part, s);
+        exact::bulk_s<StoreF32>(a, g, collision, rep_s, s);
     }
 }
 

@@ -15,12 +15,16 @@ void launch_stream_fast(int storage, int collision, int rep_s, const GridDesc& g
     else fast::stream_s<StoreF16Dev>(collision, rep_s, g, a, map, sm_count, s);
 }
 
-void launch_bulk_fast(int storage, int collision, int rep_s, const GridDesc& g, const BulkArgs& a, int part,
-                      cudaStream_t s) {
+void launch_rare_fast(int storage, int collision, int rep_s, const BulkArgs& a, cudaStream_t s) {
+    if (storage == BFX_STORAGE_BF16_DEVIATION) fast::rare_s<StoreBF16Dev>(a, collision, rep_s, s);
+    else fast::rare_s<StoreF16Dev>(a, collision, rep_s, s);
+}
+
+void launch_bulk_fast(int storage, int collision, int rep_s, const GridDesc& g, const BulkArgs& a, cudaStream_t s) {
     switch (storage) {
-    case BFX_STORAGE_F16_DEVIATION: fast::bulk_s<StoreF16Dev>(a, g, collision, rep_s, part, s); break;
-    case BFX_STORAGE_BF16_DEVIATION: fast::bulk_s<StoreBF16Dev>(a, g, collision, rep_s, part, s); break;
-    default: fast::bulk_s<StoreF32>(a, g, collision, rep_s, part, s); break;
+    case BFX_STORAGE_F16_DEVIATION: fast::bulk_s<StoreF16Dev>(a, g, collision, rep_s, s); break;
+    case BFX_STORAGE_BF16_DEVIATION: fast::bulk_s<StoreBF16Dev>(a, g, collision, rep_s, s); break;
+    default: fast::bulk_s<StoreF32>(a, g, collision, rep_s, s); break;
     }
 }
 

@@ -724,9 +724,14 @@ __global__ void __launch_bounds__(128) k_links_fraction(const GeomArgs a, int ge
 // the incoming population, write it where the fluid step will read it, and
 // accumulate the momentum-exchange load in FP64.
 // ---------------------------------------------------------------------------
+__device__ void finish_state(const GeomArgs& a, float gx, float gy, float gz, int substeps, int free_flight,
+                             const bfx_bird* bird_ptr);
+
 template <class S>
-__global__ void __launch_bounds__(256) k_links_apply(const GeomArgs a, int rep_s) {
+__global__ void __launch_bounds__(256) k_links_apply(const GeomArgs a, int rep_s, int with_topology, int fuse_finish,
+                                                     const FinishParams fin) {
     __shared__ double sh[8][256];
+    __shared__ int last_block;
     using T = typename S::T;
     using R = typename S::R;
     const FluidParams& fp = a.fp;
@@ -875,53 +880,58 @@ __global__ void __launch_bounds__(256) k_links_apply(const GeomArgs a, int rep_s
             }
         }
     }
-    block_sum<8>(acc, sh);
-    if (threadIdx.x == 0)
-        for (int k = 0; k < 8; ++k) a.b.link_partials[8 * blockIdx.x + k] = acc[k];
-}
-
-// Fixed-order sum over a 1024-thread block: shuffle tree inside each warp,
-// then the 32 warp totals in order by thread 0 (the result is valid there).
-template <int K>
-__device__ __forceinline__ void block_sum_1024(double (&v)[K], double (*sh)[32]) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int k = 0; k < K; ++k)
-        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
-    if (lane == 0)
-        for (int k = 0; k < K; ++k) sh[k][warp] = v[k];
-    __syncthreads();
-    if (threadIdx.x == 0)
-        for (int k = 0; k < K; ++k) {
-            double t = 0.0;
-            for (int w = 0; w < 32; ++w) t += sh[k][w];
-            v[k] = t;
+    // Block sums: the link loads, then this block's contiguous share of the
+    // topology partials (most blocks hold no link and no topology impulse).
+    bool nonzero = false;
+    for (int k = 0; k < 8; ++k) nonzero = nonzero || acc[k] != 0.0;
+    if (__syncthreads_or(nonzero)) block_sum<8>(acc, sh);
+    double tp[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (with_topology) {
+        const int nb = a.b.box_blocks;
+        const int per = (nb + (int)gridDim.x - 1) / (int)gridDim.x;
+        const int lo = (int)blockIdx.x * per;
+        const int hi = lo + per < nb ? lo + per : nb;
+        for (int i = lo + (int)threadIdx.x; i < hi; i += blockDim.x)
+            for (int k = 0; k < 8; ++k) tp[k] += a.b.topo_partials[8 * (int64_t)i + k];
+        bool tnz = false;
+        for (int k = 0; k < 8; ++k) tnz = tnz || tp[k] != 0.0;
+        if (__syncthreads_or(tnz)) block_sum<8>(tp, sh);
+    }
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 8; ++k) {
+            a.b.link_partials[16 * blockIdx.x + k] = acc[k];
+            a.b.link_partials[16 * blockIdx.x + 8 + k] = tp[k];
         }
+        __threadfence();
+        last_block = atomicAdd(&a.b.state->apply_done, 1u) == gridDim.x - 1 ? 1 : 0;
+    }
     __syncthreads();
-}
-
-// Final fixed-order reduction of the topology and link partials (1024 threads).
-__global__ void __launch_bounds__(1024) k_reduce_loads(const GeomArgs a, int with_topology) {
-    __shared__ double sh[8][32];
-    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    if (with_topology)
-        for (int i = threadIdx.x; i < a.b.box_blocks; i += blockDim.x)
-            for (int k = 0; k < 8; ++k) acc[k] += a.b.topo_partials[8 * i + k];
-    double acc2[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int i = threadIdx.x; i < a.b.apply_blocks; i += blockDim.x)
-        for (int k = 0; k < 8; ++k) acc2[k] += a.b.link_partials[8 * i + k];
-    block_sum_1024<8>(acc, sh);
-    block_sum_1024<8>(acc2, sh);
+    if (!last_block) return;
+    // Last block: fixed-order sums of the per-block partials (the result does
+    // not depend on which block finishes last).
+    __threadfence();
+    double l[8] = {0, 0, 0, 0, 0, 0, 0, 0}, t[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x)
+        for (int k = 0; k < 8; ++k) {
+            l[k] += __ldcg(a.b.link_partials + 16 * i + k);
+            t[k] += __ldcg(a.b.link_partials + 16 * i + 8 + k);
+        }
+    block_sum<8>(l, sh);
+    block_sum<8>(t, sh);
     if (threadIdx.x == 0) {
         DeviceState* st = a.b.state;
         for (int k = 0; k < 3; ++k) {
-            st->loads_lattice[k] = acc[k] + acc2[k];
-            st->loads_torque[k] = acc[3 + k] + acc2[3 + k];
+            st->loads_lattice[k] = t[k] + l[k];
+            st->loads_torque[k] = t[3 + k] + l[3 + k];
         }
-        st->power_lattice = acc2[6];
+        st->power_lattice = l[6];
         if (with_topology) {
-            st->covered_count = (int64_t)acc[6];
-            st->uncovered_count = (int64_t)acc[7];
+            st->covered_count = (int64_t)t[6];
+            st->uncovered_count = (int64_t)t[7];
         }
+        st->apply_done = 0;
+        if (fuse_finish)
+            finish_state(a, fin.gravity[0], fin.gravity[1], fin.gravity[2], fin.substeps, fin.free_flight, a.b.bird);
     }
 }
 
@@ -941,8 +951,8 @@ __device__ void qnormalize_d(double* q) {
     }
 }
 
-__global__ void k_finish(const GeomArgs a, float gx, float gy, float gz, int substeps, int free_flight,
-                         const bfx_bird* bird_ptr) {
+__device__ void finish_state(const GeomArgs& a, float gx, float gy, float gz, int substeps, int free_flight,
+                             const bfx_bird* bird_ptr) {
     DeviceState* st = a.b.state;
     const FluidParams& fp = a.fp;
     if (free_flight) {
@@ -1051,6 +1061,11 @@ __global__ void k_finish(const GeomArgs a, float gx, float gy, float gz, int sub
     st->step += 1;
 }
 
+__global__ void k_finish(const GeomArgs a, float gx, float gy, float gz, int substeps, int free_flight,
+                         const bfx_bird* bird_ptr) {
+    finish_state(a, gx, gy, gz, substeps, free_flight, bird_ptr);
+}
+
 __global__ void k_record_sample(const GeomArgs a, bfx_run_sample* samples, uint64_t index, float dt) {
     const DeviceState* st = a.b.state;
     bfx_run_sample& s = samples[index];
@@ -1137,23 +1152,16 @@ void launch_links_emit(int geometry, int link_rule, const GridDesc& g, const Flu
 }
 
 template <class S>
-static void apply_s(const GeomArgs& a, int rep_s, cudaStream_t s) {
-    k_links_apply<S><<<a.b.apply_blocks, 256, 0, s>>>(a, rep_s);
+static void apply_s(const GeomArgs& a, int rep_s, int with_topology, const FinishParams* fin, cudaStream_t s) {
+    const FinishParams none = {};
+    k_links_apply<S><<<a.b.apply_blocks, 256, 0, s>>>(a, rep_s, with_topology, fin ? 1 : 0, fin ? *fin : none);
 }
 
 void launch_links_apply(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const GeomBuffers& gb,
-                        const FluidBuffers& fb, cudaStream_t s) {
+                        const FluidBuffers& fb, int with_topology, const FinishParams* fin, cudaStream_t s) {
     BoxDesc box = {1, 1, 1, 1};
     GeomArgs a = make_geom(g, fp, box, gb, fb.pops);
-    BFX_DISPATCH_STORAGE(storage, apply_s, a, rep_s, s);
-}
-
-void launch_reduce_loads(const GeomBuffers& gb, int with_topology, cudaStream_t s) {
-    GridDesc g = {};
-    FluidParams fp = {};
-    BoxDesc box = {1, 1, 1, 1};
-    GeomArgs a = make_geom(g, fp, box, gb, nullptr);
-    k_reduce_loads<<<1, 1024, 0, s>>>(a, with_topology);
+    BFX_DISPATCH_STORAGE(storage, apply_s, a, rep_s, with_topology, fin, s);
 }
 
 void launch_integrate(const GridDesc& g, const FluidParams& fp, const GeomBuffers& gb, float gravity_x,

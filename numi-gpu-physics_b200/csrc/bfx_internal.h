@@ -30,12 +30,13 @@ struct FluidBuffers {
     int sm_count;
 };
 
-// Fused stream + collide: part 0 = fluid interior cells (the hot kernel);
-// part 1 = the six domain faces (wrap, face rules, spill planes) and the solid /
-// newly uncovered interior cells of the geometry box (box = extent or null).
-// One step launches both parts.
+// Fused stream + collide of every cell: fluid cells collide, solid cells take
+// the moving-wall equilibrium and newly uncovered cells refill and collide.
+// box: extent of the geometry box (origin in DeviceState), null without
+// geometry; the staged 16-bit kernel leaves the box's solid / uncovered cells
+// to a second launch over the box.
 void launch_bulk(int storage, int collision, int rep_s, const GridDesc& g, const FluidParams& fp,
-                 const FluidBuffers& b, int capture, int part, const int* box, cudaStream_t s);
+                 const FluidBuffers& b, int capture, const int* box, cudaStream_t s);
 // Halo fill: the values boundary cells pull from outside the lattice (before the step).
 void launch_halo(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const FluidBuffers& b,
                  cudaStream_t s);
@@ -84,7 +85,7 @@ struct GeomBuffers {
     uint32_t* block_offsets;
     int box_blocks;
     double* topo_partials;          // 8 per box block
-    double* link_partials;          // 8 per apply block
+    double* link_partials;          // 16 per apply block (link sums, topology sums)
     int apply_blocks;
     DeviceState* state;
     Objective* objective;           // load objective accumulated by the step end (may be null)
@@ -101,9 +102,17 @@ void launch_boundary_scan(int storage, int rep_s, const GridDesc& g, const Fluid
                           const GeomBuffers& gb, const FluidBuffers& fb, cudaStream_t s);
 void launch_links_emit(int geometry, int link_rule, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
                        const GeomBuffers& gb, cudaStream_t s);
+// End-of-step body update parameters (k_finish).
+struct FinishParams {
+    float gravity[3];
+    int substeps;
+    int free_flight;
+};
+// Cut-link bounce-back and loads; the launch's last block also reduces the
+// link and topology partials into the step's loads and, with `fin`, runs the
+// end-of-step body update that launch_integrate would run.
 void launch_links_apply(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const GeomBuffers& gb,
-                        const FluidBuffers& fb, cudaStream_t s);
-void launch_reduce_loads(const GeomBuffers& gb, int with_topology, cudaStream_t s);
+                        const FluidBuffers& fb, int with_topology, const FinishParams* fin, cudaStream_t s);
 void launch_integrate(const GridDesc& g, const FluidParams& fp, const GeomBuffers& gb, float gravity_x,
                       float gravity_y, float gravity_z, int substeps, int free_flight, cudaStream_t s);
 void launch_record_sample(const GeomBuffers& gb, const FluidParams& fp, bfx_run_sample* samples, uint64_t index,
@@ -163,6 +172,8 @@ void launch_fill_wall(float4* wall, int64_t n, float w, cudaStream_t s);
 bool encode_population_map(CUtensorMap* map, void* pops, int storage, int64_t px, int64_t py, int64_t pz);
 // Collision operators whose 16-bit fluid step runs the staged kernel.
 bool staged_collision(int collision);
+// Kernel launches of one launch_bulk call.
+int launch_bulk_count(int storage, int collision, int capture, bool tma_ok, bool geometry);
 // Raises the staged kernel's shared-memory limit for a 16-bit storage format
 // and collision operator (call before any graph capture).
 void prepare_stream(int storage, int collision);

@@ -228,6 +228,7 @@ __global__ void __launch_bounds__(kStreamThreads, 4)
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(empty0 + 8 * s);
+        // solid and newly uncovered cells (mask byte set) are left to k_rare
         va = va && ma == 0;
         vb = vb && mb == 0;
         if (!__any_sync(0xffffffffu, va || vb)) continue;

@@ -68,7 +68,7 @@ struct DeviceState {
     uint64_t launches_device;
     double power_lattice;          // last step: sum over cut links of F_link . u_wall (lattice units)
     uint32_t stream_error;         // nonzero: a staged-kernel pipeline wait timed out (1 producer, 2 consumer)
-    uint32_t _pad1;
+    uint32_t apply_done;           // link-kernel blocks finished this launch (0 between launches)
     SegmentFrame seg[4];           // mesh segments 3..6: left / right middle, left / right outer
 };
 
