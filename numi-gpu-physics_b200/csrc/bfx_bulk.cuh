@@ -18,6 +18,7 @@ struct BulkArgs {
     int32_t doff[19];       // c_q . (1, px, px*py): padded neighbour offset of direction q
     float far_eq_f[19];     // equilibrium(q, far density, far velocity), FP32
     double far_eq_d[19];    // same in FP64 (FP64 storage)
+    float far_dev[19];      // (far_eq_f - w_q) x the storage's deviation scale (16-bit formats)
     int box[3];             // geometry box extent (origin in DeviceState); rare-cell launch
     void* pops;
     const uint8_t* mask;

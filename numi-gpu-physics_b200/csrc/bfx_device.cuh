@@ -130,6 +130,10 @@ struct StoreF16Dev {
         float w = q == 0 ? Lat<float>::w0 : (q <= 6 ? Lat<float>::w1 : Lat<float>::w2);
         *p = __float2half_rn(__fmaf_rn(v, kF16Scale, -w * kF16Scale));
     }
+    // the stored value itself: the deviation f - w_q scaled by kDevScale
+    static constexpr float kDevScale = kF16Scale;
+    __device__ __forceinline__ static float ld_dev(const T* p) { return __half2float(*p); }
+    __device__ __forceinline__ static void st_dev(T* p, float v) { *p = __float2half_rn(v); }
 };
 struct StoreBF16Dev {
     using T = __nv_bfloat16;
@@ -147,6 +151,9 @@ struct StoreBF16Dev {
         float w = q == 0 ? Lat<float>::w0 : (q <= 6 ? Lat<float>::w1 : Lat<float>::w2);
         *p = __float2bfloat16_rn(v - w);
     }
+    static constexpr float kDevScale = 1.0f;
+    __device__ __forceinline__ static float ld_dev(const T* p) { return __bfloat162float(*p); }
+    __device__ __forceinline__ static void st_dev(T* p, float v) { *p = __float2bfloat16_rn(v); }
 };
 
 // ---------------------------------------------------------------------------

@@ -278,6 +278,8 @@ BulkArgs make_bulk_args(const GridDesc& gd, const FluidParams& fp, const FluidBu
         a.doff[q] = (int32_t)((int64_t)cx(q) + (int64_t)a.g.px * cy(q) + a.g.pxy * cz(q));
         a.far_eq_f[q] = host_feq<float>(q, fp.far[3], fp.far[0], fp.far[1], fp.far[2]);
         a.far_eq_d[q] = host_feq<double>(q, (double)fp.far[3], (double)fp.far[0], (double)fp.far[1], (double)fp.far[2]);
+        const double scale = storage == BFX_STORAGE_F16_DEVIATION ? (double)StoreF16Dev::kDevScale : 1.0;
+        a.far_dev[q] = (float)((a.far_eq_d[q] - wq<double>(q)) * scale);
     }
     a.pops = b.pops;
     a.mask = b.mask;

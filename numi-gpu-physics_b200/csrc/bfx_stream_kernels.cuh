@@ -1,6 +1,6 @@
 // TMA-staged fused stream + collide (see bfx_stream.cuh for the pipeline), for
-// the 16-bit deviation formats with the TRT operator.  Included in the
-// contracted translation unit only (bfx_fluid_fast.cu, after
+// the 16-bit deviation formats with the TRT, regularized and RR3 operators.
+// Included in the contracted translation unit only (bfx_fluid_fast.cu, after
 // bfx_bulk_kernels.cuh).
 //
 // Two cells per lane (x and x + 32 of the warp's 64-cell row) are collided in
@@ -9,6 +9,17 @@
 // bit-identical FP32 step: the assembler fuses packed multiply / add pairs into
 // FFMA2 even when each carries an explicit rounding mode (measured: a 1-ulp
 // change of x*x + y*y + z*z in 17 % of cases under --fmad=false).
+//
+// The collision runs on the stored quantity itself, the scaled deviation
+// d_q = s (f_q - w_q) (s = 4096 for FP16, 1 for BF16): a load or store is one
+// conversion with no offset arithmetic, and the moments and non-equilibrium
+// parts are formed from numbers of size s |f - w| rather than differences of
+// numbers of size w.  With D = sum d / s (so rho = 1 + D) every term of the
+// operator is linear in d or in the equilibrium deviation
+//   e_q = s (feq_q - w_q) = w_q s D + s rho w_q (3 cu + 4.5 cu^2 - 1.5 u^2),
+// split into its even part E_q (w_q s D + s rho w_q (4.5 cu^2 - 1.5 u^2)) and
+// odd part O_q (3 s rho w_q cu), so TRT and the regularized operators keep
+// their form with f -> d and feq -> e.
 #include "bfx_stream.cuh"
 
 #if !defined(BFX_VARIANT) || !defined(BFX_CONTRACTED)
@@ -18,95 +29,164 @@
 namespace bfx {
 namespace BFX_VARIANT {
 
-// c_q . u with the zero products dropped (cdotq on pairs)
-__device__ __forceinline__ P2 cdot2(int q, P2 ux, P2 uy, P2 uz) {
-    P2 r = pv(0.0f);
-    bool first = true;
-    if (cx(q) != 0) { r = cx(q) > 0 ? ux : -ux; first = false; }
-    if (cy(q) != 0) { r = first ? (cy(q) > 0 ? uy : -uy) : (cy(q) > 0 ? r + uy : r - uy); first = false; }
-    if (cz(q) != 0) { r = first ? (cz(q) > 0 ? uz : -uz) : (cz(q) > 0 ? r + uz : r - uz); }
-    return r;
-}
-
-// Moments in the reference order (moments<R> on pairs).
-__device__ __forceinline__ void moments2(const P2 (&f)[19], P2& rho, P2& ux, P2& uy, P2& uz) {
-    P2 r = pv(0.0f), mx = pv(0.0f), my = pv(0.0f), mz = pv(0.0f);
-#pragma unroll
-    for (int q = 0; q < 19; ++q) {
-        r = r + f[q];
-        if (cx(q) > 0) mx = mx + f[q];
-        if (cx(q) < 0) mx = mx - f[q];
-        if (cy(q) > 0) my = my + f[q];
-        if (cy(q) < 0) my = my - f[q];
-        if (cz(q) > 0) mz = mz + f[q];
-        if (cz(q) < 0) mz = mz - f[q];
-    }
-    r.x = r.x > 1.0e-8f ? r.x : 1.0e-8f;
-    r.y = r.y > 1.0e-8f ? r.y : 1.0e-8f;
-    rho = r;
-    const P2 inv = make_float2(1.0f / r.x, 1.0f / r.y);
-    ux = mx * inv;
-    uy = my * inv;
-    uz = mz * inv;
-}
-
-// collide<float, COLL> on two cells; the limiter runs lane by lane through
-// the scalar operator.
+// Collision of two cells in scaled deviation space (see above).  d: incoming
+// deviations; post: outgoing deviations.  For the regularized operators,
+// `slow` flags a lane where some outgoing population may fall below its
+// positivity floor; the caller then runs admit_dev_lane on it.
 template <int COLL>
-__device__ __forceinline__ void collide2(const P2 (&f)[19], P2 rho, P2 ux, P2 uy, P2 uz, float omega_p, float omega_m,
-                                         P2 (&post)[19], float (&activation)[2], float (&restriction)[2]) {
-    if (COLL == BFX_COLLISION_TRT_LIMITER) {
-#pragma unroll
-        for (int l = 0; l < 2; ++l) {
-            float fs[19], ps[19];
-#pragma unroll
-            for (int q = 0; q < 19; ++q) fs[q] = l ? f[q].y : f[q].x;
-            collide<float, COLL>(fs, l ? rho.y : rho.x, l ? ux.y : ux.x, l ? uy.y : uy.x, l ? uz.y : uz.x, omega_p,
-                                 omega_m, ps, activation[l], restriction[l]);
-#pragma unroll
-            for (int q = 0; q < 19; ++q) {
-                if (l) post[q].y = ps[q];
-                else post[q].x = ps[q];
-            }
-        }
-        return;
-    }
-    const P2 u2 = ux * ux + uy * uy + uz * uz;
-    const P2 t15 = 1.5f * u2;
-    const P2 wr0 = Lat<float>::w0 * rho, wr1 = Lat<float>::w1 * rho, wr2 = Lat<float>::w2 * rho;
-    P2 feqv[19];
-    // 1 + 3*0 + 4.5*0*0 is exactly 1
-    feqv[0] = wr0 * (pv(1.0f) - t15);
+__device__ __forceinline__ void collide_dev2(const P2 (&d)[19], float s, float inv_s, float omega_p, float omega_m,
+                                             P2 (&post)[19], P2& rho, P2& ux, P2& uy, P2& uz, bool (&slow)[2]) {
+    constexpr float cs2 = Lat<float>::cs2;
+    P2 ps[19], md[19];
+    P2 dsum = d[0];
 #pragma unroll
     for (int q = 1; q < 19; q += 2) {
-        const P2 cu = cdot2(q, ux, uy, uz);
-        const P2 t3 = 3.0f * cu;
-        const P2 t45 = (4.5f * cu) * cu;
-        const P2 wr = q <= 6 ? wr1 : wr2;
-        feqv[q] = wr * (((pv(1.0f) + t3) + t45) - t15);
-        feqv[q + 1] = wr * (((pv(1.0f) - t3) + t45) - t15);
+        ps[q] = d[q] + d[q + 1];
+        md[q] = d[q] - d[q + 1];
+        dsum = dsum + ps[q];
     }
-    {
-        // TRT; the regularized operators run through collide_pairs
-        post[0] = f[0] - omega_p * (f[0] - feqv[0]);
+    const P2 mx = pair_dot<0>(md), my = pair_dot<1>(md), mz = pair_dot<2>(md);
+    P2 k;
+#pragma unroll
+    for (int l = 0; l < 2; ++l) {
+        float r = __fmaf_rn(Lanes<P2>::get(dsum, l), inv_s, 1.0f);
+        r = r > 1.0e-8f ? r : 1.0e-8f;
+        Lanes<P2>::set(rho, l, r);
+        Lanes<P2>::set(k, l, inv_s / r);
+        slow[l] = r > 1.0e3f;
+    }
+    ux = mx * k;
+    uy = my * k;
+    uz = mz * k;
+    const P2 t15 = 1.5f * ((ux * ux + uy * uy) + uz * uz);
+    const P2 sr = s * rho;
+    const P2 sr1 = Lat<float>::w1 * sr, sr2 = Lat<float>::w2 * sr;
+    const P2 wd1 = Lat<float>::w1 * dsum, wd2 = Lat<float>::w2 * dsum;
+    const P2 e0 = Lat<float>::w0 * dsum - (Lat<float>::w0 * sr) * t15;
+    auto even_odd = [&](int q, P2& E, P2& O) {
+        const P2 cu = cdot_pair(q, ux, uy, uz);
+        const P2 srw = q <= 6 ? sr1 : sr2;
+        E = (q <= 6 ? wd1 : wd2) + srw * ((4.5f * cu) * cu - t15);
+        O = srw * (3.0f * cu);
+    };
+    if (COLL == BFX_COLLISION_TRT) {
+        // BF.metal:3063-3093 on the deviations (w_q is its own even part):
+        // with d_q = p + m, d_q' = p - m (p, m the pair's even and odd halves)
+        // post_q = P + M, post_q' = P - M, P = p - w+ (p - E), M = m - w- (m - O)
+        post[0] = d[0] - omega_p * (d[0] - e0);
+        const float kp = 0.5f * (1.0f - omega_p), km = 0.5f * (1.0f - omega_m);
 #pragma unroll
         for (int q = 1; q < 19; q += 2) {
-            const P2 fp_ = 0.5f * (f[q] + f[q + 1]);
-            const P2 fm = 0.5f * (f[q] - f[q + 1]);
-            const P2 ep = 0.5f * (feqv[q] + feqv[q + 1]);
-            const P2 em = 0.5f * (feqv[q] - feqv[q + 1]);
-            const P2 A = omega_p * (fp_ - ep);
-            const P2 B = omega_m * (fm - em);
-            post[q] = (f[q] - A) - B;
-            post[q + 1] = (f[q + 1] - A) + B;
+            P2 E, O;
+            even_odd(q, E, O);
+            const P2 P = kp * ps[q] + omega_p * E;
+            const P2 M = km * md[q] + omega_m * O;
+            post[q] = P + M;
+            post[q + 1] = P - M;
         }
+        slow[0] = slow[1] = false;
+        return;
+    }
+    P2 E[19], O[19];
+#pragma unroll
+    for (int q = 1; q < 19; q += 2) even_odd(q, E[q], O[q]);
+    // regularized / RR3 (BF.metal:2917-3062), pair-restated as in collide_pairs
+    P2 nps[19];
+    P2 ntot = d[0] - e0;
+#pragma unroll
+    for (int q = 1; q < 19; q += 2) {
+        nps[q] = ps[q] - 2.0f * E[q];
+        ntot = ntot + nps[q];
+    }
+    const P2 dsx = pair_second<0, 0>(nps) - cs2 * ntot;
+    const P2 dsy = pair_second<1, 1>(nps) - cs2 * ntot;
+    const P2 dsz = pair_second<2, 2>(nps) - cs2 * ntot;
+    const P2 odx = pair_second<0, 1>(nps), ody = pair_second<0, 2>(nps), odz = pair_second<1, 2>(nps);
+    const P2 aXxy = (2.0f * ux) * odx + uy * dsx;
+    const P2 aXxz = (2.0f * ux) * ody + uz * dsx;
+    const P2 aXyy = ux * dsy + (2.0f * uy) * odx;
+    const P2 aXzz = ux * dsz + (2.0f * uz) * ody;
+    const P2 aYyz = (2.0f * uy) * odz + uz * dsy;
+    const P2 aYzz = uy * dsz + (2.0f * uz) * odz;
+    const P2 trace = (dsx + dsy) + dsz;
+    const P2 cax = dsx - cs2 * trace, cay = dsy - cs2 * trace, caz = dsz - cs2 * trace;
+    const float om = 1.0f - omega_p;
+    const float om0 = om * (Lat<float>::w0 * 4.5f * -cs2);
+    const float om1 = om * (Lat<float>::w1 * 4.5f), om2 = om * (Lat<float>::w2 * 4.5f);
+    const float ot1 = om * (Lat<float>::w1 * 13.5f), ot2 = om * (Lat<float>::w2 * 13.5f);
+    // positivity floor max(1e-12, 1e-6 feq) <= w_q / 2 unless rho > 1e3 (flagged
+    // above), so a population at or above w_q / 2 needs no admission:
+    // the exact test runs only on a lane with a deviation below -s w_q / 2
+    post[0] = e0 + om0 * trace;
+    const float h0 = -0.5f * Lat<float>::w0 * s, h1 = -0.5f * Lat<float>::w1 * s, h2 = -0.5f * Lat<float>::w2 * s;
+#pragma unroll
+    for (int l = 0; l < 2; ++l) slow[l] = slow[l] || Lanes<P2>::get(post[0], l) < h0;
+#pragma unroll
+    for (int q = 1; q < 19; q += 2) {
+        const float hx = (float)(cx(q) * cx(q)) - cs2, hy = (float)(cy(q) * cy(q)) - cs2,
+                    hz = (float)(cz(q) * cz(q)) - cs2;
+        P2 contraction;
+        if (cx(q) != 0 && cy(q) != 0) contraction = (cax + dsy) + 2.0f * (cx(q) * cy(q) > 0 ? odx : -odx);
+        else if (cx(q) != 0 && cz(q) != 0) contraction = (cax + dsz) + 2.0f * (cx(q) * cz(q) > 0 ? ody : -ody);
+        else if (cy(q) != 0 && cz(q) != 0) contraction = (cay + dsz) + 2.0f * (cy(q) * cz(q) > 0 ? odz : -odz);
+        else contraction = cx(q) != 0 ? cax : (cy(q) != 0 ? cay : caz);
+        const P2 X = E[q] + (q <= 6 ? om1 : om2) * contraction;
+        P2 Y = O[q];
+        if (COLL == BFX_COLLISION_RR3) {
+            P2 third = pv(0.0f);
+            bool any = false;
+            auto add = [&](int da, float hb, P2 amp) {
+                if (da == 0) return;
+                const P2 t = ((float)da * hb) * amp;
+                third = any ? third + t : t;
+                any = true;
+            };
+            add(cy(q), hx, aXxy);
+            add(cz(q), hx, aXxz);
+            add(cx(q), hy, aXyy);
+            add(cx(q), hz, aXzz);
+            add(cz(q), hy, aYyz);
+            add(cy(q), hz, aYzz);
+            Y = Y + (q <= 6 ? ot1 : ot2) * third;
+        }
+        post[q] = X + Y;
+        post[q + 1] = X - Y;
+        const float hq = q <= 6 ? h1 : h2;
+#pragma unroll
+        for (int l = 0; l < 2; ++l)
+            slow[l] = slow[l] || Lanes<P2>::get(post[q], l) < hq || Lanes<P2>::get(post[q + 1], l) < hq;
     }
 }
 
-// Storage conversions of one population (ld_rt / st_rt on pairs).
-template <class S>
-__device__ __forceinline__ float ld1(const typename S::T* p, int q) {
-    return S::ld_rt(p, q);
+// Exact positivity admission of one lane (BF.metal:3035-3052) on absolute
+// populations f = w_q + d / s: the admissible scale over every direction, and
+// the scaled blend feq + scale (cand - feq) when it is below 1.
+__device__ __forceinline__ void admit_dev_lane(P2 (&post)[19], int l, float rho, float ux, float uy, float uz,
+                                               float s, float inv_s, float& activation, float& restriction) {
+    float scale = 1.0f;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        const float fe = feq_rt<float>(q, rho, ux, uy, uz);
+        const float cand = __fmaf_rn(Lanes<P2>::get(post[q], l), inv_s, wq<float>(q));
+        const float floor_ = admit_floor(fe);
+        if (cand < floor_) {
+            float den = fe - cand;
+            den = den > 1.0e-30f ? den : 1.0e-30f;
+            float adm = (fe - floor_) / den;
+            adm = adm < 0.0f ? 0.0f : (adm > 1.0f ? 1.0f : adm);
+            scale = scale < adm ? scale : adm;
+        }
+    }
+    if (scale < 1.0f) {
+        activation = 1.0f;
+        restriction = 1.0f - scale;
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            const float fe = feq_rt<float>(q, rho, ux, uy, uz);
+            const float cand = __fmaf_rn(Lanes<P2>::get(post[q], l), inv_s, wq<float>(q));
+            Lanes<P2>::set(post[q], l, (fe + scale * (cand - fe) - wq<float>(q)) * s);
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -218,13 +298,13 @@ __global__ void __launch_bounds__(kStreamThreads, 4)
             break;
         }
         const T* row = (const T*)(smem + s * G::stage_bytes) + warp * G::row;
-        P2 f[19];
+        constexpr float dscale = S::kDevScale, inv_dscale = 1.0f / S::kDevScale;
+        P2 dv[19];
 #pragma unroll
         for (int q = 0; q < 19; ++q) {
             const int base = REP_S ? 1 : 1 - cx(q);
             const T* p = row + q * (G::plane_bytes / (int)sizeof(T)) + base + lane;
-            const int slot = REP_S ? q : opp(q);
-            f[q] = make_float2(S::ld_rt(p, slot), S::ld_rt(p + 32, slot));
+            dv[q] = make_float2(S::ld_dev(p), S::ld_dev(p + 32));
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(empty0 + 8 * s);
@@ -232,24 +312,27 @@ __global__ void __launch_bounds__(kStreamThreads, 4)
         va = va && ma == 0;
         vb = vb && mb == 0;
         if (!__any_sync(0xffffffffu, va || vb)) continue;
-        P2 post[19];
+        P2 post[19], rho, ux, uy, uz;
+        bool slow[2];
         float activation[2] = {0.0f, 0.0f}, restriction[2] = {0.0f, 0.0f};
-        if constexpr (COLL == BFX_COLLISION_RR3 || COLL == BFX_COLLISION_REGULARIZED) {
-            collide_pairs<P2, COLL>(f, fp.omega_p, post, activation, restriction);
-        } else {
-            P2 rho, ux, uy, uz;
-            moments2(f, rho, ux, uy, uz);
-            collide2<COLL>(f, rho, ux, uy, uz, fp.omega_p, fp.omega_m, post, activation, restriction);
+        collide_dev2<COLL>(dv, dscale, inv_dscale, fp.omega_p, fp.omega_m, post, rho, ux, uy, uz, slow);
+        if (COLL != BFX_COLLISION_TRT) {
+#pragma unroll
+            for (int l = 0; l < 2; ++l)
+                if (slow[l])
+                    admit_dev_lane(post, l, Lanes<P2>::get(rho, l), Lanes<P2>::get(ux, l), Lanes<P2>::get(uy, l),
+                                   Lanes<P2>::get(uz, l), dscale, inv_dscale, activation[l], restriction[l]);
         }
         if (fp.has_sponge) {
             const float spa = va ? sponge_factor(g, fp, xa, y, z) : 0.0f;
             const float spb = vb ? sponge_factor(g, fp, xb, y, z) : 0.0f;
             if (spa > 0.0f || spb > 0.0f) {
-                // post + (far - post) * sp, a zero factor leaving the lane unchanged
+                // post + (far - post) * sp on the deviations, a zero factor
+                // leaving the lane unchanged
                 const P2 sp = make_float2(spa, spb);
 #pragma unroll
                 for (int q = 0; q < 19; ++q) {
-                    const P2 d = (pv(a.far_eq_f[q]) - post[q]) * sp;
+                    const P2 d = (pv(a.far_dev[q]) - post[q]) * sp;
                     post[q] = make_float2(spa > 0.0f ? post[q].x + d.x : post[q].x,
                                           spb > 0.0f ? post[q].y + d.y : post[q].y);
                 }
@@ -267,15 +350,17 @@ __global__ void __launch_bounds__(kStreamThreads, 4)
                 if (cz(q) > 0) cmz = cmz + post[q];
                 if (cz(q) < 0) cmz = cmz - post[q];
             }
-            cd.x = cd.x > 1.0e-8f ? cd.x : 1.0e-8f;
-            cd.y = cd.y > 1.0e-8f ? cd.y : 1.0e-8f;
-            if (va) {
-                a.density[gida] = cd.x;
-                a.velocity[gida] = make_float4(cmx.x / cd.x, cmy.x / cd.x, cmz.x / cd.x, 0.0f);
-            }
-            if (vb) {
-                a.density[gida + 32] = cd.y;
-                a.velocity[gida + 32] = make_float4(cmx.y / cd.y, cmy.y / cd.y, cmz.y / cd.y, 0.0f);
+            // rho = 1 + sum d / s, momentum = sum c d / s (sum w_q c_q = 0)
+#pragma unroll
+            for (int l = 0; l < 2; ++l) {
+                if (!(l ? vb : va)) continue;
+                float r = __fmaf_rn(Lanes<P2>::get(cd, l), inv_dscale, 1.0f);
+                r = r > 1.0e-8f ? r : 1.0e-8f;
+                const uint32_t gl = gida + 32 * l;
+                a.density[gl] = r;
+                a.velocity[gl] = make_float4(Lanes<P2>::get(cmx, l) * inv_dscale / r,
+                                             Lanes<P2>::get(cmy, l) * inv_dscale / r,
+                                             Lanes<P2>::get(cmz, l) * inv_dscale / r, 0.0f);
             }
         }
         if (COLL != BFX_COLLISION_TRT) {
@@ -290,9 +375,8 @@ __global__ void __launch_bounds__(kStreamThreads, 4)
 #pragma unroll
         for (int q = 0; q < 19; ++q) {
             T* p = REP_S ? (T*)a.plane[opp(q)] + pid : (T*)a.plane[q] + (uint32_t)(pid + (uint32_t)a.doff[q]);
-            const int slot = REP_S ? opp(q) : q;
-            if (va) S::st_rt(p, slot, post[q].x);
-            if (vb) S::st_rt(p + 32, slot, post[q].y);
+            if (va) S::st_dev(p, post[q].x);
+            if (vb) S::st_dev(p + 32, post[q].y);
         }
     }
 }
