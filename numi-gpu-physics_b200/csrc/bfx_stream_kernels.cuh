@@ -69,7 +69,7 @@ __device__ __forceinline__ void collide_dev2(const P2 (&d)[19], float s, float i
         E = (q <= 6 ? wd1 : wd2) + srw * ((4.5f * cu) * cu - t15);
         O = srw * (3.0f * cu);
     };
-    if (COLL == BFX_COLLISION_TRT) {
+    if constexpr (COLL == BFX_COLLISION_TRT) {
         // BF.metal:3063-3093 on the deviations (w_q is its own even part):
         // with d_q = p + m, d_q' = p - m (p, m the pair's even and odd halves)
         // post_q = P + M, post_q' = P - M, P = p - w+ (p - E), M = m - w- (m - O)
@@ -85,76 +85,76 @@ __device__ __forceinline__ void collide_dev2(const P2 (&d)[19], float s, float i
             post[q + 1] = P - M;
         }
         slow[0] = slow[1] = false;
-        return;
-    }
-    P2 E[19], O[19];
+    } else {
+        P2 E[19], O[19];
 #pragma unroll
-    for (int q = 1; q < 19; q += 2) even_odd(q, E[q], O[q]);
-    // regularized / RR3 (BF.metal:2917-3062), pair-restated as in collide_pairs
-    P2 nps[19];
-    P2 ntot = d[0] - e0;
+        for (int q = 1; q < 19; q += 2) even_odd(q, E[q], O[q]);
+        // regularized / RR3 (BF.metal:2917-3062), pair-restated as in collide_pairs
+        P2 nps[19];
+        P2 ntot = d[0] - e0;
 #pragma unroll
-    for (int q = 1; q < 19; q += 2) {
-        nps[q] = ps[q] - 2.0f * E[q];
-        ntot = ntot + nps[q];
-    }
-    const P2 dsx = pair_second<0, 0>(nps) - cs2 * ntot;
-    const P2 dsy = pair_second<1, 1>(nps) - cs2 * ntot;
-    const P2 dsz = pair_second<2, 2>(nps) - cs2 * ntot;
-    const P2 odx = pair_second<0, 1>(nps), ody = pair_second<0, 2>(nps), odz = pair_second<1, 2>(nps);
-    const P2 aXxy = (2.0f * ux) * odx + uy * dsx;
-    const P2 aXxz = (2.0f * ux) * ody + uz * dsx;
-    const P2 aXyy = ux * dsy + (2.0f * uy) * odx;
-    const P2 aXzz = ux * dsz + (2.0f * uz) * ody;
-    const P2 aYyz = (2.0f * uy) * odz + uz * dsy;
-    const P2 aYzz = uy * dsz + (2.0f * uz) * odz;
-    const P2 trace = (dsx + dsy) + dsz;
-    const P2 cax = dsx - cs2 * trace, cay = dsy - cs2 * trace, caz = dsz - cs2 * trace;
-    const float om = 1.0f - omega_p;
-    const float om0 = om * (Lat<float>::w0 * 4.5f * -cs2);
-    const float om1 = om * (Lat<float>::w1 * 4.5f), om2 = om * (Lat<float>::w2 * 4.5f);
-    const float ot1 = om * (Lat<float>::w1 * 13.5f), ot2 = om * (Lat<float>::w2 * 13.5f);
-    // positivity floor max(1e-12, 1e-6 feq) <= w_q / 2 unless rho > 1e3 (flagged
-    // above), so a population at or above w_q / 2 needs no admission:
-    // the exact test runs only on a lane with a deviation below -s w_q / 2
-    post[0] = e0 + om0 * trace;
-    const float h0 = -0.5f * Lat<float>::w0 * s, h1 = -0.5f * Lat<float>::w1 * s, h2 = -0.5f * Lat<float>::w2 * s;
-#pragma unroll
-    for (int l = 0; l < 2; ++l) slow[l] = slow[l] || Lanes<P2>::get(post[0], l) < h0;
-#pragma unroll
-    for (int q = 1; q < 19; q += 2) {
-        const float hx = (float)(cx(q) * cx(q)) - cs2, hy = (float)(cy(q) * cy(q)) - cs2,
-                    hz = (float)(cz(q) * cz(q)) - cs2;
-        P2 contraction;
-        if (cx(q) != 0 && cy(q) != 0) contraction = (cax + dsy) + 2.0f * (cx(q) * cy(q) > 0 ? odx : -odx);
-        else if (cx(q) != 0 && cz(q) != 0) contraction = (cax + dsz) + 2.0f * (cx(q) * cz(q) > 0 ? ody : -ody);
-        else if (cy(q) != 0 && cz(q) != 0) contraction = (cay + dsz) + 2.0f * (cy(q) * cz(q) > 0 ? odz : -odz);
-        else contraction = cx(q) != 0 ? cax : (cy(q) != 0 ? cay : caz);
-        const P2 X = E[q] + (q <= 6 ? om1 : om2) * contraction;
-        P2 Y = O[q];
-        if (COLL == BFX_COLLISION_RR3) {
-            P2 third = pv(0.0f);
-            bool any = false;
-            auto add = [&](int da, float hb, P2 amp) {
-                if (da == 0) return;
-                const P2 t = ((float)da * hb) * amp;
-                third = any ? third + t : t;
-                any = true;
-            };
-            add(cy(q), hx, aXxy);
-            add(cz(q), hx, aXxz);
-            add(cx(q), hy, aXyy);
-            add(cx(q), hz, aXzz);
-            add(cz(q), hy, aYyz);
-            add(cy(q), hz, aYzz);
-            Y = Y + (q <= 6 ? ot1 : ot2) * third;
+        for (int q = 1; q < 19; q += 2) {
+            nps[q] = ps[q] - 2.0f * E[q];
+            ntot = ntot + nps[q];
         }
-        post[q] = X + Y;
-        post[q + 1] = X - Y;
-        const float hq = q <= 6 ? h1 : h2;
+        const P2 dsx = pair_second<0, 0>(nps) - cs2 * ntot;
+        const P2 dsy = pair_second<1, 1>(nps) - cs2 * ntot;
+        const P2 dsz = pair_second<2, 2>(nps) - cs2 * ntot;
+        const P2 odx = pair_second<0, 1>(nps), ody = pair_second<0, 2>(nps), odz = pair_second<1, 2>(nps);
+        const P2 aXxy = (2.0f * ux) * odx + uy * dsx;
+        const P2 aXxz = (2.0f * ux) * ody + uz * dsx;
+        const P2 aXyy = ux * dsy + (2.0f * uy) * odx;
+        const P2 aXzz = ux * dsz + (2.0f * uz) * ody;
+        const P2 aYyz = (2.0f * uy) * odz + uz * dsy;
+        const P2 aYzz = uy * dsz + (2.0f * uz) * odz;
+        const P2 trace = (dsx + dsy) + dsz;
+        const P2 cax = dsx - cs2 * trace, cay = dsy - cs2 * trace, caz = dsz - cs2 * trace;
+        const float om = 1.0f - omega_p;
+        const float om0 = om * (Lat<float>::w0 * 4.5f * -cs2);
+        const float om1 = om * (Lat<float>::w1 * 4.5f), om2 = om * (Lat<float>::w2 * 4.5f);
+        const float ot1 = om * (Lat<float>::w1 * 13.5f), ot2 = om * (Lat<float>::w2 * 13.5f);
+        // positivity floor max(1e-12, 1e-6 feq) <= w_q / 2 unless rho > 1e3 (flagged
+        // above), so a population at or above w_q / 2 needs no admission:
+        // the exact test runs only on a lane with a deviation below -s w_q / 2
+        post[0] = e0 + om0 * trace;
+        const float h0 = -0.5f * Lat<float>::w0 * s, h1 = -0.5f * Lat<float>::w1 * s, h2 = -0.5f * Lat<float>::w2 * s;
 #pragma unroll
-        for (int l = 0; l < 2; ++l)
-            slow[l] = slow[l] || Lanes<P2>::get(post[q], l) < hq || Lanes<P2>::get(post[q + 1], l) < hq;
+        for (int l = 0; l < 2; ++l) slow[l] = slow[l] || Lanes<P2>::get(post[0], l) < h0;
+#pragma unroll
+        for (int q = 1; q < 19; q += 2) {
+            const float hx = (float)(cx(q) * cx(q)) - cs2, hy = (float)(cy(q) * cy(q)) - cs2,
+                        hz = (float)(cz(q) * cz(q)) - cs2;
+            P2 contraction;
+            if (cx(q) != 0 && cy(q) != 0) contraction = (cax + dsy) + 2.0f * (cx(q) * cy(q) > 0 ? odx : -odx);
+            else if (cx(q) != 0 && cz(q) != 0) contraction = (cax + dsz) + 2.0f * (cx(q) * cz(q) > 0 ? ody : -ody);
+            else if (cy(q) != 0 && cz(q) != 0) contraction = (cay + dsz) + 2.0f * (cy(q) * cz(q) > 0 ? odz : -odz);
+            else contraction = cx(q) != 0 ? cax : (cy(q) != 0 ? cay : caz);
+            const P2 X = E[q] + (q <= 6 ? om1 : om2) * contraction;
+            P2 Y = O[q];
+            if (COLL == BFX_COLLISION_RR3) {
+                P2 third = pv(0.0f);
+                bool any = false;
+                auto add = [&](int da, float hb, P2 amp) {
+                    if (da == 0) return;
+                    const P2 t = ((float)da * hb) * amp;
+                    third = any ? third + t : t;
+                    any = true;
+                };
+                add(cy(q), hx, aXxy);
+                add(cz(q), hx, aXxz);
+                add(cx(q), hy, aXyy);
+                add(cx(q), hz, aXzz);
+                add(cz(q), hy, aYyz);
+                add(cy(q), hz, aYzz);
+                Y = Y + (q <= 6 ? ot1 : ot2) * third;
+            }
+            post[q] = X + Y;
+            post[q + 1] = X - Y;
+            const float hq = q <= 6 ? h1 : h2;
+#pragma unroll
+            for (int l = 0; l < 2; ++l)
+                slow[l] = slow[l] || Lanes<P2>::get(post[q], l) < hq || Lanes<P2>::get(post[q + 1], l) < hq;
+        }
     }
 }
 
