@@ -116,7 +116,13 @@ struct bfx_sim {
     // pair starts from (the launch sequence repeats with period two).
     cudaGraphExec_t pair_graph[2] = {nullptr, nullptr};
     uint64_t pair_launches[2] = {0, 0};
+    // single steps (an odd step count, one-step calls), same keying
+    cudaGraphExec_t step_graph[2] = {nullptr, nullptr};
+    uint64_t step_launches[2] = {0, 0};
     bool graphs_enabled = true;
+    // pinned host staging of the device state: read-backs and body uploads
+    // without a pageable-copy bounce
+    DeviceState* hstate = nullptr;
 
     bool geometry() const { return cfg.geometry != BFX_GEOMETRY_NONE; }
     bool moving() const { return geometry() && !cfg.static_geometry; }
@@ -336,28 +342,42 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
 // Replays (capturing on first use) the two-step graph for the current parity.
 // Host-side state (representation, mask index) returns to its starting value
 // after two steps, so the captured launches stay valid for every later pair.
-int run_pair_graph(bfx_sim* s) {
+// Replays (capturing on first use) the graph of `nsteps` (1 or 2) plain steps
+// for the current parity.  Host-side state (representation, mask index)
+// alternates with period two, so a pair graph leaves it where it started and
+// the single-step graph of each parity hands over to the other's.
+int run_steps_graph(bfx_sim* s, int nsteps) {
     const int key = s->rep_s;
-    if (!s->pair_graph[key]) {
+    cudaGraphExec_t* slot = nsteps == 2 ? &s->pair_graph[key] : &s->step_graph[key];
+    uint64_t* count = nsteps == 2 ? &s->pair_launches[key] : &s->step_launches[key];
+    if (!*slot) {
+        const int rep0 = s->rep_s, cur0 = s->cur;
         cudaGraph_t graph = nullptr;
         uint64_t before = s->launches;
         cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return cuda_fail(s, e, "graph capture begin");
-        encode_step(s, 0, nullptr, 0);
-        encode_step(s, 0, nullptr, 0);
+        for (int i = 0; i < nsteps; ++i) encode_step(s, 0, nullptr, 0);
         e = cudaStreamEndCapture(s->stream, &graph);
         if (e != cudaSuccess) return cuda_fail(s, e, "graph capture end");
-        e = cudaGraphInstantiate(&s->pair_graph[key], graph, 0);
+        e = cudaGraphInstantiate(slot, graph, 0);
         cudaGraphDestroy(graph);
         if (e != cudaSuccess) return cuda_fail(s, e, "graph instantiate");
-        s->pair_launches[key] = s->launches - before;
+        *count = s->launches - before;
         s->launches = before;
+        // capture only recorded the steps: the host state advances at launch
+        s->rep_s = rep0;
+        s->cur = cur0;
     }
-    cudaError_t e = cudaGraphLaunch(s->pair_graph[key], s->stream);
+    cudaError_t e = cudaGraphLaunch(*slot, s->stream);
     if (e != cudaSuccess) return cuda_fail(s, e, "graph launch");
-    s->launches += s->pair_launches[key];
+    s->launches += *count;
+    for (int i = 0; i < nsteps; ++i) {
+        s->rep_s ^= 1;
+        if (s->moving()) s->cur ^= 1;
+    }
     return BFX_OK;
 }
+int run_pair_graph(bfx_sim* s) { return run_steps_graph(s, 2); }
 
 int sync_check(bfx_sim* s, const char* what) {
     cudaError_t e = cudaStreamSynchronize(s->stream);
@@ -496,6 +516,9 @@ void bfx_destroy(bfx_sim* s) {
         if (e) cudaEventDestroy(e);
     for (auto g : s->pair_graph)
         if (g) cudaGraphExecDestroy(g);
+    for (auto g : s->step_graph)
+        if (g) cudaGraphExecDestroy(g);
+    if (s->hstate) cudaFreeHost(s->hstate);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -587,6 +610,10 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
     BFX_ALLOC(s->density, (size_t)g.n * sizeof(float));
     BFX_ALLOC(s->velocity, (size_t)g.n * sizeof(float4));
     BFX_ALLOC(s->dstate, sizeof(DeviceState));
+    if (cudaMallocHost((void**)&s->hstate, sizeof(DeviceState)) != cudaSuccess) {
+        (void)cudaGetLastError();
+        s->hstate = nullptr;  // pageable copies instead
+    }
     BFX_ALLOC(s->dobjective, sizeof(Objective));
     s->mm_blocks = 4 * s->sm_count;
     BFX_ALLOC(s->mm_partials, (size_t)s->mm_blocks * 4 * sizeof(double));
@@ -699,6 +726,21 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
         cudaSetDevice((s)->device);                              \
     } while (0)
 
+static int read_state(bfx_sim* s, DeviceState* st) {
+    int rc = sync_check(s, "read-back");
+    if (rc != BFX_OK) return rc;
+    cudaError_t e;
+    if (s->hstate) {
+        e = cudaMemcpyAsync(s->hstate, s->dstate, sizeof(*st), cudaMemcpyDeviceToHost, s->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+        if (e == cudaSuccess) *st = *s->hstate;
+    } else {
+        e = cudaMemcpy(st, s->dstate, sizeof(*st), cudaMemcpyDeviceToHost);
+    }
+    if (e != cudaSuccess) return cuda_fail(s, e, "state read-back");
+    return BFX_OK;
+}
+
 int bfx_advance(bfx_sim* s, uint64_t steps, uint32_t batch_size, uint32_t flags, bfx_run_sample* samples,
                 size_t sample_capacity, bfx_advance_result* result) {
     BFX_GUARD(s);
@@ -731,6 +773,11 @@ int bfx_advance(bfx_sim* s, uint64_t steps, uint32_t batch_size, uint32_t flags,
                 int rc = run_pair_graph(s);
                 if (rc != BFX_OK) return rc;
             }
+            if (k < plain) {
+                int rc = run_steps_graph(s, 1);
+                if (rc != BFX_OK) return rc;
+                ++k;
+            }
         }
         for (; k < count; ++k) {
             bool last = done + k + 1 == steps;
@@ -740,10 +787,9 @@ int bfx_advance(bfx_sim* s, uint64_t steps, uint32_t batch_size, uint32_t flags,
         if (le != cudaSuccess) return cuda_fail(s, le, "kernel launch");
         done += count;
         if (s->cfg.free_flight || s->moving() || done == steps) {
-            int rc = sync_check(s, "advance");
-            if (rc != BFX_OK) return rc;
             DeviceState st;
-            cudaMemcpy(&st, s->dstate, sizeof(st), cudaMemcpyDeviceToHost);
+            int rc = read_state(s, &st);
+            if (rc != BFX_OK) return rc;
             s->step = st.step;
             if (st.link_overflow) return fail(s, BFX_ERR_KERNEL, "the cut-link list exceeded its capacity; raise link_capacity");
             if (st.stream_error) return fail(s, BFX_ERR_KERNEL, "a fused-kernel pipeline wait timed out");
@@ -765,7 +811,8 @@ int bfx_advance(bfx_sim* s, uint64_t steps, uint32_t batch_size, uint32_t flags,
     }
     if (result) {
         DeviceState st;
-        cudaMemcpy(&st, s->dstate, sizeof(st), cudaMemcpyDeviceToHost);
+        int rc = read_state(s, &st);
+        if (rc != BFX_OK) return rc;
         result->steps_done = steps;
         result->field_frame_published = capture ? 1 : 0;
         result->safety_passed = st.safety_event[2] == 0 ? 1 : 0;
@@ -775,13 +822,6 @@ int bfx_advance(bfx_sim* s, uint64_t steps, uint32_t batch_size, uint32_t flags,
     return BFX_OK;
 }
 
-static int read_state(bfx_sim* s, DeviceState* st) {
-    int rc = sync_check(s, "read-back");
-    if (rc != BFX_OK) return rc;
-    cudaError_t e = cudaMemcpy(st, s->dstate, sizeof(*st), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) return cuda_fail(s, e, "state read-back");
-    return BFX_OK;
-}
 
 static void loads_from_state(const bfx_sim* s, const DeviceState& st, bfx_loads* out) {
     std::memset(out, 0, sizeof(*out));
@@ -1027,6 +1067,9 @@ int bfx_restore_state(bfx_sim* s, const void* buf, size_t size) {
     uint64_t sum;
     std::memcpy(&sum, (const char*)buf + need - sizeof(uint64_t), sizeof(sum));
     if (sum != fnv1a(buf, need - sizeof(uint64_t))) return fail(s, BFX_ERR_INVALID_ARGUMENT, "state checksum mismatch");
+    // nothing queued (a body upload) may land after the restored state
+    const int synced = sync_check(s, "restore state");
+    if (synced != BFX_OK) return synced;
     const char* p = (const char*)buf + sizeof(h);
     cudaMemcpy(s->dstate, p, sizeof(DeviceState), cudaMemcpyHostToDevice);
     p += sizeof(DeviceState);
@@ -1075,7 +1118,17 @@ int bfx_set_body(bfx_sim* s, const bfx_body_state* in) {
     for (int k = 0; k < 3; ++k) b[10 + k] = in->omega_body[k];
     int rc = sync_check(s, "set body");
     if (rc != BFX_OK) return rc;
-    cudaMemcpy((char*)s->dstate + offsetof(DeviceState, body), b, sizeof(b), cudaMemcpyHostToDevice);
+    cudaError_t e;
+    if (s->hstate) {
+        // stream-ordered upload from pinned staging (the stream is idle, so no
+        // earlier copy still reads the staging)
+        std::memcpy(s->hstate->body, b, sizeof(b));
+        e = cudaMemcpyAsync((char*)s->dstate + offsetof(DeviceState, body), s->hstate->body, sizeof(b),
+                            cudaMemcpyHostToDevice, s->stream);
+    } else {
+        e = cudaMemcpy((char*)s->dstate + offsetof(DeviceState, body), b, sizeof(b), cudaMemcpyHostToDevice);
+    }
+    if (e != cudaSuccess) return cuda_fail(s, e, "body upload");
     return BFX_OK;
 }
 
