@@ -12,8 +12,152 @@ namespace BFX_VARIANT {
 #include "bfx_pair_math.cuh"
 #endif
 
-// Collision (BF.metal:2907-3174).  Directions are processed in opposite pairs
-// (q odd, q+1 = opp(q)): the equilibrium, TRT and regularized terms of the pair
+// Sums over the pairs (q odd) of c_a(q) v[q] (B < 0) or c_a(q) c_b(q) v[q],
+// the first nonzero term taken as is or negated, then added or subtracted in
+// direction order.
+template <int A, int B, class R>
+__device__ __forceinline__ R pair_sum(const R (&v)[19]) {
+    R r = R(0);
+    bool first = true;
+#pragma unroll
+    for (int q = 1; q < 19; q += 2) {
+        const int ca = A == 0 ? cx(q) : (A == 1 ? cy(q) : cz(q));
+        const int cb = B < 0 ? 1 : (B == 0 ? cx(q) : (B == 1 ? cy(q) : cz(q)));
+        const int c = ca * cb;
+        if (c == 0) continue;
+        r = first ? (c > 0 ? v[q] : -v[q]) : (c > 0 ? r + v[q] : r - v[q]);
+        first = false;
+    }
+    return r;
+}
+
+// Regularized / RR3 collision (BF.metal:2917-3062) evaluated on
+// opposite-direction pairs (q odd, q + 1 = opp q), the oracle's
+// regularized_pairs operation for operation (FP32 results bit-identical to
+// it; the reference's literal per-direction order agrees with it to FP32
+// rounding):
+//   moments from pair sums p = f_q + f_q' and differences m = f_q - f_q';
+//   feq_q = E + O, feq_q' = E - O with E = w rho (1 - 1.5u^2 + 4.5cu^2),
+//   O = 3 w rho cu;
+//   stress from the pair non-equilibria n = p - 2E:
+//   ds_a = sum_{c_a != 0} n - cs2 (ne_0 + sum n), od_ab = sum sign(c_a c_b) n;
+//   post_q = X + Y, post_q' = X - Y with X = E + (1 - w+) w 4.5 H2:ds,
+//   Y = O + (1 - w+) w 13.5 H3:a3;
+//   positivity admission over every direction, and the scaled blend
+//   feq + s (cand - feq) only where s < 1.
+// It takes about two thirds of the literal form's instructions.  A cheap
+// superset test (min over the populations against 1e-12 + 1e-6 max feq, with
+// E + |O| bounding each pair's equilibria) skips the exact admission for the
+// cells that cannot need it; the exact test then decides as the oracle does.
+template <class R, int COLL>
+__device__ __forceinline__ void regularized_pairs(const R (&f)[19], R omega_p, R (&post)[19], float& activation,
+                                                  float& restriction) {
+    const R cs2 = Lat<R>::cs2;
+    R ps[19], md[19], E[19], O[19], nps[19];
+    R rho = f[0];
+#pragma unroll
+    for (int q = 1; q < 19; q += 2) {
+        ps[q] = f[q] + f[q + 1];
+        md[q] = f[q] - f[q + 1];
+        rho = rho + ps[q];
+    }
+    const R mx = pair_sum<0, -1>(md), my = pair_sum<1, -1>(md), mz = pair_sum<2, -1>(md);
+    rho = rho > R(1.0e-8) ? rho : R(1.0e-8);
+    const R ux = mx / rho, uy = my / rho, uz = mz / rho;
+    const R u2 = ux * ux + uy * uy + uz * uz;
+    const R base = R(1) - R(1.5) * u2;
+    const R wr1 = Lat<R>::w1 * rho, wr2 = Lat<R>::w2 * rho;
+    const R feq0 = (Lat<R>::w0 * rho) * base;
+    R ntot = f[0] - feq0;
+#pragma unroll
+    for (int q = 1; q < 19; q += 2) {
+        const R cu = cdotq<R>(q, ux, uy, uz);
+        const R wr = q <= 6 ? wr1 : wr2;
+        E[q] = wr * (base + (R(4.5) * cu) * cu);
+        O[q] = wr * (R(3) * cu);
+        nps[q] = ps[q] - R(2) * E[q];
+        ntot = ntot + nps[q];
+    }
+    const R dsx = pair_sum<0, 0>(nps) - cs2 * ntot;
+    const R dsy = pair_sum<1, 1>(nps) - cs2 * ntot;
+    const R dsz = pair_sum<2, 2>(nps) - cs2 * ntot;
+    const R odx = pair_sum<0, 1>(nps), ody = pair_sum<0, 2>(nps), odz = pair_sum<1, 2>(nps);
+    const R aXxy = (R(2) * ux) * odx + uy * dsx;
+    const R aXxz = (R(2) * ux) * ody + uz * dsx;
+    const R aXyy = ux * dsy + (R(2) * uy) * odx;
+    const R aXzz = ux * dsz + (R(2) * uz) * ody;
+    const R aYyz = (R(2) * uy) * odz + uz * dsy;
+    const R aYzz = uy * dsz + (R(2) * uz) * odz;
+    const R trace = dsx + dsy + dsz;
+    const R cax = dsx - cs2 * trace, cay = dsy - cs2 * trace, caz = dsz - cs2 * trace;
+    const R om = R(1) - omega_p;
+    const R om0 = om * (Lat<R>::w0 * R(4.5) * -cs2);
+    const R om1 = om * (Lat<R>::w1 * R(4.5)), om2 = om * (Lat<R>::w2 * R(4.5));
+    const R ot1 = om * (Lat<R>::w1 * R(13.5)), ot2 = om * (Lat<R>::w2 * R(13.5));
+    post[0] = feq0 + om0 * trace;
+    R lo = post[0], hi = feq0;
+#pragma unroll
+    for (int q = 1; q < 19; q += 2) {
+        R contraction;
+        if (cx(q) != 0 && cy(q) != 0) contraction = (cax + dsy) + R(2) * (cx(q) * cy(q) > 0 ? odx : -odx);
+        else if (cx(q) != 0 && cz(q) != 0) contraction = (cax + dsz) + R(2) * (cx(q) * cz(q) > 0 ? ody : -ody);
+        else if (cy(q) != 0 && cz(q) != 0) contraction = (cay + dsz) + R(2) * (cy(q) * cz(q) > 0 ? odz : -odz);
+        else contraction = cx(q) != 0 ? cax : (cy(q) != 0 ? cay : caz);
+        const R X = E[q] + (q <= 6 ? om1 : om2) * contraction;
+        R Y = O[q];
+        if (COLL == BFX_COLLISION_RR3) {
+            const R hx = (R)(cx(q) * cx(q)) - cs2, hy = (R)(cy(q) * cy(q)) - cs2, hz = (R)(cz(q) * cz(q)) - cs2;
+            R third = R(0);
+            bool any = false;
+            auto add = [&](int da, R hb, R amp) {
+                if (da == 0) return;
+                const R t = ((R)da * hb) * amp;
+                third = any ? third + t : t;
+                any = true;
+            };
+            add(cy(q), hx, aXxy);
+            add(cz(q), hx, aXxz);
+            add(cx(q), hy, aXyy);
+            add(cx(q), hz, aXzz);
+            add(cz(q), hy, aYyz);
+            add(cy(q), hz, aYzz);
+            Y = Y + (q <= 6 ? ot1 : ot2) * third;
+        }
+        post[q] = X + Y;
+        post[q + 1] = X - Y;
+        lo = fmin(lo, fmin(post[q], post[q + 1]));
+        hi = fmax(hi, E[q] + fabs(O[q]));
+    }
+    // every floor max(1e-12, 1e-6 max(feq_q, 0)) is at most 1e-12 + 1e-6 max(hi, 0)
+    if (!(lo < R(1.0e-12) + R(1.0e-6) * fmax(hi, R(0)))) return;
+    R scale = R(1);
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        const R fe = q == 0 ? feq0 : ((q & 1) ? E[q] + O[q] : E[q - 1] - O[q - 1]);
+        const R fl = R(1.0e-6) * (fe > R(0) ? fe : R(0));
+        const R floor_ = R(1.0e-12) > fl ? R(1.0e-12) : fl;
+        if (post[q] < floor_) {
+            R den = fe - post[q];
+            den = den > R(1.0e-30) ? den : R(1.0e-30);
+            R adm = (fe - floor_) / den;
+            adm = adm < R(0) ? R(0) : (adm > R(1) ? R(1) : adm);
+            scale = scale < adm ? scale : adm;
+        }
+    }
+    if (scale < R(1)) {
+        activation = 1.0f;
+        restriction = (float)(R(1) - scale);
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            const R fe = q == 0 ? feq0 : ((q & 1) ? E[q] + O[q] : E[q - 1] - O[q - 1]);
+            post[q] = fe + scale * (post[q] - fe);
+        }
+    }
+}
+
+// TRT and symmetric-limiter collision (BF.metal:3063-3174; the regularized
+// operators are regularized_pairs).  Directions are processed in opposite pairs
+// (q odd, q+1 = opp(q)): the equilibrium and TRT terms of the pair
 // share their even parts and negate their odd parts, and in IEEE arithmetic
 // -(a-b) == b-a, (-a)*b == -(a*b), x-(-y) == x+y exactly.  Every value is
 // therefore bit-identical to evaluating the reference expression once per
@@ -21,6 +165,8 @@ namespace BFX_VARIANT {
 template <class R, int COLL>
 __device__ __forceinline__ void collide(const R (&f)[19], R rho, R ux, R uy, R uz, R omega_p, R omega_m,
                                         R (&post)[19], float& activation, float& restriction) {
+    static_assert(COLL == BFX_COLLISION_TRT || COLL == BFX_COLLISION_TRT_LIMITER,
+                  "the regularized operators run through regularized_pairs");
     const R cs2 = Lat<R>::cs2;
     const R u2 = ux * ux + uy * uy + uz * uz;
     const R t15 = R(1.5) * u2;
@@ -38,118 +184,7 @@ __device__ __forceinline__ void collide(const R (&f)[19], R rho, R ux, R uy, R u
         feqv[q + 1] = wr * (R(1) - t3 + t45 - t15);
     }
 
-    if (COLL == BFX_COLLISION_REGULARIZED || COLL == BFX_COLLISION_RR3) {
-        // Projected second-order non-equilibrium stress; products with a zero
-        // lattice coefficient are dropped and +-1 products become sign flips
-        // (exact for finite values).
-        R dsx = 0, dsy = 0, dsz = 0, odx = 0, ody = 0, odz = 0;
-#pragma unroll
-        for (int q = 0; q < 19; ++q) {
-            R ne = f[q] - feqv[q];
-            dsx += ne * ((R)(cx(q) * cx(q)) - cs2);
-            dsy += ne * ((R)(cy(q) * cy(q)) - cs2);
-            dsz += ne * ((R)(cz(q) * cz(q)) - cs2);
-            if (cx(q) * cy(q) > 0) odx += ne;
-            if (cx(q) * cy(q) < 0) odx -= ne;
-            if (cx(q) * cz(q) > 0) ody += ne;
-            if (cx(q) * cz(q) < 0) ody -= ne;
-            if (cy(q) * cz(q) > 0) odz += ne;
-            if (cy(q) * cz(q) < 0) odz -= ne;
-        }
-        R aXxy = R(2) * ux * odx + uy * dsx;
-        R aXxz = R(2) * ux * ody + uz * dsx;
-        R aXyy = ux * dsy + R(2) * uy * odx;
-        R aXzz = ux * dsz + R(2) * uz * ody;
-        R aYyz = R(2) * uy * odz + uz * dsy;
-        R aYzz = uy * dsz + R(2) * uz * odz;
-        const R one_minus = R(1) - omega_p;
-        R scale = R(1);
-        // Positivity admission (BF.metal:3035-3052).  The floor test runs on
-        // every population; the admissible scale, which only a population below
-        // its floor changes, is evaluated afterwards in the same direction order
-        // for the rare cell that has one.
-        bool need = false;
-        auto below = [&](R fe, R cand) {
-            R fl = R(1.0e-6) * (fe > R(0) ? fe : R(0));
-            R floor_ = R(1.0e-12) > fl ? R(1.0e-12) : fl;
-            need = need || cand < floor_;
-        };
-        auto admit = [&](R fe, R cand) {
-            R fl = R(1.0e-6) * (fe > R(0) ? fe : R(0));
-            R floor_ = R(1.0e-12) > fl ? R(1.0e-12) : fl;
-            if (cand < floor_) {
-                R den = fe - cand;
-                den = den > R(1.0e-30) ? den : R(1.0e-30);
-                R adm = (fe - floor_) / den;
-                adm = adm < R(0) ? R(0) : (adm > R(1) ? R(1) : adm);
-                scale = scale < adm ? scale : adm;
-            }
-        };
-        {
-            // rest direction: contraction = -cs2 (dsx + dsy + dsz), no third-order part
-            const R h = -cs2;
-            const R contraction = h * dsx + h * dsy + h * dsz;
-            const R rne = Lat<R>::w0 * R(4.5) * contraction;
-            post[0] = feqv[0] + one_minus * rne;
-            below(feqv[0], post[0]);
-        }
-#pragma unroll
-        for (int q = 1; q < 19; q += 2) {
-            // the contraction is even in c (shared by q and opp q), the third-order sum is odd
-            const R hx = (R)(cx(q) * cx(q)) - cs2, hy = (R)(cy(q) * cy(q)) - cs2, hz = (R)(cz(q) * cz(q)) - cs2;
-            R contraction = hx * dsx + hy * dsy + hz * dsz;
-            {
-                const int xy = cx(q) * cy(q), xz = cx(q) * cz(q), yz = cy(q) * cz(q);
-                if (xy != 0) contraction = contraction + R(2) * (xy > 0 ? odx : -odx);
-                else if (xz != 0) contraction = contraction + R(2) * (xz > 0 ? ody : -ody);
-                else if (yz != 0) contraction = contraction + R(2) * (yz > 0 ? odz : -odz);
-            }
-            const R a = wq<R>(q) * R(4.5) * contraction;
-            R rq = a, ro = a;
-            if (COLL == BFX_COLLISION_RR3) {
-                R third = R(0);
-                bool any = false;
-                auto add = [&](int da, R hb, R amp) {
-                    if (da == 0) return;
-                    R t = ((R)da * hb) * amp;
-                    third = any ? third + t : t;
-                    any = true;
-                };
-                add(cy(q), hx, aXxy);
-                add(cz(q), hx, aXxz);
-                add(cx(q), hy, aXyy);
-                add(cx(q), hz, aXzz);
-                add(cz(q), hy, aYyz);
-                add(cy(q), hz, aYzz);
-                const R b = wq<R>(q) * R(13.5) * third;
-                rq = a + b;
-                ro = a - b;
-            }
-            post[q] = feqv[q] + one_minus * rq;
-            post[q + 1] = feqv[q + 1] + one_minus * ro;
-            below(feqv[q], post[q]);
-            below(feqv[q + 1], post[q + 1]);
-        }
-        if (need) {
-#pragma unroll
-            for (int q = 0; q < 19; ++q) admit(feqv[q], post[q]);
-        }
-        if (scale < R(1)) {
-            activation = 1.0f;
-            restriction = (float)(R(1) - scale);
-#pragma unroll
-            for (int q = 0; q < 19; ++q) post[q] = feqv[q] + scale * (post[q] - feqv[q]);
-        } else if (scale == R(1)) {
-            // 1 * d == d exactly, but feq + (cand - feq) equals cand only up to
-            // rounding, so the rest of the reference expression stays
-#pragma unroll
-            for (int q = 0; q < 19; ++q) post[q] = feqv[q] + (post[q] - feqv[q]);
-        } else {
-            // NaN scale (a non-finite equilibrium): the reference expression as is
-#pragma unroll
-            for (int q = 0; q < 19; ++q) post[q] = feqv[q] + scale * (post[q] - feqv[q]);
-        }
-    } else if (COLL == BFX_COLLISION_TRT) {
+    if (COLL == BFX_COLLISION_TRT) {
         // BF.metal:3063-3093, pairwise
         post[0] = f[0] - omega_p * (f[0] - feqv[0]);
 #pragma unroll
@@ -324,10 +359,14 @@ __device__ __forceinline__ void rare_cell(const BulkArgs& a, uint32_t gid, int x
     R f[19];
 #pragma unroll
     for (int q = 0; q < 19; ++q) f[q] = feqq<R>(q, R(1), ux, uy, uz, u2);
-    R rho, vx, vy, vz;
-    moments<R>(f, rho, vx, vy, vz);
     float activation = 0.0f, restriction = 0.0f;
-    collide<R, COLL>(f, rho, vx, vy, vz, (R)a.fp.omega_p, (R)a.fp.omega_m, post, activation, restriction);
+    if constexpr (COLL == BFX_COLLISION_RR3 || COLL == BFX_COLLISION_REGULARIZED) {
+        regularized_pairs<R, COLL>(f, (R)a.fp.omega_p, post, activation, restriction);
+    } else {
+        R rho, vx, vy, vz;
+        moments<R>(f, rho, vx, vy, vz);
+        collide<R, COLL>(f, rho, vx, vy, vz, (R)a.fp.omega_p, (R)a.fp.omega_m, post, activation, restriction);
+    }
     finish_cell<S, COLL>(a, gid, x, y, z, a.capture == 1, post, activation, restriction);
     store_cell<S, REP_S>(a, pid, post);
 }
@@ -358,15 +397,16 @@ __global__ void __launch_bounds__(256, sizeof(typename S::R) == 8 ? 1 : (COLL ==
     load_cell<S, REP_S>(a, pid, f);
     R post[19];
     float activation = 0.0f, restriction = 0.0f;
-#ifdef BFX_CONTRACTED
     if constexpr (COLL == BFX_COLLISION_RR3 || COLL == BFX_COLLISION_REGULARIZED) {
+#ifdef BFX_CONTRACTED
         float act[1] = {0.0f}, res[1] = {0.0f};
         collide_pairs<R, COLL>(f, a.fp.omega_p, post, act, res);
         activation = act[0];
         restriction = res[0];
-    } else
+#else
+        regularized_pairs<R, COLL>(f, (R)a.fp.omega_p, post, activation, restriction);
 #endif
-    {
+    } else {
         R rho, ux, uy, uz;
         moments<R>(f, rho, ux, uy, uz);
         if (CAPTURE == 2) {

@@ -239,6 +239,215 @@ static float outside_value(const or_params* p, int q, int cx, int cy, int cz, in
 }
 
 /* ------------------------------------------------------------------ */
+/* Regularized / RR3 collision (BF.metal:2917-3062).                    */
+/* ------------------------------------------------------------------ */
+/* The reference's literal per-direction evaluation: the projected
+ * second-order non-equilibrium stress summed over q, the third-order
+ * Hermite closure per direction, positivity admission and the scaled blend
+ * feq + scale (cand - feq) for every direction. */
+static void regularized_literal(const float f[19], const float u[3], const float feq[19], float omega_p, int rr3,
+                                float post[19], float* act, float* restr) {
+    float ds[3] = {0, 0, 0}, od[3] = {0, 0, 0};
+    for (int q = 0; q < 19; ++q) {
+        float d[3] = {(float)C[q][0], (float)C[q][1], (float)C[q][2]};
+        float ne = f[q] - feq[q];
+        ds[0] += ne * (d[0] * d[0] - CS2);
+        ds[1] += ne * (d[1] * d[1] - CS2);
+        ds[2] += ne * (d[2] * d[2] - CS2);
+        od[0] += ne * (d[0] * d[1]);
+        od[1] += ne * (d[0] * d[2]);
+        od[2] += ne * (d[1] * d[2]);
+    }
+    float aXxy = 2.0f * u[0] * od[0] + u[1] * ds[0];
+    float aXxz = 2.0f * u[0] * od[1] + u[2] * ds[0];
+    float aXyy = u[0] * ds[1] + 2.0f * u[1] * od[0];
+    float aXzz = u[0] * ds[2] + 2.0f * u[2] * od[1];
+    float aYyz = 2.0f * u[1] * od[2] + u[2] * ds[1];
+    float aYzz = u[1] * ds[2] + 2.0f * u[2] * od[2];
+    float unb[19];
+    float scale = 1.0f;
+    for (int q = 0; q < 19; ++q) {
+        float d[3] = {(float)C[q][0], (float)C[q][1], (float)C[q][2]};
+        float h[3] = {d[0] * d[0] - CS2, d[1] * d[1] - CS2, d[2] * d[2] - CS2};
+        float o[3] = {d[0] * d[1], d[0] * d[2], d[1] * d[2]};
+        float contraction = dot3(h, ds) + 2.0f * dot3(o, od);
+        float third = 0.0f;
+        if (rr3) {
+            third = d[1] * (d[0] * d[0] - CS2) * aXxy + d[2] * (d[0] * d[0] - CS2) * aXxz +
+                    d[0] * (d[1] * d[1] - CS2) * aXyy + d[0] * (d[2] * d[2] - CS2) * aXzz +
+                    d[2] * (d[1] * d[1] - CS2) * aYyz + d[1] * (d[2] * d[2] - CS2) * aYzz;
+        }
+        float rne = W[q] * 4.5f * contraction;
+        if (rr3) rne += W[q] * 13.5f * third;
+        float cand = feq[q] + (1.0f - omega_p) * rne;
+        unb[q] = cand;
+        float floor_ = fmaxf(1.0e-12f, 1.0e-6f * fmaxf(feq[q], 0.0f));
+        if (cand < floor_) {
+            float adm = clampf((feq[q] - floor_) / fmaxf(feq[q] - cand, 1.0e-30f), 0.0f, 1.0f);
+            scale = fminf(scale, adm);
+        }
+    }
+    if (scale < 1.0f) {
+        *act = 1.0f;
+        *restr = 1.0f - scale;
+    }
+    for (int q = 0; q < 19; ++q) post[q] = feq[q] + scale * (unb[q] - feq[q]);
+}
+
+/* The first nonzero term taken as is (or negated), the rest added or
+ * subtracted in direction order: sum over the odd (pair-leading) q of
+ * c_a(q) v[q] (b < 0) or c_a(q) c_b(q) v[q]. */
+static float pair_sum(const float v[19], int a, int b) {
+    float r = 0.0f;
+    int first = 1;
+    for (int q = 1; q < 19; q += 2) {
+        const int c = b < 0 ? C[q][a] : C[q][a] * C[q][b];
+        if (c == 0) continue;
+        if (first) r = c > 0 ? v[q] : -v[q];
+        else r = c > 0 ? r + v[q] : r - v[q];
+        first = 0;
+    }
+    return r;
+}
+/* c_q . u over the nonzero components of c_q. */
+static float cdot_nz(int q, const float u[3]) {
+    float r = 0.0f;
+    int first = 1;
+    for (int k = 0; k < 3; ++k) {
+        if (C[q][k] == 0) continue;
+        if (first) r = C[q][k] > 0 ? u[k] : -u[k];
+        else r = C[q][k] > 0 ? r + u[k] : r - u[k];
+        first = 0;
+    }
+    return r;
+}
+
+/* The same operator evaluated on opposite-direction pairs (q odd, q + 1 =
+ * OPP[q]), the order the FP32 fluid kernel uses:
+ *   moments from pair sums p = f_q + f_q' and differences m = f_q - f_q';
+ *   feq_q = E + O, feq_q' = E - O with E = w rho (1 - 1.5u^2 + 4.5cu^2),
+ *   O = 3 w rho cu;
+ *   stress from the pair non-equilibria n = p - 2E:
+ *   ds_a = sum_{c_a != 0} n - cs2 (ne_0 + sum n), od_ab = sum sign(c_a c_b) n;
+ *   post_q = X + Y, post_q' = X - Y with X = E + (1 - w+) w 4.5 (H2 : ds),
+ *   Y = O + (1 - w+) w 13.5 (H3 : a3).
+ * Mathematically the literal operator; the two orders agree to FP32
+ * rounding.  The scaled blend runs only where the admission scale is below
+ * one (a blend with scale 1 is the identity up to rounding). */
+static void regularized_pairs(const float f[19], float omega_p, int rr3, float post[19], float* act, float* restr) {
+    float ps[19], md[19], E[19], O[19], nps[19];
+    float rho = f[0];
+    for (int q = 1; q < 19; q += 2) {
+        ps[q] = f[q] + f[q + 1];
+        md[q] = f[q] - f[q + 1];
+        rho = rho + ps[q];
+    }
+    const float mx = pair_sum(md, 0, -1), my = pair_sum(md, 1, -1), mz = pair_sum(md, 2, -1);
+    rho = rho > 1.0e-8f ? rho : 1.0e-8f;
+    const float u[3] = {mx / rho, my / rho, mz / rho};
+    const float u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    const float base = 1.0f - 1.5f * u2;
+    const float wr1 = W1 * rho, wr2 = W2 * rho;
+    const float feq0 = (W0 * rho) * base;
+    float ntot = f[0] - feq0;
+    for (int q = 1; q < 19; q += 2) {
+        const float cu = cdot_nz(q, u);
+        const float wr = q <= 6 ? wr1 : wr2;
+        E[q] = wr * (base + (4.5f * cu) * cu);
+        O[q] = wr * (3.0f * cu);
+        nps[q] = ps[q] - 2.0f * E[q];
+        ntot = ntot + nps[q];
+    }
+    const float dsx = pair_sum(nps, 0, 0) - CS2 * ntot;
+    const float dsy = pair_sum(nps, 1, 1) - CS2 * ntot;
+    const float dsz = pair_sum(nps, 2, 2) - CS2 * ntot;
+    const float odx = pair_sum(nps, 0, 1), ody = pair_sum(nps, 0, 2), odz = pair_sum(nps, 1, 2);
+    const float aXxy = (2.0f * u[0]) * odx + u[1] * dsx;
+    const float aXxz = (2.0f * u[0]) * ody + u[2] * dsx;
+    const float aXyy = u[0] * dsy + (2.0f * u[1]) * odx;
+    const float aXzz = u[0] * dsz + (2.0f * u[2]) * ody;
+    const float aYyz = (2.0f * u[1]) * odz + u[2] * dsy;
+    const float aYzz = u[1] * dsz + (2.0f * u[2]) * odz;
+    const float trace = dsx + dsy + dsz;
+    const float cax = dsx - CS2 * trace, cay = dsy - CS2 * trace, caz = dsz - CS2 * trace;
+    const float om = 1.0f - omega_p;
+    const float om0 = om * (W0 * 4.5f * -CS2);
+    const float om1 = om * (W1 * 4.5f), om2 = om * (W2 * 4.5f);
+    const float ot1 = om * (W1 * 13.5f), ot2 = om * (W2 * 13.5f);
+    float fe[19];
+    fe[0] = feq0;
+    post[0] = feq0 + om0 * trace;
+    for (int q = 1; q < 19; q += 2) {
+        const int x = C[q][0], y = C[q][1], z = C[q][2];
+        float contraction;
+        if (x != 0 && y != 0) contraction = (cax + dsy) + 2.0f * (x * y > 0 ? odx : -odx);
+        else if (x != 0 && z != 0) contraction = (cax + dsz) + 2.0f * (x * z > 0 ? ody : -ody);
+        else if (y != 0 && z != 0) contraction = (cay + dsz) + 2.0f * (y * z > 0 ? odz : -odz);
+        else contraction = x != 0 ? cax : (y != 0 ? cay : caz);
+        const float X = E[q] + (q <= 6 ? om1 : om2) * contraction;
+        float Y = O[q];
+        if (rr3) {
+            const float hx = (float)(x * x) - CS2, hy = (float)(y * y) - CS2, hz = (float)(z * z) - CS2;
+            const int da[6] = {y, z, x, x, z, y};
+            const float hb[6] = {hx, hx, hy, hz, hy, hz};
+            const float amp[6] = {aXxy, aXxz, aXyy, aXzz, aYyz, aYzz};
+            float third = 0.0f;
+            int any = 0;
+            for (int k = 0; k < 6; ++k) {
+                if (da[k] == 0) continue;
+                const float t = ((float)da[k] * hb[k]) * amp[k];
+                third = any ? third + t : t;
+                any = 1;
+            }
+            Y = Y + (q <= 6 ? ot1 : ot2) * third;
+        }
+        post[q] = X + Y;
+        post[q + 1] = X - Y;
+        fe[q] = E[q] + O[q];
+        fe[q + 1] = E[q] - O[q];
+    }
+    float scale = 1.0f;
+    for (int q = 0; q < 19; ++q) {
+        const float fl = 1.0e-6f * (fe[q] > 0.0f ? fe[q] : 0.0f);
+        const float floor_ = 1.0e-12f > fl ? 1.0e-12f : fl;
+        if (post[q] < floor_) {
+            float den = fe[q] - post[q];
+            den = den > 1.0e-30f ? den : 1.0e-30f;
+            float adm = (fe[q] - floor_) / den;
+            adm = adm < 0.0f ? 0.0f : (adm > 1.0f ? 1.0f : adm);
+            scale = scale < adm ? scale : adm;
+        }
+    }
+    if (scale < 1.0f) {
+        *act = 1.0f;
+        *restr = 1.0f - scale;
+        for (int q = 0; q < 19; ++q) post[q] = fe[q] + scale * (post[q] - fe[q]);
+    }
+}
+
+void or_collide_regularized(int order, const float* f, float omega_p, int rr3, float* post, float* activation,
+                            float* restriction) {
+    *activation = 0.0f;
+    *restriction = 0.0f;
+    if (order == 1) {
+        regularized_pairs(f, omega_p, rr3, post, activation, restriction);
+        return;
+    }
+    float rho = 0.0f, mom[3] = {0.0f, 0.0f, 0.0f};
+    for (int q = 0; q < 19; ++q) {
+        rho += f[q];
+        mom[0] += f[q] * (float)C[q][0];
+        mom[1] += f[q] * (float)C[q][1];
+        mom[2] += f[q] * (float)C[q][2];
+    }
+    rho = fmaxf(rho, 1.0e-8f);
+    const float u[3] = {mom[0] / rho, mom[1] / rho, mom[2] / rho};
+    float feq[19];
+    for (int q = 0; q < 19; ++q) feq[q] = or_equilibrium(q, rho, u);
+    regularized_literal(f, u, feq, omega_p, rr3, post, activation, restriction);
+}
+
+/* ------------------------------------------------------------------ */
 /* stepFluidTRT: BF.metal:2507-3236 (all branches).                     */
 /* ------------------------------------------------------------------ */
 void or_step(const or_params* p, const float* pin, float* pout,
@@ -470,52 +679,8 @@ void or_step(const or_params* p, const float* pin, float* pout,
                     float post_all[19];
 
                     if (regularized) {
-                        /* BF.metal:2917-3062 */
-                        float ds[3] = {0, 0, 0}, od[3] = {0, 0, 0};
-                        for (int q = 0; q < 19; ++q) {
-                            float d[3] = {(float)C[q][0], (float)C[q][1], (float)C[q][2]};
-                            float ne = f[q] - feq[q];
-                            ds[0] += ne * (d[0] * d[0] - CS2);
-                            ds[1] += ne * (d[1] * d[1] - CS2);
-                            ds[2] += ne * (d[2] * d[2] - CS2);
-                            od[0] += ne * (d[0] * d[1]);
-                            od[1] += ne * (d[0] * d[2]);
-                            od[2] += ne * (d[1] * d[2]);
-                        }
-                        float aXxy = 2.0f * u[0] * od[0] + u[1] * ds[0];
-                        float aXxz = 2.0f * u[0] * od[1] + u[2] * ds[0];
-                        float aXyy = u[0] * ds[1] + 2.0f * u[1] * od[0];
-                        float aXzz = u[0] * ds[2] + 2.0f * u[2] * od[1];
-                        float aYyz = 2.0f * u[1] * od[2] + u[2] * ds[1];
-                        float aYzz = u[1] * ds[2] + 2.0f * u[2] * od[2];
-                        float unb[19];
-                        float scale = 1.0f;
-                        for (int q = 0; q < 19; ++q) {
-                            float d[3] = {(float)C[q][0], (float)C[q][1], (float)C[q][2]};
-                            float h[3] = {d[0] * d[0] - CS2, d[1] * d[1] - CS2, d[2] * d[2] - CS2};
-                            float o[3] = {d[0] * d[1], d[0] * d[2], d[1] * d[2]};
-                            float contraction = dot3(h, ds) + 2.0f * dot3(o, od);
-                            float third = 0.0f;
-                            if (rr3) {
-                                third = d[1] * (d[0] * d[0] - CS2) * aXxy + d[2] * (d[0] * d[0] - CS2) * aXxz +
-                                        d[0] * (d[1] * d[1] - CS2) * aXyy + d[0] * (d[2] * d[2] - CS2) * aXzz +
-                                        d[2] * (d[1] * d[1] - CS2) * aYyz + d[1] * (d[2] * d[2] - CS2) * aYzz;
-                            }
-                            float rne = W[q] * 4.5f * contraction;
-                            if (rr3) rne += W[q] * 13.5f * third;
-                            float cand = feq[q] + (1.0f - omega_p) * rne;
-                            unb[q] = cand;
-                            float floor_ = fmaxf(1.0e-12f, 1.0e-6f * fmaxf(feq[q], 0.0f));
-                            if (cand < floor_) {
-                                float adm = clampf((feq[q] - floor_) / fmaxf(feq[q] - cand, 1.0e-30f), 0.0f, 1.0f);
-                                scale = fminf(scale, adm);
-                            }
-                        }
-                        if (scale < 1.0f) {
-                            limiter_activation = 1.0f;
-                            limiter_restriction = 1.0f - scale;
-                        }
-                        for (int q = 0; q < 19; ++q) post_all[q] = feq[q] + scale * (unb[q] - feq[q]);
+                        /* BF.metal:2917-3062, in the pair order of regularized_pairs */
+                        regularized_pairs(f, omega_p, rr3, post_all, &limiter_activation, &limiter_restriction);
                     } else if (!limiter) {
                         /* TRT: BF.metal:3063-3093 */
                         for (int q = 0; q < 19; ++q) {

@@ -88,6 +88,13 @@ typedef struct or_body_f64 { double position[3], orientation[4], velocity[3], om
 /* ---- lattice --------------------------------------------------------- */
 void or_lattice(int32_t* c /*19x3*/, int32_t* opp /*19*/, float* w /*19*/);
 float or_equilibrium(int q, float rho, const float u[3]);
+/* One regularized (rr3 = 0) or RR3 (rr3 = 1) collision of the 19 populations
+ * f (BF.metal:2917-3062).  order 0: the reference's literal per-direction
+ * expressions; order 1: the opposite-direction pair order the stepping (and
+ * the FP32 fluid kernel) uses.  activation / restriction report the
+ * positivity admission. */
+void or_collide_regularized(int order, const float* f, float omega_p, int rr3, float* post, float* activation,
+                            float* restriction);
 void or_trt_collision(const float* f, float rho, const float u[3], float omega_p, float omega_m, float* out);
 
 /* ---- field initialisation (BF.metal:2078-2162) ----------------------- */

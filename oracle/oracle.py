@@ -98,6 +98,7 @@ def lib():
         fp, u8p, dp = P(ct.c_float), P(ct.c_uint8), P(ct.c_double)
         L.or_equilibrium.restype = ct.c_float
         L.or_equilibrium.argtypes = [ct.c_int, ct.c_float, fp]
+        L.or_collide_regularized.argtypes = [ct.c_int, fp, ct.c_float, ct.c_int, fp, fp, fp]
         L.or_trt_collision.argtypes = [fp, ct.c_float, fp, ct.c_float, ct.c_float, fp]
         L.or_init_equilibrium.argtypes = [P(Params), fp, u8p, fp, fp, fp]
         L.or_init_shear_wave.argtypes = [P(Params), ct.c_float, ct.c_int, fp, fp, fp]
@@ -198,6 +199,18 @@ def prepared_to_array(prep: Prepared) -> np.ndarray:
 def equilibrium(q: int, rho: float, u) -> float:
     u = np.asarray(u, dtype=np.float32)
     return lib().or_equilibrium(q, rho, fptr(u))
+
+
+def collide_regularized(f, omega_p: float, rr3: bool, order: int):
+    """One regularized / RR3 collision of 19 populations: order 0 = the
+    reference's literal per-direction form, 1 = the pair order the stepping
+    uses.  Returns (post, activation, restriction)."""
+    f = np.ascontiguousarray(f, dtype=np.float32)
+    post = np.zeros(19, np.float32)
+    act = np.zeros(1, np.float32)
+    res = np.zeros(1, np.float32)
+    lib().or_collide_regularized(order, fptr(f), omega_p, 1 if rr3 else 0, fptr(post), fptr(act), fptr(res))
+    return post, float(act[0]), float(res[0])
 
 
 def lattice():
