@@ -589,6 +589,12 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
     fp.accumulate = c.accumulate_loads ? 1 : 0;
     fp.has_sponge = c.sponge_strength > 0.0f ? 1 : 0;
     fp.fast_math = c.fast_math ? 1 : 0;
+    // A mesh touches cells within the raster guard (half thickness + 2 cells)
+    // of its vertices' bounding box; three more cells cover the cells solid or
+    // flagged in the two previous steps (bounded motion, Mach <= 0.25).
+    fp.act_margin = c.geometry == BFX_GEOMETRY_MESH
+                        ? (int)std::ceil(c.mesh_half_thickness / c.cell_size) + 2 + 3
+                        : 0;
 
     s->elem = storage_bytes(c.storage);
     size_t pop_bytes = (size_t)19 * (size_t)g.padded * s->elem;
@@ -1287,19 +1293,23 @@ int bfx_adjoint(bfx_sim* s, uint64_t steps, const bfx_adjoint_objective* objecti
     uint8_t* snap_mask = nullptr;
     DeviceState* snap_state = nullptr;
     BFX_ADJ_ALLOC(snap_pops, (nseg + 1) * pop_bytes);
-    BFX_ADJ_ALLOC(snap_mask, (nseg + 1) * n);
+    // both mask buffers: the geometry rewrites only its active bounds, and the
+    // cells outside them keep the zeros the other buffer holds
+    BFX_ADJ_ALLOC(snap_mask, (nseg + 1) * 2 * n);
     BFX_ADJ_ALLOC(snap_state, (nseg + 1) * sizeof(DeviceState));
     std::vector<int> snap_rep(nseg + 1), snap_cur(nseg + 1);
     auto snapshot = [&](uint64_t i) {
         cudaMemcpyAsync(snap_pops + i * pop_bytes, s->pops, pop_bytes, cudaMemcpyDeviceToDevice, s->stream);
-        cudaMemcpyAsync(snap_mask + i * n, s->mask[s->cur], n, cudaMemcpyDeviceToDevice, s->stream);
+        cudaMemcpyAsync(snap_mask + i * 2 * n, s->mask[s->cur], n, cudaMemcpyDeviceToDevice, s->stream);
+        cudaMemcpyAsync(snap_mask + i * 2 * n + n, s->mask[s->cur ^ 1], n, cudaMemcpyDeviceToDevice, s->stream);
         cudaMemcpyAsync(snap_state + i, s->dstate, sizeof(DeviceState), cudaMemcpyDeviceToDevice, s->stream);
         snap_rep[i] = s->rep_s;
         snap_cur[i] = s->cur;
     };
     auto restore = [&](uint64_t i) {
         cudaMemcpyAsync(s->pops, snap_pops + i * pop_bytes, pop_bytes, cudaMemcpyDeviceToDevice, s->stream);
-        cudaMemcpyAsync(s->mask[snap_cur[i]], snap_mask + i * n, n, cudaMemcpyDeviceToDevice, s->stream);
+        cudaMemcpyAsync(s->mask[snap_cur[i]], snap_mask + i * 2 * n, n, cudaMemcpyDeviceToDevice, s->stream);
+        cudaMemcpyAsync(s->mask[snap_cur[i] ^ 1], snap_mask + i * 2 * n + n, n, cudaMemcpyDeviceToDevice, s->stream);
         cudaMemcpyAsync(s->dstate, snap_state + i, sizeof(DeviceState), cudaMemcpyDeviceToDevice, s->stream);
         s->rep_s = snap_rep[i];
         s->cur = snap_cur[i];

@@ -431,10 +431,16 @@ template <class S, int REP_S, int COLL>
 __global__ void __launch_bounds__(128) k_rare(const BulkArgs a) {
     const int lx = blockIdx.x * blockDim.x + threadIdx.x;
     if (lx >= a.box[0]) return;
-    const int x = a.state->box_origin[0] + lx;
-    const int y = a.state->box_origin[1] + (int)blockIdx.y;
-    const int z0 = a.state->box_origin[2] + (int)blockIdx.z * kRareZ;
+    const DeviceState* st = a.state;
+    const int x = st->box_origin[0] + lx;
+    const int y = st->box_origin[1] + (int)blockIdx.y;
+    const int z0 = st->box_origin[2] + (int)blockIdx.z * kRareZ;
     if (x < 0 || x >= a.g.nx || y < 0 || y >= a.g.ny) return;
+    // flagged cells lie within the geometry's active bounds
+    const int am = a.fp.act_margin;
+    if (x < st->act_lo[0] - am || x > st->act_hi[0] + am || y < st->act_lo[1] - am || y > st->act_hi[1] + am ||
+        z0 + kRareZ - 1 < st->act_lo[2] - am || z0 > st->act_hi[2] + am)
+        return;
     const int lz_end = a.box[2] - (int)blockIdx.z * kRareZ;
     const uint32_t plane = (uint32_t)a.g.nx * (uint32_t)a.g.ny;
     uint8_t m[kRareZ];

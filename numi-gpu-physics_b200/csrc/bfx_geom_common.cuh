@@ -87,6 +87,38 @@ __device__ __forceinline__ bool box_cell(const GeomArgs& a, int& x, int& y, int&
     return x < a.g.nx && y < a.g.ny && z < a.g.nz;
 }
 
+// Active bounds of the step: the cells of the geometry box within
+// fp.act_margin of the mesh vertices' bounding box (the whole box for the
+// analytic shapes).  Cells outside hold no key, no link and no topology
+// change, and their mask bytes are 0 in both buffers.
+__device__ __forceinline__ void active_bounds(const GeomArgs& a, int (&lo)[3], int (&hi)[3]) {
+    const DeviceState* st = a.b.state;
+    const int ext[3] = {a.bx, a.by, a.bz};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int l = st->act_lo[k] - a.fp.act_margin, h = st->act_hi[k] + a.fp.act_margin;
+        lo[k] = l > st->box_origin[k] ? l : st->box_origin[k];
+        const int top = st->box_origin[k] + ext[k] - 1;
+        hi[k] = h < top ? h : top;
+    }
+}
+// The cells of box_cell's block all lie outside the active bounds (uniform
+// over the block).
+__device__ __forceinline__ bool block_inactive(const GeomArgs& a) {
+    int lo[3], hi[3];
+    active_bounds(a, lo, hi);
+    const int32_t* o = a.b.state->box_origin;
+    const int x0 = o[0] + (int)(blockIdx.x * blockDim.x), x1 = x0 + (int)blockDim.x - 1;
+    const int y0 = o[1] + (int)(blockIdx.y * blockDim.y), y1 = y0 + (int)blockDim.y - 1;
+    const int z = o[2] + (int)blockIdx.z;
+    return x1 < lo[0] || x0 > hi[0] || y1 < lo[1] || y0 > hi[1] || z < lo[2] || z > hi[2];
+}
+__device__ __forceinline__ bool cell_active(const GeomArgs& a, int x, int y, int z) {
+    int lo[3], hi[3];
+    active_bounds(a, lo, hi);
+    return x >= lo[0] && x <= hi[0] && y >= lo[1] && y <= hi[1] && z >= lo[2] && z <= hi[2];
+}
+
 __device__ __forceinline__ uint8_t topo_flags(uint8_t part, uint8_t prev_part, int has_prev) {
     if (!has_prev) return part;
     if (part && !prev_part) return (uint8_t)(part | kCovered);

@@ -193,6 +193,11 @@ __global__ void k_prepare(const GeomArgs a, int init, float dt, float box_radius
         lo = lo < 0 ? 0 : lo;
         lo = lo > dims[k] - ext[k] ? dims[k] - ext[k] : lo;
         st->box_origin[k] = lo < 0 ? 0 : lo;
+        // active bounds: open for the analytic shapes; for a mesh, empty until
+        // k_mesh_prepare places the vertices
+        const bool mesh = a.b.mesh_local != nullptr;
+        st->act_lo[k] = mesh ? (1 << 30) : -(1 << 30);
+        st->act_hi[k] = mesh ? -(1 << 30) : (1 << 30);
     }
     (void)box_radius;
 }
@@ -324,12 +329,50 @@ __global__ void k_classify_ellipsoid(const GeomArgs a, int has_prev) {
 }
 
 // driven by the rigid frames instead of keyframes).
+__device__ void mesh_vertex(const GeomArgs& a, uint32_t i, V3& w, V3& v);
+
+// Vertex positions and velocities, and the bounding box of the vertices in
+// cells (warp min / max, then one atomic per warp and bound: order-free).
 __global__ void k_mesh_prepare(const GeomArgs a) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.b.nverts) return;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < a.b.nverts;
+    int lo[3] = {1 << 30, 1 << 30, 1 << 30}, hi[3] = {-(1 << 30), -(1 << 30), -(1 << 30)};
+    if (valid) {
+        V3 w, v;
+        mesh_vertex(a, i, w, v);
+        a.b.mesh_pos[i] = f4(w, 0.0f);
+        a.b.mesh_vel[i] = make_float4(v.x * a.fp.v2l, v.y * a.fp.v2l, v.z * a.fp.v2l, 0.0f);
+        const float c[3] = {(w.x - a.fp.origin[0]) / a.fp.dx - 0.5f, (w.y - a.fp.origin[1]) / a.fp.dx - 0.5f,
+                            (w.z - a.fp.origin[2]) / a.fp.dx - 0.5f};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            // clamp before the conversion (a non-finite position opens the bounds)
+            const float ck = c[k] == c[k] ? fminf(fmaxf(c[k], -1.0e9f), 1.0e9f) : 0.0f;
+            lo[k] = c[k] == c[k] ? (int)floorf(ck) : -(1 << 30);
+            hi[k] = c[k] == c[k] ? (int)ceilf(ck) : (1 << 30);
+            lo[k] = lo[k] < -(1 << 30) ? -(1 << 30) : lo[k];
+            hi[k] = hi[k] > (1 << 30) ? (1 << 30) : hi[k];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        for (int o = 16; o > 0; o >>= 1) {
+            const int l = __shfl_down_sync(0xffffffffu, lo[k], o), h = __shfl_down_sync(0xffffffffu, hi[k], o);
+            lo[k] = l < lo[k] ? l : lo[k];
+            hi[k] = h > hi[k] ? h : hi[k];
+        }
+    }
+    if ((threadIdx.x & 31) == 0 && lo[0] <= hi[0]) {
+        for (int k = 0; k < 3; ++k) {
+            atomicMin(&a.b.state->act_lo[k], lo[k]);
+            atomicMax(&a.b.state->act_hi[k], hi[k]);
+        }
+    }
+}
+
+__device__ void mesh_vertex(const GeomArgs& a, uint32_t i, V3& w, V3& v) {
     const Prepared& p = a.b.state->prep;
     V3 l = v3(a.b.mesh_local[3 * i], a.b.mesh_local[3 * i + 1], a.b.mesh_local[3 * i + 2]);
-    V3 w, v;
     uint8_t seg = a.b.mesh_segment[i];
     if (seg == 0) {
         V3 r = qrotate(p.orientation, l);
@@ -360,13 +403,15 @@ __global__ void k_mesh_prepare(const GeomArgs a) {
         v = v3(p.linear_velocity.x + cr.x + cw.x, p.linear_velocity.y + cr.y + cw.y,
                p.linear_velocity.z + cr.z + cw.z);
     }
-    a.b.mesh_pos[i] = f4(w, 0.0f);
-    a.b.mesh_vel[i] = make_float4(v.x * a.fp.v2l, v.y * a.fp.v2l, v.z * a.fp.v2l, 0.0f);
 }
 
+// Clears the keys of the active cells (only those are read this step).
 __global__ void k_mesh_clear(const GeomArgs a) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < a.box_cells) a.b.keys[i] = 0xFFFFFFFFFFFFFFFFull;
+    if (block_inactive(a)) return;
+    int x, y, z;
+    int64_t bidx;
+    if (!box_cell(a, x, y, z, bidx) || !cell_active(a, x, y, z)) return;
+    a.b.keys[bidx] = 0xFFFFFFFFFFFFFFFFull;
 }
 
 // One warp per triangle: the lanes share the triangle's voxel box (its AABB
@@ -414,10 +459,13 @@ __global__ void __launch_bounds__(128) k_mesh_raster(const GeomArgs a) {
     }
 }
 
+// Mask byte and wall value of every active cell (cells outside the active
+// bounds keep mask 0; their wall value is never read).
 __global__ void k_mesh_resolve(const GeomArgs a, int has_prev) {
+    if (block_inactive(a)) return;
     int x, y, z;
     int64_t bidx;
-    if (!box_cell(a, x, y, z, bidx)) return;
+    if (!box_cell(a, x, y, z, bidx) || !cell_active(a, x, y, z)) return;
     const int64_t gid = flat(a.g, x, y, z);
     uint8_t prev_part = a.b.mask_prev[gid] & kPartMask;
     unsigned long long key = a.b.keys[bidx];
@@ -520,7 +568,16 @@ __global__ void __launch_bounds__(256) k_boundary_scan(const GeomArgs a, int rep
     uint32_t links = 0;
     int x, y, z;
     int64_t bidx;
-    if (box_cell(a, x, y, z, bidx)) {
+    if (block_inactive(a)) {
+        // no key, link or topology change in this block
+        if (linear_tid() == 0) {
+            const int block = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+            a.b.block_counts[block] = 0;
+            for (int k = 0; k < 8; ++k) a.b.topo_partials[8 * block + k] = 0.0;
+        }
+        return;
+    }
+    if (box_cell(a, x, y, z, bidx) && cell_active(a, x, y, z)) {
         const Grid& g = a.g;
         const int64_t gid = flat(g, x, y, z);
         const uint8_t m1 = a.b.mask_next[gid];
@@ -640,6 +697,8 @@ __global__ void k_scan(const GeomArgs a) {
 // the preceding threads, so the list is ordered by box cell then direction.
 __global__ void __launch_bounds__(256) k_links_emit(const GeomArgs a, int geometry, int link_rule, int interpolated) {
     __shared__ uint32_t wsum[8];
+    // blocks without links (most of the box) emit nothing
+    if (a.b.block_counts[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] == 0) return;
     int x = 0, y = 0, z = 0;
     int64_t bidx;
     const Grid& g = a.g;
@@ -1113,7 +1172,7 @@ void launch_classify(int geometry, int has_prev, const GridDesc& g, const FluidP
         k_classify_ellipsoid<<<grid, block, 0, s>>>(a, has_prev);
     } else if (geometry == BFX_GEOMETRY_MESH) {
         k_mesh_prepare<<<(gb.nverts + 255) / 256, 256, 0, s>>>(a);
-        k_mesh_clear<<<(unsigned)((box.cells + 255) / 256), 256, 0, s>>>(a);
+        k_mesh_clear<<<grid, block, 0, s>>>(a);
         k_mesh_raster<<<(unsigned)(((int64_t)gb.ntris * 32 + 127) / 128), 128, 0, s>>>(a);
         k_mesh_resolve<<<grid, block, 0, s>>>(a, has_prev);
     }

@@ -30,6 +30,7 @@ struct FluidParams {
     int has_sponge;
     int any_outflow;
     int fast_math;
+    int act_margin;          // cells around the mesh vertices' bounding box the geometry can touch
 };
 
 // Prepared articulated geometry (GPUPreparedBirdGeometry, BF.metal:112-127).
@@ -53,6 +54,9 @@ struct DeviceState {
     Prepared prep;
     int32_t box_origin[3];         // geometry region origin (cells)
     int32_t _pad0;
+    // bounding box (cells, inclusive) of this step's mesh vertices; open
+    // (+-2^30) for the analytic shapes, empty before the vertices are placed
+    int32_t act_lo[3], act_hi[3];
     float wing_prev[16];           // GPUWingMomentumState
     float wing_reaction[16];       // GPUWingInertialReaction
     float safety_metrics[4];
