@@ -87,6 +87,7 @@ struct bfx_sim {
     uint32_t* block_counts = nullptr;
     uint32_t* block_offsets = nullptr;
     int box_blocks = 0;
+    int scan_blocks = 0;
     double* topo_partials = nullptr;
     double* link_partials = nullptr;
     int apply_blocks = 0;
@@ -202,6 +203,7 @@ GeomBuffers geom_buffers(bfx_sim* s, uint8_t* mprev, uint8_t* mnext) {
     b.block_counts = s->block_counts;
     b.block_offsets = s->block_offsets;
     b.box_blocks = s->box_blocks;
+    b.scan_blocks = s->scan_blocks;
     b.topo_partials = s->topo_partials;
     b.link_partials = s->link_partials;
     b.apply_blocks = s->apply_blocks;
@@ -653,6 +655,7 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
         s->box.sz = std::min(ext, g.nz);
         s->box.cells = (int64_t)s->box.sx * s->box.sy * s->box.sz;
         s->box_blocks = box_block_count(s->box);
+        s->scan_blocks = s->box_blocks;
         BFX_ALLOC(s->block_counts, (size_t)s->box_blocks * sizeof(uint32_t));
         BFX_ALLOC(s->block_offsets, (size_t)s->box_blocks * sizeof(uint32_t));
         BFX_ALLOC(s->topo_partials, (size_t)s->box_blocks * 8 * sizeof(double));

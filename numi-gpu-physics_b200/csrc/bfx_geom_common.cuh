@@ -102,6 +102,33 @@ __device__ __forceinline__ void active_bounds(const GeomArgs& a, int (&lo)[3], i
         hi[k] = h < top ? h : top;
     }
 }
+// Slab launches: a block covers kSlabZ consecutive z slices of its (x, y)
+// tile, one cell per thread and slice, so empty parts of the box cost a
+// quarter of the blocks.
+constexpr int kSlabZ = 4;
+__device__ __forceinline__ bool slab_cell(const GeomArgs& a, int k, int& x, int& y, int& z, int64_t& bidx) {
+    int lx = blockIdx.x * blockDim.x + threadIdx.x;
+    int ly = blockIdx.y * blockDim.y + threadIdx.y;
+    int lz = blockIdx.z * kSlabZ + k;
+    if (lx >= a.bx || ly >= a.by || lz >= a.bz) return false;
+    const int32_t* o = a.b.state->box_origin;
+    x = o[0] + lx;
+    y = o[1] + ly;
+    z = o[2] + lz;
+    bidx = (int64_t)lx + (int64_t)a.bx * ((int64_t)ly + (int64_t)a.by * lz);
+    return x < a.g.nx && y < a.g.ny && z < a.g.nz;
+}
+// Every cell of the slab block lies outside the active bounds (uniform over the block).
+__device__ __forceinline__ bool slab_inactive(const GeomArgs& a) {
+    int lo[3], hi[3];
+    active_bounds(a, lo, hi);
+    const int32_t* o = a.b.state->box_origin;
+    const int x0 = o[0] + (int)(blockIdx.x * blockDim.x), x1 = x0 + (int)blockDim.x - 1;
+    const int y0 = o[1] + (int)(blockIdx.y * blockDim.y), y1 = y0 + (int)blockDim.y - 1;
+    const int z0 = o[2] + (int)blockIdx.z * kSlabZ, z1 = z0 + kSlabZ - 1;
+    return x1 < lo[0] || x0 > hi[0] || y1 < lo[1] || y0 > hi[1] || z1 < lo[2] || z0 > hi[2];
+}
+
 // The cells of box_cell's block all lie outside the active bounds (uniform
 // over the block).
 __device__ __forceinline__ bool block_inactive(const GeomArgs& a) {
@@ -113,10 +140,13 @@ __device__ __forceinline__ bool block_inactive(const GeomArgs& a) {
     const int z = o[2] + (int)blockIdx.z;
     return x1 < lo[0] || x0 > hi[0] || y1 < lo[1] || y0 > hi[1] || z < lo[2] || z > hi[2];
 }
+__device__ __forceinline__ bool in_bounds(const int (&lo)[3], const int (&hi)[3], int x, int y, int z) {
+    return x >= lo[0] && x <= hi[0] && y >= lo[1] && y <= hi[1] && z >= lo[2] && z <= hi[2];
+}
 __device__ __forceinline__ bool cell_active(const GeomArgs& a, int x, int y, int z) {
     int lo[3], hi[3];
     active_bounds(a, lo, hi);
-    return x >= lo[0] && x <= hi[0] && y >= lo[1] && y <= hi[1] && z >= lo[2] && z <= hi[2];
+    return in_bounds(lo, hi, x, y, z);
 }
 
 __device__ __forceinline__ uint8_t topo_flags(uint8_t part, uint8_t prev_part, int has_prev) {
@@ -280,6 +310,10 @@ static inline void box_shape(const BoxDesc& box, dim3& grid, dim3& block) {
     int by = 256 / bx;
     block = dim3(bx, by, 1);
     grid = dim3((box.sx + bx - 1) / bx, (box.sy + by - 1) / by, box.sz);
+}
+static inline void slab_shape(const BoxDesc& box, dim3& grid, dim3& block) {
+    box_shape(box, grid, block);
+    grid.z = (unsigned)((box.sz + kSlabZ - 1) / kSlabZ);
 }
 
 }  // namespace bfx

@@ -405,13 +405,17 @@ __device__ void mesh_vertex(const GeomArgs& a, uint32_t i, V3& w, V3& v) {
     }
 }
 
-// Clears the keys of the active cells (only those are read this step).
+// Clears the keys of the active cells (only those are read this step); slab launch.
 __global__ void k_mesh_clear(const GeomArgs a) {
-    if (block_inactive(a)) return;
-    int x, y, z;
-    int64_t bidx;
-    if (!box_cell(a, x, y, z, bidx) || !cell_active(a, x, y, z)) return;
-    a.b.keys[bidx] = 0xFFFFFFFFFFFFFFFFull;
+    if (slab_inactive(a)) return;
+    int lo[3], hi[3];
+    active_bounds(a, lo, hi);
+#pragma unroll
+    for (int k = 0; k < kSlabZ; ++k) {
+        int x, y, z;
+        int64_t bidx;
+        if (slab_cell(a, k, x, y, z, bidx) && in_bounds(lo, hi, x, y, z)) a.b.keys[bidx] = 0xFFFFFFFFFFFFFFFFull;
+    }
 }
 
 // One warp per triangle: the lanes share the triangle's voxel box (its AABB
@@ -444,11 +448,27 @@ __global__ void __launch_bounds__(128) k_mesh_raster(const GeomArgs a) {
     const int ex = hi[0] - lo[0] + 1, ey = hi[1] - lo[1] + 1, ez = hi[2] - lo[2] + 1;
     if (ex <= 0 || ey <= 0 || ez <= 0) return;
     const int total = ex * ey * ez;
+    // Voxels farther than the guard from the triangle decide nothing (a cell
+    // next to a solid one lies within h + sqrt(3) dx of its triangle, inside
+    // the guard), so only voxels within the guard of the triangle's bounding
+    // sphere compute their distance: a superset, with a relative slack that
+    // covers the rounding of the squared distances.
+    const V3 cen = v3((A.x + B.x + C.x) * (1.0f / 3.0f), (A.y + B.y + C.y) * (1.0f / 3.0f),
+                      (A.z + B.z + C.z) * (1.0f / 3.0f));
+    const float r2 = fmaxf(dot(A - cen, A - cen), fmaxf(dot(B - cen, B - cen), dot(C - cen, C - cen)));
+    const float reach = sqrtf(r2) + guard;
+    const float reach2 = reach * reach * 1.0001f;
+    // voxel index -> (x, y, z) by reciprocal multiplication (exact for these small extents)
+    const float inv_ex = 1.0f / (float)ex, inv_ey = 1.0f / (float)ey;
     for (int i = lane; i < total; i += 32) {
-        const int xi = i % ex;
-        const int r = i / ex;
-        const int x = lo[0] + xi, y = lo[1] + r % ey, z = lo[2] + r / ey;
+        const int r = (int)(((float)i + 0.5f) * inv_ex);
+        const int xi = i - r * ex;
+        const int zi = (int)(((float)r + 0.5f) * inv_ey);
+        const int yi = r - zi * ey;
+        const int x = lo[0] + xi, y = lo[1] + yi, z = lo[2] + zi;
         V3 w = cell_world(a.fp, x, y, z), bary;
+        const V3 dcen = w - cen;
+        if (dot(dcen, dcen) > reach2) continue;
         V3 cp = closest_point(w, A, B, C, bary);
         float dc = length(w - cp) / cs;
         float bin = roundf(dc * 65536.0f);
@@ -459,13 +479,23 @@ __global__ void __launch_bounds__(128) k_mesh_raster(const GeomArgs a) {
     }
 }
 
+__device__ void resolve_cell(const GeomArgs& a, int has_prev, int x, int y, int z, int64_t bidx);
+
 // Mask byte and wall value of every active cell (cells outside the active
-// bounds keep mask 0; their wall value is never read).
+// bounds keep mask 0; their wall value is never read); slab launch.
 __global__ void k_mesh_resolve(const GeomArgs a, int has_prev) {
-    if (block_inactive(a)) return;
-    int x, y, z;
-    int64_t bidx;
-    if (!box_cell(a, x, y, z, bidx) || !cell_active(a, x, y, z)) return;
+    if (slab_inactive(a)) return;
+    int lo[3], hi[3];
+    active_bounds(a, lo, hi);
+#pragma unroll
+    for (int k = 0; k < kSlabZ; ++k) {
+        int x, y, z;
+        int64_t bidx;
+        if (slab_cell(a, k, x, y, z, bidx) && in_bounds(lo, hi, x, y, z)) resolve_cell(a, has_prev, x, y, z, bidx);
+    }
+}
+
+__device__ void resolve_cell(const GeomArgs& a, int has_prev, int x, int y, int z, int64_t bidx) {
     const int64_t gid = flat(a.g, x, y, z);
     uint8_t prev_part = a.b.mask_prev[gid] & kPartMask;
     unsigned long long key = a.b.keys[bidx];
@@ -548,26 +578,90 @@ __device__ float mesh_ray_root(const GeomArgs& a, int fx, int fy, int fz, int sx
 // raster's h + 2 dx guard, so it owns a key: keyless cells are skipped without
 // reading their 18 neighbours.  Link counting and emission use this same test.
 __device__ __forceinline__ bool may_have_links(const GeomArgs& a, int64_t bidx, uint8_t m_next, uint8_t m_prev) {
-    if (!persistent_fluid(m_next, m_prev)) return false;
-    return a.b.keys == nullptr || a.b.keys[bidx] != 0xFFFFFFFFFFFFFFFFull;
+    // the key is loaded unconditionally, so its load overlaps the mask loads
+    const bool keyed = a.b.keys == nullptr || a.b.keys[bidx] != 0xFFFFFFFFFFFFFFFFull;
+    return persistent_fluid(m_next, m_prev) && keyed;
 }
 
 // ---------------------------------------------------------------------------
 // Topology impulses (BF.metal:2557-2609 covered, 2616-2666 uncovered) and the
 // per-block cut-link count.  Reads populations only; runs before any link write.
 // ---------------------------------------------------------------------------
+// Topology impulses and cut-link count of one cell (BF.metal:2557-2609
+// covered, 2616-2666 uncovered).
 template <class S>
-__global__ void __launch_bounds__(256) k_boundary_scan(const GeomArgs a, int rep_s) {
-    __shared__ double sh[8][256];
+__device__ __forceinline__ void scan_cell(const GeomArgs& a, int rep_s, int x, int y, int z, int64_t bidx,
+                                          double (&acc)[8], uint32_t& links) {
     using R = typename S::R;
     const FluidParams& fp = a.fp;
     const int sel = fp.interpolated;
     const int mode = sel ? fp.force_mode : 6;
     const int include_topo = !sel || fp.load_component != 1;
+    const Grid& g = a.g;
+    const int64_t gid = flat(g, x, y, z);
+    const uint8_t m1 = a.b.mask_next[gid];
+    const uint8_t m0 = a.b.mask_prev[gid];
+    const typename S::T* A = (const typename S::T*)a.pops;
+    const double* body = a.b.state->body;
+    const V3 world = cell_world(fp, x, y, z);
+    if ((m1 & kCovered) && fp.accumulate && include_topo) {
+        // newly covered: previous fluid momentum (minus the wall-moving density for estimators 0-5)
+        R pd = 0, pmx = 0, pmy = 0, pmz = 0;
+        for (int q = 0; q < 19; ++q) {
+            R prev = canon_load<S>(A, g, rep_s, q, x, y, z);
+            pd += prev;
+            pmx += prev * (R)cx(q);
+            pmy += prev * (R)cy(q);
+            pmz += prev * (R)cz(q);
+        }
+        float4 w = a.b.wall[gid];
+        R ix = pmx, iy = pmy, iz = pmz;
+        if (mode != 6) {
+            ix = pmx - pd * (R)w.x;
+            iy = pmy - pd * (R)w.y;
+            iz = pmz - pd * (R)w.z;
+        }
+        add_load<R>(acc, ix, iy, iz, (R)world.x, (R)world.y, (R)world.z, body, fp.f2p);
+        acc[6] += 1.0;
+    } else if ((m1 & kUncovered) && fp.accumulate && include_topo && mode == 6) {
+        // newly uncovered: refill momentum plus the moving-domain stencil
+        float4 w = a.b.wall[gid];
+        R mx = 0, my = 0, mz = 0;
+        for (int q = 0; q < 19; ++q) {
+            R v = feq_rt<R>(q, R(1), (R)w.x, (R)w.y, (R)w.z);
+            mx += v * (R)cx(q);
+            my += v * (R)cy(q);
+            mz += v * (R)cz(q);
+        }
+        R tx = -mx, ty = -my, tz = -mz;
+        for (int q = 1; q < 19; ++q) {
+            int bx = x + cx(q), by = y + cy(q), bz = z + cz(q);
+            if (!inside(g, bx, by, bz)) continue;
+            int64_t nb = flat(g, bx, by, bz);
+            if (!((a.b.mask_prev[nb] & kPartMask) == 0 && (a.b.mask_next[nb] & kPartMask) == 0)) continue;
+            R old_out = canon_load<S>(A, g, rep_s, q, x, y, z);
+            R sup_in = canon_load<S>(A, g, rep_s, opp(q), bx, by, bz);
+            R sum = old_out + sup_in;
+            tx -= sum * (R)cx(q);
+            ty -= sum * (R)cy(q);
+            tz -= sum * (R)cz(q);
+        }
+        add_load<R>(acc, tx, ty, tz, (R)world.x, (R)world.y, (R)world.z, body, fp.f2p);
+        acc[7] += 1.0;
+    }
+    if (may_have_links(a, bidx, m1, m0)) {
+        for (int q = 1; q < 19; ++q) {
+            int sx, sy, sz;
+            if (link_source(g, a.b.mask_next, x, y, z, q, sx, sy, sz) >= 0) ++links;
+        }
+    }
+}
+
+template <class S>
+__global__ void __launch_bounds__(256) k_boundary_scan(const GeomArgs a, int rep_s) {
+    __shared__ double sh[8][256];
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     uint32_t links = 0;
-    int x, y, z;
-    int64_t bidx;
     if (block_inactive(a)) {
         // no key, link or topology change in this block
         if (linear_tid() == 0) {
@@ -577,65 +671,10 @@ __global__ void __launch_bounds__(256) k_boundary_scan(const GeomArgs a, int rep
         }
         return;
     }
-    if (box_cell(a, x, y, z, bidx) && cell_active(a, x, y, z)) {
-        const Grid& g = a.g;
-        const int64_t gid = flat(g, x, y, z);
-        const uint8_t m1 = a.b.mask_next[gid];
-        const uint8_t m0 = a.b.mask_prev[gid];
-        const typename S::T* A = (const typename S::T*)a.pops;
-        const double* body = a.b.state->body;
-        const V3 world = cell_world(fp, x, y, z);
-        if ((m1 & kCovered) && fp.accumulate && include_topo) {
-            // newly covered: previous fluid momentum (minus the wall-moving density for estimators 0-5)
-            R pd = 0, pmx = 0, pmy = 0, pmz = 0;
-            for (int q = 0; q < 19; ++q) {
-                R prev = canon_load<S>(A, g, rep_s, q, x, y, z);
-                pd += prev;
-                pmx += prev * (R)cx(q);
-                pmy += prev * (R)cy(q);
-                pmz += prev * (R)cz(q);
-            }
-            float4 w = a.b.wall[gid];
-            R ix = pmx, iy = pmy, iz = pmz;
-            if (mode != 6) {
-                ix = pmx - pd * (R)w.x;
-                iy = pmy - pd * (R)w.y;
-                iz = pmz - pd * (R)w.z;
-            }
-            add_load<R>(acc, ix, iy, iz, (R)world.x, (R)world.y, (R)world.z, body, fp.f2p);
-            acc[6] += 1.0;
-        } else if ((m1 & kUncovered) && fp.accumulate && include_topo && mode == 6) {
-            // newly uncovered: refill momentum plus the moving-domain stencil
-            float4 w = a.b.wall[gid];
-            R mx = 0, my = 0, mz = 0;
-            for (int q = 0; q < 19; ++q) {
-                R v = feq_rt<R>(q, R(1), (R)w.x, (R)w.y, (R)w.z);
-                mx += v * (R)cx(q);
-                my += v * (R)cy(q);
-                mz += v * (R)cz(q);
-            }
-            R tx = -mx, ty = -my, tz = -mz;
-            for (int q = 1; q < 19; ++q) {
-                int bx = x + cx(q), by = y + cy(q), bz = z + cz(q);
-                if (!inside(g, bx, by, bz)) continue;
-                int64_t nb = flat(g, bx, by, bz);
-                if (!((a.b.mask_prev[nb] & kPartMask) == 0 && (a.b.mask_next[nb] & kPartMask) == 0)) continue;
-                R old_out = canon_load<S>(A, g, rep_s, q, x, y, z);
-                R sup_in = canon_load<S>(A, g, rep_s, opp(q), bx, by, bz);
-                R sum = old_out + sup_in;
-                tx -= sum * (R)cx(q);
-                ty -= sum * (R)cy(q);
-                tz -= sum * (R)cz(q);
-            }
-            add_load<R>(acc, tx, ty, tz, (R)world.x, (R)world.y, (R)world.z, body, fp.f2p);
-            acc[7] += 1.0;
-        }
-        if (may_have_links(a, bidx, m1, m0)) {
-            for (int q = 1; q < 19; ++q) {
-                int sx, sy, sz;
-                if (link_source(g, a.b.mask_next, x, y, z, q, sx, sy, sz) >= 0) ++links;
-            }
-        }
+    {
+        int x, y, z;
+        int64_t bidx;
+        if (box_cell(a, x, y, z, bidx) && cell_active(a, x, y, z)) scan_cell<S>(a, rep_s, x, y, z, bidx, acc, links);
     }
     // most blocks hold no covered / uncovered cell: skip their FP64 tree
     bool nonzero = false;
@@ -657,36 +696,40 @@ __global__ void __launch_bounds__(256) k_boundary_scan(const GeomArgs a, int rep
     }
 }
 
-// Exclusive scan of the per-block link counts (one block, fixed order).
-__global__ void k_scan(const GeomArgs a) {
-    __shared__ uint32_t sh[1024];
-    const int nb = a.b.box_blocks;
-    const int per = (nb + 1023) / 1024;
-    const int t = threadIdx.x;
-    uint32_t local = 0;
-    for (int i = 0; i < per; ++i) {
-        int idx = t * per + i;
-        if (idx < nb) local += a.b.block_counts[idx];
-    }
-    sh[t] = local;
+// Exclusive scan of the per-block link counts (one block of 1024 threads).
+// Warp w owns a contiguous chunk of the counts: a coalesced pass sums it, the
+// warp totals give each chunk's base, and a second coalesced pass writes the
+// offsets 32 at a time with a shuffle scan carrying the running total.
+__global__ void __launch_bounds__(1024) k_scan(const GeomArgs a) {
+    __shared__ uint32_t wtot[32];
+    const int nb = a.b.scan_blocks;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int chunk = (nb + 31) / 32;
+    const int lo = warp * chunk;
+    const int hi = lo + chunk < nb ? lo + chunk : nb;
+    uint32_t tot = 0;
+#pragma unroll 8
+    for (int i = lo + lane; i < hi; i += 32) tot += a.b.block_counts[i];
+    for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+    if (lane == 0) wtot[warp] = tot;
     __syncthreads();
-    for (int s = 1; s < 1024; s <<= 1) {
-        uint32_t v = t >= s ? sh[t - s] : 0;
-        __syncthreads();
-        sh[t] += v;
-        __syncthreads();
-    }
-    uint32_t run = t > 0 ? sh[t - 1] : 0;
-    for (int i = 0; i < per; ++i) {
-        int idx = t * per + i;
-        if (idx < nb) {
-            uint32_t c = a.b.block_counts[idx];
-            a.b.block_offsets[idx] = run;
-            run += c;
+    uint32_t base = 0;
+    for (int w = 0; w < warp; ++w) base += wtot[w];
+#pragma unroll 4
+    for (int i0 = lo; i0 < hi; i0 += 32) {
+        const int i = i0 + lane;
+        const uint32_t c = i < hi ? a.b.block_counts[i] : 0u;
+        uint32_t incl = c;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
         }
+        if (i < hi) a.b.block_offsets[i] = base + incl - c;
+        base += __shfl_sync(0xffffffffu, incl, 31);
     }
-    if (t == 1023) {
-        uint64_t total = sh[1023];
+    if (threadIdx.x == 0) {
+        uint64_t total = 0;
+        for (int w = 0; w < 32; ++w) total += wtot[w];
         a.b.state->link_count = (int64_t)total;
         a.b.state->link_overflow = total > a.b.link_capacity ? 1u : 0u;
     }
@@ -697,23 +740,22 @@ __global__ void k_scan(const GeomArgs a) {
 // the preceding threads, so the list is ordered by box cell then direction.
 __global__ void __launch_bounds__(256) k_links_emit(const GeomArgs a, int geometry, int link_rule, int interpolated) {
     __shared__ uint32_t wsum[8];
+    const int block = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     // blocks without links (most of the box) emit nothing
-    if (a.b.block_counts[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] == 0) return;
-    int x = 0, y = 0, z = 0;
-    int64_t bidx;
+    if (a.b.block_counts[block] == 0) return;
     const Grid& g = a.g;
     uint32_t mine = 0;
-    int64_t gid = 0;
-    bool valid = box_cell(a, x, y, z, bidx);
+    int x = 0, y = 0, z = 0;
+    int64_t bidx = 0, gid = 0;
+    bool valid = box_cell(a, x, y, z, bidx) && cell_active(a, x, y, z);
     if (valid) {
         gid = flat(g, x, y, z);
-        if (may_have_links(a, bidx, a.b.mask_next[gid], a.b.mask_prev[gid])) {
-            for (int q = 1; q < 19; ++q) {
-                int sx, sy, sz;
-                if (link_source(g, a.b.mask_next, x, y, z, q, sx, sy, sz) >= 0) ++mine;
-            }
-        } else {
-            valid = false;
+        valid = may_have_links(a, bidx, a.b.mask_next[gid], a.b.mask_prev[gid]);
+    }
+    if (valid) {
+        for (int q = 1; q < 19; ++q) {
+            int sx, sy, sz;
+            if (link_source(g, a.b.mask_next, x, y, z, q, sx, sy, sz) >= 0) ++mine;
         }
     }
     // block-exclusive prefix of `mine`
@@ -728,16 +770,15 @@ __global__ void __launch_bounds__(256) k_links_emit(const GeomArgs a, int geomet
     __syncthreads();
     uint32_t wbase = 0;
     for (int w = 0; w < warp; ++w) wbase += wsum[w];
-    const int block = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     uint32_t pos = a.b.block_offsets[block] + wbase + incl - mine;
-    if (!valid || mine == 0) return;
+    if (mine == 0) return;
     for (int q = 1; q < 19; ++q) {
         int sx, sy, sz;
-        int64_t s = link_source(g, a.b.mask_next, x, y, z, q, sx, sy, sz);
-        if (s < 0) continue;
+        int64_t src = link_source(g, a.b.mask_next, x, y, z, q, sx, sy, sz);
+        if (src < 0) continue;
         if (pos < a.b.link_capacity) {
             a.b.link_cell[pos] = (uint32_t)gid;
-            a.b.link_meta[pos] = (uint32_t)q | ((uint32_t)(a.b.mask_next[s] & kPartMask) << 8);
+            a.b.link_meta[pos] = (uint32_t)q | ((uint32_t)(a.b.mask_next[src] & kPartMask) << 8);
         }
         ++pos;
     }
@@ -946,7 +987,7 @@ __global__ void __launch_bounds__(256) k_links_apply(const GeomArgs a, int rep_s
     if (__syncthreads_or(nonzero)) block_sum<8>(acc, sh);
     double tp[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     if (with_topology) {
-        const int nb = a.b.box_blocks;
+        const int nb = a.b.scan_blocks;
         const int per = (nb + (int)gridDim.x - 1) / (int)gridDim.x;
         const int lo = (int)blockIdx.x * per;
         const int hi = lo + per < nb ? lo + per : nb;
@@ -1148,6 +1189,12 @@ __global__ void k_record_sample(const GeomArgs a, bfx_run_sample* samples, uint6
 // Host launchers
 // ---------------------------------------------------------------------------
 
+int slab_block_count(const BoxDesc& box) {
+    dim3 grid, block;
+    slab_shape(box, grid, block);
+    return (int)(grid.x * grid.y * grid.z);
+}
+
 int box_block_count(const BoxDesc& box) {
     dim3 grid, block;
     box_shape(box, grid, block);
@@ -1171,10 +1218,12 @@ void launch_classify(int geometry, int has_prev, const GridDesc& g, const FluidP
     } else if (geometry == BFX_GEOMETRY_ELLIPSOID) {
         k_classify_ellipsoid<<<grid, block, 0, s>>>(a, has_prev);
     } else if (geometry == BFX_GEOMETRY_MESH) {
+        dim3 sgrid, sblock;
+        slab_shape(box, sgrid, sblock);
         k_mesh_prepare<<<(gb.nverts + 255) / 256, 256, 0, s>>>(a);
-        k_mesh_clear<<<grid, block, 0, s>>>(a);
+        k_mesh_clear<<<sgrid, sblock, 0, s>>>(a);
         k_mesh_raster<<<(unsigned)(((int64_t)gb.ntris * 32 + 127) / 128), 128, 0, s>>>(a);
-        k_mesh_resolve<<<grid, block, 0, s>>>(a, has_prev);
+        k_mesh_resolve<<<sgrid, sblock, 0, s>>>(a, has_prev);
     }
 }
 

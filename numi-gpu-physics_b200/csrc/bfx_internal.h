@@ -83,7 +83,8 @@ struct GeomBuffers {
     uint32_t link_capacity;
     uint32_t* block_counts;         // per box block
     uint32_t* block_offsets;
-    int box_blocks;
+    int box_blocks;                 // blocks of a one-slice-per-block box launch (allocations)
+    int scan_blocks;                // blocks of the link count / scan / emission launch
     double* topo_partials;          // 8 per box block
     double* link_partials;          // 16 per apply block (link sums, topology sums)
     int apply_blocks;
@@ -165,6 +166,7 @@ namespace bfx {
 struct Grid;
 Grid device_grid(const GridDesc& gd);
 int box_block_count(const BoxDesc& box);
+int slab_block_count(const BoxDesc& box);
 void launch_fill_wall(float4* wall, int64_t n, float w, cudaStream_t s);
 // Tensor map (px, py, pz, 19) of a 16-bit population array for the staged
 // fused kernel; false when the driver entry point is missing or the format is
