@@ -97,6 +97,7 @@ class Lattice:
                  mesh: dict | None = None):
         self.lib = L.load()
         self.config = config
+        self.bird = bird
         self.n = int(config.nx) * int(config.ny) * int(config.nz)
         self._mesh_keep = None
         mesh_ptr = None
@@ -241,6 +242,36 @@ class Lattice:
         buf = ct.create_string_buffer(data, len(data))
         _check(self.lib.bfx_restore_state(self.handle, buf, len(data)), self.handle)
 
+    def save_archive(self, destination: str, extra: dict | None = None):
+        """Writes a checkpoint archive (bfx.checkpoint): the canonical FP32
+        populations, the current solid mask and the exact restart state, with
+        their SHA-256 digests, configuration, bird, step, time, body and loads
+        in the manifest.  `extra` adds manifest entries."""
+        from . import checkpoint as C
+        step, time = self.step_index()
+        manifest = {"configuration": C.struct_dict(self.config),
+                    "bird": C.struct_dict(self.bird) if self.bird is not None else None,
+                    "step": int(step), "timeSeconds": float(time), "body": C.struct_dict(self.body()),
+                    "load": C.struct_dict(self.loads())}
+        if extra:
+            manifest.update(extra)
+        files = {C.POPULATIONS: self.populations().tobytes(), C.SOLID_MASK: self.mask().tobytes(),
+                 C.RESTART_STATE: self.save_state()}
+        C.write_archive(destination, manifest, files)
+
+    def restore_archive(self, source: str) -> dict:
+        """Restores a checkpoint archive written by save_archive after checking
+        every digest; the restored populations must equal the archive's
+        populations file byte for byte.  Returns the manifest."""
+        from . import checkpoint as C
+        manifest, files = C.read_archive(source)
+        self.restore_state(files[C.RESTART_STATE])
+        if self.populations().tobytes() != files[C.POPULATIONS]:
+            raise C.CheckpointError("populations file does not match the restart state")
+        if self.mask().tobytes() != files[C.SOLID_MASK]:
+            raise C.CheckpointError("solid-mask file does not match the restart state")
+        return manifest
+
     def adjoint(self, steps: int, force_weight=(0.0, 0.0, 0.0), power_weight: float = 0.0, window=None,
                 checkpoint_interval: int = 0) -> L.AdjointResult:
         """Advances `steps` steps and runs the discrete adjoint backward
@@ -359,6 +390,19 @@ class BirdFlowSimulation:
     def restore_checkpoint(self, data: bytes):
         self.lattice.restore_state(data)
         self.step_index, self.time_seconds = self.lattice.step_index()
+
+    def save_checkpoint_archive(self, destination: str):
+        """CheckpointArchive.write (CheckpointArchive.swift:45-80): a directory
+        with manifest.json, the populations, the solid mask and the exact
+        restart state, each with its SHA-256 digest (bfx.checkpoint)."""
+        self.lattice.save_archive(destination)
+
+    def restore_checkpoint_archive(self, source: str):
+        """CheckpointArchive.read (CheckpointArchive.swift:82-110): verifies the
+        schema, sizes and digests, then restores."""
+        manifest = self.lattice.restore_archive(source)
+        self.step_index, self.time_seconds = self.lattice.step_index()
+        return manifest
 
     def close(self):
         self.lattice.close()
