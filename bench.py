@@ -529,8 +529,8 @@ def main():
     traffic = profiled_traffic(args.workload, args.storage)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "peak_kind": f"of {peak_kind}",
-                "kernel": ("k_stream (TMA-staged fused AA stream+collide, 16-bit TRT)"
-                           if coll == "trt" and args.storage in ("f16dev", "bf16dev")
+                "kernel": ("k_stream (TMA-staged fused AA stream+collide, 16-bit storage)"
+                           if coll in ("trt", "rr3", "reg") and args.storage in ("f16dev", "bf16dev")
                            else "k_bulk (fused AA stream+collide over every fluid cell)"),
                 "bytes_per_launch": bytes_per_launch, "bytes_rule": "fluid cells x 19 x 2 x storage bytes",
                 "kernel_ms": kernel_s * 1000.0}
