@@ -574,7 +574,10 @@ __global__ void __launch_bounds__(256) k_adj_bulk(const AdjArgs a) {
 template <int K>
 __device__ __forceinline__ void write_partials(double (&v)[K], double* out) {
     __shared__ double sh[K][256];
-    block_sum<K>(v, sh);
+    // most blocks contribute nothing: skip their tree (a sum of zeros is 0)
+    bool nonzero = false;
+    for (int k = 0; k < K; ++k) nonzero = nonzero || v[k] != 0.0;
+    if (__syncthreads_or(nonzero)) block_sum<K>(v, sh);
     const int block = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     if (linear_tid() == 0)
         for (int k = 0; k < K; ++k) out[K * block + k] = v[k];
@@ -589,7 +592,14 @@ __global__ void __launch_bounds__(256) k_adj_rare(const AdjArgs a) {
     double grad[NP] = {0.0, 0.0, 0.0, 0.0};
     int x, y, z;
     int64_t bidx;
-    if (box_cell(ga, x, y, z, bidx)) {
+    if (block_inactive(ga)) {
+        // flagged cells lie within the active bounds
+        const int block = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+        if (linear_tid() == 0)
+            for (int k = 0; k < NP; ++k) a.part_rare[NP * block + k] = 0.0;
+        return;
+    }
+    if (box_cell(ga, x, y, z, bidx) && cell_active(ga, x, y, z)) {
         const int64_t gid = flat(g, x, y, z);
         const uint8_t mk = ga.b.mask_next[gid];
         if (mk) {
@@ -729,14 +739,28 @@ __global__ void __launch_bounds__(128) k_adj_halo(const AdjArgs a, int rep_s, in
     hy -= 1;
     hz -= 1;
     R* A = (R*)a.lam;
+    // two passes, as in k_halo: the loads read halo-facing slots (rep E:
+    // A[opp q][h]; rep S: A[q][h + c_q]) and the image stores write
+    // A[opp q][w] / A[q][w + c_q] of a real cell w, which no load reads
+    R v[19];
+    uint32_t live = 0;
+#pragma unroll
     for (int q = 1; q < 19; ++q) {
         const int bx = hx + cx(q), by = hy + cy(q), bz = hz + cz(q);
         if (!inside(g, bx, by, bz)) continue;
+        live |= 1u << q;
+        const R* slot = rep_s ? A + (int64_t)q * g.pn + pflat(g, bx, by, bz) : A + (int64_t)opp(q) * g.pn + pflat(g, hx, hy, hz);
+        v[q] = *slot;
+    }
+    int wx = hx, wy = hy, wz = hz;
+    const bool image = wrap(g, wx, wy, wz);
+#pragma unroll
+    for (int q = 1; q < 19; ++q) {
+        if (!(live & (1u << q))) continue;
+        const int bx = hx + cx(q), by = hy + cy(q), bz = hz + cz(q);
         R* slot = rep_s ? A + (int64_t)q * g.pn + pflat(g, bx, by, bz) : A + (int64_t)opp(q) * g.pn + pflat(g, hx, hy, hz);
-        const R v = *slot;
         *slot = R(0);
-        int wx = hx, wy = hy, wz = hz;
-        if (wrap(g, wx, wy, wz)) *canon_slot(A, g, rep_s, q, wx, wy, wz) = v;
+        if (image) *canon_slot(A, g, rep_s, q, wx, wy, wz) = v[q];
     }
 }
 
@@ -748,7 +772,8 @@ __global__ void __launch_bounds__(256) k_adj_topology(const AdjArgs a, int rep_s
     const FluidParams& fp = ga.fp;
     int x, y, z;
     int64_t bidx;
-    if (!box_cell(ga, x, y, z, bidx)) return;
+    if (block_inactive(ga)) return;
+    if (!box_cell(ga, x, y, z, bidx) || !cell_active(ga, x, y, z)) return;
     if (!fp.accumulate || (fp.interpolated && fp.load_component == 1)) return;
     const int64_t gid = flat(g, x, y, z);
     const uint8_t mk = ga.b.mask_next[gid];
