@@ -124,6 +124,9 @@ struct bfx_sim {
     // pinned host staging of the device state: read-backs and body uploads
     // without a pageable-copy bounce
     DeviceState* hstate = nullptr;
+    // hstate holds the device state as of now: no launch, copy or state
+    // change since it was read (the read-only entry points reuse it)
+    bool hstate_fresh = false;
 
     bool geometry() const { return cfg.geometry != BFX_GEOMETRY_NONE; }
     bool moving() const { return geometry() && !cfg.static_geometry; }
@@ -274,6 +277,7 @@ void timing_collect(bfx_sim* s) {
 // and link tangents, the link values, masks, keys, state and pre-collision moments.
 void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint64_t sample_index,
                  const TapeSlot* tape = nullptr) {
+    s->hstate_fresh = false;
     uint8_t* mprev = s->mask[s->cur];
     uint8_t* mnext = s->moving() ? s->mask[s->cur ^ 1] : s->mask[s->cur];
     if (s->moving()) {
@@ -349,6 +353,7 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
 // alternates with period two, so a pair graph leaves it where it started and
 // the single-step graph of each parity hands over to the other's.
 int run_steps_graph(bfx_sim* s, int nsteps) {
+    s->hstate_fresh = false;
     const int key = s->rep_s;
     cudaGraphExec_t* slot = nsteps == 2 ? &s->pair_graph[key] : &s->step_graph[key];
     uint64_t* count = nsteps == 2 ? &s->pair_launches[key] : &s->step_launches[key];
@@ -728,22 +733,37 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
     return BFX_OK;
 }
 
-#define BFX_GUARD(s)                                             \
+#define BFX_GUARD_READ(s)                                        \
     do {                                                         \
         if (!(s)) return BFX_ERR_INVALID_ARGUMENT;               \
         if ((s)->invalid) return BFX_ERR_INVALIDATED;            \
         cudaSetDevice((s)->device);                              \
     } while (0)
+// every entry point that may change the device state drops the host copy
+#define BFX_GUARD(s)                                             \
+    do {                                                         \
+        BFX_GUARD_READ(s);                                       \
+        (s)->hstate_fresh = false;                               \
+    } while (0)
 
 static int read_state(bfx_sim* s, DeviceState* st) {
-    int rc = sync_check(s, "read-back");
-    if (rc != BFX_OK) return rc;
+    if (s->hstate && s->hstate_fresh) {
+        *st = *s->hstate;
+        return BFX_OK;
+    }
     cudaError_t e;
     if (s->hstate) {
+        // one synchronisation: the copy queues behind the pending work
         e = cudaMemcpyAsync(s->hstate, s->dstate, sizeof(*st), cudaMemcpyDeviceToHost, s->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
-        if (e == cudaSuccess) *st = *s->hstate;
+        if (e == cudaSuccess) e = cudaGetLastError();
+        if (e == cudaSuccess) {
+            *st = *s->hstate;
+            s->hstate_fresh = true;
+        }
     } else {
+        int rc = sync_check(s, "read-back");
+        if (rc != BFX_OK) return rc;
         e = cudaMemcpy(st, s->dstate, sizeof(*st), cudaMemcpyDeviceToHost);
     }
     if (e != cudaSuccess) return cuda_fail(s, e, "state read-back");
@@ -850,7 +870,7 @@ static void loads_from_state(const bfx_sim* s, const DeviceState& st, bfx_loads*
 }
 
 int bfx_last_loads(bfx_sim* s, bfx_loads* out) {
-    BFX_GUARD(s);
+    BFX_GUARD_READ(s);
     if (!out) return BFX_ERR_INVALID_ARGUMENT;
     DeviceState st;
     int rc = read_state(s, &st);
@@ -860,7 +880,7 @@ int bfx_last_loads(bfx_sim* s, bfx_loads* out) {
 }
 
 int bfx_snapshot(bfx_sim* s, bfx_snapshot_data* out) {
-    BFX_GUARD(s);
+    BFX_GUARD_READ(s);
     if (!out) return BFX_ERR_INVALID_ARGUMENT;
     DeviceState st;
     int rc = read_state(s, &st);
@@ -1142,7 +1162,7 @@ int bfx_set_body(bfx_sim* s, const bfx_body_state* in) {
 }
 
 int bfx_step_index(bfx_sim* s, uint64_t* step, double* time) {
-    BFX_GUARD(s);
+    BFX_GUARD_READ(s);
     DeviceState st;
     int rc = read_state(s, &st);
     if (rc != BFX_OK) return rc;
@@ -1310,6 +1330,7 @@ int bfx_adjoint(bfx_sim* s, uint64_t steps, const bfx_adjoint_objective* objecti
         snap_cur[i] = s->cur;
     };
     auto restore = [&](uint64_t i) {
+        s->hstate_fresh = false;
         cudaMemcpyAsync(s->pops, snap_pops + i * pop_bytes, pop_bytes, cudaMemcpyDeviceToDevice, s->stream);
         cudaMemcpyAsync(s->mask[snap_cur[i]], snap_mask + i * 2 * n, n, cudaMemcpyDeviceToDevice, s->stream);
         cudaMemcpyAsync(s->mask[snap_cur[i] ^ 1], snap_mask + i * 2 * n + n, n, cudaMemcpyDeviceToDevice, s->stream);
