@@ -386,6 +386,36 @@ typedef struct bfx_adjoint_result {
 BFX_API int bfx_adjoint(bfx_sim* sim, uint64_t steps, const bfx_adjoint_objective* objective,
                         uint32_t checkpoint_interval, bfx_adjoint_result* result);
 
+/* ---- coupled momentum ledger ------------------------------------------------
+ * One linear-momentum balance per step of a free-flight run, all impulses in
+ * SI (kg m / s): the fluid momentum reduced directly from the populations
+ * before and after the step, the whole-bird and prescribed-wing momenta, and
+ * the external sources the fluid receives (open far-field faces, sponge) with
+ * the persistent cut-link exchange reconstructed from the pre-step
+ * populations.  Replaces BirdFlowSimulation.advanceWithCoupledMomentumLedger
+ * (BirdFlowSimulation.swift:806-1085, BF.metal:4322-4552); the report (RMS,
+ * relative residuals, verdict) is assembled by the caller. */
+typedef struct bfx_ledger_sample {
+    uint64_t step;
+    double time;
+    double fluid_momentum_before[3], fluid_momentum_after[3], fluid_momentum_change[3];
+    double body_momentum_before[3], body_momentum_after[3];
+    double wing_momentum_before[3], wing_momentum_after[3];
+    double aerodynamic_impulse[3], gravity_impulse[3];
+    double far_field_impulse[3], sponge_impulse[3], link_exchange_impulse[3], topology_impulse[3];
+    double fluid_boundary_impulse[3], boundary_residual[3];
+    double total_momentum_change[3], external_impulse[3], system_residual[3];
+    uint64_t far_field_links, sponge_cells, boundary_links, topology_cells;
+} bfx_ledger_sample;
+
+/* Advances `steps` steps one at a time and records a ledger sample per step
+ * (capacity >= steps).  Free flight only, sponge strength below 1 - 1e-6 (the
+ * pre-sponge populations are reconstructed from the post-sponge ones):
+ * BFX_ERR_UNSUPPORTED otherwise.  *steps_done reports the samples written,
+ * also when a safety violation (BFX_ERR_SAFETY) stops the run. */
+BFX_API int bfx_advance_ledger(bfx_sim* sim, uint64_t steps, bfx_ledger_sample* samples, size_t capacity,
+                               uint64_t* steps_done);
+
 /* Message of the last failure on this handle (or of the last failed create when sim is NULL). */
 BFX_API int bfx_last_error(bfx_sim* sim, char* buf, size_t capacity);
 

@@ -123,13 +123,27 @@ class AdjointResult(ct.Structure):
                 ("reverse_ms", ct.c_double), ("max_links", ct.c_uint64), ("work_bytes", ct.c_uint64)]
 
 
+LEDGER_VECTORS = ("fluid_momentum_before", "fluid_momentum_after", "fluid_momentum_change", "body_momentum_before",
+                  "body_momentum_after", "wing_momentum_before", "wing_momentum_after", "aerodynamic_impulse",
+                  "gravity_impulse", "far_field_impulse", "sponge_impulse", "link_exchange_impulse",
+                  "topology_impulse", "fluid_boundary_impulse", "boundary_residual", "total_momentum_change",
+                  "external_impulse", "system_residual")
+LEDGER_COUNTS = ("far_field_links", "sponge_cells", "boundary_links", "topology_cells")
+
+
+class LedgerSample(ct.Structure):
+    _fields_ = ([("step", ct.c_uint64), ("time", ct.c_double)] + [(n, ct.c_double * 3) for n in LEDGER_VECTORS] +
+                [(n, ct.c_uint64) for n in LEDGER_COUNTS])
+
+
 EXPORTED = (
     "bfx_version", "bfx_abi_version", "bfx_device_count", "bfx_create", "bfx_destroy", "bfx_advance",
     "bfx_snapshot", "bfx_copy_fields", "bfx_copy_gauge_pressure", "bfx_runtime_safety", "bfx_last_loads",
     "bfx_copy_populations", "bfx_set_populations", "bfx_copy_mask", "bfx_copy_wall", "bfx_copy_links",
     "bfx_fluid_mass_momentum", "bfx_save_state", "bfx_restore_state", "bfx_get_body", "bfx_set_body",
     "bfx_step_index", "bfx_set_kernel_timing", "bfx_kernel_timing", "bfx_timer_begin", "bfx_timer_end",
-    "bfx_launch_count", "bfx_device_bytes", "bfx_fluid_mass_momentum_noalloc", "bfx_adjoint", "bfx_last_error",
+    "bfx_launch_count", "bfx_device_bytes", "bfx_fluid_mass_momentum_noalloc", "bfx_adjoint", "bfx_advance_ledger",
+    "bfx_last_error",
 )
 
 _lib = None
@@ -181,6 +195,7 @@ def load(path: str | None = None):
     L.bfx_device_bytes.argtypes = [vp, P(ct.c_uint64)]
     L.bfx_fluid_mass_momentum_noalloc.argtypes = [vp, vp, ct.c_uint32, ct.c_uint32, ct.c_uint32, vp]
     L.bfx_adjoint.argtypes = [vp, ct.c_uint64, P(AdjointObjective), ct.c_uint32, P(AdjointResult)]
+    L.bfx_advance_ledger.argtypes = [vp, ct.c_uint64, P(LedgerSample), ct.c_size_t, P(ct.c_uint64)]
     L.bfx_last_error.argtypes = [vp, ct.c_char_p, ct.c_size_t]
     if path is None:
         _lib = L

@@ -10,6 +10,7 @@ record_run_samples)`` semantics and the same error kinds (``BirdFlowError``).
 from __future__ import annotations
 
 import ctypes as ct
+import math
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -242,6 +243,18 @@ class Lattice:
         buf = ct.create_string_buffer(data, len(data))
         _check(self.lib.bfx_restore_state(self.handle, buf, len(data)), self.handle)
 
+    def advance_ledger(self, steps: int):
+        """Advances `steps` steps one at a time with the coupled momentum
+        ledger (bfx_advance_ledger): one L.LedgerSample per step, impulses in
+        kg m / s.  A safety violation raises after the samples written so far
+        are kept in ``self.last_ledger``."""
+        samples = (L.LedgerSample * max(steps, 1))()
+        done = ct.c_uint64()
+        st = self.lib.bfx_advance_ledger(self.handle, steps, samples, max(steps, 1), ct.byref(done))
+        self.last_ledger = [samples[i] for i in range(done.value)]
+        _check(st, self.handle)
+        return self.last_ledger
+
     def save_archive(self, destination: str, extra: dict | None = None):
         """Writes a checkpoint archive (bfx.checkpoint): the canonical FP32
         populations, the current solid mask and the exact restart state, with
@@ -391,6 +404,22 @@ class BirdFlowSimulation:
         self.lattice.restore_state(data)
         self.step_index, self.time_seconds = self.lattice.step_index()
 
+    def advance_with_coupled_momentum_ledger(self, steps: int, maximum_relative_residual: float = 0.005) -> dict:
+        """advanceWithCoupledMomentumLedger (BirdFlowSimulation.swift:806-1085):
+        steps one at a time recording the total-system linear-momentum
+        balance, and gates it: the boundary closure (aerodynamic impulse +
+        fluid boundary impulse) and the external-system closure (total
+        momentum change - far field - sponge - gravity) must each stay within
+        `maximum_relative_residual` in RMS, relative to the RMS aerodynamic
+        impulse (and the RMS external impulse for the system closure)."""
+        if not self.configuration.free_flight:
+            raise BirdFlowError(10, "the total-system ledger requires freeFlight=true")
+        if steps <= 0 or not math.isfinite(maximum_relative_residual) or maximum_relative_residual <= 0:
+            raise BirdFlowError(3, f"invalid advance request steps={steps} batchSize=1")
+        samples = self.lattice.advance_ledger(steps)
+        self.step_index, self.time_seconds = self.lattice.step_index()
+        return ledger_report(samples, self.configuration.scaling.time_step_seconds, maximum_relative_residual)
+
     def save_checkpoint_archive(self, destination: str):
         """CheckpointArchive.write (CheckpointArchive.swift:45-80): a directory
         with manifest.json, the populations, the solid mask and the exact
@@ -406,3 +435,49 @@ class BirdFlowSimulation:
 
     def close(self):
         self.lattice.close()
+
+
+def ledger_report(samples, time_step_seconds: float, maximum_relative_residual: float = 0.005) -> dict:
+    """CoupledMomentumLedgerReport (CoupledMomentumLedger.swift:36-60) from
+    ledger samples: RMS and maximum residuals, their relative values and the
+    verdict of the two closure gates."""
+    rows = []
+    for s in samples:
+        d = {"step": int(s.step), "time_seconds": float(s.time)}
+        for n in L.LEDGER_VECTORS:
+            d[n] = [float(v) for v in getattr(s, n)]
+        for n in L.LEDGER_COUNTS:
+            d[n] = int(getattr(s, n))
+        rows.append(d)
+
+    def rms(key):
+        return math.sqrt(sum(sum(v * v for v in r[key]) for r in rows) / len(rows)) if rows else 0.0
+
+    def maximum(key):
+        return max((math.sqrt(sum(v * v for v in r[key])) for r in rows), default=0.0)
+
+    aero, external = rms("aerodynamic_impulse"), rms("external_impulse")
+    boundary, system = rms("boundary_residual"), rms("system_residual")
+    rel_boundary = boundary / max(aero, 1.0e-30)
+    rel_system = system / max(max(aero, external), 1.0e-30)
+    finite = all(math.isfinite(v) for r in rows for n in L.LEDGER_VECTORS for v in r[n])
+    passed = bool(rows) and finite and rel_boundary <= maximum_relative_residual and rel_system <= maximum_relative_residual
+    return {
+        "schema_version": 1, "steps": len(rows), "time_step_seconds": time_step_seconds,
+        "momentum_definition": "direct population momentum + whole-bird translational momentum + prescribed-wing "
+                               "momentum relative to the registered body frame; external impulse = open far field + "
+                               "sponge + gravity",
+        "topology_definition": "fluid boundary impulse minus the persistent-link exchange reconstructed from the "
+                               "pre-step populations; the remainder includes cover / uncover conversion",
+        "samples": rows, "rms_aerodynamic_impulse": aero, "rms_external_impulse": external,
+        "rms_boundary_closure_residual": boundary, "rms_external_system_closure_residual": system,
+        "maximum_boundary_closure_residual": maximum("boundary_residual"),
+        "maximum_external_system_closure_residual": maximum("system_residual"),
+        "relative_rms_boundary_closure_residual": rel_boundary,
+        "relative_rms_external_system_closure_residual": rel_system,
+        "maximum_allowed_relative_rms_residual": maximum_relative_residual,
+        "finite": finite, "passed": passed,
+        "scientific_verdict": "coupled external linear-momentum and fluid/boundary impulse gates passed" if passed
+        else "coupled momentum closure failed; do not accept quantitative free-flight loads",
+    }
+

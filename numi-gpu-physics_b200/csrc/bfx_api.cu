@@ -124,6 +124,10 @@ struct bfx_sim {
     // pinned host staging of the device state: read-backs and body uploads
     // without a pageable-copy bounce
     DeviceState* hstate = nullptr;
+    // coupled momentum ledger partial sums (allocated on first use)
+    double* ledger_in = nullptr;
+    double* ledger_out = nullptr;
+    int ledger_blocks = 0;
     // hstate holds the device state as of now: no launch, copy or state
     // change since it was read (the read-only entry points reuse it)
     bool hstate_fresh = false;
@@ -276,7 +280,7 @@ void timing_collect(bfx_sim* s) {
 // With a tape slot the step also records what its adjoint needs: the wing-frame
 // and link tangents, the link values, masks, keys, state and pre-collision moments.
 void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint64_t sample_index,
-                 const TapeSlot* tape = nullptr) {
+                 const TapeSlot* tape = nullptr, double* ledger_in = nullptr) {
     s->hstate_fresh = false;
     uint8_t* mprev = s->mask[s->cur];
     uint8_t* mnext = s->moving() ? s->mask[s->cur ^ 1] : s->mask[s->cur];
@@ -294,6 +298,12 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
         gb.frames = tape->frames;
         launch_link_tangent(s->cfg.link_rule, s->fp.interpolated, s->g, s->fp, s->box, gb, tape->link_tangent,
                             s->stream);
+        s->launches += 1;
+    }
+    if (ledger_in) {
+        // the ledger's pre-step pass: geometry built, no population written yet
+        launch_ledger_in(s->cfg.storage, s->rep_s, s->g, s->fp, fb, s->geometry() ? mprev : nullptr,
+                         s->geometry() ? mnext : nullptr, ledger_in, s->ledger_blocks, s->stream);
         s->launches += 1;
     }
     // halo fill before the link writes: a link whose solid source is a periodic
@@ -1223,6 +1233,92 @@ int bfx_launch_count(bfx_sim* s, uint64_t* launches) {
 int bfx_device_bytes(bfx_sim* s, uint64_t* bytes) {
     if (!s || !bytes) return BFX_ERR_INVALID_ARGUMENT;
     *bytes = s->device_bytes;
+    return BFX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Coupled momentum ledger (BirdFlowSimulation.advanceWithCoupledMomentumLedger,
+// BirdFlowSimulation.swift:806-1085): steps one at a time with the ledger's
+// pre- and post-step passes (bfx_ledger.cu) and forms the balance in SI.
+// ---------------------------------------------------------------------------
+int bfx_advance_ledger(bfx_sim* s, uint64_t steps, bfx_ledger_sample* samples, size_t capacity,
+                       uint64_t* steps_done) {
+    BFX_GUARD(s);
+    if (steps_done) *steps_done = 0;
+    if (!s->cfg.free_flight || !s->has_bird)
+        return fail(s, BFX_ERR_UNSUPPORTED, "the total-system ledger requires free flight with a bird");
+    if (!(s->cfg.sponge_strength < 1.0f - 1.0e-6f))
+        return fail(s, BFX_ERR_UNSUPPORTED, "sponge strength must be below 0.999999 to reconstruct the pre-sponge populations");
+    if (steps == 0) return BFX_OK;
+    if (!samples || capacity < steps) return fail(s, BFX_ERR_CAPACITY, "ledger sample buffer smaller than the step count");
+    if (!s->ledger_in) {
+        s->ledger_blocks = 4 * s->sm_count;
+        cudaError_t e = dalloc(s, &s->ledger_in, (size_t)s->ledger_blocks * kLedgerInWidth * sizeof(double));
+        if (e == cudaSuccess) e = dalloc(s, &s->ledger_out, (size_t)s->ledger_blocks * kLedgerOutWidth * sizeof(double));
+        if (e != cudaSuccess) return cuda_fail(s, e, "ledger allocation");
+    }
+    std::vector<double> pin((size_t)s->ledger_blocks * kLedgerInWidth), pout((size_t)s->ledger_blocks * kLedgerOutWidth);
+    const double dt = (double)s->cfg.time_step;
+    const double f2p = (double)s->fp.f2p;
+    const double mscale = f2p * dt;  // lattice momentum -> kg m / s
+    const double mass = (double)s->bird.body_radii_mass.v[3];
+    for (uint64_t k = 0; k < steps; ++k) {
+        DeviceState before, after;
+        int rc = read_state(s, &before);
+        if (rc != BFX_OK) return rc;
+        encode_step(s, 0, nullptr, 0, nullptr, s->ledger_in);
+        uint8_t* mcur = s->geometry() ? s->mask[s->cur] : nullptr;
+        launch_ledger_out(s->cfg.storage, s->rep_s, s->g, s->fp, fluid_buffers(s, mcur), mcur, s->ledger_out,
+                          s->ledger_blocks, s->stream);
+        s->launches += 1;
+        cudaError_t e = cudaMemcpyAsync(pin.data(), s->ledger_in, pin.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                        s->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(pout.data(), s->ledger_out, pout.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                s->stream);
+        if (e != cudaSuccess) return cuda_fail(s, e, "ledger read-back");
+        rc = read_state(s, &after);
+        if (rc != BFX_OK) return rc;
+        s->step = after.step;
+        double in[kLedgerInWidth] = {}, out[kLedgerOutWidth] = {};
+        for (int b = 0; b < s->ledger_blocks; ++b) {
+            for (int j = 0; j < kLedgerInWidth; ++j) in[j] += pin[(size_t)b * kLedgerInWidth + j];
+            for (int j = 0; j < kLedgerOutWidth; ++j) out[j] += pout[(size_t)b * kLedgerOutWidth + j];
+        }
+        bfx_ledger_sample& r = samples[k];
+        std::memset(&r, 0, sizeof(r));
+        r.step = after.step;
+        r.time = (double)(float)((double)after.step * dt);
+        for (int c = 0; c < 3; ++c) {
+            r.fluid_momentum_before[c] = in[1 + c] * mscale;
+            r.fluid_momentum_after[c] = out[1 + c] * mscale;
+            r.fluid_momentum_change[c] = r.fluid_momentum_after[c] - r.fluid_momentum_before[c];
+            r.body_momentum_before[c] = before.body[7 + c] * mass;
+            r.body_momentum_after[c] = after.body[7 + c] * mass;
+            r.wing_momentum_before[c] = (double)before.wing_prev[c] + (double)before.wing_prev[8 + c];
+            r.wing_momentum_after[c] = (double)after.wing_prev[c] + (double)after.wing_prev[8 + c];
+            r.aerodynamic_impulse[c] = after.loads_lattice[c] * f2p * dt;
+            r.gravity_impulse[c] = (double)s->cfg.gravity[c] * (mass * dt);
+            r.far_field_impulse[c] = in[5 + c] * mscale;
+            r.sponge_impulse[c] = out[5 + c] * mscale;
+            r.link_exchange_impulse[c] = in[9 + c] * mscale;
+            r.fluid_boundary_impulse[c] = r.fluid_momentum_change[c] - r.far_field_impulse[c] - r.sponge_impulse[c];
+            r.topology_impulse[c] = r.fluid_boundary_impulse[c] - r.link_exchange_impulse[c];
+            r.boundary_residual[c] = r.aerodynamic_impulse[c] + r.fluid_boundary_impulse[c];
+            r.total_momentum_change[c] = r.fluid_momentum_change[c] + (r.body_momentum_after[c] - r.body_momentum_before[c]) +
+                                         (r.wing_momentum_after[c] - r.wing_momentum_before[c]);
+            r.external_impulse[c] = r.far_field_impulse[c] + r.sponge_impulse[c] + r.gravity_impulse[c];
+            r.system_residual[c] = r.total_momentum_change[c] - r.external_impulse[c];
+        }
+        r.far_field_links = (uint64_t)in[12];
+        r.boundary_links = (uint64_t)in[14];
+        r.topology_cells = (uint64_t)in[15];
+        r.sponge_cells = (uint64_t)out[8];
+        if (steps_done) *steps_done = k + 1;
+        if (after.link_overflow) return fail(s, BFX_ERR_KERNEL, "the cut-link list exceeded its capacity; raise link_capacity");
+        if (after.safety_event[2] != 0)
+            return fail(s, BFX_ERR_SAFETY, "runtime safety violation (Mach, clearance or non-finite state)");
+    }
     return BFX_OK;
 }
 

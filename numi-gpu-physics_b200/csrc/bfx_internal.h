@@ -103,6 +103,15 @@ void launch_boundary_scan(int storage, int rep_s, const GridDesc& g, const Fluid
                           const GeomBuffers& gb, const FluidBuffers& fb, cudaStream_t s);
 void launch_links_emit(int geometry, int link_rule, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
                        const GeomBuffers& gb, cudaStream_t s);
+// Coupled momentum ledger passes (bfx_ledger.cu): `blocks` rows of 16 (in) or
+// 9 (out) FP64 partial sums.
+constexpr int kLedgerInWidth = 16;
+constexpr int kLedgerOutWidth = 9;
+void launch_ledger_in(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const FluidBuffers& b,
+                      const uint8_t* mprev, const uint8_t* mnext, double* partials, int blocks, cudaStream_t s);
+void launch_ledger_out(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const FluidBuffers& b,
+                       const uint8_t* mnext, double* partials, int blocks, cudaStream_t s);
+
 // End-of-step body update parameters (k_finish).
 struct FinishParams {
     float gravity[3];

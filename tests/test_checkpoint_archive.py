@@ -74,3 +74,25 @@ def test_refuses_schema_size_and_missing_files(tmp_path):
         C.read_archive(path)
     with pytest.raises(C.CheckpointError, match="manifest"):
         C.read_archive(str(tmp_path / "missing"))
+
+
+def test_ledger_report_gates_on_the_relative_residuals():
+    """The ledger report's RMS arithmetic and gates (CoupledMomentumLedger.swift:36-60)
+    on synthetic samples: 1 % boundary residual fails a 0.5 % gate, 0.1 % passes."""
+    import bfx._lib as L
+    from bfx.simulation import ledger_report
+
+    def sample(step, residual):
+        s = L.LedgerSample()
+        s.step = step
+        s.aerodynamic_impulse[:] = [0.0, 0.0, 2.0]
+        s.boundary_residual[:] = [0.0, 0.0, 2.0 * residual]
+        s.external_impulse[:] = [0.0, 0.0, 1.0]
+        s.system_residual[:] = [0.0, 0.0, 1.0e-4]
+        return s
+
+    bad = ledger_report([sample(i, 0.01) for i in range(4)], 1e-4, 0.005)
+    good = ledger_report([sample(i, 0.001) for i in range(4)], 1e-4, 0.005)
+    assert not bad["passed"] and good["passed"]
+    assert abs(good["relative_rms_boundary_closure_residual"] - 0.001) < 1e-12
+    assert abs(good["rms_aerodynamic_impulse"] - 2.0) < 1e-12
