@@ -53,7 +53,8 @@ typedef enum bfx_status {
     BFX_ERR_INVALID_CONFIG = 7,     /* BirdFlowConfigurationError */
     BFX_ERR_INVALID_ARGUMENT = 8,
     BFX_ERR_CAPACITY = 9,           /* caller buffer or link list too small */
-    BFX_ERR_UNSUPPORTED = 10        /* configuration outside the adjoint's scope */
+    BFX_ERR_UNSUPPORTED = 10,       /* configuration outside the adjoint's scope */
+    BFX_ERR_TIMEOUT = 11            /* a required field capture found no free observation slot in time */
 } bfx_status;
 
 /* Collision operator.  The reference selects these through caseParameters.w
@@ -254,17 +255,50 @@ typedef struct bfx_snapshot_data {  /* SimulationSnapshot (Diagnostics.swift) */
     bfx_loads loads;
 } bfx_snapshot_data;
 
+/* FieldCaptureMode (GPUFieldObservation.swift:4-13): with neither capture
+ * flag the advance runs with capture disabled. */
 enum {
-    BFX_ADVANCE_CAPTURE_FIELDS = 1,   /* FieldCaptureMode.required: rho/u on the last step */
-    BFX_ADVANCE_RECORD_SAMPLES = 2    /* recordRunSamples */
+    BFX_ADVANCE_CAPTURE_FIELDS = 1,       /* .required: rho/u of the last step, waiting for a slot if need be */
+    BFX_ADVANCE_RECORD_SAMPLES = 2,       /* recordRunSamples */
+    BFX_ADVANCE_CAPTURE_BEST_EFFORT = 4   /* .bestEffort: publish only if a slot is free now, else drop */
 };
+enum { BFX_FIELD_CAPTURE_REQUIRED = 0, BFX_FIELD_CAPTURE_BEST_EFFORT = 1, BFX_FIELD_CAPTURE_DISABLED = 2 };
 
-typedef struct bfx_advance_result { /* AdvanceResult (GPUFieldObservation.swift) */
+typedef struct bfx_advance_result { /* AdvanceResult (GPUFieldObservation.swift:90-108) */
     uint64_t steps_done;
     uint32_t field_frame_published;
     uint32_t safety_passed;
     bfx_safety_record safety;
+    uint64_t dropped_field_frames;  /* droppedFieldFrameCount after the call */
 } bfx_advance_result;
+
+/* BirdGeometryFrame (GPUFieldObservation.swift:111-160): the prepared frame of
+ * the step a field was captured on.  omega_body_world.w is the conservative
+ * geometry radius. */
+typedef struct bfx_geometry_frame {
+    float body_position[4], orientation[4], linear_velocity[4], omega_body_world[4];
+    float left_root[4], left_chord[4], left_span[4], left_normal[4], left_angular_velocity[4];
+    float right_root[4], right_chord[4], right_span[4], right_normal[4], right_angular_velocity[4];
+} bfx_geometry_frame;
+
+/* GPUFieldFrameMetadata + GPUFieldFrameLease (GPUFieldObservation.swift:162-262).
+ * density (n floats) and velocity (n float4: lattice velocity xyz, w = 0) are
+ * device pointers into the leased slot, valid for reading until the lease is
+ * released; nothing may write through them. */
+typedef struct bfx_field_frame {
+    uint64_t lease;                 /* 0: no frame was leased */
+    bfx_snapshot_data snapshot;
+    uint32_t grid[3];
+    uint32_t slot;
+    float domain_origin[3];
+    float cell_size;                /* m */
+    float velocity_to_physical;     /* m/s per lattice velocity unit */
+    float _pad[3];
+    bfx_geometry_frame geometry;
+    double publication_uptime_seconds;  /* CLOCK_MONOTONIC at publication */
+    const float* density;
+    const float* velocity;
+} bfx_field_frame;
 
 BFX_API const char* bfx_version(void);
 BFX_API int bfx_abi_version(void);
@@ -283,11 +317,36 @@ BFX_API int bfx_advance(bfx_sim* sim, uint64_t steps, uint32_t batch_size, uint3
 
 /* snapshot() (BirdFlowSimulation.swift:1087) */
 BFX_API int bfx_snapshot(bfx_sim* sim, bfx_snapshot_data* out);
-/* copyMacroscopicFields() (BirdFlowSimulation.swift:1109): the fields captured by
- * the last advance with BFX_ADVANCE_CAPTURE_FIELDS (density[n], velocity[3n]). */
+/* copyMacroscopicFields() (BirdFlowSimulation.swift:1109): the newest published
+ * field frame, else observation slot 0 (density[n], velocity[3n], lattice units). */
 BFX_API int bfx_copy_fields(bfx_sim* sim, float* density, float* velocity_xyz, size_t cells);
 /* copyGaugePressureFieldPascals() (BirdFlowSimulation.swift:1132) */
 BFX_API int bfx_copy_gauge_pressure(bfx_sim* sim, float pressure_scale_pascals, float* out, size_t cells);
+/* observationBufferCount (BirdFlowSimulation.swift:480-488, 540-600): the
+ * number of field observation slots, 1...4 (default 1).  Allowed before the
+ * first step only.  wait_limit_ms bounds how long a required capture waits for
+ * a lease to be released (0: without limit, as the reference does); when it
+ * runs out the call fails with BFX_ERR_TIMEOUT and the handle stays usable. */
+BFX_API int bfx_set_observation_buffers(bfx_sim* sim, uint32_t count, uint32_t wait_limit_ms);
+/* acquireLatestGPUFieldFrame(afterStep:) (BirdFlowSimulation.swift:1148-1171):
+ * leases the newest published frame, if its step is above after_step when
+ * has_after_step is set; out->lease == 0 when there is none.  Thread-safe with
+ * respect to bfx_advance on the same handle. */
+BFX_API int bfx_acquire_field_frame(bfx_sim* sim, int has_after_step, uint64_t after_step, bfx_field_frame* out);
+/* Copies a leased frame to host memory (density[n], velocity[3n], lattice units). */
+BFX_API int bfx_field_frame_copy(bfx_sim* sim, uint64_t lease, float* density, float* velocity_xyz, size_t cells);
+/* GPUFieldFrameLease.releaseImmediately (GPUFieldObservation.swift:247-249).
+ * Releasing twice is a no-op.  Thread-safe. */
+BFX_API int bfx_release_field_frame(bfx_sim* sim, uint64_t lease);
+/* GPUFieldFrameLease.releaseAfterCompletion(of:) (GPUFieldObservation.swift:241-245):
+ * the release runs once the work queued so far on cuda_stream (a cudaStream_t;
+ * NULL: the simulation's own stream) has completed. */
+BFX_API int bfx_release_field_frame_after(bfx_sim* sim, uint64_t lease, void* cuda_stream);
+/* captureCurrentMacroscopicField(mode:) (BirdFlowSimulation.swift:1176-1210):
+ * publishes rho/u of the current populations without a step. */
+BFX_API int bfx_capture_current_fields(bfx_sim* sim, uint32_t mode, uint32_t* published);
+/* droppedFieldFrameCount, fieldCaptureWaitCount (BirdFlowSimulation.swift:466-478) */
+BFX_API int bfx_observation_counters(bfx_sim* sim, uint64_t* dropped_frames, uint64_t* capture_waits);
 /* runtimeSafetyReport() (BirdFlowSimulation.swift:1766) */
 BFX_API int bfx_runtime_safety(bfx_sim* sim, bfx_safety_record* out);
 BFX_API int bfx_last_loads(bfx_sim* sim, bfx_loads* out);

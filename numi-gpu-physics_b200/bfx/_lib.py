@@ -17,7 +17,7 @@ BFX_OK = 0
 STATUS_NAMES = {
     0: "ok", 1: "deviceUnavailable", 2: "allocationFailed", 3: "invalidAdvanceRequest",
     4: "commandBufferFailed", 5: "runtimeSafetyViolation", 6: "simulationStateInvalidated",
-    7: "invalidConfiguration", 8: "invalidArgument", 9: "capacity",
+    7: "invalidConfiguration", 8: "invalidArgument", 9: "capacity", 10: "unsupported", 11: "timeout",
 }
 
 COLLISION_TRT, COLLISION_TRT_LIMITER, COLLISION_REGULARIZED, COLLISION_RR3 = 0, 1, 2, 3
@@ -27,7 +27,10 @@ BC_FARFIELD, BC_PERIODIC, BC_VELOCITY, BC_OUTFLOW = 0, 1, 2, 3
 GEOMETRY_NONE, GEOMETRY_BIRD, GEOMETRY_ELLIPSOID, GEOMETRY_MESH = 0, 1, 2, 3
 LINK_LINEAR, LINK_RAY_ROOT = 0, 1
 INIT_EQUILIBRIUM, INIT_SHEAR_WAVE_Y, INIT_SHEAR_WAVE_Z = 0, 1, 2
-ADVANCE_CAPTURE_FIELDS, ADVANCE_RECORD_SAMPLES = 1, 2
+ADVANCE_CAPTURE_FIELDS, ADVANCE_RECORD_SAMPLES, ADVANCE_CAPTURE_BEST_EFFORT = 1, 2, 4
+FIELD_CAPTURE_REQUIRED, FIELD_CAPTURE_BEST_EFFORT, FIELD_CAPTURE_DISABLED = 0, 1, 2
+FIELD_CAPTURE_MODES = {"required": FIELD_CAPTURE_REQUIRED, "bestEffort": FIELD_CAPTURE_BEST_EFFORT,
+                       "disabled": FIELD_CAPTURE_DISABLED}
 
 STORAGE_BYTES = {STORAGE_F32: 4, STORAGE_F16_DEVIATION: 2, STORAGE_BF16_DEVIATION: 2, STORAGE_F64: 8}
 STORAGE_NAMES = {STORAGE_F32: "f32", STORAGE_F16_DEVIATION: "f16dev", STORAGE_BF16_DEVIATION: "bf16dev",
@@ -109,7 +112,23 @@ class Snapshot(ct.Structure):
 
 class AdvanceResult(ct.Structure):
     _fields_ = [("steps_done", ct.c_uint64), ("field_frame_published", ct.c_uint32),
-                ("safety_passed", ct.c_uint32), ("safety", SafetyRecord)]
+                ("safety_passed", ct.c_uint32), ("safety", SafetyRecord), ("dropped_field_frames", ct.c_uint64)]
+
+
+GEOMETRY_FRAME_FIELDS = ("body_position", "orientation", "linear_velocity", "omega_body_world", "left_root",
+                         "left_chord", "left_span", "left_normal", "left_angular_velocity", "right_root",
+                         "right_chord", "right_span", "right_normal", "right_angular_velocity")
+
+
+class GeometryFrame(ct.Structure):
+    _fields_ = [(name, ct.c_float * 4) for name in GEOMETRY_FRAME_FIELDS]
+
+
+class FieldFrame(ct.Structure):
+    _fields_ = [("lease", ct.c_uint64), ("snapshot", Snapshot), ("grid", ct.c_uint32 * 3), ("slot", ct.c_uint32),
+                ("domain_origin", ct.c_float * 3), ("cell_size", ct.c_float), ("velocity_to_physical", ct.c_float),
+                ("_pad", ct.c_float * 3), ("geometry", GeometryFrame), ("publication_uptime_seconds", ct.c_double),
+                ("density", ct.c_void_p), ("velocity", ct.c_void_p)]
 
 
 class AdjointObjective(ct.Structure):
@@ -143,7 +162,9 @@ EXPORTED = (
     "bfx_fluid_mass_momentum", "bfx_save_state", "bfx_restore_state", "bfx_get_body", "bfx_set_body",
     "bfx_step_index", "bfx_set_kernel_timing", "bfx_kernel_timing", "bfx_timer_begin", "bfx_timer_end",
     "bfx_launch_count", "bfx_device_bytes", "bfx_fluid_mass_momentum_noalloc", "bfx_adjoint", "bfx_advance_ledger",
-    "bfx_last_error",
+    "bfx_last_error", "bfx_set_observation_buffers", "bfx_acquire_field_frame", "bfx_field_frame_copy",
+    "bfx_release_field_frame", "bfx_release_field_frame_after", "bfx_capture_current_fields",
+    "bfx_observation_counters",
 )
 
 _lib = None
@@ -197,6 +218,13 @@ def load(path: str | None = None):
     L.bfx_adjoint.argtypes = [vp, ct.c_uint64, P(AdjointObjective), ct.c_uint32, P(AdjointResult)]
     L.bfx_advance_ledger.argtypes = [vp, ct.c_uint64, P(LedgerSample), ct.c_size_t, P(ct.c_uint64)]
     L.bfx_last_error.argtypes = [vp, ct.c_char_p, ct.c_size_t]
+    L.bfx_set_observation_buffers.argtypes = [vp, ct.c_uint32, ct.c_uint32]
+    L.bfx_acquire_field_frame.argtypes = [vp, ct.c_int, ct.c_uint64, P(FieldFrame)]
+    L.bfx_field_frame_copy.argtypes = [vp, ct.c_uint64, P(ct.c_float), P(ct.c_float), ct.c_size_t]
+    L.bfx_release_field_frame.argtypes = [vp, ct.c_uint64]
+    L.bfx_release_field_frame_after.argtypes = [vp, ct.c_uint64, vp]
+    L.bfx_capture_current_fields.argtypes = [vp, ct.c_uint32, P(ct.c_uint32)]
+    L.bfx_observation_counters.argtypes = [vp, P(ct.c_uint64), P(ct.c_uint64)]
     if path is None:
         _lib = L
     return L

@@ -39,10 +39,96 @@ def _fp(a):
 
 @dataclass
 class AdvanceResult:
-    """AdvanceResult (Sources/BirdFlowMetal/GPUFieldObservation.swift)."""
+    """AdvanceResult (Sources/BirdFlowMetal/GPUFieldObservation.swift:90-108)."""
     run_samples: list = field(default_factory=list)
     field_frame_published: bool = False
+    dropped_field_frame_count: int = 0
     runtime_safety: dict | None = None
+
+
+def _capture_mode(mode) -> int:
+    """FieldCaptureMode (GPUFieldObservation.swift:4-13) by name, or a bool
+    (True: required, False: disabled)."""
+    if isinstance(mode, bool):
+        return L.FIELD_CAPTURE_REQUIRED if mode else L.FIELD_CAPTURE_DISABLED
+    if mode in L.FIELD_CAPTURE_MODES:
+        return L.FIELD_CAPTURE_MODES[mode]
+    raise ValueError(f"unknown field capture mode {mode!r}")
+
+
+class _DeviceArray:
+    """__cuda_array_interface__ over a leased slot's device memory, so torch
+    (torch.as_tensor(view, device="cuda")) reads it without a copy."""
+
+    def __init__(self, ptr: int, shape, typestr: str = "<f4"):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(ptr), False),
+                                         "version": 3, "strides": None}
+
+
+class FieldFrameLease:
+    """GPUFieldFrameLease (GPUFieldObservation.swift:205-262): a read-only
+    view of one published field frame.  The slot stays out of the capture
+    rotation until the lease is released (explicitly, on leaving a ``with``
+    block, after a CUDA stream's work completes, or when the object is
+    collected)."""
+
+    def __init__(self, lattice: "Lattice", frame: L.FieldFrame, metadata: dict):
+        self._lattice = lattice
+        self._frame = frame
+        self.lease = int(frame.lease)
+        self.metadata = metadata
+
+    @property
+    def step(self) -> int:
+        return int(self._frame.snapshot.step)
+
+    def copy(self):
+        """(density[n], velocity[n, 3]) in lattice units, copied to the host."""
+        n = self._lattice.n
+        rho = np.empty(n, np.float32)
+        vel = np.empty(3 * n, np.float32)
+        _check(self._lattice.lib.bfx_field_frame_copy(self._lattice.handle, self.lease, _fp(rho), _fp(vel), n),
+               self._lattice.handle)
+        return rho, vel.reshape(-1, 3)
+
+    def device_views(self):
+        """bindMacroscopicFields: (density[nz, ny, nx], velocity[nz, ny, nx, 4])
+        as __cuda_array_interface__ objects over the slot.  Read only by
+        contract: nothing may write through them."""
+        c = self._lattice.config
+        return (_DeviceArray(self._frame.density, (c.nz, c.ny, c.nx)),
+                _DeviceArray(self._frame.velocity, (c.nz, c.ny, c.nx, 4)))
+
+    def release(self):
+        """releaseImmediately (GPUFieldObservation.swift:247-249); releasing twice is a no-op."""
+        if self.lease and self._lattice.handle:
+            self._lattice.lib.bfx_release_field_frame(self._lattice.handle, self.lease)
+        self.lease = 0
+
+    def release_after(self, stream=None):
+        """releaseAfterCompletion(of:) (GPUFieldObservation.swift:241-245): the
+        slot is released once the work queued so far on ``stream`` (a
+        torch.cuda.Stream, a raw cudaStream_t, or None for the simulation's
+        own stream) has completed."""
+        if not self.lease:
+            return
+        raw = getattr(stream, "cuda_stream", stream)
+        _check(self._lattice.lib.bfx_release_field_frame_after(self._lattice.handle, self.lease,
+                                                               ct.c_void_p(raw) if raw else None),
+               self._lattice.handle)
+        self.lease = 0
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.release()
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
 
 
 def default_config(nx: int, ny: int, nz: int, **kw) -> L.Config:
@@ -151,8 +237,13 @@ class Lattice:
         self.close()
 
     # -- stepping ---------------------------------------------------------
-    def advance(self, steps: int, batch_size: int = 32, capture_fields: bool = False, record_samples: bool = False):
-        flags = (L.ADVANCE_CAPTURE_FIELDS if capture_fields else 0) | (L.ADVANCE_RECORD_SAMPLES if record_samples else 0)
+    def advance(self, steps: int, batch_size: int = 32, capture_fields=False, record_samples: bool = False):
+        """capture_fields: a FieldCaptureMode name ("required", "bestEffort",
+        "disabled") or a bool (True: required)."""
+        mode = _capture_mode(capture_fields)
+        flags = ({L.FIELD_CAPTURE_REQUIRED: L.ADVANCE_CAPTURE_FIELDS,
+                  L.FIELD_CAPTURE_BEST_EFFORT: L.ADVANCE_CAPTURE_BEST_EFFORT}.get(mode, 0) |
+                 (L.ADVANCE_RECORD_SAMPLES if record_samples else 0))
         samples = (L.RunSample * max(steps, 1))() if record_samples else None
         res = L.AdvanceResult()
         st = self.lib.bfx_advance(self.handle, steps, batch_size, flags, samples, steps if record_samples else 0,
@@ -175,6 +266,38 @@ class Lattice:
         vel = np.empty(3 * self.n, np.float32)
         _check(self.lib.bfx_copy_fields(self.handle, _fp(rho), _fp(vel), self.n), self.handle)
         return rho, vel.reshape(-1, 3)
+
+    # -- field observation (BirdFlowSimulation.swift:1148-1210, 1806-1918) ----
+    def set_observation_buffers(self, count: int, wait_limit_ms: int = 0):
+        _check(self.lib.bfx_set_observation_buffers(self.handle, count, wait_limit_ms), self.handle)
+
+    def acquire_field_frame(self, after_step: int | None = None) -> FieldFrameLease | None:
+        frame = L.FieldFrame()
+        _check(self.lib.bfx_acquire_field_frame(self.handle, int(after_step is not None), after_step or 0,
+                                                ct.byref(frame)), self.handle)
+        if frame.lease == 0:
+            return None
+        meta = {
+            "step": int(frame.snapshot.step), "time_seconds": float(frame.snapshot.time),
+            "body": frame.snapshot.body, "aerodynamic_load": frame.snapshot.loads,
+            "grid": tuple(frame.grid), "slot": int(frame.slot), "domain_origin_meters": tuple(frame.domain_origin),
+            "cell_size_meters": float(frame.cell_size), "velocity_to_physical": float(frame.velocity_to_physical),
+            "geometry": {name: tuple(getattr(frame.geometry, name)) for name in L.GEOMETRY_FRAME_FIELDS},
+            "publication_uptime_seconds": float(frame.publication_uptime_seconds),
+        }
+        return FieldFrameLease(self, frame, meta)
+
+    def capture_current_fields(self, mode="required") -> bool:
+        published = ct.c_uint32(0)
+        _check(self.lib.bfx_capture_current_fields(self.handle, _capture_mode(mode), ct.byref(published)),
+               self.handle)
+        return bool(published.value)
+
+    def observation_counters(self):
+        """(droppedFieldFrameCount, fieldCaptureWaitCount)."""
+        d, w = ct.c_uint64(0), ct.c_uint64(0)
+        _check(self.lib.bfx_observation_counters(self.handle, ct.byref(d), ct.byref(w)), self.handle)
+        return int(d.value), int(w.value)
 
     def mask(self) -> np.ndarray:
         out = np.empty(self.n, np.uint8)
@@ -341,8 +464,11 @@ class BirdFlowSimulation:
     """
 
     def __init__(self, configuration: SimulationConfiguration, bird: BirdParameters,
-                 initial_body_state: BirdBodyState, *, storage: int = L.STORAGE_F32,
-                 collision: int = L.COLLISION_TRT, device: int = 0):
+                 initial_body_state: BirdBodyState, observation_buffer_count: int = 1, *, storage: int = L.STORAGE_F32,
+                 collision: int = L.COLLISION_TRT, device: int = 0, field_wait_limit_ms: int = 0):
+        if not 1 <= observation_buffer_count <= 4:
+            raise BirdFlowError(8,
+                                f"invalidObservationBufferCount({observation_buffer_count})")
         bird.validate(configuration)
         self.configuration = configuration
         self.bird = bird
@@ -361,6 +487,8 @@ class BirdFlowSimulation:
             collision=collision, wall_rule=L.WALL_HALFWAY, storage=storage, geometry=L.GEOMETRY_BIRD,
             free_flight=int(configuration.free_flight), accumulate_loads=1)
         self.lattice = Lattice(cfg, bird_struct(bird.packed()), body_struct(initial_body_state))
+        if observation_buffer_count != 1 or field_wait_limit_ms:
+            self.lattice.set_observation_buffers(observation_buffer_count, field_wait_limit_ms)
         self.step_index = 0
         self.time_seconds = 0.0
 
@@ -368,12 +496,14 @@ class BirdFlowSimulation:
                 record_run_samples: bool = False) -> AdvanceResult:
         if steps < 0 or batch_size <= 0:
             raise BirdFlowError(3, f"invalid advance request steps={steps} batchSize={batch_size}")
+        mode = _capture_mode(field_capture)
         if steps == 0:
-            return AdvanceResult(runtime_safety=self.runtime_safety_report() if self.configuration.free_flight else None)
-        capture = field_capture in ("required", "latest")
-        res, samples = self.lattice.advance(steps, batch_size, capture, record_run_samples)
+            return AdvanceResult(dropped_field_frame_count=self.dropped_field_frame_count,
+                                 runtime_safety=self.runtime_safety_report() if self.configuration.free_flight else None)
+        res, samples = self.lattice.advance(steps, batch_size, field_capture, record_run_samples)
         self.step_index, self.time_seconds = self.lattice.step_index()
-        out = AdvanceResult(field_frame_published=bool(res.field_frame_published))
+        out = AdvanceResult(field_frame_published=bool(res.field_frame_published),
+                            dropped_field_frame_count=int(res.dropped_field_frames))
         if record_run_samples:
             out.run_samples = [samples[i] for i in range(steps)]
         if self.configuration.free_flight:
@@ -384,12 +514,45 @@ class BirdFlowSimulation:
         return self.lattice.snapshot()
 
     def copy_macroscopic_fields(self):
-        return self.lattice.fields()
+        """copyMacroscopicFields (BirdFlowSimulation.swift:1107-1130): density
+        and velocity in m/s (lattice velocity x velocityToPhysical) of the
+        newest published frame."""
+        rho, vel = self.lattice.fields()
+        return rho, (vel * np.float32(self.configuration.scaling.velocity_to_physical)).astype(np.float32)
 
     def copy_gauge_pressure_field_pascals(self):
         rho, _ = self.lattice.fields()
         sc = self.configuration.scaling
         return (np.float32(1.0 / 3.0) * (rho - np.float32(1.0)) * np.float32(sc.pressure_scale_pascals)).astype(np.float32)
+
+    def acquire_latest_gpu_field_frame(self, after_step: int | None = None) -> FieldFrameLease | None:
+        """acquireLatestGPUFieldFrame(afterStep:) (BirdFlowSimulation.swift:1145-1171)
+        with the GPUFieldFrameMetadata scales (GPUFieldObservation.swift:162-203)."""
+        lease = self.lattice.acquire_field_frame(after_step)
+        if lease is not None:
+            sc = self.configuration.scaling
+            v2p = np.float32(sc.velocity_to_physical)
+            lease.metadata.update(
+                velocity_to_physical=float(v2p),
+                pressure_scale_pascals=float(np.float32(sc.pressure_scale_pascals)),
+                reference_dynamic_pressure_pascals=float(
+                    np.float32(0.5) * np.float32(self.configuration.physical_air_density) *
+                    (np.float32(sc.lattice_reference_speed) * v2p) ** 2),
+                physical_air_density=float(np.float32(self.configuration.physical_air_density)),
+                bird=self.bird)
+        return lease
+
+    def capture_current_macroscopic_field(self, mode: str = "required") -> bool:
+        """captureCurrentMacroscopicField(mode:) (BirdFlowSimulation.swift:1173-1210)."""
+        return self.lattice.capture_current_fields(mode)
+
+    @property
+    def dropped_field_frame_count(self) -> int:
+        return self.lattice.observation_counters()[0]
+
+    @property
+    def field_capture_wait_count(self) -> int:
+        return self.lattice.observation_counters()[1]
 
     def runtime_safety_report(self) -> dict:
         r = self.lattice.safety()

@@ -9,11 +9,14 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <ctime>
+#include <memory>
 #include <string>
 #include <vector>
 
 #include "../../include/bfx.h"
 #include "bfx_internal.h"
+#include "bfx_observation.h"
 
 using namespace bfx;
 
@@ -63,8 +66,17 @@ struct bfx_sim {
     uint8_t* mask[2] = {nullptr, nullptr};
     int cur = 0;
     float4* wall = nullptr;
-    float* density = nullptr;
+    float* density = nullptr;      // observation slot 0
     float4* velocity = nullptr;
+    // field observation slots: density / velocity volumes (slot 0 is the pair
+    // above), the slot the next capture writes, and the publication protocol
+    // (shared with pending stream-ordered releases)
+    static constexpr int kMaxSlots = 4;
+    float* slot_density[kMaxSlots] = {};
+    float4* slot_velocity[kMaxSlots] = {};
+    int capture_slot = 0;
+    uint32_t slot_wait_ms = 0;
+    std::shared_ptr<FieldSlots<bfx_field_frame>> slots;
     DeviceState* dstate = nullptr;
     Objective* dobjective = nullptr;
     bfx_bird* dbird = nullptr;
@@ -176,8 +188,8 @@ FluidBuffers fluid_buffers(bfx_sim* s, uint8_t* mask) {
     b.pops = s->pops;
     b.mask = mask;
     b.wall = s->wall;
-    b.density = s->density;
-    b.velocity = s->velocity;
+    b.density = s->slot_density[s->capture_slot];
+    b.velocity = s->slot_velocity[s->capture_slot];
     b.state = s->dstate;
     b.tape = nullptr;
     b.tmap = s->tma_ok ? &s->tmap : nullptr;
@@ -520,6 +532,10 @@ int bfx_device_count(int* count) {
     return e == cudaSuccess ? BFX_OK : BFX_ERR_DEVICE_UNAVAILABLE;
 }
 
+static int read_state(bfx_sim* s, DeviceState* st);
+static bfx_field_frame field_frame_meta(const bfx_sim* s, const DeviceState& st, int slot);
+static int copy_slot(bfx_sim* s, int slot, float* density, float* velocity_xyz);
+
 void bfx_destroy(bfx_sim* s) {
     if (!s) return;
     if (s->stream) {
@@ -632,6 +648,9 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
     if (s->tma_ok) prepare_stream(c.storage, c.collision);
     BFX_ALLOC(s->density, (size_t)g.n * sizeof(float));
     BFX_ALLOC(s->velocity, (size_t)g.n * sizeof(float4));
+    s->slot_density[0] = s->density;
+    s->slot_velocity[0] = s->velocity;
+    s->slots = std::make_shared<FieldSlots<bfx_field_frame>>(1);
     BFX_ALLOC(s->dstate, sizeof(DeviceState));
     if (cudaMallocHost((void**)&s->hstate, sizeof(DeviceState)) != cudaSuccess) {
         (void)cudaGetLastError();
@@ -739,6 +758,14 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
             return BFX_ERR_CAPACITY;
         }
     }
+    // the initial fields are published in slot 0 (BirdFlowSimulation.swift:626-640)
+    DeviceState st0;
+    if (read_state(s, &st0) != BFX_OK) {
+        g_create_error = s->err;
+        bfx_destroy(s);
+        return BFX_ERR_KERNEL;
+    }
+    s->slots->reset(field_frame_meta(s, st0, 0));
     *out = s;
     return BFX_OK;
 }
@@ -785,9 +812,24 @@ int bfx_advance(bfx_sim* s, uint64_t steps, uint32_t batch_size, uint32_t flags,
     BFX_GUARD(s);
     if (batch_size == 0) return fail(s, BFX_ERR_INVALID_ADVANCE, "batch size must be positive");
     const bool record = (flags & BFX_ADVANCE_RECORD_SAMPLES) != 0;
-    const bool capture = (flags & BFX_ADVANCE_CAPTURE_FIELDS) != 0;
+    const CaptureMode mode = (flags & BFX_ADVANCE_CAPTURE_FIELDS)        ? CaptureMode::Required
+                             : (flags & BFX_ADVANCE_CAPTURE_BEST_EFFORT) ? CaptureMode::BestEffort
+                                                                         : CaptureMode::Disabled;
     if (record && (samples == nullptr || sample_capacity < steps))
         return fail(s, BFX_ERR_CAPACITY, "run-sample buffer smaller than the step count");
+    // selectCaptureSlot (BirdFlowSimulation.swift:711): a slot for the last
+    // step's fields, given back if the advance fails
+    const int slot = steps > 0 ? s->slots->select(mode, s->slot_wait_ms) : kNoSlot;
+    if (slot == kSlotWaitTimeout)
+        return fail(s, BFX_ERR_TIMEOUT, "no field observation slot was released within the wait limit");
+    const bool capture = slot >= 0;
+    struct SlotGuard {
+        FieldSlots<bfx_field_frame>* slots;
+        int index;
+        ~SlotGuard() {
+            if (index >= 0) slots->abandon(index);
+        }
+    } slot_guard{s->slots.get(), slot};
     if (record && steps > s->dsamples_cap) {
         void* p = nullptr;
         cudaError_t e = cudaMalloc(&p, steps * sizeof(bfx_run_sample));
@@ -820,7 +862,9 @@ int bfx_advance(bfx_sim* s, uint64_t steps, uint32_t batch_size, uint32_t flags,
         }
         for (; k < count; ++k) {
             bool last = done + k + 1 == steps;
+            if (capture && last) s->capture_slot = slot;
             encode_step(s, capture && last ? 1 : 0, record ? s->dsamples : nullptr, done + k);
+            s->capture_slot = 0;
         }
         cudaError_t le = cudaGetLastError();
         if (le != cudaSuccess) return cuda_fail(s, le, "kernel launch");
@@ -843,7 +887,15 @@ int bfx_advance(bfx_sim* s, uint64_t steps, uint32_t batch_size, uint32_t flags,
             }
         }
     }
-    if (capture) s->fields_valid = true;
+    if (capture) {
+        // the state read after the last batch completed the captured step
+        DeviceState st;
+        int rc = read_state(s, &st);
+        if (rc != BFX_OK) return rc;
+        s->slots->publish(slot, field_frame_meta(s, st, slot));
+        slot_guard.index = -1;
+        s->fields_valid = true;
+    }
     if (record && steps > 0) {
         cudaError_t e = cudaMemcpy(samples, s->dsamples, steps * sizeof(bfx_run_sample), cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) return cuda_fail(s, e, "run-sample read-back");
@@ -854,6 +906,7 @@ int bfx_advance(bfx_sim* s, uint64_t steps, uint32_t batch_size, uint32_t flags,
         if (rc != BFX_OK) return rc;
         result->steps_done = steps;
         result->field_frame_published = capture ? 1 : 0;
+        result->dropped_field_frames = s->slots->dropped();
         result->safety_passed = st.safety_event[2] == 0 ? 1 : 0;
         std::memcpy(result->safety.metrics, st.safety_metrics, sizeof(st.safety_metrics));
         std::memcpy(result->safety.event, st.safety_event, sizeof(st.safety_event));
@@ -889,12 +942,7 @@ int bfx_last_loads(bfx_sim* s, bfx_loads* out) {
     return BFX_OK;
 }
 
-int bfx_snapshot(bfx_sim* s, bfx_snapshot_data* out) {
-    BFX_GUARD_READ(s);
-    if (!out) return BFX_ERR_INVALID_ARGUMENT;
-    DeviceState st;
-    int rc = read_state(s, &st);
-    if (rc != BFX_OK) return rc;
+static void snapshot_from_state(const bfx_sim* s, const DeviceState& st, bfx_snapshot_data* out) {
     out->step = st.step;
     out->time = (double)(float)((double)st.step * (double)s->cfg.time_step);
     for (int k = 0; k < 3; ++k) out->body.position[k] = st.body[k];
@@ -902,7 +950,39 @@ int bfx_snapshot(bfx_sim* s, bfx_snapshot_data* out) {
     for (int k = 0; k < 3; ++k) out->body.velocity[k] = st.body[7 + k];
     for (int k = 0; k < 3; ++k) out->body.omega_body[k] = st.body[10 + k];
     loads_from_state(s, st, &out->loads);
+}
+
+int bfx_snapshot(bfx_sim* s, bfx_snapshot_data* out) {
+    BFX_GUARD_READ(s);
+    if (!out) return BFX_ERR_INVALID_ARGUMENT;
+    DeviceState st;
+    int rc = read_state(s, &st);
+    if (rc != BFX_OK) return rc;
+    snapshot_from_state(s, st, out);
     return BFX_OK;
+}
+
+static_assert(sizeof(bfx_geometry_frame) == sizeof(Prepared), "BirdGeometryFrame is the prepared frame");
+
+// GPUFieldFrameMetadata of a capture (publishFieldSlot, BirdFlowSimulation.swift:1832-1880)
+static bfx_field_frame field_frame_meta(const bfx_sim* s, const DeviceState& st, int slot) {
+    bfx_field_frame m;
+    std::memset(&m, 0, sizeof(m));
+    snapshot_from_state(s, st, &m.snapshot);
+    m.grid[0] = s->cfg.nx;
+    m.grid[1] = s->cfg.ny;
+    m.grid[2] = s->cfg.nz;
+    m.slot = (uint32_t)slot;
+    for (int k = 0; k < 3; ++k) m.domain_origin[k] = s->cfg.origin[k];
+    m.cell_size = s->cfg.cell_size;
+    m.velocity_to_physical = s->cfg.cell_size / s->cfg.time_step;
+    std::memcpy(&m.geometry, &st.prep, sizeof(m.geometry));
+    timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    m.publication_uptime_seconds = (double)ts.tv_sec + 1.0e-9 * (double)ts.tv_nsec;
+    m.density = s->slot_density[slot];
+    m.velocity = (const float*)s->slot_velocity[slot];
+    return m;
 }
 
 int bfx_copy_fields(bfx_sim* s, float* density, float* velocity_xyz, size_t cells) {
@@ -910,10 +990,21 @@ int bfx_copy_fields(bfx_sim* s, float* density, float* velocity_xyz, size_t cell
     if (cells < (size_t)s->g.n) return fail(s, BFX_ERR_CAPACITY, "field buffers smaller than the lattice");
     int rc = sync_check(s, "fields");
     if (rc != BFX_OK) return rc;
-    if (density) cudaMemcpy(density, s->density, (size_t)s->g.n * sizeof(float), cudaMemcpyDeviceToHost);
+    // currentPublishedFieldSlot (BirdFlowSimulation.swift:1906-1918)
+    return copy_slot(s, s->slots->current(), density, velocity_xyz);
+}
+
+static int copy_slot(bfx_sim* s, int slot, float* density, float* velocity_xyz) {
+    if (density) {
+        cudaError_t e =
+            cudaMemcpy(density, s->slot_density[slot], (size_t)s->g.n * sizeof(float), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return cuda_fail(s, e, "field read-back");
+    }
     if (velocity_xyz) {
         std::vector<float> v4((size_t)s->g.n * 4);
-        cudaMemcpy(v4.data(), s->velocity, v4.size() * sizeof(float), cudaMemcpyDeviceToHost);
+        cudaError_t e =
+            cudaMemcpy(v4.data(), s->slot_velocity[slot], v4.size() * sizeof(float), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return cuda_fail(s, e, "field read-back");
         for (int64_t i = 0; i < s->g.n; ++i) {
             velocity_xyz[3 * i] = v4[4 * i];
             velocity_xyz[3 * i + 1] = v4[4 * i + 1];
@@ -1127,10 +1218,16 @@ int bfx_restore_state(bfx_sim* s, const void* buf, size_t size) {
         // rebuild the static link list for the restored representation
         encode_links(s, s->mask[s->cur], s->mask[s->cur]);
     }
+    // every slot is freed and slot 0 republished from the restored
+    // populations (restoreCheckpointState, BirdFlowSimulation.swift:1990-2023)
+    s->capture_slot = 0;
+    launch_macroscopic(s->cfg.storage, s->rep_s, s->g, fluid_buffers(s, nullptr), s->stream);
+    s->launches += 1;
     DeviceState st;
     int rc = read_state(s, &st);
     if (rc != BFX_OK) return rc;
     s->step = st.step;
+    s->slots->reset(field_frame_meta(s, st, 0));
     return BFX_OK;
 }
 
@@ -1604,6 +1701,141 @@ int bfx_adjoint(bfx_sim* s, uint64_t steps, const bfx_adjoint_objective* objecti
         result->max_links = (uint64_t)ob.max_links;
         result->work_bytes = mem.bytes;
     }
+    return BFX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Field observation slots (BirdFlowSimulation.swift:1148-1210, 1806-1918)
+
+int bfx_set_observation_buffers(bfx_sim* s, uint32_t count, uint32_t wait_limit_ms) {
+    BFX_GUARD(s);
+    if (count < 1 || count > (uint32_t)bfx_sim::kMaxSlots)
+        return fail(s, BFX_ERR_INVALID_ARGUMENT, "observationBufferCount must be in 1...4");
+    if (!s->slots->idle()) return fail(s, BFX_ERR_INVALID_ARGUMENT, "a field frame is leased or being written");
+    int rc = sync_check(s, "observation buffers");
+    if (rc != BFX_OK) return rc;
+    for (uint32_t i = 1; i < count; ++i) {
+        if (s->slot_density[i]) continue;
+        cudaError_t e = dalloc(s, &s->slot_density[i], (size_t)s->g.n * sizeof(float));
+        if (e == cudaSuccess) e = dalloc(s, &s->slot_velocity[i], (size_t)s->g.n * sizeof(float4));
+        if (e != cudaSuccess) return cuda_fail(s, e, "observation slot allocation");
+    }
+    // The newest published frame carries over into slot 0 of the new set;
+    // without one, slot 0 is extracted from the current populations.
+    bfx_field_frame meta;
+    int newest = 0;
+    if (s->slots->acquire(false, 0, &meta, &newest) != 0) {
+        if (newest != 0) {
+            cudaMemcpyAsync(s->slot_density[0], s->slot_density[newest], (size_t)s->g.n * sizeof(float),
+                            cudaMemcpyDeviceToDevice, s->stream);
+            cudaMemcpyAsync(s->slot_velocity[0], s->slot_velocity[newest], (size_t)s->g.n * sizeof(float4),
+                            cudaMemcpyDeviceToDevice, s->stream);
+        }
+        meta.slot = 0;
+        meta.density = s->slot_density[0];
+        meta.velocity = (const float*)s->slot_velocity[0];
+        rc = sync_check(s, "observation buffers");
+        if (rc != BFX_OK) return rc;
+    } else {
+        s->capture_slot = 0;
+        launch_macroscopic(s->cfg.storage, s->rep_s, s->g, fluid_buffers(s, nullptr), s->stream);
+        s->launches += 1;
+        DeviceState st;
+        rc = read_state(s, &st);
+        if (rc != BFX_OK) return rc;
+        meta = field_frame_meta(s, st, 0);
+    }
+    auto slots = std::make_shared<FieldSlots<bfx_field_frame>>((int)count);
+    slots->reset(meta);
+    slots->add_counters(s->slots->dropped(), s->slots->waits());
+    s->slots = slots;
+    s->slot_wait_ms = wait_limit_ms;
+    return BFX_OK;
+}
+
+int bfx_acquire_field_frame(bfx_sim* s, int has_after_step, uint64_t after_step, bfx_field_frame* out) {
+    if (!s || !out) return BFX_ERR_INVALID_ARGUMENT;
+    std::memset(out, 0, sizeof(*out));
+    bfx_field_frame meta;
+    int slot = 0;
+    const uint64_t lease = s->slots->acquire(has_after_step != 0, after_step, &meta, &slot);
+    if (lease == 0) return BFX_OK;
+    *out = meta;
+    out->lease = lease;
+    return BFX_OK;
+}
+
+int bfx_field_frame_copy(bfx_sim* s, uint64_t lease, float* density, float* velocity_xyz, size_t cells) {
+    BFX_GUARD_READ(s);
+    if (cells < (size_t)s->g.n) return fail(s, BFX_ERR_CAPACITY, "field buffers smaller than the lattice");
+    const int slot = s->slots->leased_slot(lease);
+    if (slot < 0) return fail(s, BFX_ERR_INVALID_ARGUMENT, "the field frame lease is not live");
+    return copy_slot(s, slot, density, velocity_xyz);
+}
+
+int bfx_release_field_frame(bfx_sim* s, uint64_t lease) {
+    if (!s) return BFX_ERR_INVALID_ARGUMENT;
+    s->slots->release(lease);
+    return BFX_OK;
+}
+
+namespace {
+struct PendingRelease {
+    std::shared_ptr<FieldSlots<bfx_field_frame>> slots;
+    uint64_t lease;
+};
+void CUDART_CB release_when_done(void* p) {
+    auto* r = static_cast<PendingRelease*>(p);
+    r->slots->release(r->lease);
+    delete r;
+}
+}  // namespace
+
+int bfx_release_field_frame_after(bfx_sim* s, uint64_t lease, void* cuda_stream) {
+    if (!s) return BFX_ERR_INVALID_ARGUMENT;
+    if (s->slots->leased_slot(lease) < 0) return BFX_OK;  // released already
+    cudaSetDevice(s->device);
+    auto* r = new PendingRelease{s->slots, lease};
+    cudaStream_t st = cuda_stream ? (cudaStream_t)cuda_stream : s->stream;
+    cudaError_t e = cudaLaunchHostFunc(st, release_when_done, r);
+    if (e != cudaSuccess) {
+        delete r;
+        (void)cudaGetLastError();
+        return fail(s, BFX_ERR_INVALID_ARGUMENT, std::string("release after completion: ") + cudaGetErrorString(e));
+    }
+    return BFX_OK;
+}
+
+int bfx_capture_current_fields(bfx_sim* s, uint32_t mode, uint32_t* published) {
+    BFX_GUARD(s);
+    if (published) *published = 0;
+    if (mode > BFX_FIELD_CAPTURE_DISABLED) return fail(s, BFX_ERR_INVALID_ARGUMENT, "unknown field capture mode");
+    int rc = sync_check(s, "field capture");
+    if (rc != BFX_OK) return rc;
+    const int slot = s->slots->select((CaptureMode)mode, s->slot_wait_ms);
+    if (slot == kSlotWaitTimeout)
+        return fail(s, BFX_ERR_TIMEOUT, "no field observation slot was released within the wait limit");
+    if (slot < 0) return BFX_OK;
+    s->capture_slot = slot;
+    launch_macroscopic(s->cfg.storage, s->rep_s, s->g, fluid_buffers(s, nullptr), s->stream);
+    s->capture_slot = 0;
+    s->launches += 1;
+    DeviceState st;
+    rc = read_state(s, &st);
+    if (rc != BFX_OK) {
+        s->slots->abandon(slot);
+        return rc;
+    }
+    s->slots->publish(slot, field_frame_meta(s, st, slot));
+    s->fields_valid = true;
+    if (published) *published = 1;
+    return BFX_OK;
+}
+
+int bfx_observation_counters(bfx_sim* s, uint64_t* dropped_frames, uint64_t* capture_waits) {
+    if (!s) return BFX_ERR_INVALID_ARGUMENT;
+    if (dropped_frames) *dropped_frames = s->slots->dropped();
+    if (capture_waits) *capture_waits = s->slots->waits();
     return BFX_OK;
 }
 

@@ -46,11 +46,12 @@ def test_struct_layout_matches_c_header():
 #include <stddef.h>
 #include "bfx.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(bfx_config), sizeof(bfx_bird),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(bfx_config), sizeof(bfx_bird),
          sizeof(bfx_body_state), sizeof(bfx_mesh), sizeof(bfx_loads), sizeof(bfx_run_sample),
          sizeof(bfx_safety_record), sizeof(bfx_snapshot_data), sizeof(bfx_advance_result),
          offsetof(bfx_config, mesh_half_thickness), sizeof(bfx_adjoint_objective), sizeof(bfx_adjoint_result),
-         sizeof(bfx_ledger_sample), offsetof(bfx_ledger_sample, far_field_links));
+         sizeof(bfx_ledger_sample), offsetof(bfx_ledger_sample, far_field_links), sizeof(bfx_field_frame),
+         offsetof(bfx_field_frame, geometry), offsetof(bfx_field_frame, density));
   return 0;
 }
 '''
@@ -64,7 +65,8 @@ int main(void) {
     mine = [ct.sizeof(L.Config), ct.sizeof(L.Bird), ct.sizeof(L.BodyState), ct.sizeof(L.Mesh), ct.sizeof(L.Loads),
             ct.sizeof(L.RunSample), ct.sizeof(L.SafetyRecord), ct.sizeof(L.Snapshot), ct.sizeof(L.AdvanceResult),
             L.Config.mesh_half_thickness.offset, ct.sizeof(L.AdjointObjective), ct.sizeof(L.AdjointResult),
-            ct.sizeof(L.LedgerSample), L.LedgerSample.far_field_links.offset]
+            ct.sizeof(L.LedgerSample), L.LedgerSample.far_field_links.offset, ct.sizeof(L.FieldFrame),
+            L.FieldFrame.geometry.offset, L.FieldFrame.density.offset]
     assert sizes == mine
     # GPUBirdParameters is 13 float4 (GPUDataLayoutTests.swift:5-40)
     assert ct.sizeof(L.Bird) == 13 * 16

@@ -257,3 +257,152 @@ def test_coupled_momentum_ledger_requires_free_flight():
         sim.lattice.advance_ledger(2)
     assert e.value.status == 10
     sim.close()
+
+
+def test_observation_modes_do_not_change_numerical_state():
+    """ObservationAndCheckpointTests.swift:9-60: six free-flight steps with
+    capture disabled (one slot, then captureCurrentMacroscopicField) and with
+    best-effort capture (three slots) end in the same snapshot, and the
+    extracted fields equal the fields the fused kernel captured to 1e-6
+    (density, and velocity in lattice units)."""
+    from bfx.simulation import BirdFlowSimulation
+    config, bird, state = cases.compact_bird(free_flight=True)
+    disabled = BirdFlowSimulation(config, bird, state, observation_buffer_count=1)
+    observed = BirdFlowSimulation(config, bird, state, observation_buffer_count=3)
+    r0 = disabled.advance(6, batch_size=3, field_capture="disabled")
+    r1 = observed.advance(6, batch_size=3, field_capture="bestEffort")
+    assert not r0.field_frame_published and r1.field_frame_published
+    assert disabled.capture_current_macroscopic_field()
+    a, b = disabled.snapshot(), observed.snapshot()
+    assert a.step == b.step == 6 and a.time == b.time
+    assert bytes(a.body) == bytes(b.body) and bytes(a.loads) == bytes(b.loads)
+    ra, va = disabled.lattice.fields()
+    rb, vb = observed.lattice.fields()
+    assert np.max(np.abs(ra - rb)) < 1e-6
+    assert np.max(np.linalg.norm(va - vb, axis=1)) < 1e-6
+    # copyMacroscopicFields reports m/s
+    _, vphys = observed.copy_macroscopic_fields()
+    assert np.array_equal(vphys, (vb * np.float32(config.scaling.velocity_to_physical)).astype(np.float32))
+    disabled.close()
+    observed.close()
+
+
+def test_exhausted_viewer_slots_drop_without_waiting():
+    """ObservationAndCheckpointTests.swift:62-87."""
+    from bfx.simulation import BirdFlowSimulation
+    config, bird, state = cases.compact_bird()
+    sim = BirdFlowSimulation(config, bird, state, observation_buffer_count=3)
+    first = sim.acquire_latest_gpu_field_frame()
+    assert first is not None and first.step == 0
+    sim.advance(1, field_capture="bestEffort")
+    second = sim.acquire_latest_gpu_field_frame()
+    sim.advance(1, field_capture="bestEffort")
+    third = sim.acquire_latest_gpu_field_frame()
+    assert second is not None and third is not None
+    result = sim.advance(1, field_capture="bestEffort")
+    assert not result.field_frame_published
+    assert result.dropped_field_frame_count == 1
+    assert sim.field_capture_wait_count == 0
+    assert sim.step_index == 3
+    first.release()
+    second.release()
+    third.release()
+    assert sim.advance(1, field_capture="bestEffort").field_frame_published
+    sim.close()
+
+
+def test_field_frame_lease_holds_its_frame():
+    """A leased frame keeps its step's fields while later captures publish
+    into the other slots; afterStep filters; the metadata carries the
+    snapshot and the prepared geometry frame of that step; the device views
+    read the same bytes as the host copy."""
+    import torch
+    from bfx.simulation import BirdFlowSimulation
+    config, bird, state = cases.compact_bird()
+    sim = BirdFlowSimulation(config, bird, state, observation_buffer_count=2)
+    sim.advance(3, field_capture="required")
+    rho3, vel3 = sim.lattice.fields()
+    snap3 = sim.snapshot()
+    lease = sim.acquire_latest_gpu_field_frame()
+    assert lease is not None and lease.step == 3
+    assert lease.metadata["grid"] == (config.grid.x, config.grid.y, config.grid.z)
+    assert lease.metadata["time_seconds"] == snap3.time
+    assert bytes(lease.metadata["body"]) == bytes(snap3.body)
+    assert lease.metadata["geometry"]["body_position"][:3] == pytest.approx(list(snap3.body.position), abs=1e-5)
+    assert lease.metadata["pressure_scale_pascals"] > 0 and lease.metadata["reference_dynamic_pressure_pascals"] > 0
+    sim.advance(2, field_capture="required")
+    rho5, vel5 = sim.lattice.fields()
+    assert not np.array_equal(rho3, rho5)
+    r, v = lease.copy()
+    assert np.array_equal(r, rho3) and np.array_equal(v, vel3)
+    d, u = lease.device_views()
+    td = torch.as_tensor(d, device="cuda")
+    tu = torch.as_tensor(u, device="cuda")
+    assert np.array_equal(td.cpu().numpy().ravel(), rho3)
+    assert np.array_equal(tu.cpu().numpy().reshape(-1, 4)[:, :3], vel3)
+    assert sim.acquire_latest_gpu_field_frame(after_step=5) is None
+    newer = sim.acquire_latest_gpu_field_frame(after_step=4)
+    assert newer is not None and newer.step == 5
+    lease.release()
+    lease.release()  # a no-op
+    newer.release()
+    sim.close()
+
+
+def test_required_capture_waits_for_a_lease_release():
+    """A required capture with every slot leased waits until another thread
+    releases one (fieldCaptureWaitCount counts it); with a wait limit it
+    fails with a timeout instead, runs no step, and the handle stays usable."""
+    import threading
+    import time
+    from bfx.simulation import BirdFlowSimulation
+    config, bird, state = cases.compact_bird()
+    sim = BirdFlowSimulation(config, bird, state, observation_buffer_count=1, field_wait_limit_ms=20000)
+    lease = sim.acquire_latest_gpu_field_frame()
+    t = threading.Thread(target=lambda: (time.sleep(0.3), lease.release()))
+    t.start()
+    res = sim.advance(2, field_capture="required")
+    t.join()
+    assert res.field_frame_published and sim.field_capture_wait_count >= 1
+    sim.close()
+    lat = lattice(cases.shear_wave(n=16, axis="y")[0])
+    lat.set_observation_buffers(1, 200)
+    held = lat.acquire_field_frame()
+    with pytest.raises(BirdFlowError) as e:
+        lat.advance(1, capture_fields="required")
+    assert e.value.status == 11
+    assert lat.step_index()[0] == 0
+    held.release()
+    lat.advance(1, capture_fields="required")
+    assert lat.step_index()[0] == 1
+    lat.close()
+
+
+def test_release_after_stream_completion_and_restore_republishes():
+    """releaseAfterCompletion(of:) on a torch stream frees the slot once the
+    stream's work is done; a restore republishes slot 0 from the restored
+    populations at the restored step."""
+    import torch
+    cfg, _, _, _ = cases.shear_wave(n=16, viscosity=0.03, magic=3.0 / 16.0, axis="y")
+    lat = lattice(cfg)
+    lat.advance(3, capture_fields=True)
+    state = lat.save_state()
+    rho3, vel3 = lat.fields()
+    lease = lat.acquire_field_frame()
+    d, _ = lease.device_views()
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        total = torch.as_tensor(d, device="cuda").sum()
+    lease.release_after(stream)
+    stream.synchronize()
+    assert float(total) == pytest.approx(float(rho3.astype(np.float64).sum()), rel=1e-5)
+    res, _ = lat.advance(1, capture_fields="bestEffort")
+    assert res.field_frame_published
+    lat.advance(2)
+    lat.restore_state(state)
+    frame = lat.acquire_field_frame()
+    assert frame is not None and frame.step == 3
+    r, v = frame.copy()
+    assert np.max(np.abs(r - rho3)) < 1e-6 and np.max(np.abs(v - vel3)) < 1e-6
+    frame.release()
+    lat.close()
