@@ -644,7 +644,7 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
     std::memset(&s->tmap, 0, sizeof(s->tmap));
     s->tma_ok = (c.storage == BFX_STORAGE_F16_DEVIATION || c.storage == BFX_STORAGE_BF16_DEVIATION) &&
                 staged_collision(c.collision) &&
-                encode_population_map(&s->tmap, s->pops, c.storage, g.px, g.ny + 2, g.nz + 2);
+                encode_population_map(&s->tmap, s->pops, c.storage, c.collision, g.px, g.ny + 2, g.nz + 2);
     if (s->tma_ok) prepare_stream(c.storage, c.collision);
     BFX_ALLOC(s->density, (size_t)g.n * sizeof(float));
     BFX_ALLOC(s->velocity, (size_t)g.n * sizeof(float4));

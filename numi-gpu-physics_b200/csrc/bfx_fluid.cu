@@ -313,7 +313,8 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-bool encode_population_map(CUtensorMap* map, void* pops, int storage, int64_t px, int64_t py, int64_t pz) {
+bool encode_population_map(CUtensorMap* map, void* pops, int storage, int collision, int64_t px, int64_t py,
+                           int64_t pz) {
     static EncodeTiledFn fn = nullptr;
     if (!fn) {
         void* p = nullptr;
@@ -324,20 +325,22 @@ bool encode_population_map(CUtensorMap* map, void* pops, int storage, int64_t px
         fn = (EncodeTiledFn)p;
     }
     CUtensorMapDataType dt;
-    size_t e;
-    cuuint32_t row;
     switch (storage) {
-    case BFX_STORAGE_F16_DEVIATION: dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT16; e = 2; row = StreamGeom<__half>::row; break;
-    case BFX_STORAGE_BF16_DEVIATION:
-        dt = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
-        e = 2;
-        row = StreamGeom<__nv_bfloat16>::row;
-        break;
+    case BFX_STORAGE_F16_DEVIATION: dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT16; break;
+    case BFX_STORAGE_BF16_DEVIATION: dt = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16; break;
     default: return false;
     }
+    // the box is the tile shape of the operator's staged kernel (both formats are 2 bytes)
+    const size_t e = 2;
+    const bool trt = collision == BFX_COLLISION_TRT;
+    const cuuint32_t row = trt ? StreamGeom<__half, BFX_COLLISION_TRT>::row : StreamGeom<__half, BFX_COLLISION_RR3>::row;
+    const cuuint32_t rows = trt ? StreamShape<BFX_COLLISION_TRT>::Y : StreamShape<BFX_COLLISION_RR3>::Y;
+    static_assert(StreamGeom<__half, BFX_COLLISION_RR3>::row == StreamGeom<__half, BFX_COLLISION_REGULARIZED>::row &&
+                      StreamShape<BFX_COLLISION_RR3>::Y == StreamShape<BFX_COLLISION_REGULARIZED>::Y,
+                  "the regularized operators share one tile shape");
     const cuuint64_t dims[4] = {(cuuint64_t)px, (cuuint64_t)py, (cuuint64_t)pz, 19};
     const cuuint64_t strides[3] = {(cuuint64_t)(px * e), (cuuint64_t)(px * py * e), (cuuint64_t)(px * py * pz * e)};
-    const cuuint32_t box[4] = {row, (cuuint32_t)kTileY, 1, 1};
+    const cuuint32_t box[4] = {row, rows, 1, 1};
     const cuuint32_t elem_strides[4] = {1, 1, 1, 1};
     return fn(map, dt, 4, pops, dims, strides, box, elem_strides, CU_TENSOR_MAP_INTERLEAVE_NONE,
               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==

@@ -178,9 +178,10 @@ int box_block_count(const BoxDesc& box);
 int slab_block_count(const BoxDesc& box);
 void launch_fill_wall(float4* wall, int64_t n, float w, cudaStream_t s);
 // Tensor map (px, py, pz, 19) of a 16-bit population array for the staged
-// fused kernel; false when the driver entry point is missing or the format is
-// not 16-bit.
-bool encode_population_map(CUtensorMap* map, void* pops, int storage, int64_t px, int64_t py, int64_t pz);
+// fused kernel, with the box of the collision operator's tile shape; false when
+// the driver entry point is missing or the format is not 16-bit.
+bool encode_population_map(CUtensorMap* map, void* pops, int storage, int collision, int64_t px, int64_t py,
+                           int64_t pz);
 // Collision operators whose 16-bit fluid step runs the staged kernel.
 bool staged_collision(int collision);
 // Kernel launches of one launch_bulk call.

@@ -2,14 +2,14 @@
 // TRT step (bfx_stream_kernels.cuh): tile geometry, the launch interface and the
 // mbarrier / bulk-tensor PTX wrappers.
 //
-// Pipeline.  A persistent CTA owns a strided set of tiles (64 cells along x,
-// 4 rows along y, one z plane).  One producer thread issues, per tile, one 4-D
-// TMA box load per direction q (the 19 source rows of the AA pull, plus a
-// 2-cell x margin) into a ring of shared-memory stages; four consumer warps
-// each take one row, two cells per lane, read the 19 populations from shared
-// memory, release the stage, collide in packed f32x2 arithmetic and store
-// straight to HBM.  Loads of later tiles are in flight while a tile computes,
-// so the kernel is bounded by HBM bandwidth or by issue, not by load latency.
+// Pipeline.  A persistent CTA (one per SM) owns a strided set of tiles: W
+// consumer warps side by side along x (64 cells each), Y rows along y, one z
+// plane (StreamShape).  One producer thread issues, per tile, one 4-D TMA box
+// load per direction q (the 19 source rows of the AA pull, plus the x margin)
+// into a ring of shared-memory stages; each consumer warp takes 64 cells of
+// one row, two cells per lane, reads the 19 populations from shared memory,
+// releases the stage, collides in packed f32x2 arithmetic and stores straight
+// to HBM.  Loads of later tiles are in flight while a tile computes.
 #pragma once
 
 #include <cuda.h>
@@ -18,22 +18,42 @@
 
 namespace bfx {
 
-constexpr int kTileX = 64;                  // cells along x per tile (one warp row, two cells per lane)
-constexpr int kTileY = 4;                   // rows per tile = consumer warps per CTA
-constexpr int kStreamThreads = 32 * (kTileY + 1);
+constexpr int kTileX = 64;  // cells along x per consumer warp (two per lane)
 
-template <class T>
+// Tile shape and ring depth per collision operator.  Measured on B200 on the
+// 512x256x256 flapping plates in FP16 (kernel time per step):
+//   TRT          64x4, 3 stages, 4 CTAs/SM 0.705 ms; 64x16, 2 stages 0.536 ms;
+//                128x8, 2 stages 0.522 ms (chosen)
+//   RR3          64x4, 3 stages 0.733 ms; 64x12, 2 stages 0.680 ms;
+//                64x12, 3 stages 0.662 ms (chosen)
+// Taller and wider boxes make fewer, longer TMA requests with less x-margin
+// overhead per byte; for the memory-bound TRT step a shallow ring (about
+// 85 KB of loads in flight per SM) is faster than a deep one, while the
+// arithmetic-heavier regularized operators want twelve consumer warps and
+// one more stage to cover their longer tiles.
+template <int COLL>
+struct StreamShape {
+    static constexpr bool trt = COLL == BFX_COLLISION_TRT;
+    static constexpr int W = trt ? 2 : 1;         // consumer warps per row
+    static constexpr int Y = trt ? 8 : 12;        // rows per tile
+    static constexpr int stages = trt ? 2 : 3;    // shared-memory ring depth
+    static constexpr int consumers = W * Y;
+    static constexpr int threads = 32 * (consumers + 1);  // + one producer warp
+};
+
+template <class T, int COLL>
 struct StreamGeom {
-    // box row: 64 cells plus the -1 / +1 x neighbours, rounded to 16 bytes
-    static constexpr int row = (((kTileX + 2) * (int)sizeof(T) + 15) / 16) * 16 / (int)sizeof(T);
-    static constexpr int plane_bytes = ((kTileY * row * (int)sizeof(T) + 127) / 128) * 128;
+    using SH = StreamShape<COLL>;
+    // box row: the tile's cells plus the -1 / +1 x neighbours, rounded to 16 bytes
+    static constexpr int row = (((kTileX * SH::W + 2) * (int)sizeof(T) + 15) / 16) * 16 / (int)sizeof(T);
+    static constexpr int plane_bytes = ((SH::Y * row * (int)sizeof(T) + 127) / 128) * 128;
     static constexpr int stage_bytes = 19 * plane_bytes;
-    static constexpr int tx_bytes = 19 * kTileY * row * (int)sizeof(T);
-    // ring depth: 3 stages of 12 KB (16-bit), four CTAs per SM, about 100 KB
-    // of loads in flight per SM
-    static constexpr int stages = 3;
+    static constexpr int tx_bytes = 19 * SH::Y * row * (int)sizeof(T);
+    static constexpr int stages = SH::stages;
     // stages, their full / empty mbarriers, and slack to align the base to 128 B
     static constexpr int smem_bytes = stages * stage_bytes + 2 * stages * 8 + 128;
+    static_assert(row <= 256 && SH::Y <= 256, "a TMA box spans at most 256 elements per dimension");
+    static_assert(smem_bytes <= 227 * 1024, "shared memory of one CTA");
 };
 
 struct StreamTiles {

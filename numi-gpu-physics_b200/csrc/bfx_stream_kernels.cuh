@@ -192,13 +192,13 @@ __device__ __forceinline__ void admit_dev_lane(P2 (&post)[19], int l, float rho,
 // ---------------------------------------------------------------------------
 // The staged kernel.  CAPTURE 1 also writes the macroscopic fields.
 // ---------------------------------------------------------------------------
-// Four CTAs per SM (16 consumer warps) for TRT; the heavier operators keep
-// their registers at three.
+// One CTA per SM with the operator's tile shape (StreamShape).
 template <class S, int REP_S, int COLL, int CAPTURE>
-__global__ void __launch_bounds__(kStreamThreads, 4)
+__global__ void __launch_bounds__(StreamShape<COLL>::threads, 1)
     k_stream(const __grid_constant__ CUtensorMap map, const BulkArgs a, const StreamTiles tl) {
     using T = typename S::T;
-    using G = StreamGeom<T>;
+    using G = StreamGeom<T, COLL>;
+    using SH = StreamShape<COLL>;
     constexpr int NS = G::stages;
     extern __shared__ __align__(128) uint8_t smem_raw[];
     // bulk-tensor destinations must start on 128 B: align the ring explicitly
@@ -211,13 +211,13 @@ __global__ void __launch_bounds__(kStreamThreads, 4)
     if (threadIdx.x == 0) {
         for (int s = 0; s < NS; ++s) {
             mbar_init(full0 + 8 * s, 1);
-            mbar_init(empty0 + 8 * s, kTileY);
+            mbar_init(empty0 + 8 * s, SH::consumers);
         }
         mbar_fence_init();
     }
     __syncthreads();
     const Grid& g = a.g;
-    if (warp == kTileY) {
+    if (warp == SH::consumers) {
         // producer: one thread issues the 19 box loads of each tile
         if (lane != 0) return;
         int issued = 0;
@@ -233,9 +233,9 @@ __global__ void __launch_bounds__(kStreamThreads, 4)
             }
             const int txi = tile % tl.tiles_x;
             const int rest = tile / tl.tiles_x;
-            const int y0 = (rest % tl.tiles_y) * kTileY;
+            const int y0 = (rest % tl.tiles_y) * SH::Y;
             const int z = rest / tl.tiles_y;
-            const int x0 = txi * kTileX;
+            const int x0 = txi * kTileX * SH::W;
             const uint32_t bar = full0 + 8 * s;
             mbar_expect_tx(bar, G::tx_bytes);
             const uint32_t dst = sbase + s * G::stage_bytes;
@@ -254,7 +254,8 @@ __global__ void __launch_bounds__(kStreamThreads, 4)
         }
         return;
     }
-    // consumers: warp w takes row y0 + w, lane l the cells x0 + l and x0 + l + 32.
+    // consumers: warp w takes row y0 + w % Y and the 64 cells from
+    // x0 + 64 (w / Y); lane l the cells at +l and +l + 32 of those.
     // The mask bytes of the next tile are loaded one tile ahead, so their HBM
     // latency overlaps the current tile's collision.
     const FluidParams& fp = a.fp;
@@ -267,9 +268,9 @@ __global__ void __launch_bounds__(kStreamThreads, 4)
     auto locate = [&](int tile, Cells& c) {
         const int txi = tile % tl.tiles_x;
         const int rest = tile / tl.tiles_x;
-        c.y = (rest % tl.tiles_y) * kTileY + warp;
+        c.y = (rest % tl.tiles_y) * SH::Y + warp % SH::Y;
         c.z = rest / tl.tiles_y;
-        c.xa = txi * kTileX + lane;
+        c.xa = txi * kTileX * SH::W + kTileX * (warp / SH::Y) + lane;
         const bool row_ok = c.y < g.ny;
         c.gida = (uint32_t)c.xa + (uint32_t)g.nx * ((uint32_t)c.y + (uint32_t)g.ny * (uint32_t)c.z);
         c.va = row_ok && c.xa < g.nx;
@@ -297,7 +298,7 @@ __global__ void __launch_bounds__(kStreamThreads, 4)
             atomicOr(&a.state->stream_error, 2u);
             break;
         }
-        const T* row = (const T*)(smem + s * G::stage_bytes) + warp * G::row;
+        const T* row = (const T*)(smem + s * G::stage_bytes) + (warp % SH::Y) * G::row + kTileX * (warp / SH::Y);
         constexpr float dscale = S::kDevScale, inv_dscale = 1.0f / S::kDevScale;
         P2 dv[19];
 #pragma unroll
@@ -385,13 +386,13 @@ __global__ void __launch_bounds__(kStreamThreads, 4)
 // dynamic shared-memory limit (done at simulation creation, outside any capture).
 template <class S, int REP, int COLL, int CAPTURE>
 static int stream_blocks_per_sm() {
-    using G = StreamGeom<typename S::T>;
+    using G = StreamGeom<typename S::T, COLL>;
     static int per_sm = 0;
     if (per_sm == 0) {
         cudaFuncSetAttribute(k_stream<S, REP, COLL, CAPTURE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              G::smem_bytes);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stream<S, REP, COLL, CAPTURE>, kStreamThreads,
-                                                      G::smem_bytes);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stream<S, REP, COLL, CAPTURE>,
+                                                      StreamShape<COLL>::threads, G::smem_bytes);
         if (per_sm < 1) per_sm = 1;
     }
     return per_sm;
@@ -400,14 +401,15 @@ static int stream_blocks_per_sm() {
 template <class S, int REP, int COLL, int C>
 static void stream_launch(const GridDesc& gd, const BulkArgs& a, const CUtensorMap& map, int sm_count,
                           cudaStream_t s) {
-    using G = StreamGeom<typename S::T>;
+    using G = StreamGeom<typename S::T, COLL>;
+    using SH = StreamShape<COLL>;
     StreamTiles tl;
-    tl.tiles_x = (gd.nx + kTileX - 1) / kTileX;
-    tl.tiles_y = (gd.ny + kTileY - 1) / kTileY;
+    tl.tiles_x = (gd.nx + kTileX * SH::W - 1) / (kTileX * SH::W);
+    tl.tiles_y = (gd.ny + SH::Y - 1) / SH::Y;
     tl.ntiles = tl.tiles_x * tl.tiles_y * gd.nz;
     int blocks = stream_blocks_per_sm<S, REP, COLL, C>() * sm_count;
     if (blocks > tl.ntiles) blocks = tl.ntiles;
-    k_stream<S, REP, COLL, C><<<blocks, kStreamThreads, G::smem_bytes, s>>>(map, a, tl);
+    k_stream<S, REP, COLL, C><<<blocks, SH::threads, G::smem_bytes, s>>>(map, a, tl);
 }
 
 template <class S, int REP, int COLL>
