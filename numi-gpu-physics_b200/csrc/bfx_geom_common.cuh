@@ -61,13 +61,16 @@ __device__ __forceinline__ V3 qrotate(float4 q, V3 v) {
     return v3(v.x + q.w * t.x + c2.x, v.y + q.w * t.y + c2.y, v.z + q.w * t.z + c2.z);
 }
 __device__ __forceinline__ V3 qunrotate(float4 q, V3 v) { return qrotate(make_float4(-q.x, -q.y, -q.z, q.w), v); }
-// rotateAroundAxis: BF.metal:466-473
-__device__ __forceinline__ V3 rotate_axis(V3 v, V3 axis, float angle) {
-    float s = bfx_sinf(angle), c = bfx_cosf(angle);
+// rotateAroundAxis (BF.metal:466-473) with the angle's sine and cosine given
+__device__ __forceinline__ V3 rotate_axis_sc(V3 v, V3 axis, float s, float c) {
     V3 cr = cross(axis, v);
     float d = dot(axis, v);
     return v3(v.x * c + cr.x * s + axis.x * d * (1.0f - c), v.y * c + cr.y * s + axis.y * d * (1.0f - c),
               v.z * c + cr.z * s + axis.z * d * (1.0f - c));
+}
+// rotateAroundAxis: BF.metal:466-473
+__device__ __forceinline__ V3 rotate_axis(V3 v, V3 axis, float angle) {
+    return rotate_axis_sc(v, axis, bfx_sinf(angle), bfx_cosf(angle));
 }
 __device__ __forceinline__ V3 normalize3(V3 v) {
     float l = length(v);

@@ -21,23 +21,27 @@ struct WingFrame {
     float tip_twist, tip_rate;
 };
 
-// makeWingFrame: BF.metal:611-684
-__device__ void make_wing_frame(float side, float stroke, float stroke_rate, float deviation, float deviation_rate,
-                                float pitch, float pitch_rate, const bfx_bird& bird, V3 pos, float4 orient,
+// Sine and cosine of one rotation angle.
+struct SinCos {
+    float s, c;
+};
+
+// makeWingFrame: BF.metal:611-684, with the sines and cosines of the signed
+// stroke, the deviation and the signed pitch given.
+__device__ void make_wing_frame(float side, SinCos stroke, float stroke_rate, SinCos deviation, float deviation_rate,
+                                SinCos pitch, float pitch_rate, const bfx_bird& bird, V3 pos, float4 orient,
                                 WingFrame& fr) {
     float4 o = qnormalize(orient);
     V3 bx = qrotate(o, v3(1, 0, 0)), by = qrotate(o, v3(0, 1, 0)), bz = qrotate(o, v3(0, 0, 1));
     V3 root_local = v3(bird.wing_geometry1.v[1], side * bird.wing_geometry1.v[2], bird.wing_geometry1.v[3]);
     V3 rr = qrotate(o, root_local);
     V3 root = pos + rr;
-    float signed_stroke = side * stroke;
-    V3 span_after = rotate_axis(v3(side * by.x, side * by.y, side * by.z), bx, signed_stroke);
-    V3 normal_after = rotate_axis(v3(side * bz.x, side * bz.y, side * bz.z), bx, signed_stroke);
-    V3 span = rotate_axis(span_after, normal_after, deviation);
-    V3 chord_before = rotate_axis(bx, normal_after, deviation);
-    float signed_pitch = side * pitch;
-    V3 chord = rotate_axis(chord_before, span, signed_pitch);
-    V3 normal = rotate_axis(normal_after, span, signed_pitch);
+    V3 span_after = rotate_axis_sc(v3(side * by.x, side * by.y, side * by.z), bx, stroke.s, stroke.c);
+    V3 normal_after = rotate_axis_sc(v3(side * bz.x, side * bz.y, side * bz.z), bx, stroke.s, stroke.c);
+    V3 span = rotate_axis_sc(span_after, normal_after, deviation.s, deviation.c);
+    V3 chord_before = rotate_axis_sc(bx, normal_after, deviation.s, deviation.c);
+    V3 chord = rotate_axis_sc(chord_before, span, pitch.s, pitch.c);
+    V3 normal = rotate_axis_sc(normal_after, span, pitch.s, pitch.c);
     fr.root = root;
     fr.chord = normalize3(chord);
     fr.span = normalize3(span);
@@ -69,35 +73,92 @@ __device__ void wing_momentum(V3 root, V3 chord, V3 span, V3 normal, V3 rel, con
 }
 
 __global__ void k_prepare(const GeomArgs a, int init, float dt, float box_radius) {
+    // One warp stages what the single-thread update reads (bird parameters,
+    // joints, step, body state, previous wing momentum) into shared memory
+    // with parallel loads.  The update then reads no global memory: its
+    // stores into the device state may alias global loads, which would
+    // otherwise wait one load latency after another.
+    __shared__ bfx_bird sbird;
+    __shared__ bfx_joint sjoint[2];
+    __shared__ double sbody[13];
+    __shared__ float sprev[16];
+    __shared__ uint64_t sstep;
     DeviceState* st = a.b.state;
-    const bfx_bird& bird = *a.b.bird;
-    uint64_t absolute = init ? 0 : st->step + 1;
+    {
+        const int t = threadIdx.x;
+        const uint32_t* bsrc = (const uint32_t*)a.b.bird;
+        for (int i = t; i < (int)(sizeof(bfx_bird) / 4); i += blockDim.x) ((uint32_t*)&sbird)[i] = bsrc[i];
+        const int nj = a.b.joint_count < 2 ? a.b.joint_count : 2;
+        const uint32_t* jsrc = (const uint32_t*)a.b.joints;
+        for (int i = t; i < nj * (int)(sizeof(bfx_joint) / 4); i += blockDim.x) ((uint32_t*)sjoint)[i] = jsrc[i];
+        if (t < 13) sbody[t] = st->body[t];
+        if (t < 16) sprev[t] = st->wing_prev[t];
+        if (t == 0) sstep = st->step;
+        __syncthreads();
+    }
+    const bfx_bird& bird = sbird;
+    uint64_t absolute = init ? 0 : sstep + 1;
     float time = (float)((double)absolute * (double)dt);
-    V3 pos = v3((float)st->body[0], (float)st->body[1], (float)st->body[2]);
-    float4 orient = make_float4((float)st->body[3], (float)st->body[4], (float)st->body[5], (float)st->body[6]);
-    V3 vel = v3((float)st->body[7], (float)st->body[8], (float)st->body[9]);
-    V3 omb = v3((float)st->body[10], (float)st->body[11], (float)st->body[12]);
     float af = 2.0f * 3.14159265358979323846f * bird.wing_kinematics0.v[0];
     float phase = af * time;
-    float stroke = bird.wing_kinematics0.v[2] + bird.wing_kinematics0.v[1] * bfx_sinf(phase);
-    float stroke_rate = af * bird.wing_kinematics0.v[1] * bfx_cosf(phase);
-    float pitch = bird.wing_kinematics0.v[3] + bird.wing_kinematics1.v[0] * bfx_sinf(phase + bird.wing_kinematics1.v[1]);
-    float pitch_rate = af * bird.wing_kinematics1.v[0] * bfx_cosf(phase + bird.wing_kinematics1.v[1]);
+    // The step's sines and cosines (portable FP64 series, bit-identical to the
+    // host) are independent of one another: the lanes evaluate them in two
+    // rounds, the phase angles and then the rotation angles built from them.
+    //   round 1: phase, phase + pitch phase, 2 phase, phase + joint phase (2)
+    //   round 2: +/- stroke, deviation, +/- pitch, +/- each joint angle
+    const int njoints = a.b.joint_count < 2 ? a.b.joint_count : 2;
+    __shared__ SinCos sc1[5], sc2[9];
+    {
+        const int t = threadIdx.x;
+        if (t < 10) {
+            const int k = t >> 1;
+            const float ang = k == 0 ? phase
+                              : k == 1 ? phase + bird.wing_kinematics1.v[1]
+                              : k == 2 ? 2.0f * phase
+                              : phase + (k - 3 < njoints ? sjoint[k - 3].phase : 0.0f);
+            if (t & 1) sc1[k].c = bfx_cosf(ang);
+            else sc1[k].s = bfx_sinf(ang);
+        }
+        __syncthreads();
+        if (t < 18) {
+            const int k = t >> 1;
+            const float stroke = bird.wing_kinematics0.v[2] + bird.wing_kinematics0.v[1] * sc1[0].s;
+            const float pitch = bird.wing_kinematics0.v[3] + bird.wing_kinematics1.v[0] * sc1[1].s;
+            float ang;
+            if (k < 2) ang = (k == 0 ? 1.0f : -1.0f) * stroke;
+            else if (k == 2) ang = bird.wing_kinematics1.v[2] * sc1[2].s;
+            else if (k < 5) ang = (k == 3 ? 1.0f : -1.0f) * pitch;
+            else {
+                const int j = (k - 5) >> 1;
+                const float sgn = ((k - 5) & 1) ? -1.0f : 1.0f;
+                ang = j < njoints ? sgn * (sjoint[j].bias + sjoint[j].amplitude * sc1[3 + j].s) : 0.0f;
+            }
+            if (t & 1) sc2[k].c = bfx_cosf(ang);
+            else sc2[k].s = bfx_sinf(ang);
+        }
+        __syncthreads();
+        if (t != 0) return;
+    }
+    V3 pos = v3((float)sbody[0], (float)sbody[1], (float)sbody[2]);
+    float4 orient = make_float4((float)sbody[3], (float)sbody[4], (float)sbody[5], (float)sbody[6]);
+    V3 vel = v3((float)sbody[7], (float)sbody[8], (float)sbody[9]);
+    V3 omb = v3((float)sbody[10], (float)sbody[11], (float)sbody[12]);
+    float stroke_rate = af * bird.wing_kinematics0.v[1] * sc1[0].c;
+    float pitch_rate = af * bird.wing_kinematics1.v[0] * sc1[1].c;
     // stroke-plane deviation at twice the flapping frequency (figure-of-eight
     // tip path); the reference feeds deviation only from measured keyframes
-    float deviation = bird.wing_kinematics1.v[2] * bfx_sinf(2.0f * phase);
-    float deviation_rate = 2.0f * af * bird.wing_kinematics1.v[2] * bfx_cosf(2.0f * phase);
+    float deviation_rate = 2.0f * af * bird.wing_kinematics1.v[2] * sc1[2].c;
     WingFrame l, r;
-    make_wing_frame(1.0f, stroke, stroke_rate, deviation, deviation_rate, pitch, pitch_rate, bird, pos, orient, l);
-    make_wing_frame(-1.0f, stroke, stroke_rate, deviation, deviation_rate, pitch, pitch_rate, bird, pos, orient, r);
+    make_wing_frame(1.0f, sc2[0], stroke_rate, sc2[2], deviation_rate, sc2[3], pitch_rate, bird, pos, orient, l);
+    make_wing_frame(-1.0f, sc2[1], stroke_rate, sc2[2], deviation_rate, sc2[4], pitch_rate, bird, pos, orient, r);
     // articulated segments: each joint rotates its parent's frame about the
     // hinge axis and moves it to the joint (angles mirrored on the right wing)
-    for (int side = 0; side < 2 && a.b.joint_count > 0; ++side) {
+    for (int side = 0; side < 2 && njoints > 0; ++side) {
         const WingFrame& wf = side == 0 ? l : r;
         const float sgn = side == 0 ? 1.0f : -1.0f;
         V3 po = wf.root, pc = wf.chord, ps = wf.span, pn = wf.normal, pw = wf.rel, pu = v3(0.0f, 0.0f, 0.0f);
-        for (int j = 0; j < a.b.joint_count; ++j) {
-            const bfx_joint& jt = a.b.joints[j];
+        for (int j = 0; j < njoints; ++j) {
+            const bfx_joint& jt = sjoint[j];
             const V3 o = v3(po.x + pc.x * jt.origin[0] + ps.x * jt.origin[1] + pn.x * jt.origin[2],
                             po.y + pc.y * jt.origin[0] + ps.y * jt.origin[1] + pn.y * jt.origin[2],
                             po.z + pc.z * jt.origin[0] + ps.z * jt.origin[1] + pn.z * jt.origin[2]);
@@ -108,9 +169,10 @@ __global__ void k_prepare(const GeomArgs a, int init, float dt, float box_radius
             const V3 ax = v3(pc.x * jt.axis[0] + ps.x * jt.axis[1] + pn.x * a2,
                              pc.y * jt.axis[0] + ps.y * jt.axis[1] + pn.y * a2,
                              pc.z * jt.axis[0] + ps.z * jt.axis[1] + pn.z * a2);
-            const float ang = sgn * (jt.bias + jt.amplitude * bfx_sinf(phase + jt.phase));
-            const float rate = sgn * (af * jt.amplitude * bfx_cosf(phase + jt.phase));
-            const V3 cc = rotate_axis(pc, ax, ang), cs = rotate_axis(ps, ax, ang), cn = rotate_axis(pn, ax, ang);
+            const SinCos rot = sc2[5 + 2 * j + side];
+            const float rate = sgn * (af * jt.amplitude * sc1[3 + j].c);
+            const V3 cc = rotate_axis_sc(pc, ax, rot.s, rot.c), cs = rotate_axis_sc(ps, ax, rot.s, rot.c),
+                     cn = rotate_axis_sc(pn, ax, rot.s, rot.c);
             const V3 om = v3(pw.x + ax.x * rate, pw.y + ax.y * rate, pw.z + ax.z * rate);
             const V3 uu = pu + cross(pw, o - po);
             SegmentFrame& f = st->seg[2 * j + side];
@@ -171,9 +233,9 @@ __global__ void k_prepare(const GeomArgs a, int init, float dt, float box_radius
             if (init) {
                 st->wing_reaction[4 * j] = st->wing_reaction[4 * j + 1] = st->wing_reaction[4 * j + 2] = 0.0f;
             } else {
-                st->wing_reaction[4 * j] = -(cur[j].x - st->wing_prev[4 * j]) * inv;
-                st->wing_reaction[4 * j + 1] = -(cur[j].y - st->wing_prev[4 * j + 1]) * inv;
-                st->wing_reaction[4 * j + 2] = -(cur[j].z - st->wing_prev[4 * j + 2]) * inv;
+                st->wing_reaction[4 * j] = -(cur[j].x - sprev[4 * j]) * inv;
+                st->wing_reaction[4 * j + 1] = -(cur[j].y - sprev[4 * j + 1]) * inv;
+                st->wing_reaction[4 * j + 2] = -(cur[j].z - sprev[4 * j + 2]) * inv;
             }
             st->wing_reaction[4 * j + 3] = 0.0f;
             st->wing_prev[4 * j] = cur[j].x;
@@ -1204,7 +1266,7 @@ int box_block_count(const BoxDesc& box) {
 void launch_prepare(int geometry, float dt, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
                     const GeomBuffers& gb, int init, cudaStream_t s) {
     GeomArgs a = make_geom(g, fp, box, gb, nullptr);
-    k_prepare<<<1, 1, 0, s>>>(a, init, dt, 0.0f);
+    k_prepare<<<1, 32, 0, s>>>(a, init, dt, 0.0f);
     (void)geometry;
 }
 
