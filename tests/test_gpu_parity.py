@@ -269,6 +269,23 @@ def test_flapping_plate_mesh_matches_oracle(link_rule):
         ld = lat.loads()
         assert ld.covered_count == osim.loads.covered_count and ld.uncovered_count == osim.loads.uncovered_count
     assert osim.loads.covered_count + osim.loads.uncovered_count > 0
+    if link_rule == L.LINK_RAY_ROOT:
+        # sampled ray-root fractions of the last step equal the oracle's search bit for bit
+        tris = mesh["tris"].astype(np.uint32).ravel()
+        c, _, _ = O.lattice()
+        nx, ny = cfg.nx, cfg.ny
+        sampled = range(0, len(cell), max(1, len(cell) // 300))
+        for i in sampled:
+            g = int(cell[i])
+            x, y, z = g % nx, (g // nx) % ny, g // (nx * ny)
+            qq = int(d[i])
+            sx, sy, sz = x - c[qq][0], y - c[qq][1], z - c[qq][2]
+            oq = O.lib().or_mesh_ray_root(ct.byref(osim.p), O.fptr(osim.mesh_pos),
+                                          tris.ctypes.data_as(ct.POINTER(ct.c_uint32)), mesh["tris"].shape[0],
+                                          cfg.mesh_half_thickness, osim.keys.ctypes.data_as(ct.POINTER(ct.c_uint64)),
+                                          x, y, z, sx, sy, sz)
+            assert q[i] == np.float32(oq), (i, float(q[i]), oq)
+        assert len(sampled) > 50
 
 
 @pytest.mark.parametrize("link_rule", [L.LINK_LINEAR, L.LINK_RAY_ROOT])
