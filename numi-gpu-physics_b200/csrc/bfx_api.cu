@@ -132,6 +132,13 @@ struct bfx_sim {
     // single steps (an odd step count, one-step calls), same keying
     cudaGraphExec_t step_graph[2] = {nullptr, nullptr};
     uint64_t step_launches[2] = {0, 0};
+    // pipelined pairs: each step's geometry was built during the previous
+    // step's fluid kernel, and each step builds the next one's the same way
+    cudaGraphExec_t pipe_graph[2] = {nullptr, nullptr};
+    uint64_t pipe_launches[2] = {0, 0};
+    // side stream of the next step's geometry build, with its fork / join events
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     bool graphs_enabled = true;
     // pinned host staging of the device state: read-backs and body uploads
     // without a pageable-copy bounce
@@ -246,13 +253,23 @@ struct TapeSlot {
     float* link_tangent;    // per-link tangent scratch shared by all slots
 };
 
-// Classification + link build for the geometry at the current state.
-void encode_geometry_build(bfx_sim* s, int init, uint8_t* mprev, uint8_t* mnext) {
+// Classification for the geometry at the current state (pose and frames,
+// occupancy, wall field, mesh keys), on the simulation's stream or another.
+void encode_geometry_build(bfx_sim* s, int init, uint8_t* mprev, uint8_t* mnext, cudaStream_t st = nullptr) {
     GeomBuffers gb = geom_buffers(s, mprev, mnext);
-    launch_prepare(s->cfg.geometry, s->cfg.time_step, s->g, s->fp, s->box, gb, init, s->stream);
-    launch_classify(s->cfg.geometry, init ? 0 : 1, s->g, s->fp, s->box, gb, s->stream);
+    if (!st) st = s->stream;
+    launch_prepare(s->cfg.geometry, s->cfg.time_step, s->g, s->fp, s->box, gb, init, st);
+    launch_classify(s->cfg.geometry, init ? 0 : 1, s->g, s->fp, s->box, gb, st);
     s->launches += 1 + (s->cfg.geometry == BFX_GEOMETRY_MESH ? 4 : 1);
 }
+
+// The next step's geometry build can overlap this step's fluid kernel: with
+// the staged 16-bit kernel the fluid cells read only the populations and this
+// step's mask, while the build writes the other mask buffer, the wall field,
+// the keys and the pose fields of the device state; the body update it reads
+// is done by the link kernel before the fluid kernel, and the box's solid
+// cells (which read the wall field) are launched before the fork.
+bool can_pipeline(const bfx_sim* s) { return s->moving() && s->tma_ok && s->side != nullptr; }
 
 void encode_links(bfx_sim* s, uint8_t* mprev, uint8_t* mnext) {
     GeomBuffers gb = geom_buffers(s, mprev, mnext);
@@ -291,12 +308,16 @@ void timing_collect(bfx_sim* s) {
 // One time step (BirdFlowSimulation.encodeBatch body, BirdFlowSimulation.swift:1374-1437).
 // With a tape slot the step also records what its adjoint needs: the wing-frame
 // and link tangents, the link values, masks, keys, state and pre-collision moments.
+// geometry_ready: this step's geometry was built by the previous step's
+// prefetch.  prefetch_next: build the next step's geometry on the side stream
+// while this step's fluid kernel runs (can_pipeline; no capture, tape or ledger).
 void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint64_t sample_index,
-                 const TapeSlot* tape = nullptr, double* ledger_in = nullptr) {
+                 const TapeSlot* tape = nullptr, double* ledger_in = nullptr, bool geometry_ready = false,
+                 bool prefetch_next = false) {
     s->hstate_fresh = false;
     uint8_t* mprev = s->mask[s->cur];
     uint8_t* mnext = s->moving() ? s->mask[s->cur ^ 1] : s->mask[s->cur];
-    if (s->moving()) {
+    if (s->moving() && !geometry_ready) {
         encode_geometry_build(s, 0, mprev, mnext);
     }
     if (tape) {
@@ -348,10 +369,22 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
         capture = 2;
     }
     const int box[3] = {s->box.sx, s->box.sy, s->box.sz};
-    timing_begin(s);
-    launch_bulk(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, capture, s->geometry() ? box : nullptr,
-                s->stream);
-    timing_end(s);
+    if (prefetch_next && capture == 0 && !tape && !ledger_in && can_pipeline(s)) {
+        // solid / uncovered cells first (they read the wall field), then fork
+        // the next step's geometry (masks swap roles) beside the fluid kernel
+        launch_bulk_rare(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, box, s->stream);
+        cudaEventRecord(s->fork_ev, s->stream);
+        cudaStreamWaitEvent(s->side, s->fork_ev, 0);
+        encode_geometry_build(s, 0, mnext, mprev, s->side);
+        cudaEventRecord(s->join_ev, s->side);
+        launch_bulk_stream(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, box, s->stream);
+        cudaStreamWaitEvent(s->stream, s->join_ev, 0);
+    } else {
+        timing_begin(s);
+        launch_bulk(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, capture,
+                    s->geometry() ? box : nullptr, s->stream);
+        timing_end(s);
+    }
     s->launches += launch_bulk_count(s->cfg.storage, s->cfg.collision, capture, s->tma_ok, s->geometry());
     GeomBuffers gb = geom_buffers(s, mprev, mnext);
     if (!finish_fused) {
@@ -367,25 +400,25 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
     if (s->moving()) s->cur ^= 1;
 }
 
-// Replays (capturing on first use) the two-step graph for the current parity.
-// Host-side state (representation, mask index) returns to its starting value
-// after two steps, so the captured launches stay valid for every later pair.
 // Replays (capturing on first use) the graph of `nsteps` (1 or 2) plain steps
 // for the current parity.  Host-side state (representation, mask index)
 // alternates with period two, so a pair graph leaves it where it started and
-// the single-step graph of each parity hands over to the other's.
-int run_steps_graph(bfx_sim* s, int nsteps) {
+// the single-step graph of each parity hands over to the other's.  A pipelined
+// pair takes its first step's geometry as built and builds the geometry of the
+// step after the pair (so one more step of the same batch must follow).
+int run_steps_graph(bfx_sim* s, int nsteps, bool pipelined = false) {
     s->hstate_fresh = false;
     const int key = s->rep_s;
-    cudaGraphExec_t* slot = nsteps == 2 ? &s->pair_graph[key] : &s->step_graph[key];
-    uint64_t* count = nsteps == 2 ? &s->pair_launches[key] : &s->step_launches[key];
+    cudaGraphExec_t* slot = pipelined ? &s->pipe_graph[key] : nsteps == 2 ? &s->pair_graph[key] : &s->step_graph[key];
+    uint64_t* count =
+        pipelined ? &s->pipe_launches[key] : nsteps == 2 ? &s->pair_launches[key] : &s->step_launches[key];
     if (!*slot) {
         const int rep0 = s->rep_s, cur0 = s->cur;
         cudaGraph_t graph = nullptr;
         uint64_t before = s->launches;
         cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return cuda_fail(s, e, "graph capture begin");
-        for (int i = 0; i < nsteps; ++i) encode_step(s, 0, nullptr, 0);
+        for (int i = 0; i < nsteps; ++i) encode_step(s, 0, nullptr, 0, nullptr, nullptr, pipelined, pipelined);
         e = cudaStreamEndCapture(s->stream, &graph);
         if (e != cudaSuccess) return cuda_fail(s, e, "graph capture end");
         e = cudaGraphInstantiate(slot, graph, 0);
@@ -551,6 +584,11 @@ void bfx_destroy(bfx_sim* s) {
         if (g) cudaGraphExecDestroy(g);
     for (auto g : s->step_graph)
         if (g) cudaGraphExecDestroy(g);
+    for (auto g : s->pipe_graph)
+        if (g) cudaGraphExecDestroy(g);
+    if (s->fork_ev) cudaEventDestroy(s->fork_ev);
+    if (s->join_ev) cudaEventDestroy(s->join_ev);
+    if (s->side) cudaStreamDestroy(s->side);
     if (s->hstate) cudaFreeHost(s->hstate);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -577,6 +615,15 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
     if (e != cudaSuccess) {
         bfx_destroy(s);
         return cuda_fail(nullptr, e, "stream creation");
+    }
+    // side stream for the pipelined geometry build (optional: without it the
+    // steps run in order on the main stream)
+    if (cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->join_ev, cudaEventDisableTiming) != cudaSuccess) {
+        (void)cudaGetLastError();
+        if (s->side) cudaStreamDestroy(s->side);
+        s->side = nullptr;
     }
     if (bird) {
         s->bird = *bird;
@@ -848,7 +895,25 @@ int bfx_advance(bfx_sim* s, uint64_t steps, uint32_t batch_size, uint32_t flags,
         uint64_t k = 0;
         // Pairs of plain steps replay a captured graph; steps that capture
         // fields, record samples or are individually timed are encoded directly.
-        if (s->graphs_enabled && !record && !s->timing) {
+        const bool last_batch = done + count == steps;
+        if (s->graphs_enabled && !record && !s->timing && can_pipeline(s) && count > 1) {
+            // Pipelined: every step but the batch's last builds the next
+            // step's geometry beside its own fluid kernel.  The batch's first
+            // step builds its own; pairs replay a graph while a step of the
+            // batch remains after them; the last one or two run directly.
+            encode_step(s, 0, nullptr, 0, nullptr, nullptr, false, true);
+            k = 1;
+            for (; k + 2 < count; k += 2) {
+                int rc = run_steps_graph(s, 2, true);
+                if (rc != BFX_OK) return rc;
+            }
+            for (; k < count; ++k) {
+                const bool last = k + 1 == count;
+                if (capture && last && last_batch) s->capture_slot = slot;
+                encode_step(s, capture && last && last_batch ? 1 : 0, nullptr, 0, nullptr, nullptr, true, !last);
+                s->capture_slot = 0;
+            }
+        } else if (s->graphs_enabled && !record && !s->timing) {
             uint64_t plain = capture && done + count == steps ? count - 1 : count;
             for (; k + 1 < plain; k += 2) {
                 int rc = run_pair_graph(s);

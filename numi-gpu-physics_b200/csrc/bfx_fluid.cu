@@ -396,6 +396,24 @@ void launch_bulk(int storage, int collision, int rep_s, const GridDesc& g, const
     }
 }
 
+// The staged path of launch_bulk in its two launches, so that other work can
+// be queued between them: the geometry box's solid and newly uncovered cells
+// (k_rare), then the fluid cells (k_stream).  Every population slot is read
+// and written by one cell only in a step, and the two launches cover disjoint
+// cells, so their order does not change the result.
+void launch_bulk_rare(int storage, int collision, int rep_s, const GridDesc& g, const FluidParams& fp,
+                      const FluidBuffers& b, const int* box, cudaStream_t s) {
+    BulkArgs a = make_bulk_args(g, fp, b, 0, storage);
+    for (int k = 0; k < 3; ++k) a.box[k] = box[k];
+    launch_rare_fast(storage, collision, rep_s, a, s);
+}
+void launch_bulk_stream(int storage, int collision, int rep_s, const GridDesc& g, const FluidParams& fp,
+                        const FluidBuffers& b, const int* box, cudaStream_t s) {
+    BulkArgs a = make_bulk_args(g, fp, b, 0, storage);
+    for (int k = 0; k < 3; ++k) a.box[k] = box[k];
+    launch_stream_fast(storage, collision, rep_s, g, &a, (const CUtensorMap*)b.tmap, b.sm_count, s);
+}
+
 template <class S>
 static void halo_s(const BulkArgs& a, int rep_s, cudaStream_t s) {
     const int64_t halo = a.g.pn - a.g.n;

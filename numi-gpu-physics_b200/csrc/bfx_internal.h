@@ -37,6 +37,13 @@ struct FluidBuffers {
 // to a second launch over the box.
 void launch_bulk(int storage, int collision, int rep_s, const GridDesc& g, const FluidParams& fp,
                  const FluidBuffers& b, int capture, const int* box, cudaStream_t s);
+// The staged path's two launches (k_rare over the geometry box, then k_stream)
+// for callers that queue work between them; only for a simulation whose
+// population tensor map was encoded (16-bit storage, staged operator).
+void launch_bulk_rare(int storage, int collision, int rep_s, const GridDesc& g, const FluidParams& fp,
+                      const FluidBuffers& b, const int* box, cudaStream_t s);
+void launch_bulk_stream(int storage, int collision, int rep_s, const GridDesc& g, const FluidParams& fp,
+                        const FluidBuffers& b, const int* box, cudaStream_t s);
 // Halo fill: the values boundary cells pull from outside the lattice (before the step).
 void launch_halo(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const FluidBuffers& b,
                  cudaStream_t s);

@@ -36,9 +36,13 @@ def small_mesh_case(**kw):
     return cases.flapping_plates(**args)
 
 
-def test_batch_partition_invariance_is_bit_exact():
-    """16 steps as 16x1, 4x4 and 1x16 give identical populations and loads."""
-    cfg, rows, body, mesh = small_mesh_case()
+@pytest.mark.parametrize("storage", [L.STORAGE_F32, L.STORAGE_F16_DEVIATION])
+def test_batch_partition_invariance_is_bit_exact(storage):
+    """16 steps as 16x1, 4x4 and 1x16 give identical populations and loads.
+    With 16-bit storage, batches of more than one step build each next step's
+    geometry on a side stream beside the fluid kernel (and replay pipelined
+    graphs); one-step batches run every stage in order."""
+    cfg, rows, body, mesh = small_mesh_case(storage=storage)
     results = []
     for batches in ((1,) * 16, (4,) * 4, (16,)):
         lat = lattice(cfg, rows, body, mesh)
@@ -50,6 +54,27 @@ def test_batch_partition_invariance_is_bit_exact():
     for pops, force in results[1:]:
         assert np.array_equal(pops, results[0][0])
         assert np.array_equal(force, results[0][1])
+
+
+def test_pipelined_free_flight_bird_is_bit_exact():
+    """The compact free-flying bird in FP16 deviation storage with RR3 (the
+    staged kernel): 12 steps in one batch (geometry of each next step built
+    beside the fluid kernel) equal 12 one-step batches bit for bit, body and
+    loads included."""
+    from bfx.simulation import BirdFlowSimulation
+    config, bird, state = cases.compact_bird(free_flight=True)
+    out = []
+    for batch in (12, 1):
+        sim = BirdFlowSimulation(config, bird, state, storage=L.STORAGE_F16_DEVIATION, collision=L.COLLISION_RR3)
+        sim.advance(12, batch_size=batch, field_capture="disabled")
+        lat = sim.lattice
+        out.append((lat.populations(), bytes(lat.body()), np.array(lat.loads().force), lat.mask()))
+        sim.close()
+    assert np.all(np.isfinite(out[0][0]))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[0][1] == out[1][1]
+    assert np.array_equal(out[0][2], out[1][2])
+    assert np.array_equal(out[0][3], out[1][3])
 
 
 def test_two_runs_are_bit_identical():
