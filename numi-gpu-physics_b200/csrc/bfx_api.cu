@@ -340,15 +340,8 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
         s->launches += 1;
     }
     // halo fill before the link writes: a link whose solid source is a periodic
-    // image writes into a halo slot and must win over the periodic copy.  With
-    // the staged kernel the far-field x faces are left to it (scattered
-    // 2-byte writes here, a substitution on two tiles per row there).
-    int halo_skip_x = 0;
-    if (s->tma_ok && !tape) {
-        if (s->cfg.face_bc[0] == BFX_BC_FARFIELD) halo_skip_x |= 1;
-        if (s->cfg.face_bc[1] == BFX_BC_FARFIELD) halo_skip_x |= 2;
-    }
-    launch_halo(s->cfg.storage, s->rep_s, s->g, s->fp, fb, s->stream, halo_skip_x);
+    // image writes into a halo slot and must win over the periodic copy
+    launch_halo(s->cfg.storage, s->rep_s, s->g, s->fp, fb, s->stream);
     s->launches += 1;
     // The end-of-step body update needs only the reduced loads: it runs in the
     // link kernel's last block, except while taping (the tape records the
@@ -384,12 +377,12 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
         cudaStreamWaitEvent(s->side, s->fork_ev, 0);
         encode_geometry_build(s, 0, mnext, mprev, s->side);
         cudaEventRecord(s->join_ev, s->side);
-        launch_bulk_stream(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, box, s->stream, halo_skip_x);
+        launch_bulk_stream(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, box, s->stream);
         cudaStreamWaitEvent(s->stream, s->join_ev, 0);
     } else {
         timing_begin(s);
         launch_bulk(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, capture,
-                    s->geometry() ? box : nullptr, s->stream, halo_skip_x);
+                    s->geometry() ? box : nullptr, s->stream);
         timing_end(s);
     }
     s->launches += launch_bulk_count(s->cfg.storage, s->cfg.collision, capture, s->tma_ok, s->geometry());

@@ -30,9 +30,6 @@ struct BulkArgs {
     Grid g;
     FluidParams fp;
     int capture;            // 0 none, 1 macroscopic fields, 2 adjoint tape
-    // far-field x faces the halo fill left out (bit 0: -x, bit 1: +x); the
-    // staged kernel substitutes their value itself
-    int halo_skip_x;
 };
 
 // Fused-step launch for the contracted variant (bfx_fluid_fast.cu).

@@ -39,12 +39,6 @@ __global__ void __launch_bounds__(128) k_halo(const BulkArgs a, int rep_s, int64
     const Grid& g = a.g;
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= halo_cells) return;
-    if (a.halo_skip_x) {
-        // the x-face columns (the last segment of the shell) of a skipped face
-        const int64_t xseg = 2 * (int64_t)g.px * g.py + 2 * (int64_t)g.px * (g.pz - 2);
-        if (t >= xseg && ((t < xseg + (int64_t)(g.py - 2) * (g.pz - 2)) ? (a.halo_skip_x & 1) : (a.halo_skip_x & 2)))
-            return;
-    }
     int hx, hy, hz;
     if (!padded_shell_cell(g, t, hx, hy, hz)) return;
     hx -= 1;
@@ -287,7 +281,6 @@ BulkArgs make_bulk_args(const GridDesc& gd, const FluidParams& fp, const FluidBu
         const double scale = storage == BFX_STORAGE_F16_DEVIATION ? (double)StoreF16Dev::kDevScale : 1.0;
         a.far_dev[q] = (float)((a.far_eq_d[q] - wq<double>(q)) * scale);
     }
-    a.halo_skip_x = 0;
     a.pops = b.pops;
     a.mask = b.mask;
     a.wall = b.wall;
@@ -374,7 +367,7 @@ int launch_bulk_count(int storage, int collision, int capture, bool tma_ok, bool
 }
 
 void launch_bulk(int storage, int collision, int rep_s, const GridDesc& g, const FluidParams& fp,
-                 const FluidBuffers& b, int capture, const int* box, cudaStream_t s, int halo_skip_x) {
+                 const FluidBuffers& b, int capture, const int* box, cudaStream_t s) {
     BulkArgs a = make_bulk_args(g, fp, b, capture, storage);
     if (box) {
         a.box[0] = box[0];
@@ -390,7 +383,6 @@ void launch_bulk(int storage, int collision, int rep_s, const GridDesc& g, const
     // their path cost the staged kernel registers).  FP32 and FP64 keep k_bulk
     // (bit-identical scalar arithmetic), which takes those cells inline.
     if (use_staged(storage, collision, capture, b.tmap != nullptr)) {
-        a.halo_skip_x = halo_skip_x;
         launch_stream_fast(storage, collision, rep_s, g, &a, (const CUtensorMap*)b.tmap, b.sm_count, s);
         if (box && a.mask) launch_rare_fast(storage, collision, rep_s, a, s);
         return;
@@ -416,25 +408,20 @@ void launch_bulk_rare(int storage, int collision, int rep_s, const GridDesc& g, 
     launch_rare_fast(storage, collision, rep_s, a, s);
 }
 void launch_bulk_stream(int storage, int collision, int rep_s, const GridDesc& g, const FluidParams& fp,
-                        const FluidBuffers& b, const int* box, cudaStream_t s, int halo_skip_x) {
+                        const FluidBuffers& b, const int* box, cudaStream_t s) {
     BulkArgs a = make_bulk_args(g, fp, b, 0, storage);
     for (int k = 0; k < 3; ++k) a.box[k] = box[k];
-    a.halo_skip_x = halo_skip_x;
     launch_stream_fast(storage, collision, rep_s, g, &a, (const CUtensorMap*)b.tmap, b.sm_count, s);
 }
 
 template <class S>
 static void halo_s(const BulkArgs& a, int rep_s, cudaStream_t s) {
-    // every shell cell (and the pad columns, which return at once); without
-    // both x faces only the z and y segments
-    const int64_t halo = a.halo_skip_x == 3 ? 2 * (int64_t)a.g.px * a.g.py + 2 * (int64_t)a.g.px * (a.g.pz - 2)
-                                            : a.g.pn - a.g.n;
+    const int64_t halo = a.g.pn - a.g.n;
     k_halo<S><<<(unsigned)((halo + 127) / 128), 128, 0, s>>>(a, rep_s, halo);
 }
 void launch_halo(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const FluidBuffers& b,
-                 cudaStream_t s, int skip_x) {
+                 cudaStream_t s) {
     BulkArgs a = make_bulk_args(g, fp, b, 0, storage);
-    a.halo_skip_x = skip_x;
     BFX_DISPATCH_STORAGE(storage, halo_s, a, rep_s, s);
 }
 

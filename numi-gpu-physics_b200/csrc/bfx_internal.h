@@ -34,24 +34,19 @@ struct FluidBuffers {
 // the moving-wall equilibrium and newly uncovered cells refill and collide.
 // box: extent of the geometry box (origin in DeviceState), null without
 // geometry; the staged 16-bit kernel leaves the box's solid / uncovered cells
-// to a second launch over the box.  halo_skip_x: the far-field x faces the halo
-// fill left out (launch_halo); only the staged kernel takes them over, so it
-// must be 0 whenever another path runs.
+// to a second launch over the box.
 void launch_bulk(int storage, int collision, int rep_s, const GridDesc& g, const FluidParams& fp,
-                 const FluidBuffers& b, int capture, const int* box, cudaStream_t s, int halo_skip_x = 0);
+                 const FluidBuffers& b, int capture, const int* box, cudaStream_t s);
 // The staged path's two launches (k_rare over the geometry box, then k_stream)
 // for callers that queue work between them; only for a simulation whose
 // population tensor map was encoded (16-bit storage, staged operator).
 void launch_bulk_rare(int storage, int collision, int rep_s, const GridDesc& g, const FluidParams& fp,
                       const FluidBuffers& b, const int* box, cudaStream_t s);
 void launch_bulk_stream(int storage, int collision, int rep_s, const GridDesc& g, const FluidParams& fp,
-                        const FluidBuffers& b, const int* box, cudaStream_t s, int halo_skip_x = 0);
-// Halo fill: the values boundary cells pull from outside the lattice (before
-// the step).  skip_x (bit 0: -x, bit 1: +x) leaves out the columns of far-field
-// x faces, whose scattered 2-byte writes the staged kernel replaces by
-// substituting the same value for the pulls that cross them.
+                        const FluidBuffers& b, const int* box, cudaStream_t s);
+// Halo fill: the values boundary cells pull from outside the lattice (before the step).
 void launch_halo(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const FluidBuffers& b,
-                 cudaStream_t s, int skip_x = 0);
+                 cudaStream_t s);
 // Equilibrium initialisation into representation E.
 void launch_init(int storage, int init_kind, float amplitude, const GridDesc& g, const FluidParams& fp,
                  const FluidBuffers& b, cudaStream_t s);

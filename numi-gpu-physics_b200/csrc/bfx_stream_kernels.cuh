@@ -309,29 +309,6 @@ __global__ void __launch_bounds__(StreamShape<COLL>::threads, 1)
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(empty0 + 8 * s);
-        // Pulls across a far-field x face that the halo fill left out take the
-        // value it would have stored there (the far-field equilibrium through
-        // the storage rule), for sources on the face itself; the edge and
-        // corner halo cells are still filled.
-        if (a.halo_skip_x) {
-            const bool lo_a = (a.halo_skip_x & 1) && xa == 0;
-            const bool hi_a = (a.halo_skip_x & 2) && xa == g.nx - 1;
-            const bool hi_b = (a.halo_skip_x & 2) && xb == g.nx - 1;
-            if (__any_sync(0xffffffffu, lo_a || hi_a || hi_b)) {
-#pragma unroll
-                for (int q = 1; q < 19; ++q) {
-                    if (cx(q) == 0) continue;
-                    const int sy = y - cy(q), sz = z - cz(q);
-                    if (sy < 0 || sy >= g.ny || sz < 0 || sz >= g.nz) continue;
-                    T h;
-                    S::st_rt(&h, q, a.far_eq_f[q]);
-                    const float v = S::ld_dev(&h);
-                    if (cx(q) > 0 && lo_a) dv[q].x = v;
-                    if (cx(q) < 0 && hi_a) dv[q].x = v;
-                    if (cx(q) < 0 && hi_b) dv[q].y = v;
-                }
-            }
-        }
         // solid and newly uncovered cells (mask byte set) are left to k_rare
         va = va && ma == 0;
         vb = vb && mb == 0;
