@@ -345,6 +345,14 @@ BFX_API int bfx_release_field_frame_after(bfx_sim* sim, uint64_t lease, void* cu
 /* captureCurrentMacroscopicField(mode:) (BirdFlowSimulation.swift:1176-1210):
  * publishes rho/u of the current populations without a step. */
 BFX_API int bfx_capture_current_fields(bfx_sim* sim, uint32_t mode, uint32_t* published);
+/* deriveFlowDiagnostics (Sources/BirdFlowVisualization/Metal/Visualization.metal:270-308)
+ * of a leased frame: vorticity (curl xyz and |curl|, 1/s) as 4 floats per
+ * cell, the Q criterion -tr(grad u . grad u) / 2 (1/s^2) and a validity byte;
+ * boundary cells and cells whose 7-point stencil touches the body of the
+ * captured step are invalid (zeros).  Outputs of `cells` >= n entries, in host
+ * memory, or device memory of this simulation's GPU when device_outputs != 0. */
+BFX_API int bfx_flow_diagnostics(bfx_sim* sim, uint64_t lease, float* vorticity4, float* q_criterion, uint8_t* valid,
+                                 size_t cells, int device_outputs);
 /* droppedFieldFrameCount, fieldCaptureWaitCount (BirdFlowSimulation.swift:466-478) */
 BFX_API int bfx_observation_counters(bfx_sim* sim, uint64_t* dropped_frames, uint64_t* capture_waits);
 /* runtimeSafetyReport() (BirdFlowSimulation.swift:1766) */

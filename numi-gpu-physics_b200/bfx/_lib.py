@@ -164,7 +164,7 @@ EXPORTED = (
     "bfx_launch_count", "bfx_device_bytes", "bfx_fluid_mass_momentum_noalloc", "bfx_adjoint", "bfx_advance_ledger",
     "bfx_last_error", "bfx_set_observation_buffers", "bfx_acquire_field_frame", "bfx_field_frame_copy",
     "bfx_release_field_frame", "bfx_release_field_frame_after", "bfx_capture_current_fields",
-    "bfx_observation_counters",
+    "bfx_observation_counters", "bfx_flow_diagnostics",
 )
 
 _lib = None
@@ -225,6 +225,7 @@ def load(path: str | None = None):
     L.bfx_release_field_frame_after.argtypes = [vp, ct.c_uint64, vp]
     L.bfx_capture_current_fields.argtypes = [vp, ct.c_uint32, P(ct.c_uint32)]
     L.bfx_observation_counters.argtypes = [vp, P(ct.c_uint64), P(ct.c_uint64)]
+    L.bfx_flow_diagnostics.argtypes = [vp, ct.c_uint64, vp, vp, vp, ct.c_size_t, ct.c_int]
     if path is None:
         _lib = L
     return L

@@ -91,6 +91,17 @@ class FieldFrameLease:
                self._lattice.handle)
         return rho, vel.reshape(-1, 3)
 
+    def flow_diagnostics(self):
+        """deriveFlowDiagnostics (Visualization.metal:270-308) of this frame:
+        (vorticity[n, 4] = curl xyz and |curl| in 1/s, q[n] in 1/s^2, valid[n])."""
+        n = self._lattice.n
+        vort = np.empty((n, 4), np.float32)
+        q = np.empty(n, np.float32)
+        valid = np.empty(n, np.uint8)
+        _check(self._lattice.lib.bfx_flow_diagnostics(self._lattice.handle, self.lease, vort.ctypes.data,
+                                                      q.ctypes.data, valid.ctypes.data, n, 0), self._lattice.handle)
+        return vort, q, valid
+
     def device_views(self):
         """bindMacroscopicFields: (density[nz, ny, nx], velocity[nz, ny, nx, 4])
         as __cuda_array_interface__ objects over the slot.  Read only by

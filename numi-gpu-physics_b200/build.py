@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libbfx.so")
 SOURCES = ["bfx_fluid.cu", "bfx_fluid_fast.cu", "bfx_geometry.cu", "bfx_adjoint.cu", "bfx_ledger.cu", "bfx_api.cu",
-           "bfx_noalloc.cu"]
+           "bfx_noalloc.cu", "bfx_fields.cu"]
 # translation units built with FMA contraction (see csrc/bfx_bulk.cuh)
 CONTRACTED = {"bfx_fluid_fast.cu"}
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

@@ -74,6 +74,8 @@ struct bfx_sim {
     static constexpr int kMaxSlots = 4;
     float* slot_density[kMaxSlots] = {};
     float4* slot_velocity[kMaxSlots] = {};
+    uint8_t* slot_mask[kMaxSlots] = {};   // occupancy of the captured step (with geometry)
+    float* diag_scratch = nullptr;        // flow-diagnostics staging for host outputs (lazily)
     int capture_slot = 0;
     uint32_t slot_wait_ms = 0;
     std::shared_ptr<FieldSlots<bfx_field_frame>> slots;
@@ -568,6 +570,7 @@ int bfx_device_count(int* count) {
 static int read_state(bfx_sim* s, DeviceState* st);
 static bfx_field_frame field_frame_meta(const bfx_sim* s, const DeviceState& st, int slot);
 static int copy_slot(bfx_sim* s, int slot, float* density, float* velocity_xyz);
+static int snapshot_slot_mask(bfx_sim* s, int slot);
 
 void bfx_destroy(bfx_sim* s) {
     if (!s) return;
@@ -697,6 +700,7 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
     BFX_ALLOC(s->velocity, (size_t)g.n * sizeof(float4));
     s->slot_density[0] = s->density;
     s->slot_velocity[0] = s->velocity;
+    if (c.geometry != BFX_GEOMETRY_NONE) BFX_ALLOC(s->slot_mask[0], (size_t)g.n);
     s->slots = std::make_shared<FieldSlots<bfx_field_frame>>(1);
     BFX_ALLOC(s->dstate, sizeof(DeviceState));
     if (cudaMallocHost((void**)&s->hstate, sizeof(DeviceState)) != cudaSuccess) {
@@ -808,6 +812,11 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
     // the initial fields are published in slot 0 (BirdFlowSimulation.swift:626-640)
     DeviceState st0;
     if (read_state(s, &st0) != BFX_OK) {
+        g_create_error = s->err;
+        bfx_destroy(s);
+        return BFX_ERR_KERNEL;
+    }
+    if (snapshot_slot_mask(s, 0) != BFX_OK) {
         g_create_error = s->err;
         bfx_destroy(s);
         return BFX_ERR_KERNEL;
@@ -957,6 +966,8 @@ int bfx_advance(bfx_sim* s, uint64_t steps, uint32_t batch_size, uint32_t flags,
         DeviceState st;
         int rc = read_state(s, &st);
         if (rc != BFX_OK) return rc;
+        rc = snapshot_slot_mask(s, slot);
+        if (rc != BFX_OK) return rc;
         s->slots->publish(slot, field_frame_meta(s, st, slot));
         slot_guard.index = -1;
         s->fields_valid = true;
@@ -1057,6 +1068,18 @@ int bfx_copy_fields(bfx_sim* s, float* density, float* velocity_xyz, size_t cell
     if (rc != BFX_OK) return rc;
     // currentPublishedFieldSlot (BirdFlowSimulation.swift:1906-1918)
     return copy_slot(s, s->slots->current(), density, velocity_xyz);
+}
+
+// The occupancy of the step a slot's fields belong to, copied beside them so
+// that its derived diagnostics exclude the body of that step; returns once the
+// copy (and everything queued before it) is done.
+static int snapshot_slot_mask(bfx_sim* s, int slot) {
+    if (s->slot_mask[slot]) {
+        cudaMemcpyAsync(s->slot_mask[slot], s->mask[s->cur], (size_t)s->g.n, cudaMemcpyDeviceToDevice, s->stream);
+        cudaError_t e = cudaStreamSynchronize(s->stream);
+        if (e != cudaSuccess) return cuda_fail(s, e, "occupancy snapshot");
+    }
+    return BFX_OK;
 }
 
 static int copy_slot(bfx_sim* s, int slot, float* density, float* velocity_xyz) {
@@ -1292,6 +1315,8 @@ int bfx_restore_state(bfx_sim* s, const void* buf, size_t size) {
     int rc = read_state(s, &st);
     if (rc != BFX_OK) return rc;
     s->step = st.step;
+    rc = snapshot_slot_mask(s, 0);
+    if (rc != BFX_OK) return rc;
     s->slots->reset(field_frame_meta(s, st, 0));
     return BFX_OK;
 }
@@ -1783,6 +1808,7 @@ int bfx_set_observation_buffers(bfx_sim* s, uint32_t count, uint32_t wait_limit_
         if (s->slot_density[i]) continue;
         cudaError_t e = dalloc(s, &s->slot_density[i], (size_t)s->g.n * sizeof(float));
         if (e == cudaSuccess) e = dalloc(s, &s->slot_velocity[i], (size_t)s->g.n * sizeof(float4));
+        if (e == cudaSuccess && s->geometry()) e = dalloc(s, &s->slot_mask[i], (size_t)s->g.n);
         if (e != cudaSuccess) return cuda_fail(s, e, "observation slot allocation");
     }
     // The newest published frame carries over into slot 0 of the new set;
@@ -1795,6 +1821,9 @@ int bfx_set_observation_buffers(bfx_sim* s, uint32_t count, uint32_t wait_limit_
                             cudaMemcpyDeviceToDevice, s->stream);
             cudaMemcpyAsync(s->slot_velocity[0], s->slot_velocity[newest], (size_t)s->g.n * sizeof(float4),
                             cudaMemcpyDeviceToDevice, s->stream);
+            if (s->slot_mask[0])
+                cudaMemcpyAsync(s->slot_mask[0], s->slot_mask[newest], (size_t)s->g.n, cudaMemcpyDeviceToDevice,
+                                s->stream);
         }
         meta.slot = 0;
         meta.density = s->slot_density[0];
@@ -1807,6 +1836,8 @@ int bfx_set_observation_buffers(bfx_sim* s, uint32_t count, uint32_t wait_limit_
         s->launches += 1;
         DeviceState st;
         rc = read_state(s, &st);
+        if (rc != BFX_OK) return rc;
+        rc = snapshot_slot_mask(s, 0);
         if (rc != BFX_OK) return rc;
         meta = field_frame_meta(s, st, 0);
     }
@@ -1891,10 +1922,49 @@ int bfx_capture_current_fields(bfx_sim* s, uint32_t mode, uint32_t* published) {
         s->slots->abandon(slot);
         return rc;
     }
+    rc = snapshot_slot_mask(s, slot);
+    if (rc != BFX_OK) {
+        s->slots->abandon(slot);
+        return rc;
+    }
     s->slots->publish(slot, field_frame_meta(s, st, slot));
     s->fields_valid = true;
     if (published) *published = 1;
     return BFX_OK;
+}
+
+int bfx_flow_diagnostics(bfx_sim* s, uint64_t lease, float* vorticity4, float* q_criterion, uint8_t* valid,
+                         size_t cells, int device_outputs) {
+    BFX_GUARD_READ(s);
+    if (!vorticity4 || !q_criterion || !valid) return BFX_ERR_INVALID_ARGUMENT;
+    if (cells < (size_t)s->g.n) return fail(s, BFX_ERR_CAPACITY, "diagnostic buffers smaller than the lattice");
+    const int slot = s->slots->leased_slot(lease);
+    if (slot < 0) return fail(s, BFX_ERR_INVALID_ARGUMENT, "the field frame lease is not live");
+    const size_t n = (size_t)s->g.n;
+    float4* dv = (float4*)vorticity4;
+    float* dq = q_criterion;
+    uint8_t* dm = valid;
+    if (!device_outputs) {
+        if (!s->diag_scratch) {
+            cudaError_t e = dalloc(s, &s->diag_scratch, n * (sizeof(float4) + sizeof(float) + 1));
+            if (e != cudaSuccess) return cuda_fail(s, e, "diagnostics staging allocation");
+        }
+        dv = (float4*)s->diag_scratch;
+        dq = (float*)(dv + n);
+        dm = (uint8_t*)(dq + n);
+    }
+    // GPUFieldFrameMetadata.velocityToPhysical over the cell size
+    const float v2p = s->cfg.cell_size / s->cfg.time_step;
+    const float scale = 0.5f * v2p / s->cfg.cell_size;
+    launch_flow_diagnostics(s->slot_velocity[slot], s->slot_mask[slot], (int)s->cfg.nx, (int)s->cfg.ny,
+                            (int)s->cfg.nz, scale, dv, dq, dm, s->stream);
+    s->launches += 1;
+    if (!device_outputs) {
+        cudaMemcpyAsync(vorticity4, dv, n * sizeof(float4), cudaMemcpyDeviceToHost, s->stream);
+        cudaMemcpyAsync(q_criterion, dq, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream);
+        cudaMemcpyAsync(valid, dm, n, cudaMemcpyDeviceToHost, s->stream);
+    }
+    return sync_check(s, "flow diagnostics");
 }
 
 int bfx_observation_counters(bfx_sim* s, uint64_t* dropped_frames, uint64_t* capture_waits) {

@@ -44,6 +44,11 @@ void launch_bulk_rare(int storage, int collision, int rep_s, const GridDesc& g, 
                       const FluidBuffers& b, const int* box, cudaStream_t s);
 void launch_bulk_stream(int storage, int collision, int rep_s, const GridDesc& g, const FluidParams& fp,
                         const FluidBuffers& b, const int* box, cudaStream_t s);
+// Vorticity (curl, |curl|), Q criterion and validity of a captured field
+// (bfx_fields.cu); velocity in lattice units, scale = 0.5 * velocity_to_physical
+// / cell_size; mask: occupancy of the captured step, or null.
+void launch_flow_diagnostics(const float4* velocity, const uint8_t* mask, int nx, int ny, int nz, float scale,
+                             float4* vorticity, float* q_criterion, uint8_t* valid, cudaStream_t s);
 // Halo fill: the values boundary cells pull from outside the lattice (before the step).
 void launch_halo(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const FluidBuffers& b,
                  cudaStream_t s);

@@ -431,3 +431,73 @@ def test_release_after_stream_completion_and_restore_republishes():
     assert np.max(np.abs(r - rho3)) < 1e-6 and np.max(np.abs(v - vel3)) < 1e-6
     frame.release()
     lat.close()
+
+
+def _flow_diagnostics_numpy(vel, mask, nx, ny, nz, cell_size, time_step):
+    """deriveFlowDiagnostics (Visualization.metal:270-308) restated in NumPy
+    float32 with the kernel's operation order."""
+    f32 = np.float32
+    u = vel.reshape(nz, ny, nx, 3).astype(f32)
+    m = mask.reshape(nz, ny, nx) & 0x3F
+    v2p = f32(cell_size) / f32(time_step)
+    scale = f32(0.5) * v2p / f32(cell_size)
+    ok = np.zeros((nz, ny, nx), bool)
+    ok[1:-1, 1:-1, 1:-1] = True
+    near = m.copy()
+    near[:, :, 1:] |= m[:, :, :-1]
+    near[:, :, :-1] |= m[:, :, 1:]
+    near[:, 1:, :] |= m[:, :-1, :]
+    near[:, :-1, :] |= m[:, 1:, :]
+    near[1:, :, :] |= m[:-1, :, :]
+    near[:-1, :, :] |= m[1:, :, :]
+    ok &= near == 0
+    c = (slice(1, -1),) * 3
+    dx = (u[1:-1, 1:-1, 2:] - u[1:-1, 1:-1, :-2]) * scale
+    dy = (u[1:-1, 2:, 1:-1] - u[1:-1, :-2, 1:-1]) * scale
+    dz = (u[2:, 1:-1, 1:-1] - u[:-2, 1:-1, 1:-1]) * scale
+    cx = dy[..., 2] - dz[..., 1]
+    cy = dz[..., 0] - dx[..., 2]
+    cz = dx[..., 1] - dy[..., 0]
+    ts = (dx[..., 0] * dx[..., 0] + dy[..., 1] * dy[..., 1] + dz[..., 2] * dz[..., 2]
+          + f32(2.0) * (dx[..., 1] * dy[..., 0] + dx[..., 2] * dz[..., 0] + dy[..., 2] * dz[..., 1]))
+    vort = np.zeros((nz, ny, nx, 4), f32)
+    q = np.zeros((nz, ny, nx), f32)
+    vort[c] = np.stack([cx, cy, cz, np.sqrt(cx * cx + cy * cy + cz * cz)], axis=-1)
+    q[c] = f32(-0.5) * ts
+    vort[~ok] = 0.0
+    q[~ok] = 0.0
+    return vort.reshape(-1, 4), q.ravel(), ok.ravel().astype(np.uint8)
+
+
+def test_flow_diagnostics_of_a_leased_frame_match_numpy():
+    """Vorticity, Q criterion and validity of a leased frame of the flapping
+    compact bird against the NumPy restatement of the same operations; the
+    body of the captured step (held with the slot) is excluded, so a later
+    step's motion does not change an older frame's diagnostics."""
+    from bfx.simulation import BirdFlowSimulation
+    config, bird, state = cases.compact_bird()
+    sim = BirdFlowSimulation(config, bird, state, observation_buffer_count=2)
+    sim.advance(8, field_capture="required")
+    lat = sim.lattice
+    mask8 = lat.mask()
+    lease = sim.acquire_latest_gpu_field_frame()
+    _, vel = lease.copy()
+    c = lat.config
+    want = _flow_diagnostics_numpy(vel, mask8, c.nx, c.ny, c.nz, c.cell_size, c.time_step)
+    # the wings move on; the leased frame keeps the occupancy of its own step
+    for _ in range(40):
+        sim.advance(10, field_capture="required")
+        if not np.array_equal(lat.mask(), mask8):
+            break
+    assert not np.array_equal(lat.mask(), mask8)
+    vort, q, valid = lease.flow_diagnostics()
+    assert np.array_equal(valid, want[2])
+    assert 0 < int(valid.sum()) < valid.size
+    scale = float(np.max(np.abs(want[0][:, 3])))
+    assert scale > 0.0
+    np.testing.assert_allclose(vort, want[0], rtol=1e-6, atol=1e-6 * scale)
+    qs = float(np.max(np.abs(want[1])))
+    np.testing.assert_allclose(q, want[1], rtol=1e-6, atol=1e-6 * qs)
+    print("exact:", np.array_equal(vort, want[0]), np.array_equal(q, want[1]))
+    lease.release()
+    sim.close()
