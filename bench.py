@@ -405,15 +405,24 @@ def adjoint_measure(device):
     return out
 
 
-def cpu_port_rate(name, seconds_budget=12.0, max_steps=64):
-    """The oracle (CPU restatement of the reference path) on the same workload."""
+def cpu_port_rate(name, seconds_budget=12.0, max_steps=64, warmup=1, warmup_budget=30.0):
+    """The oracle (CPU restatement of the reference path) on the same workload:
+    `warmup` untimed steps (fewer if they exceed `warmup_budget` seconds), then
+    timed steps until `max_steps` or `seconds_budget`.  Returns the rate, the
+    timed steps, the threads, the timed seconds and the warm-up steps run."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle as O  # noqa: F401  (checker library, CPU baseline only)
     from helpers import oracle_twin
     cfg, rows, body, mesh, desc, _ = build_case(name, 0, COLLISION_OVERRIDE)
     osim = oracle_twin(cfg, rows, body, mesh)
-    osim.step()
+    w0 = time.perf_counter()
+    warm = 0
+    while warm < max(warmup, 1):
+        osim.step()
+        warm += 1
+        if time.perf_counter() - w0 > warmup_budget:
+            break
     t0 = time.perf_counter()
     steps = 0
     while steps < max_steps:
@@ -424,7 +433,7 @@ def cpu_port_rate(name, seconds_budget=12.0, max_steps=64):
     dt = time.perf_counter() - t0
     cells = cfg.nx * cfg.ny * cfg.nz
     threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return cells * steps / dt / 1e9, steps, threads, dt
+    return cells * steps / dt / 1e9, steps, threads, dt, warm
 
 
 def run_reference_arm(args, rank, world):
@@ -434,12 +443,12 @@ def run_reference_arm(args, rank, world):
     cfg, rows, body, mesh, desc, coll = build_case(name, 0, COLLISION_OVERRIDE)
     budget = 150.0
     per_step_budget = budget / max(args.steps + args.warmup, 1)
-    rate, steps, cores, dt = cpu_port_rate(name, seconds_budget=min(60.0, per_step_budget * args.steps),
-                                           max_steps=max(1, args.steps))
+    rate, steps, cores, dt, warm = cpu_port_rate(name, seconds_budget=min(60.0, per_step_budget * args.steps),
+                                                 max_steps=max(1, args.steps), warmup=args.warmup)
     cells = cfg.nx * cfg.ny * cfg.nz
     line = {
         "impl": "reference", "metric": "D3Q19 GLUPS", "value": rate, "unit": "GLUPS", "n_gpus": world,
-        "steps": steps, "warmup": 1, "ms_per_step": dt * 1000.0 / max(steps, 1), "higher_is_better": True,
+        "steps": steps, "warmup": warm, "ms_per_step": dt * 1000.0 / max(steps, 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": desc, "lattice": [cfg.nx, cfg.ny, cfg.nz], "collision": coll, "storage": "f32"},
         "cpu_baseline": {"value": rate, "unit": "GLUPS", "cores": cores, "kind": "port",
@@ -558,7 +567,7 @@ def main():
         line["adjoint"] = adjoint_measure(local)
 
     if rank == 0 and world == 1 and not args.no_cpu:
-        rate, steps, cores, dt = cpu_port_rate(args.workload)
+        rate, steps, cores, dt, _ = cpu_port_rate(args.workload)
         line["cpu_baseline"] = {"value": rate, "unit": "GLUPS", "cores": cores, "kind": "port",
                                 "sample": f"{steps} full steps of the same workload on the CPU restatement "
                                           f"(oracle/, C + OpenMP, {dt:.1f} s)"}
