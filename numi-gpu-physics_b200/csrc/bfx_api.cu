@@ -100,6 +100,7 @@ struct bfx_sim {
     uint32_t link_capacity = 0;
     uint32_t* block_counts = nullptr;
     uint32_t* block_offsets = nullptr;
+    uint32_t* scan_sums = nullptr;
     int box_blocks = 0;
     int scan_blocks = 0;
     double* topo_partials = nullptr;
@@ -230,6 +231,7 @@ GeomBuffers geom_buffers(bfx_sim* s, uint8_t* mprev, uint8_t* mnext) {
     b.link_capacity = s->link_capacity;
     b.block_counts = s->block_counts;
     b.block_offsets = s->block_offsets;
+    b.scan_sums = s->scan_sums;
     b.box_blocks = s->box_blocks;
     b.scan_blocks = s->scan_blocks;
     b.topo_partials = s->topo_partials;
@@ -277,7 +279,7 @@ void encode_links(bfx_sim* s, uint8_t* mprev, uint8_t* mnext) {
     GeomBuffers gb = geom_buffers(s, mprev, mnext);
     launch_boundary_scan(s->cfg.storage, s->rep_s, s->g, s->fp, s->box, gb, fluid_buffers(s, mnext), s->stream);
     launch_links_emit(s->cfg.geometry, s->cfg.link_rule, s->g, s->fp, s->box, gb, s->stream);
-    s->launches += 4;
+    s->launches += 5;
 }
 
 void timing_begin(bfx_sim* s) {
@@ -743,6 +745,7 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
         s->scan_blocks = s->box_blocks;
         BFX_ALLOC(s->block_counts, (size_t)s->box_blocks * sizeof(uint32_t));
         BFX_ALLOC(s->block_offsets, (size_t)s->box_blocks * sizeof(uint32_t));
+        BFX_ALLOC(s->scan_sums, (size_t)((s->box_blocks + kScanSegment - 1) / kScanSegment) * sizeof(uint32_t));
         BFX_ALLOC(s->topo_partials, (size_t)s->box_blocks * 8 * sizeof(double));
         s->apply_blocks = 4 * s->sm_count;
         BFX_ALLOC(s->link_partials, (size_t)s->apply_blocks * 16 * sizeof(double));

@@ -819,38 +819,73 @@ __global__ void __launch_bounds__(256) k_boundary_scan(const GeomArgs a, int rep
 // Warp w owns a contiguous chunk of the counts: a coalesced pass sums it, the
 // warp totals give each chunk's base, and a second coalesced pass writes the
 // offsets 32 at a time with a shuffle scan carrying the running total.
-__global__ void __launch_bounds__(1024) k_scan(const GeomArgs a) {
+// Exclusive scan of the per-block link counts into block offsets, in two
+// levels: k_scan_reduce sums each segment of kScanSegment counts (a block per
+// segment); k_scan_apply adds the sums of the segments before its own and
+// scans its segment (eight consecutive counts per thread).  Block 0 also sets
+// the total link count and the overflow flag.  Integer sums: the offsets do
+// not depend on the split.
+__device__ __forceinline__ uint32_t block_sum_1024(uint32_t v, uint32_t* wtot) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) wtot[warp] = v;
+    __syncthreads();
+    uint32_t t = 0;
+    for (int w = 0; w < 32; ++w) t += wtot[w];
+    return t;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_reduce(const GeomArgs a) {
     __shared__ uint32_t wtot[32];
     const int nb = a.b.scan_blocks;
+    const int lo = blockIdx.x * kScanSegment;
+    const int hi = lo + kScanSegment < nb ? lo + kScanSegment : nb;
+    uint32_t t = 0;
+    for (int i = lo + threadIdx.x; i < hi; i += 1024) t += a.b.block_counts[i];
+    t = block_sum_1024(t, wtot);
+    if (threadIdx.x == 0) a.b.scan_sums[blockIdx.x] = t;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_apply(const GeomArgs a, int nseg) {
+    __shared__ uint32_t wtot[32];
+    __shared__ uint32_t seg_base;
+    const int nb = a.b.scan_blocks;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int chunk = (nb + 31) / 32;
-    const int lo = warp * chunk;
-    const int hi = lo + chunk < nb ? lo + chunk : nb;
-    uint32_t tot = 0;
-#pragma unroll 8
-    for (int i = lo + lane; i < hi; i += 32) tot += a.b.block_counts[i];
-    for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
-    if (lane == 0) wtot[warp] = tot;
-    __syncthreads();
-    uint32_t base = 0;
-    for (int w = 0; w < warp; ++w) base += wtot[w];
-#pragma unroll 4
-    for (int i0 = lo; i0 < hi; i0 += 32) {
-        const int i = i0 + lane;
-        const uint32_t c = i < hi ? a.b.block_counts[i] : 0u;
-        uint32_t incl = c;
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += v;
-        }
-        if (i < hi) a.b.block_offsets[i] = base + incl - c;
-        base += __shfl_sync(0xffffffffu, incl, 31);
-    }
     if (threadIdx.x == 0) {
-        uint64_t total = 0;
-        for (int w = 0; w < 32; ++w) total += wtot[w];
-        a.b.state->link_count = (int64_t)total;
-        a.b.state->link_overflow = total > a.b.link_capacity ? 1u : 0u;
+        uint32_t b = 0;
+        for (int k = 0; k < (int)blockIdx.x; ++k) b += a.b.scan_sums[k];
+        seg_base = b;
+        if (blockIdx.x == 0) {
+            uint64_t total = 0;
+            for (int k = 0; k < nseg; ++k) total += a.b.scan_sums[k];
+            a.b.state->link_count = (int64_t)total;
+            a.b.state->link_overflow = total > a.b.link_capacity ? 1u : 0u;
+        }
+    }
+    // eight consecutive counts per thread
+    const int first = blockIdx.x * kScanSegment + 8 * threadIdx.x;
+    uint32_t c[8];
+    uint32_t mine = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        c[k] = first + k < nb ? a.b.block_counts[first + k] : 0u;
+        mine += c[k];
+    }
+    // block-exclusive prefix of the thread sums
+    uint32_t incl = mine;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) wtot[warp] = incl;
+    __syncthreads();
+    uint32_t base = seg_base;
+    for (int w = 0; w < warp; ++w) base += wtot[w];
+    base += incl - mine;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        if (first + k < nb) a.b.block_offsets[first + k] = base;
+        base += c[k];
     }
 }
 
@@ -1392,7 +1427,9 @@ void launch_boundary_scan(int storage, int rep_s, const GridDesc& g, const Fluid
 void launch_links_emit(int geometry, int link_rule, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
                        const GeomBuffers& gb, cudaStream_t s) {
     GeomArgs a = make_geom(g, fp, box, gb, nullptr);
-    k_scan<<<1, 1024, 0, s>>>(a);
+    const int nseg = (a.b.scan_blocks + kScanSegment - 1) / kScanSegment;
+    k_scan_reduce<<<nseg, 1024, 0, s>>>(a);
+    k_scan_apply<<<nseg, 1024, 0, s>>>(a, nseg);
     dim3 grid, block;
     box_shape(box, grid, block);
     k_links_emit<<<grid, block, 0, s>>>(a, geometry, link_rule, fp.interpolated);

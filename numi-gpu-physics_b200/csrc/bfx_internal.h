@@ -44,6 +44,9 @@ void launch_bulk_rare(int storage, int collision, int rep_s, const GridDesc& g, 
                       const FluidBuffers& b, const int* box, cudaStream_t s);
 void launch_bulk_stream(int storage, int collision, int rep_s, const GridDesc& g, const FluidParams& fp,
                         const FluidBuffers& b, const int* box, cudaStream_t s);
+// Block counts per segment of the two-level link-offset scan (bfx_geometry.cu).
+constexpr int kScanSegment = 8192;
+
 // Vorticity (curl, |curl|), Q criterion and validity of a captured field
 // (bfx_fields.cu); velocity in lattice units, scale = 0.5 * velocity_to_physical
 // / cell_size; mask: occupancy of the captured step, or null.
@@ -95,6 +98,7 @@ struct GeomBuffers {
     uint32_t link_capacity;
     uint32_t* block_counts;         // per box block
     uint32_t* block_offsets;
+    uint32_t* scan_sums;            // one per kScanSegment scan blocks (two-level scan)
     int box_blocks;                 // blocks of a one-slice-per-block box launch (allocations)
     int scan_blocks;                // blocks of the link count / scan / emission launch
     double* topo_partials;          // 8 per box block

@@ -77,6 +77,25 @@ def test_pipelined_free_flight_bird_is_bit_exact():
     assert np.array_equal(out[0][3], out[1][3])
 
 
+def test_pipelined_batch_with_field_capture_is_bit_exact():
+    """A 16-bit batch with required field capture: the pipelined steps hand the
+    last one (which captures and builds no next geometry) the same state as
+    one-step batches do; fields, populations and loads agree bit for bit."""
+    from bfx.simulation import BirdFlowSimulation
+    config, bird, state = cases.compact_bird()
+    out = []
+    for batch in (6, 1):
+        sim = BirdFlowSimulation(config, bird, state, storage=L.STORAGE_F16_DEVIATION, collision=L.COLLISION_RR3)
+        res = sim.advance(6, batch_size=batch, field_capture="required")
+        assert res.field_frame_published
+        rho, vel = sim.lattice.fields()
+        out.append((rho, vel, sim.lattice.populations(), np.array(sim.lattice.loads().force)))
+        sim.close()
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
+    assert np.all(np.isfinite(out[0][0])) and float(np.max(np.abs(out[0][1]))) > 0.0
+
+
 def test_two_runs_are_bit_identical():
     cfg, rows, body, _ = cases.ellipsoid_channel(nx=64, ny=32, nz=32, radii=(9.0, 5.0, 4.5), viscosity=0.02)
     out = []
