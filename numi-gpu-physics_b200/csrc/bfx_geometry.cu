@@ -815,10 +815,6 @@ __global__ void __launch_bounds__(256) k_boundary_scan(const GeomArgs a, int rep
     }
 }
 
-// Exclusive scan of the per-block link counts (one block of 1024 threads).
-// Warp w owns a contiguous chunk of the counts: a coalesced pass sums it, the
-// warp totals give each chunk's base, and a second coalesced pass writes the
-// offsets 32 at a time with a shuffle scan carrying the running total.
 // Exclusive scan of the per-block link counts into block offsets, in two
 // levels: k_scan_reduce sums each segment of kScanSegment counts (a block per
 // segment); k_scan_apply adds the sums of the segments before its own and
