@@ -209,6 +209,18 @@ typedef struct bfx_mesh {
     uint32_t triangle_count;
     uint32_t joint_count;           /* 0, 1 (elbow) or 2 (elbow, wrist) */
     const bfx_joint* joints;
+    /* Keyframe replay (MeasuredBirdSurfaceSequence; prepareIndexedBirdSurface,
+     * BF.metal:1585-1622): keyframe_count >= 2 frames at strictly increasing
+     * keyframe_times (s); keyframe_points holds keyframe_count * vertex_count * 3
+     * body-frame offsets (m) that take the place of local_vertices.  Each step
+     * interpolates linearly inside the interval holding its time (an exact
+     * interior keyframe opens the following interval, times past the last
+     * keyframe stay on the last interval) and adds the interval's slope to the
+     * body's rigid motion.  Requires joint_count 0 and every vertex on segment 0;
+     * 0 frames: no replay. */
+    uint32_t keyframe_count;
+    const float* keyframe_times;
+    const float* keyframe_points;
 } bfx_mesh;
 
 /* ForceTorque (Sources/BirdFlowCore/Diagnostics.swift) plus step diagnostics. */

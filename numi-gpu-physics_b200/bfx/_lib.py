@@ -84,7 +84,9 @@ class Mesh(ct.Structure):
     _fields_ = [("local_vertices", ct.POINTER(ct.c_float)), ("vertex_segment", ct.POINTER(ct.c_uint8)),
                 ("vertex_count", ct.c_uint32), ("triangles", ct.POINTER(ct.c_uint32)),
                 ("triangle_part", ct.POINTER(ct.c_uint8)), ("triangle_count", ct.c_uint32),
-                ("joint_count", ct.c_uint32), ("joints", ct.POINTER(Joint))]
+                ("joint_count", ct.c_uint32), ("joints", ct.POINTER(Joint)),
+                ("keyframe_count", ct.c_uint32), ("keyframe_times", ct.POINTER(ct.c_float)),
+                ("keyframe_points", ct.POINTER(ct.c_float))]
 
 
 class Loads(ct.Structure):

@@ -111,6 +111,44 @@ def flapping_plates(nx=512, ny=256, nz=256, span=64.0, chord=12.0, thickness=2.0
     return cfg, rows, body, plate_mesh(span, chord, n_chord, n_span)
 
 
+def keyframed_plates(nx=96, ny=64, nz=64, span=16.0, chord=6.0, thickness=2.0, n_chord=6, n_span=16, frames=24,
+                     frame_interval=4.0, stroke_deg=40.0, period=1000.0, jitter=0.02, seed=7, viscosity=0.02,
+                     storage=L.STORAGE_F32, link_rule=L.LINK_RAY_ROOT, sponge_width=6.0):
+    """A keyframe replay standing in for a measured surface sequence
+    (MeasuredBirdSurfaceSequence): the two plates of flapping_plates as one
+    body-fixed mesh whose vertices are given at `frames` keyframes every
+    `frame_interval` seconds (one second per step here): a stroke rotation about
+    the body x axis, mirrored on the right plate, plus a seeded per-vertex
+    perturbation of `jitter` cells normal to the plates.  The replay
+    interpolates linearly between keyframes."""
+    cfg, rows, body, mesh = flapping_plates(nx=nx, ny=ny, nz=nz, span=span, chord=chord, thickness=thickness,
+                                            n_chord=n_chord, n_span=n_span, period=period, stroke_deg=0.0,
+                                            pitch_deg=0.0, viscosity=viscosity, storage=storage, link_rule=link_rule,
+                                            sponge_width=sponge_width)
+    nv = mesh["local"].shape[0] // 2
+    one = mesh["local"][:nv].astype(np.float64)  # (chord, span, 0) of one plate
+    root = 2.0
+    rng = np.random.default_rng(seed)
+    times = np.arange(frames, dtype=np.float64) * frame_interval
+    pts = np.zeros((frames, 2 * nv, 3), np.float64)
+    for f, t in enumerate(times):
+        phi = math.radians(stroke_deg) * math.sin(2.0 * math.pi * t / period)
+        for side, sign in ((0, 1.0), (1, -1.0)):
+            y = sign * (root + one[:, 1])
+            z = rng.uniform(-jitter, jitter, nv)
+            c, s = math.cos(sign * phi), math.sin(sign * phi)
+            blk = pts[f, side * nv:(side + 1) * nv]
+            blk[:, 0] = one[:, 0]
+            blk[:, 1] = y * c - z * s
+            blk[:, 2] = y * s + z * c
+    mesh = dict(mesh)
+    mesh["segment"] = np.zeros(2 * nv, np.uint8)
+    mesh["local"] = pts[0].astype(np.float32)
+    mesh["kf_times"] = times.astype(np.float32)
+    mesh["kf_points"] = pts.astype(np.float32)
+    return cfg, rows, body, mesh
+
+
 def compact_bird(free_flight=False, storage=L.STORAGE_F32, n=48):
     """compactMetalTestCase (Tests/BirdFlowMetalTests/MetalExecutionTests.swift:411-470)."""
     bird = BirdParameters(

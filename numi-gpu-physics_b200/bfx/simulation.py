@@ -222,6 +222,14 @@ class Lattice:
                 m.joint_count = len(joints)
                 m.joints = arr
                 self._mesh_joints = arr
+            if mesh.get("kf_times") is not None:
+                # keyframe replay: times (s) and frames x vertices x 3 body-frame offsets (m)
+                kt = np.ascontiguousarray(mesh["kf_times"], np.float32)
+                kp = np.ascontiguousarray(mesh["kf_points"], np.float32)
+                m.keyframe_count = kt.shape[0]
+                m.keyframe_times = kt.ctypes.data_as(ct.POINTER(ct.c_float))
+                m.keyframe_points = kp.ctypes.data_as(ct.POINTER(ct.c_float))
+                self._mesh_keyframes = (kt, kp)
             mesh_ptr = ct.byref(m)
             self._mesh_struct = m
         handle = ct.c_void_p()

@@ -87,6 +87,9 @@ struct bfx_sim {
     uint8_t* mesh_segment = nullptr;
     bfx_joint* joints = nullptr;
     int joint_count = 0;
+    float* kf_times = nullptr;     // keyframe replay (kf_count >= 2)
+    float* kf_points = nullptr;
+    int kf_count = 0;
     uint32_t* mesh_tris = nullptr;
     uint8_t* mesh_tri_part = nullptr;
     float4* mesh_pos = nullptr;
@@ -217,6 +220,9 @@ GeomBuffers geom_buffers(bfx_sim* s, uint8_t* mprev, uint8_t* mnext) {
     b.mesh_segment = s->mesh_segment;
     b.joints = s->joints;
     b.joint_count = s->joint_count;
+    b.kf_times = s->kf_times;
+    b.kf_points = s->kf_points;
+    b.kf_count = s->kf_count;
     b.mesh_tris = s->mesh_tris;
     b.mesh_tri_part = s->mesh_tri_part;
     b.mesh_pos = s->mesh_pos;
@@ -516,6 +522,24 @@ int validate_config(const bfx_config* c, const bfx_bird* bird, const bfx_mesh* m
         for (uint32_t i = 0; i < mesh->triangle_count; ++i)
             if (mesh->triangle_part[i] == 0 || mesh->triangle_part[i] > 63)
                 return fail(nullptr, BFX_ERR_INVALID_CONFIG, "triangle part must be 1...63");
+        if (mesh->keyframe_count > 0) {
+            if (mesh->keyframe_count < 2 || !mesh->keyframe_times || !mesh->keyframe_points)
+                return fail(nullptr, BFX_ERR_INVALID_CONFIG, "a keyframe replay needs at least two frames with times and points");
+            if (mesh->joint_count != 0)
+                return fail(nullptr, BFX_ERR_INVALID_CONFIG, "a keyframe replay takes no joints");
+            for (uint32_t i = 0; i < mesh->vertex_count; ++i)
+                if (mesh->vertex_segment[i] != 0)
+                    return fail(nullptr, BFX_ERR_INVALID_CONFIG, "keyframed vertices belong to segment 0 (the body)");
+            for (uint32_t f = 0; f < mesh->keyframe_count; ++f) {
+                if (!std::isfinite(mesh->keyframe_times[f]) ||
+                    (f > 0 && !(mesh->keyframe_times[f] > mesh->keyframe_times[f - 1])))
+                    return fail(nullptr, BFX_ERR_INVALID_CONFIG, "keyframe times must be finite and strictly increasing");
+            }
+            const size_t np = (size_t)mesh->keyframe_count * mesh->vertex_count * 3;
+            for (size_t k = 0; k < np; ++k)
+                if (!std::isfinite(mesh->keyframe_points[k]))
+                    return fail(nullptr, BFX_ERR_INVALID_CONFIG, "keyframe points must be finite");
+        }
     }
     return BFX_OK;
 }
@@ -544,6 +568,15 @@ float geometry_radius(const bfx_config* c, const bfx_bird* b, const bfx_mesh* m)
         chain[j + 1] = chain[j] + std::sqrt(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
     }
     float r = 0.0f;
+    if (m->keyframe_count >= 2) {
+        // keyframe replay: every frame's offsets (the interpolation stays inside their hull)
+        const size_t np = (size_t)m->keyframe_count * m->vertex_count;
+        for (size_t i = 0; i < np; ++i) {
+            const float* l = m->keyframe_points + 3 * i;
+            r = std::max(r, std::sqrt(l[0] * l[0] + l[1] * l[1] + l[2] * l[2]));
+        }
+        return r + c->mesh_half_thickness + 2.0f * c->cell_size;
+    }
     for (uint32_t i = 0; i < m->vertex_count; ++i) {
         const float* l = m->local_vertices + 3 * i;
         float d = std::sqrt(l[0] * l[0] + l[1] * l[1] + l[2] * l[2]);
@@ -771,6 +804,16 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
             cudaMemcpyAsync(s->mesh_tris, mesh->triangles, (size_t)s->ntris * 3 * sizeof(uint32_t),
                             cudaMemcpyHostToDevice, s->stream);
             cudaMemcpyAsync(s->mesh_tri_part, mesh->triangle_part, s->ntris, cudaMemcpyHostToDevice, s->stream);
+            if (mesh->keyframe_count >= 2) {
+                s->kf_count = (int)mesh->keyframe_count;
+                const size_t np = (size_t)s->kf_count * s->nverts * 3;
+                BFX_ALLOC(s->kf_times, (size_t)s->kf_count * sizeof(float));
+                BFX_ALLOC(s->kf_points, np * sizeof(float));
+                cudaMemcpyAsync(s->kf_times, mesh->keyframe_times, (size_t)s->kf_count * sizeof(float),
+                                cudaMemcpyHostToDevice, s->stream);
+                cudaMemcpyAsync(s->kf_points, mesh->keyframe_points, np * sizeof(float), cudaMemcpyHostToDevice,
+                                s->stream);
+            }
             if (mesh->joint_count > 0) {
                 s->joint_count = (int)mesh->joint_count;
                 BFX_ALLOC(s->joints, (size_t)s->joint_count * sizeof(bfx_joint));
@@ -1556,6 +1599,8 @@ int adjoint_scope(bfx_sim* s) {
     if (c.storage != BFX_STORAGE_F32 && c.storage != BFX_STORAGE_F64)
         return fail(s, BFX_ERR_UNSUPPORTED, "the adjoint supports F32 and F64 storage");
     if (c.fast_math) return fail(s, BFX_ERR_UNSUPPORTED, "the adjoint differentiates the non-contracted step");
+    if (s->kf_count >= 2)
+        return fail(s, BFX_ERR_UNSUPPORTED, "a keyframe replay does not depend on the kinematic parameters");
     for (int f = 0; f < 6; ++f)
         if (c.face_bc[f] == BFX_BC_OUTFLOW)
             return fail(s, BFX_ERR_UNSUPPORTED, "the adjoint does not support zero-gradient outflow faces");

@@ -190,6 +190,7 @@ __global__ void k_prepare(const GeomArgs a, int init, float dt, float box_radius
             pu = uu;
         }
     }
+    st->geom_time = time;
     float4 o = qnormalize(orient);
     Prepared& p = st->prep;
     p.body_position = f4(pos, 0.0f);
@@ -432,8 +433,47 @@ __global__ void k_mesh_prepare(const GeomArgs a) {
     }
 }
 
+// Keyframe replay of a body-frame offset (prepareIndexedBirdSurface,
+// BF.metal:1585-1622): the interval [first, first + 1] holds the geometry time
+// (an exact interior keyframe opens the following interval, times past the
+// last keyframe stay on the last one, before the first on the first), the
+// offset is mix(a, b, blend) = a + (b - a) blend with the blend clamped to
+// [0, 1], and its rate is (b - a) / duration.
+__device__ void keyframe_offset(const GeomArgs& a, uint32_t i, V3& l, V3& dl) {
+    const float t = a.b.state->geom_time;
+    const float* T = a.b.kf_times;
+    const int nf = a.b.kf_count;
+    int lo = 0, hi = nf;  // first index with T[j] > t
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (T[mid] > t) hi = mid;
+        else lo = mid + 1;
+    }
+    int first = lo - 1;
+    first = first < 0 ? 0 : (first > nf - 2 ? nf - 2 : first);
+    const float duration = T[first + 1] - T[first];
+    float blend = (t - T[first]) / duration;
+    blend = blend < 0.0f ? 0.0f : (blend > 1.0f ? 1.0f : blend);
+    const float* pa = a.b.kf_points + 3 * ((size_t)first * a.b.nverts + i);
+    const float* pb = pa + 3 * (size_t)a.b.nverts;
+    const V3 d = v3(pb[0] - pa[0], pb[1] - pa[1], pb[2] - pa[2]);
+    l = v3(pa[0] + d.x * blend, pa[1] + d.y * blend, pa[2] + d.z * blend);
+    dl = v3(d.x / duration, d.y / duration, d.z / duration);
+}
+
 __device__ void mesh_vertex(const GeomArgs& a, uint32_t i, V3& w, V3& v) {
     const Prepared& p = a.b.state->prep;
+    if (a.b.kf_count >= 2) {
+        // body-frame keyframe offset on top of the body's rigid motion
+        V3 l, dl;
+        keyframe_offset(a, i, l, dl);
+        const V3 r = qrotate(p.orientation, l), rd = qrotate(p.orientation, dl);
+        w = v3(p.body_position.x + r.x, p.body_position.y + r.y, p.body_position.z + r.z);
+        const V3 cr = cross(v3(p.omega_body_world), r);
+        v = v3(p.linear_velocity.x + cr.x + rd.x, p.linear_velocity.y + cr.y + rd.y,
+               p.linear_velocity.z + cr.z + rd.z);
+        return;
+    }
     V3 l = v3(a.b.mesh_local[3 * i], a.b.mesh_local[3 * i + 1], a.b.mesh_local[3 * i + 2]);
     uint8_t seg = a.b.mesh_segment[i];
     if (seg == 0) {

@@ -98,7 +98,10 @@ struct GeomBuffers {
     uint32_t link_capacity;
     uint32_t* block_counts;         // per box block
     uint32_t* block_offsets;
-    uint32_t* scan_sums;            // one per kScanSegment scan blocks (two-level scan)
+    uint32_t* scan_sums;
+    const float* kf_times;          // keyframe replay: times, frames x vertices x 3 offsets (kf_count >= 2)
+    const float* kf_points;
+    int kf_count;            // one per kScanSegment scan blocks (two-level scan)
     int box_blocks;                 // blocks of a one-slice-per-block box launch (allocations)
     int scan_blocks;                // blocks of the link count / scan / emission launch
     double* topo_partials;          // 8 per box block

@@ -53,7 +53,7 @@ struct DeviceState {
     double body[13];               // position 3, orientation 4, velocity 3, omega 3
     Prepared prep;
     int32_t box_origin[3];         // geometry region origin (cells)
-    int32_t _pad0;
+    float geom_time;               // time (s) of the step the geometry was built for
     // bounding box (cells, inclusive) of this step's mesh vertices; open
     // (+-2^30) for the analytic shapes, empty before the vertices are placed
     int32_t act_lo[3], act_hi[3];

@@ -1222,6 +1222,45 @@ static void closest_point(const float p[3], const float a[3], const float b[3], 
     bary[0] = 1.0f - v - w; bary[1] = v; bary[2] = w;
 }
 
+/* Keyframe replay (BF.metal:1585-1622; the reference's host picks the
+ * interval once): the interval [first, first + 1] holds `time` -- an exact
+ * interior keyframe opens the following interval, times past the last
+ * keyframe stay on the last interval and times before the first on the first
+ * -- the offset is a + (b - a) * blend with the blend clamped to [0, 1], its
+ * rate (b - a) / duration; both are rotated into the world and added to the
+ * body's rigid motion. */
+void or_mesh_prepare_keyframes(const or_prepared* prep, const float* times, uint32_t nframes, const float* points,
+                               uint32_t nverts, float time, float v2l, float* pos, float* vel) {
+    uint32_t lo = 0, hi = nframes; /* first index with times[j] > time */
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) / 2;
+        if (times[mid] > time) hi = mid;
+        else lo = mid + 1;
+    }
+    uint32_t first = lo == 0 ? 0 : lo - 1;
+    if (first > nframes - 2) first = nframes - 2;
+    const float duration = times[first + 1] - times[first];
+    float blend = (time - times[first]) / duration;
+    blend = blend < 0.0f ? 0.0f : (blend > 1.0f ? 1.0f : blend);
+    for (uint32_t i = 0; i < nverts; ++i) {
+        const float* pa = points + 3 * ((size_t)first * nverts + i);
+        const float* pb = pa + 3 * (size_t)nverts;
+        float d[3], l[3], dl[3], r[3], rd[3], cr[3], w[3], v[3];
+        for (int k = 0; k < 3; ++k) {
+            d[k] = pb[k] - pa[k];
+            l[k] = pa[k] + d[k] * blend;
+            dl[k] = d[k] / duration;
+        }
+        quat_rotate(prep->orientation.v, l, r);
+        quat_rotate(prep->orientation.v, dl, rd);
+        for (int k = 0; k < 3; ++k) w[k] = prep->body_position.v[k] + r[k];
+        cross3(prep->omega_body_world.v, r, cr);
+        for (int k = 0; k < 3; ++k) v[k] = prep->linear_velocity.v[k] + cr[k] + rd[k];
+        pos[4 * i] = w[0]; pos[4 * i + 1] = w[1]; pos[4 * i + 2] = w[2]; pos[4 * i + 3] = 0.0f;
+        vel[4 * i] = v[0] * v2l; vel[4 * i + 1] = v[1] * v2l; vel[4 * i + 2] = v[2] * v2l; vel[4 * i + 3] = 0.0f;
+    }
+}
+
 void or_mesh_prepare_articulated(const or_prepared* prep, const float* local, const uint8_t* segment,
                                  uint32_t nverts, float v2l, float* pos, float* vel) {
     for (uint32_t i = 0; i < nverts; ++i) {

@@ -156,6 +156,10 @@ void or_prepare_segments(const or_bird* bird, const or_prepared* prep, const or_
                          float time, or_segment* out /* 4: left / right middle, left / right outer */);
 void or_mesh_prepare_segments(const or_prepared* prep, const or_segment* segs, const float* local,
                               const uint8_t* segment, uint32_t nverts, float v2l, float* pos, float* vel);
+/* Keyframe replay of body-frame offsets (prepareIndexedBirdSurface,
+ * BF.metal:1585-1622) on top of the body's rigid motion at `time`. */
+void or_mesh_prepare_keyframes(const or_prepared* prep, const float* times, uint32_t nframes, const float* points,
+                               uint32_t nverts, float time, float v2l, float* pos, float* vel);
 void or_mesh_prepare_articulated(const or_prepared* prep, const float* local /*3 per vertex*/,
                                  const uint8_t* segment, uint32_t nverts, float v2l,
                                  float* pos /*4 per vertex*/, float* vel /*4 per vertex*/);

@@ -116,6 +116,8 @@ def lib():
         L.or_enumerate_links.restype = ct.c_int64
         L.or_enumerate_links.argtypes = [P(Params), u8p, u8p, P(ct.c_uint32), u8p, ct.c_int64]
         L.or_mesh_prepare_articulated.argtypes = [P(Prepared), fp, u8p, ct.c_uint32, ct.c_float, fp, fp]
+        L.or_mesh_prepare_keyframes.argtypes = [P(Prepared), fp, ct.c_uint32, fp, ct.c_uint32, ct.c_float, ct.c_float,
+                                                fp, fp]
         L.or_prepare_segments.argtypes = [P(Bird), P(Prepared), fp, ct.c_int, ct.c_float, fp]
         L.or_mesh_prepare_segments.argtypes = [P(Prepared), fp, fp, u8p, ct.c_uint32, ct.c_float, fp, fp]
         L.or_mesh_rasterize.argtypes = [P(Params), fp, P(ct.c_uint32), ct.c_uint32, ct.c_float, P(ct.c_uint64)]
@@ -314,7 +316,11 @@ class OracleSim:
             self.mesh_pos = np.zeros(4 * nv, np.float32)
             self.mesh_vel = np.zeros(4 * nv, np.float32)
             joints = m.get("joints") or []
-            if joints:
+            if m.get("kf_times") is not None:
+                L.or_mesh_prepare_keyframes(ct.byref(self.prep), fptr(m["kf_times"]), len(m["kf_times"]),
+                                            fptr(m["kf_points"]), nv, time, self.p.v2l, fptr(self.mesh_pos),
+                                            fptr(self.mesh_vel))
+            elif joints:
                 # or_joint: origin[3], axis[3], bias, amplitude, phase, reserved
                 jarr = np.array([list(j["origin"]) + list(j["axis"]) + [j["bias"], j["amplitude"], j["phase"], 0.0]
                                  for j in joints], dtype=np.float32).ravel()

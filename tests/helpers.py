@@ -37,6 +37,9 @@ def oracle_twin(cfg: L.Config, bird_rows=None, body=None, mesh=None) -> O.Oracle
         om["local"] = np.ascontiguousarray(mesh["local"], np.float32).ravel()
         om["local"] = om["local"].reshape(-1, 3)
         om["half_thickness"] = cfg.mesh_half_thickness
+        if mesh.get("kf_times") is not None:
+            om["kf_times"] = np.ascontiguousarray(mesh["kf_times"], np.float32)
+            om["kf_points"] = np.ascontiguousarray(mesh["kf_points"], np.float32).ravel()
     return O.OracleSim(p, geometry=geometry, bird=bird, body=body, mesh=om,
                        link_rule="linear" if cfg.link_rule == L.LINK_LINEAR else "ray", shear=shear)
 
