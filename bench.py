@@ -412,7 +412,7 @@ def cpu_port_rate(name, seconds_budget=12.0, max_steps=64, warmup=1, warmup_budg
     timed steps, the threads, the timed seconds and the warm-up steps run."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import oracle as O  # noqa: F401  (checker library, CPU baseline only)
+    import oracle as O  # noqa: F401  (the oracle, CPU baseline only)
     from helpers import oracle_twin
     cfg, rows, body, mesh, desc, _ = build_case(name, 0, COLLISION_OVERRIDE)
     osim = oracle_twin(cfg, rows, body, mesh)
