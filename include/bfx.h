@@ -338,7 +338,9 @@ BFX_API int bfx_copy_gauge_pressure(bfx_sim* sim, float pressure_scale_pascals, 
  * number of field observation slots, 1...4 (default 1).  Allowed before the
  * first step only.  wait_limit_ms bounds how long a required capture waits for
  * a lease to be released (0: without limit, as the reference does); when it
- * runs out the call fails with BFX_ERR_TIMEOUT and the handle stays usable. */
+ * runs out the call fails with BFX_ERR_TIMEOUT and the handle stays usable.
+ * It replaces the slot set, so no acquire or release may run concurrently
+ * with it (unlike with bfx_advance). */
 BFX_API int bfx_set_observation_buffers(bfx_sim* sim, uint32_t count, uint32_t wait_limit_ms);
 /* acquireLatestGPUFieldFrame(afterStep:) (BirdFlowSimulation.swift:1148-1171):
  * leases the newest published frame, if its step is above after_step when
