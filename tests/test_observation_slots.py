@@ -166,3 +166,83 @@ def test_capture_mode_names():
     assert _capture_mode(True) == L.FIELD_CAPTURE_REQUIRED and _capture_mode(False) == L.FIELD_CAPTURE_DISABLED
     with pytest.raises(ValueError):
         _capture_mode("latest")
+
+
+STRESS = r'''
+#include <atomic>
+#include <cstdio>
+#include <set>
+#include <thread>
+#include <vector>
+#include "bfx_observation.h"
+using namespace bfx;
+struct Snap { unsigned long long step; };
+struct Meta { Snap snapshot; };
+int main() {
+    FieldSlots<Meta> s(3);
+    Meta m0; m0.snapshot.step = 0;
+    s.reset(m0);
+    std::atomic<bool> done(false);
+    std::atomic<long> leased(0), bad(0);
+    std::vector<std::thread> consumers;
+    std::vector<std::vector<uint64_t>> ids(3);
+    for (int c = 0; c < 3; ++c) {
+        consumers.emplace_back([&, c] {
+            unsigned long long last = 0;
+            while (!done.load()) {
+                Meta m; int slot = -1;
+                uint64_t l = s.acquire(false, 0, &m, &slot);
+                if (l) {
+                    ++leased;
+                    ids[c].push_back(l);
+                    if (slot < 0 || slot > 2 || s.leased_slot(l) != slot) ++bad;
+                    if (m.snapshot.step < last) ++bad;   // newest frames only move forward per consumer
+                    last = m.snapshot.step;
+                    std::this_thread::yield();
+                    if (!s.release(l)) ++bad;
+                    if (s.release(l)) ++bad;             // a second release is a no-op
+                }
+            }
+        });
+    }
+    unsigned long long step = 0;
+    for (int i = 0; i < 20000; ++i) {
+        const CaptureMode mode = (i % 3 == 0) ? CaptureMode::Required : CaptureMode::BestEffort;
+        const int w = s.select(mode, 1000);
+        if (w == kSlotWaitTimeout) { ++bad; continue; }
+        if (w < 0) continue;
+        Meta m; m.snapshot.step = ++step;
+        if (i % 97 == 0) s.abandon(w);
+        else s.publish(w, m);
+    }
+    done = true;
+    for (auto& t : consumers) t.join();
+    std::set<uint64_t> all;
+    size_t n = 0;
+    for (auto& v : ids) { n += v.size(); all.insert(v.begin(), v.end()); }
+    if (all.size() != n) ++bad;                       // lease ids are never reused
+    if (!s.idle()) ++bad;
+    std::printf("%s leased=%ld dropped=%llu waits=%llu\n", bad.load() ? "BAD" : "OK", leased.load(),
+                (unsigned long long)s.dropped(), (unsigned long long)s.waits());
+    return bad.load() ? 1 : 0;
+}
+'''
+
+
+def test_observation_slots_under_concurrent_consumers(tmp_path):
+    """Three consumer threads lease and release the newest frame while the
+    advancing thread captures (best-effort and required with a wait limit),
+    publishes and abandons 20,000 frames; built with ThreadSanitizer when the
+    compiler has it.  Leases stay unique, each consumer's frames move forward,
+    double releases are no-ops and every slot ends free."""
+    src = tmp_path / "stress.cpp"
+    src.write_text(STRESS)
+    exe = tmp_path / "stress"
+    base = ["g++", "-std=c++17", "-O1", "-pthread", "-I", CSRC, str(src), "-o", str(exe)]
+    tsan = subprocess.run(base[:2] + ["-fsanitize=thread", "-g"] + base[2:], capture_output=True, text=True)
+    if tsan.returncode != 0:
+        subprocess.run(base, check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert out.stdout.startswith("OK"), out.stdout
+    assert "WARNING: ThreadSanitizer" not in out.stderr, out.stderr[:2000]
