@@ -98,6 +98,31 @@ def read_archive(source: str, names=(POPULATIONS, SOLID_MASK, RESTART_STATE)):
     return manifest, files
 
 
+def struct_from_dict(cls, d: dict):
+    """The inverse of struct_dict: a ctypes structure of type `cls` filled from
+    plain values (nested structures and arrays included); fields absent from
+    `d` keep their zero value."""
+    s = cls()
+    for name, _ in cls._fields_:
+        if name.startswith("_") or name not in d:
+            continue
+        value = d[name]
+        cur = getattr(s, name)
+        if hasattr(cur, "_fields_"):
+            setattr(s, name, struct_from_dict(type(cur), value))
+        elif hasattr(cur, "__len__") and not isinstance(cur, (bytes, str)):
+            for i, e in enumerate(value):
+                if hasattr(cur[i], "_fields_"):
+                    cur[i] = struct_from_dict(type(cur[i]), e)
+                elif hasattr(cur[i], "__len__"):
+                    cur[i][:] = list(e)
+                else:
+                    cur[i] = e
+        else:
+            setattr(s, name, value)
+    return s
+
+
 def struct_dict(s) -> dict:
     """A ctypes structure as plain JSON values (arrays as lists)."""
     out = {}

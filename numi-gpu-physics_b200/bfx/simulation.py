@@ -414,6 +414,23 @@ class Lattice:
                  C.RESTART_STATE: self.save_state()}
         C.write_archive(destination, manifest, files)
 
+    @classmethod
+    def from_archive(cls, source: str, mesh=None) -> "Lattice":
+        """init(checkpointURL:observationBufferCount:) (BirdFlowSimulation.swift:661-672):
+        a new simulation built from an archive's configuration, bird and body
+        and restored to its exact state.  A mesh configuration needs its mesh,
+        which the archive does not hold."""
+        from . import checkpoint as C
+        manifest, _ = C.read_archive(source)
+        cfg = C.struct_from_dict(L.Config, manifest["configuration"])
+        bird = C.struct_from_dict(L.Bird, manifest["bird"]) if manifest.get("bird") else None
+        body = C.struct_from_dict(L.BodyState, manifest["body"]) if manifest.get("body") else None
+        if cfg.geometry == L.GEOMETRY_MESH and mesh is None:
+            raise C.CheckpointError("a mesh configuration needs its mesh (meshes are not archived)")
+        lat = cls(cfg, bird, body, mesh)
+        lat.restore_archive(source)
+        return lat
+
     def restore_archive(self, source: str) -> dict:
         """Restores a checkpoint archive written by save_archive after checking
         every digest; the restored populations must equal the archive's

@@ -96,3 +96,49 @@ def test_ledger_report_gates_on_the_relative_residuals():
     assert not bad["passed"] and good["passed"]
     assert abs(good["relative_rms_boundary_closure_residual"] - 0.001) < 1e-12
     assert abs(good["rms_aerodynamic_impulse"] - 2.0) < 1e-12
+
+
+def test_struct_dict_round_trip():
+    """struct_from_dict inverts struct_dict for the structures an archive's
+    manifest holds (configuration, bird, body), nested arrays included."""
+    import json
+    import bfx._lib as L
+    import bfx.cases as cases
+    import bfx.checkpoint as C
+    from bfx.simulation import bird_struct
+    from helpers import body_struct_from_tuple
+    cfg, rows, body, _ = cases.flapping_plates(nx=96, ny=64, nz=64)
+    for s in (cfg, bird_struct(rows), body_struct_from_tuple(body)):
+        d = json.loads(json.dumps(C.struct_dict(s)))
+        back = C.struct_from_dict(type(s), d)
+        assert bytes(back) == bytes(s)
+
+
+def test_from_archive_rebuilds_a_valid_configuration(tmp_path):
+    """Lattice.from_archive rebuilds the configuration from the manifest: the
+    rebuilt configuration passes the library's checks and the call stops at
+    device creation on a machine without a GPU (deviceUnavailable, not
+    invalidConfiguration); a mesh configuration without its mesh is refused."""
+    import ctypes as ct
+    import bfx._lib as L
+    import bfx.cases as cases
+    import bfx.checkpoint as C
+    from bfx.simulation import BirdFlowError, Lattice, bird_struct
+    from helpers import body_struct_from_tuple
+    lib = L.load()
+    n = ct.c_int(0)
+    if lib.bfx_device_count(ct.byref(n)) == 0 and n.value > 0:
+        pytest.skip("a CUDA device is present")
+    cfg, rows, body, _ = cases.ellipsoid_channel(nx=64, ny=32, nz=32, radii=(8.0, 4.0, 4.0))
+    manifest = {"configuration": C.struct_dict(cfg), "bird": C.struct_dict(bird_struct(rows)),
+                "body": C.struct_dict(body_struct_from_tuple(body)), "step": 0, "timeSeconds": 0.0}
+    files = {C.POPULATIONS: b"\\0" * 16, C.SOLID_MASK: b"\\0" * 16, C.RESTART_STATE: b"\\0" * 16}
+    C.write_archive(str(tmp_path / "a"), manifest, files)
+    with pytest.raises(BirdFlowError) as e:
+        Lattice.from_archive(str(tmp_path / "a"))
+    assert e.value.status == 1
+    mcfg, mrows, mbody, _ = cases.flapping_plates(nx=96, ny=64, nz=64)
+    manifest["configuration"] = C.struct_dict(mcfg)
+    C.write_archive(str(tmp_path / "m"), manifest, files)
+    with pytest.raises(C.CheckpointError, match="mesh"):
+        Lattice.from_archive(str(tmp_path / "m"))

@@ -158,6 +158,12 @@ def test_checkpoint_archive_round_trip_and_continuation(tmp_path):
     assert fresh.step_index()[0] == 5
     fresh.advance(7)
     assert np.array_equal(fresh.populations(), cont)
+    # init(checkpointURL:): a handle built from the archive alone (plus the mesh)
+    rebuilt = Lattice.from_archive(path, mesh=mesh)
+    assert rebuilt.step_index()[0] == 5
+    rebuilt.advance(7)
+    assert np.array_equal(rebuilt.populations(), cont)
+    rebuilt.close()
     for name in (C.POPULATIONS, C.SOLID_MASK, C.RESTART_STATE):
         bad = str(tmp_path / f"bad-{name}")
         lat.save_archive(bad)
