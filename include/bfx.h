@@ -30,7 +30,9 @@
 extern "C" {
 #endif
 
-#define BFX_ABI_VERSION 1
+/* 2: bfx_mesh keyframe fields, bfx_advance_result.dropped_field_frames,
+ * field observation and flow-diagnostics entry points. */
+#define BFX_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define BFX_API __attribute__((visibility("default")))

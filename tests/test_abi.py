@@ -28,7 +28,7 @@ def test_library_loads_and_exports_every_declared_symbol():
     for s in syms:
         assert hasattr(lib, s), s
     assert set(syms) == set(L.EXPORTED)
-    assert lib.bfx_abi_version() == 1
+    assert lib.bfx_abi_version() == 2
 
 
 def test_no_device_reports_unavailable_not_crash():
