@@ -411,18 +411,28 @@ BFX_API int bfx_launch_count(bfx_sim* sim, uint64_t* launches);
 /* Bytes of device memory held by the handle. */
 BFX_API int bfx_device_bytes(bfx_sim* sim, uint64_t* bytes);
 /* Allocation-free variant of bfx_fluid_mass_momentum.  It has no counterpart in
- * the reference.  It is for callers that cannot allocate device memory when they
- * need the sum: code running while a CUDA graph is captured, loops that must
- * not touch the allocator, processes whose device memory belongs to another
- * allocator.  The caller passes device pointers it already holds:
- *   populations  canonical FP32 populations, direction-major [19][nx*ny*nz];
+ * the reference.  It is for callers that cannot call cudaMalloc where they need
+ * the sum: a host application whose device memory budget is already reserved
+ * by its own allocator (a framework's caching pool), where a fresh allocation
+ * fails or fragments that pool, and loops with a fixed time budget per
+ * iteration, where cudaMalloc / cudaFree would synchronise the device.
+ * The caller passes device pointers it already holds:
+ *   populations  canonical, dense FP32 populations, direction-major
+ *                [19][nx*ny*nz] (the layout of bfx_copy_populations).  This is
+ *                not a handle's own population buffer, which carries a halo,
+ *                a padded row pitch and possibly 16-bit storage: a caller that
+ *                holds a bfx_sim copies the populations into such an array
+ *                first;
  *   mask         part id per cell (0 = fluid), or NULL for an all-fluid lattice;
  *   out          4 doubles: fluid mass and momentum x, y, z (FP64).
  * Scratch is a fixed 1 MiB device array inside the library (kept by every GPU
- * that loads it), so lattices above 8,388,608 cells are rejected with
- * BFX_ERR_CAPACITY.  The first call on a device looks up that array's device
- * address, so make it before any stream capture.  Work runs on the legacy
- * default stream and the call returns after it finishes.  Calls share the
+ * that loads it until the process exits), so lattices above 8,388,608 cells
+ * are rejected with BFX_ERR_CAPACITY.  The first call on a device looks up
+ * that array's device address and keeps it, so make that first call before
+ * any stream capture; the address belongs to the CUDA context current at that
+ * call (a context recreated later, e.g. after cudaDeviceReset, is not
+ * supported).  The work runs on the legacy default stream, not on any
+ * handle's stream, and the call returns after it finishes.  Calls share the
  * scratch: calls that overlap on the GPU race and must be serialised. */
 BFX_API int bfx_fluid_mass_momentum_noalloc(const float* populations, const uint8_t* mask, uint32_t nx, uint32_t ny,
                                             uint32_t nz, double* out);

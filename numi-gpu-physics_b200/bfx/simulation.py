@@ -428,7 +428,11 @@ class Lattice:
         if cfg.geometry == L.GEOMETRY_MESH and mesh is None:
             raise C.CheckpointError("a mesh configuration needs its mesh (meshes are not archived)")
         lat = cls(cfg, bird, body, mesh)
-        lat.restore_archive(source)
+        try:
+            lat.restore_archive(source)
+        except BaseException:
+            lat.close()  # the handle and its device memory are not leaked on a refused archive
+            raise
         return lat
 
     def restore_archive(self, source: str) -> dict:

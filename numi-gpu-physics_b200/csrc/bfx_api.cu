@@ -848,7 +848,12 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
     }
     if (s->geometry() && !s->moving()) {
         DeviceState st;
-        cudaMemcpy(&st, s->dstate, sizeof(st), cudaMemcpyDeviceToHost);
+        cudaError_t ce = cudaMemcpy(&st, s->dstate, sizeof(st), cudaMemcpyDeviceToHost);
+        if (ce != cudaSuccess) {
+            const int rc = cuda_fail(nullptr, ce, "static link build");
+            bfx_destroy(s);
+            return rc;
+        }
         if (st.link_overflow) {
             g_create_error = "the cut-link list exceeds its capacity; raise link_capacity";
             bfx_destroy(s);
@@ -1210,7 +1215,8 @@ int bfx_copy_mask(bfx_sim* s, uint8_t* out, size_t cells) {
         std::memset(out, 0, (size_t)s->g.n);
         return BFX_OK;
     }
-    cudaMemcpy(out, s->mask[s->cur], (size_t)s->g.n, cudaMemcpyDeviceToHost);
+    cudaError_t e = cudaMemcpy(out, s->mask[s->cur], (size_t)s->g.n, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(s, e, "mask read-back");
     for (int64_t i = 0; i < s->g.n; ++i) out[i] &= 0x3F;  // part id bits
     return BFX_OK;
 }
@@ -1224,7 +1230,8 @@ int bfx_copy_wall(bfx_sim* s, float* out4, size_t cells) {
         std::memset(out4, 0, (size_t)s->g.n * 16);
         return BFX_OK;
     }
-    cudaMemcpy(out4, s->wall, (size_t)s->g.n * sizeof(float4), cudaMemcpyDeviceToHost);
+    cudaError_t e = cudaMemcpy(out4, s->wall, (size_t)s->g.n * sizeof(float4), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(s, e, "wall read-back");
     return BFX_OK;
 }
 
@@ -1240,11 +1247,13 @@ int bfx_copy_links(bfx_sim* s, uint32_t* cell, uint8_t* direction, float* fracti
     if (capacity < n) return fail(s, BFX_ERR_CAPACITY, "link buffers smaller than the link count");
     if (n == 0) return BFX_OK;
     std::vector<uint32_t> meta(n);
-    if (cell) cudaMemcpy(cell, s->link_cell, n * sizeof(uint32_t), cudaMemcpyDeviceToHost);
-    cudaMemcpy(meta.data(), s->link_meta, n * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    cudaError_t e = cudaSuccess;
+    if (cell) e = cudaMemcpy(cell, s->link_cell, n * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(meta.data(), s->link_meta, n * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && fraction) e = cudaMemcpy(fraction, s->link_q, n * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(s, e, "link read-back");
     if (direction)
         for (size_t i = 0; i < n; ++i) direction[i] = (uint8_t)(meta[i] & 0xFF);
-    if (fraction) cudaMemcpy(fraction, s->link_q, n * sizeof(float), cudaMemcpyDeviceToHost);
     return BFX_OK;
 }
 
@@ -1256,7 +1265,8 @@ int bfx_fluid_mass_momentum(bfx_sim* s, double out[4]) {
     s->launches += 2;
     int rc = sync_check(s, "mass/momentum");
     if (rc != BFX_OK) return rc;
-    cudaMemcpy(out, s->mm_result, 4 * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaError_t e = cudaMemcpy(out, s->mm_result, 4 * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(s, e, "mass/momentum read-back");
     return BFX_OK;
 }
 
@@ -1328,6 +1338,9 @@ int bfx_restore_state(bfx_sim* s, const void* buf, size_t size) {
     if (std::memcmp(h.magic, "BFXSTATE", 8) != 0 || h.version != 1 || h.storage != (uint32_t)s->cfg.storage ||
         h.nx != s->cfg.nx || h.ny != s->cfg.ny || h.nz != s->cfg.nz || h.geometry != (uint32_t)s->cfg.geometry)
         return fail(s, BFX_ERR_INVALID_ARGUMENT, "state header does not match this simulation");
+    // the representation and the mask index select device buffers: only 0 and 1 exist
+    if ((h.rep_s != 0 && h.rep_s != 1) || (h.cur != 0 && h.cur != 1))
+        return fail(s, BFX_ERR_INVALID_ARGUMENT, "state header holds an invalid representation or mask index");
     uint64_t sum;
     std::memcpy(&sum, (const char*)buf + need - sizeof(uint64_t), sizeof(sum));
     if (sum != fnv1a(buf, need - sizeof(uint64_t))) return fail(s, BFX_ERR_INVALID_ARGUMENT, "state checksum mismatch");
@@ -1335,17 +1348,19 @@ int bfx_restore_state(bfx_sim* s, const void* buf, size_t size) {
     const int synced = sync_check(s, "restore state");
     if (synced != BFX_OK) return synced;
     const char* p = (const char*)buf + sizeof(h);
-    cudaMemcpy(s->dstate, p, sizeof(DeviceState), cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpy(s->dstate, p, sizeof(DeviceState), cudaMemcpyHostToDevice);
     p += sizeof(DeviceState);
-    cudaMemcpy(s->pops, p, (size_t)19 * s->g.padded * s->elem, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(s->pops, p, (size_t)19 * s->g.padded * s->elem, cudaMemcpyHostToDevice);
     p += (size_t)19 * s->g.padded * s->elem;
     if (s->geometry()) {
-        cudaMemcpy(s->mask[0], p, (size_t)s->g.n, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(s->mask[0], p, (size_t)s->g.n, cudaMemcpyHostToDevice);
         p += s->g.n;
-        cudaMemcpy(s->mask[1], p, (size_t)s->g.n, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(s->mask[1], p, (size_t)s->g.n, cudaMemcpyHostToDevice);
         p += s->g.n;
-        cudaMemcpy(s->wall, p, (size_t)s->g.n * sizeof(float4), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(s->wall, p, (size_t)s->g.n * sizeof(float4), cudaMemcpyHostToDevice);
     }
+    // a partial restore leaves no usable state
+    if (e != cudaSuccess) return cuda_fail(s, e, "restore state upload");
     s->rep_s = h.rep_s;
     s->cur = h.cur;
     if (s->geometry() && !s->moving()) {
@@ -1718,8 +1733,9 @@ int bfx_adjoint(bfx_sim* s, uint64_t steps, const bfx_adjoint_objective* objecti
     rc = sync_check(s, "adjoint forward pass");
     if (rc != BFX_OK) return rc;
     DeviceState st_end;
-    cudaMemcpy(&st_end, s->dstate, sizeof(st_end), cudaMemcpyDeviceToHost);
-    cudaMemcpy(&ob, s->dobjective, sizeof(ob), cudaMemcpyDeviceToHost);
+    cudaError_t ce = cudaMemcpy(&st_end, s->dstate, sizeof(st_end), cudaMemcpyDeviceToHost);
+    if (ce == cudaSuccess) ce = cudaMemcpy(&ob, s->dobjective, sizeof(ob), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) return cuda_fail(s, ce, "adjoint forward read-back");
     if (st_end.link_overflow) return fail(s, BFX_ERR_KERNEL, "the cut-link list exceeded its capacity; raise link_capacity");
     const uint64_t link_slots = (uint64_t)std::max<int64_t>(1, std::min<int64_t>(ob.max_links, s->link_capacity));
 
@@ -1821,7 +1837,8 @@ int bfx_adjoint(bfx_sim* s, uint64_t steps, const bfx_adjoint_objective* objecti
     restore(nseg);
     rc = sync_check(s, "adjoint reverse pass");
     if (rc != BFX_OK) return rc;
-    cudaMemcpy(&ob, s->dobjective, sizeof(ob), cudaMemcpyDeviceToHost);
+    ce = cudaMemcpy(&ob, s->dobjective, sizeof(ob), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) return cuda_fail(s, ce, "adjoint gradient read-back");
     s->step = st_end.step;
     float f_ms = 0.0f, r_ms = 0.0f;
     cudaEventElapsedTime(&f_ms, ev[0], ev[1]);

@@ -1,11 +1,12 @@
 // FP64 fluid mass / momentum reduction that allocates no device memory.
 //
 // Some callers cannot call cudaMalloc at the point where they need this sum:
-// code running while a CUDA graph is being captured (allocation is not a
-// capturable operation), real-time loops that must not touch the allocator,
-// and processes where another allocator (for example a framework's caching
-// pool) already owns the device memory budget.  They hold the population
-// field and an output slot already; this entry point needs nothing else.
+// applications whose device memory budget is already reserved by their own
+// allocator (for example a framework's caching pool), where a fresh
+// allocation fails or fragments that pool, and loops with a fixed time budget
+// per iteration, where cudaMalloc / cudaFree would synchronise the device.
+// They hold the dense FP32 population field and an output slot already; this
+// entry point needs nothing else.
 //
 // Its scratch (the per-group partial sums) lives in one file-scope device
 // array of fixed size, 32,768 groups x 4 doubles = 1 MiB.  Every GPU that loads
@@ -96,7 +97,8 @@ double* g_scratch_address[kMaxDevices] = {};
 
 // Device address of the scratch array on the current device.  The array's
 // name is only a host-side stand-in, so the address is resolved once per
-// device with that device current and cached.
+// device with that device current and cached.  The cached address belongs to
+// the context that was current at the first call on the device.
 int scratch_address(int device, double** out) {
     std::lock_guard<std::mutex> lock(g_mutex);
     if (!g_scratch_address[device]) {

@@ -61,7 +61,10 @@ def populations_after(ref, resolution: int, steps: int, viscosity: float, amplit
 
 
 def main() -> int:
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("BFX_REFERENCE_ROOT")
+    if not root:
+        print("usage: make_golden.py <reference checkout root> (or set BFX_REFERENCE_ROOT)", file=sys.stderr)
+        return 2
     ref = load_reference(root)
     pops = populations_after(ref, 12, 8, 0.03, 0.01)
     np.savez_compressed(os.path.join(HERE, "shear_wave_ref_n12_s8.npz"), populations=pops,

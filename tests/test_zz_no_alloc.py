@@ -1,11 +1,12 @@
 """The allocation-free mass/momentum entry point against the allocating one.
 
 bfx_fluid_mass_momentum_noalloc serves callers that cannot allocate device
-memory when they need the global fluid mass and momentum (for example while a
-CUDA graph is being captured).  Here the test itself allocates the device
-input and output with torch, calls the entry point through the C ABI twice in
-a row on a lattice with solid cells, and compares each result with
-bfx_fluid_mass_momentum on the same state.  Both are FP64 sums of the same
+memory when they need the global fluid mass and momentum (an application
+whose device memory is reserved by its own allocator, or a loop that must not
+stall on cudaMalloc's device synchronisation).  Here the test itself
+allocates the device input and output with torch, calls the entry point
+through the C ABI twice in a row on a lattice with solid cells, and compares
+each result with bfx_fluid_mass_momentum on the same state.  Both are FP64 sums of the same
 FP32 values in different orders, so they agree to 1e-12 relative (the
 tolerance of the other FP64 reduction tests).  This file is collected last.
 """
