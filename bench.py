@@ -1,23 +1,27 @@
 #!/usr/bin/env python3
 """Benchmark of the D3Q19 moving-boundary step (GLUPS and fraction of the HBM roofline).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--storage S] [--impl ours|reference]
 
 One JSON line on rank 0.  A "step" is one lattice-Boltzmann time step of the
 whole workload (geometry, links, bounce-back, loads, fused stream+collide,
-body update).  ``value`` is device-timed (CUDA events on the library's stream)
-with the populations resident in HBM; ``e2e`` runs the same steps through the
-C ABI one call at a time with the body state written from pinned host memory
-and the step's loads read back every step.  ``roofline`` uses the fused
+body update).  The default is the workload the metric is quoted on: the
+flapping wing pair at 512x256x256 with FP16-deviation population storage.
+``value`` is device-timed (CUDA events on the library's stream) with the
+populations resident in HBM; ``e2e`` runs the same steps through the C ABI one
+call at a time with the body state written from pinned host memory and the
+step's loads read back every step.  ``roofline`` uses the fused
 stream+collide kernel's own CUDA-event launch times and its algorithmic
-traffic of 38 * s bytes per cell (19 reads + 19 writes of s-byte populations).
+traffic of 38 * s bytes per fluid cell (19 reads + 19 writes of s-byte
+populations); ``roofline.step_frac`` divides the same bytes by the whole step.
 
 Workloads (lattice units):
+  flapping_plates    512x256x256, two 64x12x2 plates as 2x8192 triangles,
+                     stroke 60 sin, pitch 45 cos, T = 4000, nu 0.004, TRT,
+                     ray-root links rebuilt every step (default)
   ellipsoid_channel  256x128x128, ellipsoid (24,12,12) at x=64, inflow 0.05,
                      nu 0.005, RR3, interpolated links, velocity inlet /
-                     zero-gradient outlet / periodic y,z (default)
-  flapping_plates    512x256x256, two 64x12x2 plates as 2x8192 triangles,
-                     stroke 60 sin, pitch 45 cos, T = 4000, nu 0.004, TRT
+                     zero-gradient outlet / periodic y,z
   articulated_bird   768x384x384, ellipsoid body + tail + two 3-segment wings
                      (~145k triangles), free flight, RR3
   shear_wave         64^3 periodic, nu 0.01, magic 1/4 (L2-resident)
@@ -26,10 +30,14 @@ independent replicas; ``value`` is the aggregate and ``scaling`` is weak.
 
 On one GPU the line also carries
   ``variants``  FP32 / FP16-deviation / BF16-deviation storage on the flapping
-                plates (512x256x256, TRT): GLUPS, roofline fraction, and the
-                force averaged over the first stroke period against FP64;
+                plates (512x256x256, TRT): GLUPS, the kernel's and the whole
+                step's roofline fractions, and the force averaged over the
+                third stroke period of a three-period run against FP64;
+  ``precision_form``  the metric's own figures from ``variants``: FP16 step
+                speed-up over FP32, roofline fractions, force error vs FP64;
   ``articulated``  the articulated bird at 768x384x384 in FP16-deviation
                 storage: GLUPS and the share of the step outside the fused kernel;
+  ``ellipsoid_channel``  the RR3 channel at 256x128x128 in FP32;
   ``adjoint``   the discrete adjoint on the plates at 256x128x128 over one
                 period: lift and power gradients, cost against a forward pass,
                 central differences (h = 1e-3 rad) and FP32 vs FP64 gradients
@@ -52,7 +60,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "numi-gpu-physics_b200"))
 
 FALLBACK_HBM_GBS = 6650.0
-WORKLOAD_DEFAULT = "ellipsoid_channel"
+WORKLOAD_DEFAULT = "flapping_plates"
+STORAGE_DEFAULT = "f16dev"
+METRIC = "D3Q19 GLUPS & %HBM peak, FP16-store vs FP32 at stated force error; adjoint/fwd"
 
 
 LATTICE_OVERRIDE = None  # (nx, ny, nz) for small profiling cases; geometry scales with it
@@ -132,57 +142,112 @@ def make_lattice(name, storage, device):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons of this process's GPU,
+    polled read-only through NVML every ~2 ms on a background thread (a
+    100 ms nvidia-smi loop cannot see a timed region of a few milliseconds).
+    `region()` brackets the timed region; the summary reports the samples
+    inside it, or, when the region was shorter than one poll, every sample
+    taken while the bench's GPU work ran.  Falls back to nvidia-smi when NVML
+    is unavailable."""
 
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device: int):
         self.device = device
-        self.proc = None
-        self.lines = []
+        self.samples = []  # (host time, sm MHz, set of reason names)
+        self.max_mhz = None
+        self.windows = []
+        self._stop = threading.Event()
+        self._thread = None
+        self._proc = None
+        self.source = None
 
-    def __enter__(self):
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
-                 "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except (OSError, FileNotFoundError):
-            self.proc = None
-        return self
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.device).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.device)
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
-    def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
+    def _poll_nvml(self, nv, h):
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        while not self._stop.is_set():
             try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+                mhz = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                r = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+                self.samples.append((time.perf_counter(), mhz, {k for k, b in bits.items() if r & b}))
+            except Exception:
+                return
+            self._stop.wait(0.002)
 
-    def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+    def _read_smi(self):
+        for ln in self._proc.stdout:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
             try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
+                mhz, self.max_mhz = float(parts[1]), float(parts[2])
             except ValueError:
                 continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+            self.samples.append((time.perf_counter(), mhz,
+                                 {nm for nm, v in zip(self.NAMES, parts[5:9]) if v.lower() == "active"}))
+
+    def __enter__(self):
+        try:
+            nv, h = self._nvml_handle()
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self._thread = threading.Thread(target=self._poll_nvml, args=(nv, h), daemon=True)
+            self.source = "nvml 2 ms"
+        except Exception:
+            try:
+                self._proc = subprocess.Popen(
+                    ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
+                     "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self._thread = threading.Thread(target=self._read_smi, daemon=True)
+                self.source = "nvidia-smi 100 ms"
+            except OSError:
+                return self
+        self._thread.start()
+        return self
+
+    def region(self):
+        sampler = self
+
+        class _Region:
+            def __enter__(self):
+                self.t0 = time.perf_counter()
+
+            def __exit__(self, *exc):
+                sampler.windows.append((self.t0, time.perf_counter()))
+        return _Region()
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._proc is not None:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self._proc.kill()
+        if self._thread is not None:
+            self._thread.join(timeout=5)
+
+    def summary(self):
+        inside = [s for s in self.samples if any(a <= s[0] <= b for a, b in self.windows)]
+        use = inside or self.samples
+        sm = [s[1] for s in use]
+        reasons = sorted(set().union(*[s[2] for s in use])) if use else []
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(use), "samples_in_timed_region": len(inside), "source": self.source}
 
 
 def measured_peak():
@@ -208,16 +273,23 @@ def profiled_traffic(workload: str, storage_name: str):
     return None
 
 
-def time_steps(lat, steps, warmup):
+def time_steps(lat, steps, warmup, clocks=None):
     """Device time of `steps` steps (CUDA events on the library stream), then the
     fused interior kernel's own per-launch CUDA-event times over a second run of
     the same steps (per-launch events disable the step graphs, so they are kept
-    out of the whole-step timing)."""
+    out of the whole-step timing).  `clocks` (a ClockSampler) marks the timed
+    region."""
     lat.advance(warmup, batch_size=max(warmup, 1))
     l0 = lat.launch_count()
-    lat.timer_begin()
-    lat.advance(steps, batch_size=steps)
-    ms = lat.timer_end()
+    if clocks is not None:
+        with clocks.region():
+            lat.timer_begin()
+            lat.advance(steps, batch_size=steps)
+            ms = lat.timer_end()
+    else:
+        lat.timer_begin()
+        lat.advance(steps, batch_size=steps)
+        ms = lat.timer_end()
     l1 = lat.launch_count()
     lat.set_kernel_timing(True)
     lat.advance(min(steps, 400), batch_size=min(steps, 400))
@@ -261,17 +333,23 @@ def force_history(name, storage, steps, device):
     return f
 
 
-def storage_forms(device, steps=200, warmup=5):
+def storage_forms(device, steps=200, warmup=5, periods=3):
     """FP32 / FP16-deviation / BF16-deviation on the flapping-plate workload
-    (512x256x256, TRT, links rebuilt every step): throughput, fraction of the
-    HBM roofline of the fused kernel, and the force averaged over the first
-    stroke period (4000 steps) against an FP64 run of the same kernels."""
+    (512x256x256, TRT, links rebuilt every step): whole-step throughput, the
+    fused kernel's and the whole step's fractions of the HBM roofline, and the
+    force averaged over the last stroke period of a `periods`-period run
+    (steps 8001-12000 for three periods of T = 4000) against an FP64 run of
+    the same kernels."""
     import bfx._lib as L
     peak, _ = measured_peak()
     period = 4000
-    ref = force_history("flapping_plates", L.STORAGE_F64, period, device).mean(axis=0)
+    total = periods * period
+    window = (total - period, total)  # 0-based slice: steps total-period+1 ... total
+    ref_hist = force_history("flapping_plates", L.STORAGE_F64, total, device)
+    ref = ref_hist[window[0]:window[1]].mean(axis=0)
     out = {"workload": "flapping_plates 512x256x256 TRT, stroke 60 deg, pitch 45 deg, T=4000",
-           "force_window_steps": [1, period], "force_reference": "FP64 storage, same kernels"}
+           "force_window_steps": [window[0] + 1, window[1]], "periods_run": periods,
+           "force_reference": "FP64 storage, same kernels", "force_reference_value_N": ref.tolist()}
     base = None
     for st in (L.STORAGE_F32, L.STORAGE_F16_DEVIATION, L.STORAGE_BF16_DEVIATION):
         nm = L.STORAGE_NAMES[st]
@@ -283,36 +361,47 @@ def storage_forms(device, steps=200, warmup=5):
         rate = cells * steps / (vms / 1000.0) / 1e9
         kernel_s = vkms / max(vkl, 1) / 1000.0
         ach = fluid * 38 * L.STORAGE_BYTES[st] / kernel_s / 1e9
-        f = force_history("flapping_plates", st, period, device).mean(axis=0)
+        step_s = vms / steps / 1000.0
+        hist = force_history("flapping_plates", st, total, device)
+        f = hist[window[0]:window[1]].mean(axis=0)
         err = float(np.linalg.norm(f - ref) / max(np.linalg.norm(ref), 1e-30))
         base = rate if base is None else base
-        out[nm] = {"value": rate, "unit": "GLUPS", "kernel_ms": kernel_s * 1000.0, "achieved_gbs": ach,
-                   "roofline_frac": ach / peak, "speedup_vs_f32": rate / base,
-                   "cycle_mean_force_error_vs_f64": err}
+        out[nm] = {"value": rate, "unit": "GLUPS", "ms_per_step": step_s * 1000.0, "kernel_ms": kernel_s * 1000.0,
+                   "achieved_gbs": ach, "roofline_frac": ach / peak,
+                   "step_roofline_frac": fluid * 38 * L.STORAGE_BYTES[st] / step_s / 1e9 / peak,
+                   "speedup_vs_f32": rate / base, "cycle_mean_force_error_vs_f64": err,
+                   "cycle_mean_force_N": f.tolist()}
     return out
 
 
-def articulated_measure(device, steps=100, warmup=5):
-    """The articulated bird (768x384x384, RR3, FP16-deviation storage, free
-    6-DOF flight, ~145k triangles on shoulder / elbow / wrist segments):
-    whole-step GLUPS, the fused kernel's roofline fraction and the share of the
-    step spent outside it (geometry, links, loads, body)."""
+def workload_measure(name, storage, device, steps=100, warmup=5):
+    """Whole-step GLUPS of one workload in one storage form, the fused
+    kernel's roofline fraction and the share of the step spent outside it
+    (geometry, links, loads, body)."""
     import bfx._lib as L
     peak, _ = measured_peak()
-    st = L.STORAGE_F16_DEVIATION
-    lat, cfg, desc, _ = make_lattice("articulated_bird", st, device)
+    lat, cfg, desc, coll = make_lattice(name, storage, device)
     cells = cfg.nx * cfg.ny * cfg.nz
     ms, launches, kms, kl = time_steps(lat, steps, warmup)
     fluid = cells - int(np.count_nonzero(lat.mask()))
     body = lat.body()
     lat.close()
     kernel_s = kms / max(kl, 1) / 1000.0
-    ach = fluid * 38 * L.STORAGE_BYTES[st] / kernel_s / 1e9
+    ach = fluid * 38 * L.STORAGE_BYTES[storage] / kernel_s / 1e9
     step_ms = ms / steps
-    return {"workload": desc, "storage": L.STORAGE_NAMES[st], "steps": steps, "value": cells * steps / (ms / 1e3) / 1e9,
-            "unit": "GLUPS", "ms_per_step": step_ms, "kernel_ms": kernel_s * 1e3, "achieved_gbs": ach,
-            "roofline_frac": ach / peak, "outside_kernel_share": max(0.0, 1.0 - kernel_s * 1e3 / step_ms),
-            "gpu_launches": launches, "body_position_after": [float(x) for x in body.position]}
+    return {"workload": desc, "collision": coll, "storage": L.STORAGE_NAMES[storage], "steps": steps,
+            "value": cells * steps / (ms / 1e3) / 1e9, "unit": "GLUPS", "ms_per_step": step_ms,
+            "kernel_ms": kernel_s * 1e3, "achieved_gbs": ach, "roofline_frac": ach / peak,
+            "step_roofline_frac": fluid * 38 * L.STORAGE_BYTES[storage] / (step_ms / 1e3) / 1e9 / peak,
+            "outside_kernel_share": max(0.0, 1.0 - kernel_s * 1e3 / step_ms), "gpu_launches": launches,
+            "body_position_after": [float(x) for x in body.position]}
+
+
+def articulated_measure(device, steps=100, warmup=5):
+    """The articulated bird (768x384x384, RR3, FP16-deviation storage, free
+    6-DOF flight, ~145k triangles on shoulder / elbow / wrist segments)."""
+    import bfx._lib as L
+    return workload_measure("articulated_bird", L.STORAGE_F16_DEVIATION, device, steps, warmup)
 
 
 def adjoint_measure(device):
@@ -436,6 +525,16 @@ def cpu_port_rate(name, seconds_budget=12.0, max_steps=64, warmup=1, warmup_budg
     return cells * steps / dt / 1e9, steps, threads, dt, warm
 
 
+def bench_config(desc, cfg, coll, world):
+    """The `config` object both arms print (the same workload, so the same keys)."""
+    cells = cfg.nx * cfg.ny * cfg.nz
+    return {"workload": desc, "lattice": [cfg.nx, cfg.ny, cfg.nz], "collision": coll,
+            "l2": (f"inputs larger than L2 ({19 * cells * 2 / 1e6:.0f} MB of populations at 2 B, "
+                   f"{19 * cells * 4 / 1e6:.0f} MB at 4 B; no flush needed)") if 19 * cells * 2 > 126e6
+            else "L2-resident working set",
+            "parallelism": f"replicas{world}"}
+
+
 def run_reference_arm(args, rank, world):
     name = args.workload
     if rank != 0:
@@ -447,13 +546,14 @@ def run_reference_arm(args, rank, world):
                                                  max_steps=max(1, args.steps), warmup=args.warmup)
     cells = cfg.nx * cfg.ny * cfg.nz
     line = {
-        "impl": "reference", "metric": "D3Q19 GLUPS", "value": rate, "unit": "GLUPS", "n_gpus": world,
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": "GLUPS", "n_gpus": world,
         "steps": steps, "warmup": warm, "ms_per_step": dt * 1000.0 / max(steps, 1), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": desc, "lattice": [cfg.nx, cfg.ny, cfg.nz], "collision": coll, "storage": "f32"},
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "storage": "f32", "data": "synthetic",
+        "config": bench_config(desc, cfg, coll, world),
         "cpu_baseline": {"value": rate, "unit": "GLUPS", "cores": cores, "kind": "port",
                          "sample": f"{steps} full steps of the {name} workload ({cells} cells) on the CPU "
-                                   f"restatement of the reference step (oracle/, C + OpenMP)"},
+                                   f"restatement of the reference step (oracle/, C + OpenMP, FP32 populations: "
+                                   f"the reference has no 16-bit storage)"},
         "e2e": {"value": rate, "unit": "GLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -463,8 +563,8 @@ def run_reference_arm(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--workload", default=WORKLOAD_DEFAULT)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-variants", action="store_true")
@@ -472,7 +572,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--lattice", type=int, nargs=3, default=None, help="profiling override of the lattice size")
     ap.add_argument("--collision", default=None, choices=["trt", "rr3", "reg", "limiter"])
-    ap.add_argument("--storage", default="f32", choices=["f32", "f16dev", "bf16dev", "f64"])
+    ap.add_argument("--storage", default=STORAGE_DEFAULT, choices=["f32", "f16dev", "bf16dev", "f64"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     global LATTICE_OVERRIDE, COLLISION_OVERRIDE
@@ -511,7 +611,7 @@ def main():
 
     barrier()
     with ClockSampler(local) as clocks:
-        ms, launches, kms, klaunch = time_steps(lat, args.steps, args.warmup)
+        ms, launches, kms, klaunch = time_steps(lat, args.steps, args.warmup, clocks)
     barrier()
     if dist is not None:
         import torch
@@ -536,22 +636,21 @@ def main():
     kernel_s = kms / max(klaunch, 1) / 1000.0
     achieved = bytes_per_launch / kernel_s / 1e9
     traffic = profiled_traffic(args.workload, args.storage)
+    staged = coll in ("trt", "rr3", "reg") and args.storage in ("f16dev", "bf16dev")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "peak_kind": f"of {peak_kind}",
-                "kernel": ("k_stream (TMA-staged fused AA stream+collide, 16-bit storage)"
-                           if coll in ("trt", "rr3", "reg") and args.storage in ("f16dev", "bf16dev")
+                "kernel": ("k_stream (TMA-staged fused AA stream+collide, 16-bit storage)" if staged
                            else "k_bulk (fused AA stream+collide over every fluid cell)"),
                 "bytes_per_launch": bytes_per_launch, "bytes_rule": "fluid cells x 19 x 2 x storage bytes",
-                "kernel_ms": kernel_s * 1000.0}
+                "kernel_ms": kernel_s * 1000.0,
+                "step_frac": bytes_per_launch / (ms / args.steps / 1000.0) / 1e9 / peak}
 
     line = {
-        "metric": "D3Q19 GLUPS", "value": value, "unit": "GLUPS", "n_gpus": world, "steps": args.steps,
+        "metric": METRIC, "value": value, "unit": "GLUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": desc, "lattice": [cfg.nx, cfg.ny, cfg.nz], "collision": coll, "storage": args.storage,
-                   "l2": f"inputs larger than L2 ({19 * cells * sbytes / 1e6:.1f} MB of populations)"
-                   if 19 * cells * sbytes > 126e6 else "L2-resident working set",
-                   "parallelism": f"replicas{world}"},
+        "vs_baseline": None, "dtype": "f32" if main_storage != L.STORAGE_F64 else "f64",
+        "storage": args.storage, "data": "synthetic",
+        "config": bench_config(desc, cfg, coll, world),
         "e2e": {"value": e2e_value, "unit": "GLUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": e2e_n, "calls": "bfx_set_body + bfx_advance(1) + bfx_last_loads per step"},
         "roofline": roofline,
@@ -560,9 +659,19 @@ def main():
     }
 
     if rank == 0 and world == 1 and not args.no_variants:
-        line["variants"] = storage_forms(local)
-    if rank == 0 and world == 1 and not args.no_variants:
+        v = storage_forms(local)
+        line["variants"] = v
+        if args.workload == "flapping_plates":
+            line["precision_form"] = {
+                "f16dev_step_speedup_vs_f32": v["f16dev"]["speedup_vs_f32"],
+                "bf16dev_step_speedup_vs_f32": v["bf16dev"]["speedup_vs_f32"],
+                "f16dev_kernel_roofline_frac": v["f16dev"]["roofline_frac"],
+                "f16dev_step_roofline_frac": v["f16dev"]["step_roofline_frac"],
+                "f16dev_cycle_mean_force_error_vs_f64": v["f16dev"]["cycle_mean_force_error_vs_f64"],
+                "bf16dev_cycle_mean_force_error_vs_f64": v["bf16dev"]["cycle_mean_force_error_vs_f64"],
+                "force_window_steps": v["force_window_steps"]}
         line["articulated"] = articulated_measure(local)
+        line["ellipsoid_channel"] = workload_measure("ellipsoid_channel", L.STORAGE_F32, local)
     if rank == 0 and world == 1 and not args.no_adjoint:
         line["adjoint"] = adjoint_measure(local)
 
@@ -570,7 +679,7 @@ def main():
         rate, steps, cores, dt, _ = cpu_port_rate(args.workload)
         line["cpu_baseline"] = {"value": rate, "unit": "GLUPS", "cores": cores, "kind": "port",
                                 "sample": f"{steps} full steps of the same workload on the CPU restatement "
-                                          f"(oracle/, C + OpenMP, {dt:.1f} s)"}
+                                          f"(oracle/, C + OpenMP, FP32 populations, {dt:.1f} s)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

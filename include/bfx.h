@@ -31,8 +31,10 @@ extern "C" {
 #endif
 
 /* 2: bfx_mesh keyframe fields, bfx_advance_result.dropped_field_frames,
- * field observation and flow-diagnostics entry points. */
-#define BFX_ABI_VERSION 2
+ * field observation and flow-diagnostics entry points.
+ * 3: the prescribed flapping wing (BFX_GEOMETRY_FLAPPING_WING,
+ * bfx_flapping_wing, bfx_create_flapping_wing). */
+#define BFX_ABI_VERSION 3
 
 #if defined(__GNUC__)
 #define BFX_API __attribute__((visibility("default")))
@@ -97,7 +99,9 @@ typedef enum bfx_geometry_kind {
     BFX_GEOMETRY_NONE = 0,       /* all fluid */
     BFX_GEOMETRY_BIRD = 1,       /* analytic bird: ellipsoid body, tapered wings, tail (BF.metal:816-938) */
     BFX_GEOMETRY_ELLIPSOID = 2,  /* body ellipsoid alone, link fractions by bisection (BF.metal:1144-1175 rule) */
-    BFX_GEOMETRY_MESH = 3        /* articulated triangle mesh (BF.metal:1638-2076) */
+    BFX_GEOMETRY_MESH = 3,       /* articulated triangle mesh (BF.metal:1638-2076) */
+    BFX_GEOMETRY_FLAPPING_WING = 4 /* prescribed Li-Nabawy beta-planform wing, link fractions by
+                                      10-step bisection (BF.metal:940-1297); see bfx_create_flapping_wing */
 } bfx_geometry_kind;
 
 /* Link fraction rule for mesh geometry. */
@@ -172,6 +176,28 @@ typedef struct bfx_bird {
     bfx_float4 right_wing_mass_com;
     bfx_float4 right_wing_inertia;
 } bfx_bird;
+
+/* GPUFlappingWingParameters (Sources/BirdFlowMetal/GPUData.swift:383-388): the
+ * analytic single wing of MetalFlappingWingValidation (Li and Nabawy's
+ * beta-planform benchmark).  Lengths in metres, as the world coordinates; the
+ * reference runs this wing with a 1 m cell, i.e. in lattice units
+ * (MetalFlappingWingValidation.swift:3333-3367), and the wall velocity is the
+ * wing's rotation rate (rad per step) times the distance from the root divided
+ * by the cell size.  Angles in radians; the stroke rotates about the world z
+ * axis through the root.
+ *   root_and_chord  root position xyz (m), mean chord c
+ *   geometry        radius R (span), thickness, beta shape - 1, beta normalisation
+ *                   (local chord = c * geometry.w * (r (1 - r))^geometry.z at r = radial / R)
+ *   kinematics0     cycle steps, stroke half amplitude, stroke acceleration duration,
+ *                   pitch flip duration (the durations as cycle fractions, below 1/2)
+ *   kinematics1     pitch angle low, pitch angle high, maximum stroke rate (rad per cycle),
+ *                   reference speed (unused by the geometry) */
+typedef struct bfx_flapping_wing {
+    bfx_float4 root_and_chord;
+    bfx_float4 geometry;
+    bfx_float4 kinematics0;
+    bfx_float4 kinematics1;
+} bfx_flapping_wing;
 
 /* BirdBodyState (Sources/BirdFlowCore/BirdModel.swift:53-68), FP64. */
 typedef struct bfx_body_state {
@@ -323,6 +349,11 @@ BFX_API int bfx_device_count(int* count);
 BFX_API int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_state* body,
                const bfx_mesh* mesh, bfx_sim** out);
 BFX_API void bfx_destroy(bfx_sim* sim);
+/* MetalFlappingWingValidator's prescribed-wing setup (MetalFlappingWingValidation.swift:3312-3600:
+ * preparePrescribedFlappingWing + buildPrescribedFlappingWing around stepFluidTRT).  config->geometry
+ * must be BFX_GEOMETRY_FLAPPING_WING and free_flight 0; the body sits at the wing root (loads and
+ * torques about it).  Each step t (1, 2, ...) builds the wing at the phase of t / cycle steps. */
+BFX_API int bfx_create_flapping_wing(const bfx_config* config, const bfx_flapping_wing* wing, bfx_sim** out);
 
 /* advance(steps:batchSize:fieldCapture:recordRunSamples:) (BirdFlowSimulation.swift:688-799).
  * samples may be NULL unless BFX_ADVANCE_RECORD_SAMPLES is set (capacity >= steps). */

@@ -24,7 +24,7 @@ COLLISION_TRT, COLLISION_TRT_LIMITER, COLLISION_REGULARIZED, COLLISION_RR3 = 0, 
 WALL_HALFWAY, WALL_INTERPOLATED = 0, 1
 STORAGE_F32, STORAGE_F16_DEVIATION, STORAGE_BF16_DEVIATION, STORAGE_F64 = 0, 1, 2, 3
 BC_FARFIELD, BC_PERIODIC, BC_VELOCITY, BC_OUTFLOW = 0, 1, 2, 3
-GEOMETRY_NONE, GEOMETRY_BIRD, GEOMETRY_ELLIPSOID, GEOMETRY_MESH = 0, 1, 2, 3
+GEOMETRY_NONE, GEOMETRY_BIRD, GEOMETRY_ELLIPSOID, GEOMETRY_MESH, GEOMETRY_FLAPPING_WING = 0, 1, 2, 3, 4
 LINK_LINEAR, LINK_RAY_ROOT = 0, 1
 INIT_EQUILIBRIUM, INIT_SHEAR_WAVE_Y, INIT_SHEAR_WAVE_Z = 0, 1, 2
 ADVANCE_CAPTURE_FIELDS, ADVANCE_RECORD_SAMPLES, ADVANCE_CAPTURE_BEST_EFFORT = 1, 2, 4
@@ -68,6 +68,11 @@ BIRD_FIELDS = ("body_radii_mass", "inertia", "wing_geometry0", "wing_geometry1",
 
 class Bird(ct.Structure):
     _fields_ = [(name, Float4) for name in BIRD_FIELDS]
+
+
+class FlappingWing(ct.Structure):
+    """bfx_flapping_wing (GPUFlappingWingParameters, GPUData.swift:383-388)."""
+    _fields_ = [(name, Float4) for name in ("root_and_chord", "geometry", "kinematics0", "kinematics1")]
 
 
 class BodyState(ct.Structure):
@@ -166,7 +171,7 @@ EXPORTED = (
     "bfx_launch_count", "bfx_device_bytes", "bfx_fluid_mass_momentum_noalloc", "bfx_adjoint", "bfx_advance_ledger",
     "bfx_last_error", "bfx_set_observation_buffers", "bfx_acquire_field_frame", "bfx_field_frame_copy",
     "bfx_release_field_frame", "bfx_release_field_frame_after", "bfx_capture_current_fields",
-    "bfx_observation_counters", "bfx_flow_diagnostics",
+    "bfx_observation_counters", "bfx_flow_diagnostics", "bfx_create_flapping_wing",
 )
 
 _lib = None
@@ -191,6 +196,7 @@ def load(path: str | None = None):
     L.bfx_abi_version.restype = ct.c_int
     L.bfx_device_count.argtypes = [P(ct.c_int)]
     L.bfx_create.argtypes = [P(Config), P(Bird), P(BodyState), P(Mesh), P(vp)]
+    L.bfx_create_flapping_wing.argtypes = [P(Config), P(FlappingWing), P(vp)]
     L.bfx_destroy.argtypes = [vp]
     L.bfx_destroy.restype = None
     L.bfx_advance.argtypes = [vp, ct.c_uint64, ct.c_uint32, ct.c_uint32, P(RunSample), ct.c_size_t, P(AdvanceResult)]

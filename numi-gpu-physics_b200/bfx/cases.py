@@ -8,6 +8,8 @@ All sizes are in lattice units (dx = dt = 1) unless a case says otherwise.
   flapping_plates       two rectangular flat-plate wings as a triangle mesh,
                         stroke 60 deg sin, pitch 45 deg cos, links rebuilt each step
   compact_bird          the reference's compact analytic bird on 48^3
+  flapping_wing         the prescribed Li-Nabawy beta-planform wing of
+                        MetalFlappingWingValidation (analytic link fractions)
 """
 from __future__ import annotations
 
@@ -356,3 +358,47 @@ def articulated_bird(nx=768, ny=384, nz=384, storage=L.STORAGE_F16_DEVIATION, co
                          sponge_strength=0.05, free_flight=1 if free_flight else 0)
     body = ((nx * 0.4, ny / 2.0, nz / 2.0), (0.0, 0.0, 0.0, 1.0), (0.0, 0.0, 0.0), (0.0, 0.0, 0.0))
     return cfg, rows, body, mesh
+
+
+# Li and Nabawy's Re = 100 beta-planform baseline as MetalFlappingWingValidator
+# states it (Sources/BirdFlowMetal/MetalFlappingWingValidation.swift:535-566).
+LI_NABAWY = dict(reynolds=100.0, aspect_ratio=3.0, radius_of_gyration=0.5593218135819926,
+                 beta_shape=1.4891506583557845, beta_normalization=2.497931737168364,
+                 stroke_half_amplitude=80.0 * math.pi / 180.0, acceleration_duration=0.25, pitch_duration=0.25,
+                 pitch_low=45.0 * math.pi / 180.0, pitch_high=135.0 * math.pi / 180.0, lattice_speed=0.035,
+                 horizontal_chords=10, vertical_chords=8)
+
+
+def flapping_wing(chord=8, storage=L.STORAGE_F32, collision=L.COLLISION_TRT, cycle_steps=None, nx=None, ny=None,
+                  nz=None, viscosity=None):
+    """The validator's prescribed-wing simulation (MetalPrescribedWingSimulation,
+    MetalFlappingWingValidation.swift:3312-3600 with the batchDifference grid of
+    :3103-3125): a (10 c, 10 c, 8 c) lattice in lattice units, the root at
+    (0.5, 0.5, 0.65) of it, one cycle of round(4 A r_g AR c / U) steps, the
+    wing's radius AR c and thickness 0.05 c, Re 100 on the radius-of-gyration
+    speed U, a far-field sponge of max(4, c / 2) cells at strength 0.04,
+    interpolated links and the conservative moving-domain estimator (6).
+    ``viscosity`` overrides the Re = 100 value (tests run faster cycles at a
+    higher viscosity).  Returns (config, wing record)."""
+    p = LI_NABAWY
+    nx = nx or p["horizontal_chords"] * chord
+    ny = ny or p["horizontal_chords"] * chord
+    nz = nz or p["vertical_chords"] * chord
+    if cycle_steps is None:
+        travel = 4.0 * p["stroke_half_amplitude"] * p["radius_of_gyration"] * p["aspect_ratio"]
+        cycle_steps = int(round(travel * chord / p["lattice_speed"]))
+    if viscosity is None:
+        viscosity = p["lattice_speed"] * chord / p["reynolds"]
+    op, om = _trt_rates(viscosity, 3.0 / 16.0)
+    cfg = default_config(nx, ny, nz, omega_plus=op, omega_minus=om, geometry=L.GEOMETRY_FLAPPING_WING,
+                         wall_rule=L.WALL_INTERPOLATED, collision=collision, storage=storage,
+                         sponge_strength=0.04, sponge_width=float(max(4, chord // 2)))
+    max_rate = 2.0 * p["stroke_half_amplitude"] / (p["acceleration_duration"] +
+                                                   2.0 * p["acceleration_duration"] / math.pi)
+    w = L.FlappingWing()
+    w.root_and_chord.v[:] = [float(f32(0.5 * nx)), float(f32(0.5 * ny)), float(f32(0.65) * f32(nz)), float(chord)]
+    w.geometry.v[:] = [p["aspect_ratio"] * chord, 0.05 * chord, p["beta_shape"] - 1.0, p["beta_normalization"]]
+    w.kinematics0.v[:] = [float(cycle_steps), p["stroke_half_amplitude"], p["acceleration_duration"],
+                          p["pitch_duration"]]
+    w.kinematics1.v[:] = [p["pitch_low"], p["pitch_high"], max_rate, p["lattice_speed"]]
+    return cfg, w

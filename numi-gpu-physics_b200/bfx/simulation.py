@@ -192,12 +192,21 @@ class Lattice:
     """One simulation handle on the GPU (bfx_create / bfx_destroy)."""
 
     def __init__(self, config: L.Config, bird: L.Bird | None = None, body: L.BodyState | None = None,
-                 mesh: dict | None = None):
+                 mesh: dict | None = None, wing: L.FlappingWing | None = None):
+        """bird / body / mesh: bfx_create; wing (with geometry
+        GEOMETRY_FLAPPING_WING): bfx_create_flapping_wing, the prescribed wing of
+        MetalFlappingWingValidator held at its root."""
         self.lib = L.load()
         self.config = config
         self.bird = bird
+        self.wing = wing
         self.n = int(config.nx) * int(config.ny) * int(config.nz)
         self._mesh_keep = None
+        if wing is not None:
+            handle = ct.c_void_p()
+            _check(self.lib.bfx_create_flapping_wing(ct.byref(config), ct.byref(wing), ct.byref(handle)), None)
+            self.handle = handle
+            return
         mesh_ptr = None
         if mesh is not None:
             local = np.ascontiguousarray(mesh["local"], np.float32)

@@ -472,7 +472,7 @@ int validate_config(const bfx_config* c, const bfx_bird* bird, const bfx_mesh* m
     }
     if (c->collision < 0 || c->collision > 3) return fail(nullptr, BFX_ERR_INVALID_CONFIG, "unknown collision operator");
     if (c->storage < 0 || c->storage > 3) return fail(nullptr, BFX_ERR_INVALID_CONFIG, "unknown storage format");
-    if (c->geometry < 0 || c->geometry > 3) return fail(nullptr, BFX_ERR_INVALID_CONFIG, "unknown geometry kind");
+    if (c->geometry < 0 || c->geometry > 4) return fail(nullptr, BFX_ERR_INVALID_CONFIG, "unknown geometry kind");
     if (c->wall_rule < 0 || c->wall_rule > 1) return fail(nullptr, BFX_ERR_INVALID_CONFIG, "unknown wall rule");
     if (c->force_estimator < 0 || c->force_estimator > 6)
         return fail(nullptr, BFX_ERR_INVALID_CONFIG, "force estimator must be 0...6");
@@ -503,6 +503,8 @@ int validate_config(const bfx_config* c, const bfx_bird* bird, const bfx_mesh* m
         return fail(nullptr, BFX_ERR_INVALID_CONFIG, "measured keyframe kinematics are not supported");
     if (c->free_flight && c->static_geometry)
         return fail(nullptr, BFX_ERR_INVALID_CONFIG, "a free-flying body cannot be static geometry");
+    if (c->geometry == BFX_GEOMETRY_FLAPPING_WING && c->free_flight)
+        return fail(nullptr, BFX_ERR_INVALID_CONFIG, "the prescribed flapping wing is held at its root (no free flight)");
     if (mesh && mesh->triangles) {
         for (uint32_t i = 0; i < 3 * mesh->triangle_count; ++i)
             if (mesh->triangles[i] >= mesh->vertex_count)
@@ -553,6 +555,8 @@ float geometry_radius(const bfx_config* c, const bfx_bird* b, const bfx_mesh* m)
     const float* w1 = b->wing_geometry1.v;
     float body = std::sqrt(br[0] * br[0] + br[1] * br[1] + br[2] * br[2]);
     if (c->geometry == BFX_GEOMETRY_ELLIPSOID) return std::max(br[0], std::max(br[1], br[2])) + 2.0f * c->cell_size;
+    // the prescribed wing's bounding sphere about its root (buildPrescribedFlappingWing, BF.metal:1203-1206)
+    if (c->geometry == BFX_GEOMETRY_FLAPPING_WING) return w1[0] + 1.5f * w0[3] + 2.0f * c->cell_size;
     float root = std::sqrt(w1[1] * w1[1] + w1[2] * w1[2] + w1[3] * w1[3]);
     if (c->geometry == BFX_GEOMETRY_BIRD) {
         float tx = br[0] + tg[0], ty = std::max(br[1], tg[1]), tz = br[2] + 0.5f * tg[2];
@@ -875,6 +879,39 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
     s->slots->reset(field_frame_meta(s, st0, 0));
     *out = s;
     return BFX_OK;
+}
+
+int bfx_create_flapping_wing(const bfx_config* config, const bfx_flapping_wing* wing, bfx_sim** out) {
+    if (!config || !wing || !out) return fail(nullptr, BFX_ERR_INVALID_ARGUMENT, "config, wing and out must not be null");
+    *out = nullptr;
+    if (config->geometry != BFX_GEOMETRY_FLAPPING_WING)
+        return fail(nullptr, BFX_ERR_INVALID_CONFIG, "a flapping-wing simulation needs geometry BFX_GEOMETRY_FLAPPING_WING");
+    const float* rc = wing->root_and_chord.v;
+    const float* ge = wing->geometry.v;
+    const float* k0 = wing->kinematics0.v;
+    const float* k1 = wing->kinematics1.v;
+    for (int k = 0; k < 4; ++k)
+        if (!std::isfinite(rc[k]) || !std::isfinite(ge[k]) || !std::isfinite(k0[k]) || !std::isfinite(k1[k]))
+            return fail(nullptr, BFX_ERR_INVALID_CONFIG, "flapping-wing parameters must be finite");
+    if (!(rc[3] > 0.0f) || !(ge[0] > 0.0f) || !(ge[1] >= 0.0f) || !(ge[3] > 0.0f) || !(ge[2] > -1.0f))
+        return fail(nullptr, BFX_ERR_INVALID_CONFIG,
+                    "flapping wing: chord, radius and beta normalisation must be positive, thickness non-negative");
+    if (!(k0[0] >= 1.0f) || !(k0[2] > 0.0f && k0[2] < 0.5f) || !(k0[3] > 0.0f && k0[3] < 0.5f))
+        return fail(nullptr, BFX_ERR_INVALID_CONFIG,
+                    "flapping wing: cycle steps >= 1 and the stroke / pitch transition durations in (0, 1/2)");
+    // the wing record travels in the bird record's wing rows (see bfx_geometry.cu)
+    bfx_bird packed;
+    std::memset(&packed, 0, sizeof(packed));
+    packed.wing_geometry0 = wing->root_and_chord;
+    packed.wing_geometry1 = wing->geometry;
+    packed.wing_kinematics0 = wing->kinematics0;
+    packed.wing_kinematics1 = wing->kinematics1;
+    packed.wing_kinematics1.v[3] = 0.0f;  // reference speed: not part of the geometry
+    bfx_body_state body;
+    std::memset(&body, 0, sizeof(body));
+    for (int k = 0; k < 3; ++k) body.position[k] = rc[k];
+    body.orientation[3] = 1.0;
+    return bfx_create(config, &packed, &body, nullptr, out);
 }
 
 #define BFX_GUARD_READ(s)                                        \

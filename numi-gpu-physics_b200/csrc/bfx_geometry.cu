@@ -391,6 +391,215 @@ __global__ void k_classify_ellipsoid(const GeomArgs a, int has_prev) {
                                 (p.linear_velocity.z + cr.z) * a.fp.v2l, imp);
 }
 
+// ---------------------------------------------------------------------------
+// Prescribed flapping wing: the analytic Li-Nabawy beta-planform wing of
+// MetalFlappingWingValidation (BF.metal:940-1297).  The runtime packs the
+// bfx_flapping_wing record into the device bird record: root_and_chord in
+// wing_geometry0, geometry in wing_geometry1, kinematics0 / kinematics1 in
+// wing_kinematics0 / wing_kinematics1.  Its lengths are in cells (the
+// reference runs it in lattice units); the prepared frame sits in the left
+// wing slots of Prepared, the kinematic state (stroke, pitch and their rates
+// per step) in right_root.
+// ---------------------------------------------------------------------------
+struct WingRec {
+    const float* root_and_chord;
+    const float* geometry;
+    const float* k0;
+    const float* k1;
+};
+__device__ __forceinline__ WingRec wing_rec(const bfx_bird& b) {
+    return WingRec{b.wing_geometry0.v, b.wing_geometry1.v, b.wing_kinematics0.v, b.wing_kinematics1.v};
+}
+
+// prescribedStrokeKinematics: BF.metal:945-1001 (angle, rate per cycle)
+__device__ void wing_stroke(float phase, const WingRec& w, float& angle, float& rate) {
+    const float pi = 3.14159265358979323846f;
+    const float amplitude = w.k0[1], duration = w.k0[2], half = 0.5f * duration, max_rate = w.k1[2];
+    if (phase < half) {
+        const float arg = pi * (phase + half) / duration;
+        angle = amplitude + max_rate * duration / pi * (bfx_sinf(arg) - 1.0f);
+        rate = max_rate * bfx_cosf(arg);
+    } else if (phase < 0.5f - half) {
+        const float at_end = amplitude - max_rate * duration / pi;
+        angle = at_end - max_rate * (phase - half);
+        rate = -max_rate;
+    } else if (phase < 0.5f + half) {
+        const float start = 0.5f - half;
+        const float at_start = -amplitude + max_rate * duration / pi;
+        const float arg = pi * (phase - start) / duration;
+        angle = at_start - max_rate * duration / pi * bfx_sinf(arg);
+        rate = -max_rate * bfx_cosf(arg);
+    } else if (phase < 1.0f - half) {
+        const float at_end = -amplitude + max_rate * duration / pi;
+        angle = at_end + max_rate * (phase - (0.5f + half));
+        rate = max_rate;
+    } else {
+        const float start = 1.0f - half;
+        const float at_start = amplitude - max_rate * duration / pi;
+        const float arg = pi * (phase - start) / duration;
+        angle = at_start + max_rate * duration / pi * bfx_sinf(arg);
+        rate = max_rate * bfx_cosf(arg);
+    }
+}
+
+// prescribedPitchKinematics: BF.metal:1003-1035
+__device__ void wing_pitch(float phase, const WingRec& w, float& angle, float& rate) {
+    const float pi = 3.14159265358979323846f;
+    const float duration = w.k0[3], half = 0.5f * duration;
+    const float low = w.k1[0], high = w.k1[1], delta = high - low;
+    float x, start, change;
+    if (phase < half || phase >= 1.0f - half) {
+        const float wrapped = phase < half ? phase + 1.0f : phase;
+        x = (wrapped - (1.0f - half)) / duration;
+        start = high;
+        change = -delta;
+    } else if (phase >= 0.5f - half && phase < 0.5f + half) {
+        x = (phase - (0.5f - half)) / duration;
+        start = low;
+        change = delta;
+    } else {
+        angle = phase < 0.5f ? low : high;
+        rate = 0.0f;
+        return;
+    }
+    const float blend = x - bfx_sinf(2.0f * pi * x) / (2.0f * pi);
+    rate = change / duration * (1.0f - bfx_cosf(2.0f * pi * x));
+    angle = start + change * blend;
+}
+
+// preparePrescribedFlappingWing (BF.metal:1038-1078) and the geometry box,
+// one thread.  The phase runs on the absolute step index, as the reference's
+// validator passes Float(absoluteStep) as the time.
+__global__ void k_prepare_wing(const GeomArgs a, int init, float dt) {
+    if (threadIdx.x != 0) return;
+    DeviceState* st = a.b.state;
+    const WingRec w = wing_rec(*a.b.bird);
+    const uint64_t absolute = init ? 0 : st->step + 1;
+    const float time = (float)absolute;
+    const float cycle_steps = w.k0[0];
+    float phase = fmodf(time / cycle_steps, 1.0f);
+    phase = phase < 0.0f ? phase + 1.0f : phase;
+    float stroke, stroke_rate, pitch, pitch_rate;
+    wing_stroke(phase, w, stroke, stroke_rate);
+    wing_pitch(phase, w, pitch, pitch_rate);
+    const V3 axis = v3(0.0f, 0.0f, 1.0f);
+    const V3 span = v3(bfx_cosf(stroke), bfx_sinf(stroke), 0.0f);
+    const V3 tangent = cross(axis, span);
+    const float ps = bfx_sinf(-pitch), pc = bfx_cosf(-pitch);
+    const V3 chord = rotate_axis_sc(tangent, span, ps, pc);
+    const V3 normal = normalize3(cross(span, chord));
+    const float inv = 1.0f / cycle_steps;
+    const V3 omega = v3(axis.x * (stroke_rate * inv) - span.x * (pitch_rate * inv),
+                        axis.y * (stroke_rate * inv) - span.y * (pitch_rate * inv),
+                        axis.z * (stroke_rate * inv) - span.z * (pitch_rate * inv));
+    Prepared& p = st->prep;
+    const V3 pos = v3((float)st->body[0], (float)st->body[1], (float)st->body[2]);
+    p.body_position = f4(pos, 0.0f);
+    p.orientation = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+    p.linear_velocity = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float radius = w.geometry[0] + 1.5f * w.root_and_chord[3] + 2.0f * a.fp.dx;
+    p.omega_body_world = make_float4(0.0f, 0.0f, 0.0f, radius);
+    p.left_root = make_float4(w.root_and_chord[0], w.root_and_chord[1], w.root_and_chord[2], w.root_and_chord[3]);
+    p.left_chord = f4(normalize3(chord), 0.0f);
+    p.left_span = f4(normalize3(span), 0.0f);
+    p.left_normal = f4(normal, 0.0f);
+    p.left_angular_velocity = f4(omega, 0.0f);
+    p.right_root = make_float4(stroke, pitch, stroke_rate * inv, pitch_rate * inv);
+    p.right_chord = p.right_span = p.right_normal = p.right_angular_velocity = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    for (int k = 0; k < 16; ++k) {
+        st->wing_prev[k] = 0.0f;
+        st->wing_reaction[k] = 0.0f;
+    }
+    st->geom_time = (float)((double)absolute * (double)dt);
+    // geometry box centred on the wing root, clamped into the lattice
+    const int ext[3] = {a.bx, a.by, a.bz};
+    const int dims[3] = {a.g.nx, a.g.ny, a.g.nz};
+    const float c[3] = {w.root_and_chord[0], w.root_and_chord[1], w.root_and_chord[2]};
+    for (int k = 0; k < 3; ++k) {
+        const float cc = (c[k] - a.fp.origin[k]) / a.fp.dx - 0.5f;
+        int lo = (int)floorf(cc) - ext[k] / 2;
+        lo = lo < 0 ? 0 : lo;
+        lo = lo > dims[k] - ext[k] ? dims[k] - ext[k] : lo;
+        st->box_origin[k] = lo < 0 ? 0 : lo;
+        st->act_lo[k] = -(1 << 30);
+        st->act_hi[k] = 1 << 30;
+    }
+}
+
+// prescribedWingBoundaryCoordinates + prescribedWingMaximumViolation
+// (BF.metal:1091-1142): positive outside the wing.
+__device__ float wing_violation(const WingRec& w, const Prepared& p, float dx, V3 world) {
+    const V3 rel = world - v3(p.left_root);
+    const float radial = dot(rel, v3(p.left_span)), normal = dot(rel, v3(p.left_normal)),
+                chord = dot(rel, v3(p.left_chord));
+    const float radius = w.geometry[0], chord_mean = w.root_and_chord[3];
+    const float half = 0.5f * fmaxf(w.geometry[1], dx);
+    const float fraction = clampf(radial / radius, 0.0f, 1.0f);
+    const float beta_base = fmaxf(fraction * (1.0f - fraction), 0.0f);
+    const float local_chord = chord_mean * w.geometry[3] * bfx_powf(beta_base, w.geometry[2]);
+    const float leading = -0.25f * chord_mean;
+    const float root_v = -radial, tip_v = radial - radius, normal_v = fabsf(normal) - half;
+    const float lead_v = leading - chord, trail_v = chord - (leading + local_chord);
+    return fmaxf(fmaxf(root_v, tip_v), fmaxf(normal_v, fmaxf(lead_v, trail_v)));
+}
+
+// buildPrescribedFlappingWing, classification (BF.metal:1179-1249): part 1;
+// wall = rigid rotation about the root in lattice velocity, w = -1 solid /
+// +1 fluid, (0, 0, 0, radius) outside the bounding sphere.
+__global__ void k_classify_wing(const GeomArgs a, int has_prev) {
+    int x, y, z;
+    int64_t bidx;
+    if (!box_cell(a, x, y, z, bidx)) return;
+    const Prepared& p = a.b.state->prep;
+    const WingRec w = wing_rec(*a.b.bird);
+    const int64_t gid = flat(a.g, x, y, z);
+    const float chord_mean = w.root_and_chord[3];
+    const float radius = w.geometry[0] + 1.5f * chord_mean + 2.0f * a.fp.dx;
+    const V3 world = cell_world(a.fp, x, y, z);
+    const V3 rel = world - v3(p.left_root);
+    const uint8_t prev_part = a.b.mask_prev[gid] & kPartMask;
+    const bool was_solid = has_prev && prev_part != 0;
+    if (!was_solid && dot(rel, rel) > radius * radius) {
+        a.b.mask_next[gid] = topo_flags(0, prev_part, has_prev);
+        a.b.wall[gid] = make_float4(0.0f, 0.0f, 0.0f, radius);
+        return;
+    }
+    const float cc = dot(rel, v3(p.left_chord)), rc = dot(rel, v3(p.left_span)), nc = dot(rel, v3(p.left_normal));
+    const float half = 0.5f * fmaxf(w.geometry[1], a.fp.dx);
+    const bool in_radial = rc >= 0.0f && rc <= w.geometry[0];
+    const bool in_normal = fabsf(nc) <= half;
+    bool is_wing = false;
+    if (in_radial && in_normal) {
+        const float fraction = clampf(rc / w.geometry[0], 0.0f, 1.0f);
+        const float beta_base = fmaxf(fraction * (1.0f - fraction), 0.0f);
+        const float local_chord = chord_mean * w.geometry[3] * bfx_powf(beta_base, w.geometry[2]);
+        const float leading = -0.25f * chord_mean;
+        const float trailing = leading + local_chord;
+        is_wing = cc >= leading && cc <= trailing;
+    }
+    const V3 u = cross(v3(p.left_angular_velocity), rel);
+    a.b.mask_next[gid] = topo_flags(is_wing ? 1 : 0, prev_part, has_prev);
+    a.b.wall[gid] = make_float4(u.x / a.fp.dx, u.y / a.fp.dx, u.z / a.fp.dx, is_wing ? -1.0f : 1.0f);
+}
+
+// prescribedWingLinkFraction (BF.metal:1144-1175) of the link from solid s
+// toward s + c_q, the fluid end placed at s's position plus c_q dx as
+// buildPrescribedFlappingWing places it (BF.metal:1276-1278).
+__device__ float wing_link_fraction(const GeomArgs& a, int q, int sx, int sy, int sz) {
+    const Prepared& p = a.b.state->prep;
+    const WingRec w = wing_rec(*a.b.bird);
+    const V3 sw = cell_world(a.fp, sx, sy, sz);
+    const V3 fw = v3(sw.x + (float)cx(q) * a.fp.dx, sw.y + (float)cy(q) * a.fp.dx, sw.z + (float)cz(q) * a.fp.dx);
+    float lo = 0.0f, hi = 1.0f;
+    for (int it = 0; it < 10; ++it) {
+        const float mid = 0.5f * (lo + hi);
+        const V3 smp = v3(mixf(fw.x, sw.x, mid), mixf(fw.y, sw.y, mid), mixf(fw.z, sw.z, mid));
+        if (wing_violation(w, p, a.fp.dx, smp) > 0.0f) lo = mid;
+        else hi = mid;
+    }
+    return clampf(0.5f * (lo + hi), 1.0e-4f, 1.0f);
+}
+
 // driven by the rigid frames instead of keyframes).
 __device__ void mesh_vertex(const GeomArgs& a, uint32_t i, V3& w, V3& v);
 
@@ -995,6 +1204,8 @@ __global__ void __launch_bounds__(128) k_links_fraction(const GeomArgs a, int ge
             const int64_t s = flat(g, sx, sy, sz);
             if (geometry == BFX_GEOMETRY_ELLIPSOID) {
                 qf = ellipsoid_link_fraction(a, x, y, z, sx, sy, sz);
+            } else if (geometry == BFX_GEOMETRY_FLAPPING_WING) {
+                qf = wing_link_fraction(a, q, sx, sy, sz);
             } else if (geometry == BFX_GEOMETRY_MESH) {
                 if (link_rule == BFX_LINK_RAY_ROOT) {
                     qf = mesh_ray_root(a, x, y, z, sx, sy, sz);
@@ -1416,8 +1627,8 @@ int box_block_count(const BoxDesc& box) {
 void launch_prepare(int geometry, float dt, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
                     const GeomBuffers& gb, int init, cudaStream_t s) {
     GeomArgs a = make_geom(g, fp, box, gb, nullptr);
-    k_prepare<<<1, 32, 0, s>>>(a, init, dt, 0.0f);
-    (void)geometry;
+    if (geometry == BFX_GEOMETRY_FLAPPING_WING) k_prepare_wing<<<1, 32, 0, s>>>(a, init, dt);
+    else k_prepare<<<1, 32, 0, s>>>(a, init, dt, 0.0f);
 }
 
 void launch_classify(int geometry, int has_prev, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
@@ -1429,6 +1640,8 @@ void launch_classify(int geometry, int has_prev, const GridDesc& g, const FluidP
         k_classify_bird<<<grid, block, 0, s>>>(a, has_prev);
     } else if (geometry == BFX_GEOMETRY_ELLIPSOID) {
         k_classify_ellipsoid<<<grid, block, 0, s>>>(a, has_prev);
+    } else if (geometry == BFX_GEOMETRY_FLAPPING_WING) {
+        k_classify_wing<<<grid, block, 0, s>>>(a, has_prev);
     } else if (geometry == BFX_GEOMETRY_MESH) {
         dim3 sgrid, sblock;
         slab_shape(box, sgrid, sblock);

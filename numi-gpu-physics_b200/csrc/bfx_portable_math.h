@@ -112,4 +112,104 @@ BFX_HD double bfx_cos(double x) {
 BFX_HD float bfx_sinf(float x) { return (float)bfx_sin((double)x); }
 BFX_HD float bfx_cosf(float x) { return (float)bfx_cos((double)x); }
 
+/*
+ * Natural logarithm, exponential and power for the beta-planform chord law
+ * (pow of a number in [0, 1/4]), with the same IEEE double operations on
+ * host and device:
+ *
+ *   log x = e ln 2 + log m,  x = m 2^e with m in [sqrt(1/2), sqrt(2)),
+ *           log m = 2 atanh s = 2 (s + s^3/3 + ... + s^25/25), s = (m-1)/(m+1),
+ *           |s| <= 0.1716, so the first omitted term is below 1e-20;
+ *   exp y = 2^k exp r,  k = round(y / ln 2), r = y - k ln 2 (two-part ln 2:
+ *           a 29-bit head, exact times |k| < 2^24, and the double tail),
+ *           |r| <= 0.35, exp r by its Taylor series to r^17/17!.
+ *
+ * ln 2 was evaluated to 60 digits with Python's decimal module; the series
+ * coefficients are exact rational expressions folded by the compiler.
+ */
+#define BFX_LN2_HI 0.6931471806019545
+#define BFX_LN2_LO -4.2009150726810846e-11
+#define BFX_INV_LN2 1.4426950408889634
+
+/* Bits of a double and back, by bit pattern (no arithmetic). */
+BFX_HD unsigned long long bfx_dbits(double x) {
+#if defined(__CUDA_ARCH__)
+    return (unsigned long long)__double_as_longlong(x);
+#else
+    union { double d; unsigned long long u; } v;
+    v.d = x;
+    return v.u;
+#endif
+}
+BFX_HD double bfx_dfrombits(unsigned long long u) {
+#if defined(__CUDA_ARCH__)
+    return __longlong_as_double((long long)u);
+#else
+    union { double d; unsigned long long u; } v;
+    v.u = u;
+    return v.d;
+#endif
+}
+
+/* log x for a positive, finite, normal double x. */
+BFX_HD double bfx_log(double x) {
+    const unsigned long long b = bfx_dbits(x);
+    int e = (int)((b >> 52) & 0x7FFull) - 1023;
+    double m = bfx_dfrombits((b & 0x000FFFFFFFFFFFFFull) | 0x3FF0000000000000ull); /* [1, 2) */
+    if (m > 1.4142135623730951) {
+        m = m * 0.5;
+        e += 1;
+    }
+    const double s = (m - 1.0) / (m + 1.0);
+    const double s2 = s * s;
+    double p = 1.0 / 25.0;
+    p = p * s2 + 1.0 / 23.0;
+    p = p * s2 + 1.0 / 21.0;
+    p = p * s2 + 1.0 / 19.0;
+    p = p * s2 + 1.0 / 17.0;
+    p = p * s2 + 1.0 / 15.0;
+    p = p * s2 + 1.0 / 13.0;
+    p = p * s2 + 1.0 / 11.0;
+    p = p * s2 + 1.0 / 9.0;
+    p = p * s2 + 1.0 / 7.0;
+    p = p * s2 + 1.0 / 5.0;
+    p = p * s2 + 1.0 / 3.0;
+    const double log_m = 2.0 * s + (2.0 * s) * (s2 * p);
+    const double de = (double)e;
+    return de * BFX_LN2_HI + (de * BFX_LN2_LO + log_m);
+}
+
+/* exp y for y in [-700, 700]. */
+BFX_HD double bfx_exp(double y) {
+    const double k = bfx_round_d(y * BFX_INV_LN2);
+    const double r = (y - k * BFX_LN2_HI) - k * BFX_LN2_LO;
+    double p = 1.0 / 355687428096000.0;    /* 1/17! */
+    p = p * r + 1.0 / 20922789888000.0;    /* 1/16! */
+    p = p * r + 1.0 / 1307674368000.0;
+    p = p * r + 1.0 / 87178291200.0;
+    p = p * r + 1.0 / 6227020800.0;
+    p = p * r + 1.0 / 479001600.0;
+    p = p * r + 1.0 / 39916800.0;
+    p = p * r + 1.0 / 3628800.0;
+    p = p * r + 1.0 / 362880.0;
+    p = p * r + 1.0 / 40320.0;
+    p = p * r + 1.0 / 5040.0;
+    p = p * r + 1.0 / 720.0;
+    p = p * r + 1.0 / 120.0;
+    p = p * r + 1.0 / 24.0;
+    p = p * r + 1.0 / 6.0;
+    p = p * r + 0.5;
+    p = p * r + 1.0;
+    p = p * r + 1.0;
+    const long long ki = (long long)k;
+    return p * bfx_dfrombits((unsigned long long)(ki + 1023) << 52);
+}
+
+/* pow(b, e) for a finite float b >= 0 and |e * log b| <= 700: evaluated in
+ * double, rounded once.  pow(0, e) is 0 for e > 0 and 1 for e == 0. */
+BFX_HD float bfx_powf(float b, float e) {
+    if (b == 0.0f) return e > 0.0f ? 0.0f : 1.0f;
+    return (float)bfx_exp((double)e * bfx_log((double)b));
+}
+
 #endif /* BFX_PORTABLE_MATH_H */

@@ -1167,6 +1167,202 @@ float or_ellipsoid_link_fraction(const or_params* p, const or_bird* bird, const 
 }
 
 /* ------------------------------------------------------------------ */
+/* Prescribed flapping wing (Li-Nabawy beta planform): the analytic      */
+/* geometry of MetalFlappingWingValidation (BF.metal:940-1297).          */
+/* ------------------------------------------------------------------ */
+/* unitCyclePhase: BF.metal:940-943 */
+static float wing_unit_phase(float time, float cycle_steps) {
+    float phase = fmodf(time / cycle_steps, 1.0f);
+    return phase < 0.0f ? phase + 1.0f : phase;
+}
+
+/* prescribedStrokeKinematics: BF.metal:945-1001 (angle, rate per cycle) */
+static void wing_stroke(float phase, const or_wing* w, float out[2]) {
+    const float pi = 3.14159265358979323846f;
+    float amplitude = w->kinematics0.v[1], duration = w->kinematics0.v[2];
+    float half = 0.5f * duration, max_rate = w->kinematics1.v[2];
+    if (phase < half) {
+        float arg = pi * (phase + half) / duration;
+        out[0] = amplitude + max_rate * duration / pi * (bfx_sinf(arg) - 1.0f);
+        out[1] = max_rate * bfx_cosf(arg);
+    } else if (phase < 0.5f - half) {
+        float at_end = amplitude - max_rate * duration / pi;
+        out[0] = at_end - max_rate * (phase - half);
+        out[1] = -max_rate;
+    } else if (phase < 0.5f + half) {
+        float start = 0.5f - half;
+        float at_start = -amplitude + max_rate * duration / pi;
+        float arg = pi * (phase - start) / duration;
+        out[0] = at_start - max_rate * duration / pi * bfx_sinf(arg);
+        out[1] = -max_rate * bfx_cosf(arg);
+    } else if (phase < 1.0f - half) {
+        float at_end = -amplitude + max_rate * duration / pi;
+        out[0] = at_end + max_rate * (phase - (0.5f + half));
+        out[1] = max_rate;
+    } else {
+        float start = 1.0f - half;
+        float at_start = amplitude - max_rate * duration / pi;
+        float arg = pi * (phase - start) / duration;
+        out[0] = at_start + max_rate * duration / pi * bfx_sinf(arg);
+        out[1] = max_rate * bfx_cosf(arg);
+    }
+}
+
+/* prescribedPitchKinematics: BF.metal:1003-1035 */
+static void wing_pitch(float phase, const or_wing* w, float out[2]) {
+    const float pi = 3.14159265358979323846f;
+    float duration = w->kinematics0.v[3], half = 0.5f * duration;
+    float low = w->kinematics1.v[0], high = w->kinematics1.v[1], delta = high - low;
+    float x, start, change;
+    if (phase < half || phase >= 1.0f - half) {
+        float wrapped = phase < half ? phase + 1.0f : phase;
+        x = (wrapped - (1.0f - half)) / duration;
+        start = high;
+        change = -delta;
+    } else if (phase >= 0.5f - half && phase < 0.5f + half) {
+        x = (phase - (0.5f - half)) / duration;
+        start = low;
+        change = delta;
+    } else {
+        out[0] = phase < 0.5f ? low : high;
+        out[1] = 0.0f;
+        return;
+    }
+    float blend = x - bfx_sinf(2.0f * pi * x) / (2.0f * pi);
+    out[1] = change / duration * (1.0f - bfx_cosf(2.0f * pi * x));
+    out[0] = start + change * blend;
+}
+
+/* preparePrescribedFlappingWing: BF.metal:1038-1078.  time is the absolute
+ * step index (the reference passes Float(absoluteStep)). */
+void or_prepare_wing(const or_wing* w, float time, or_wing_prepared* out) {
+    float cycle_steps = w->kinematics0.v[0];
+    float phase = wing_unit_phase(time, cycle_steps);
+    float stroke[2], pitch[2];
+    wing_stroke(phase, w, stroke);
+    wing_pitch(phase, w, pitch);
+    const float axis[3] = {0.0f, 0.0f, 1.0f};
+    float span[3] = {bfx_cosf(stroke[0]), bfx_sinf(stroke[0]), 0.0f};
+    float tangent[3], chord[3], cn[3], normal[3], sn[3];
+    cross3(axis, span, tangent);
+    rotate_axis(tangent, span, -pitch[0], chord);
+    cross3(span, chord, cn);
+    normalize3(cn, normal);
+    float inv = 1.0f / cycle_steps;
+    float omega[3];
+    for (int k = 0; k < 3; ++k) omega[k] = axis[k] * (stroke[1] * inv) - span[k] * (pitch[1] * inv);
+    out->root = w->root_and_chord;
+    normalize3(chord, cn);
+    set4(&out->chord, cn, 0.0f);
+    normalize3(span, sn);
+    set4(&out->span, sn, 0.0f);
+    set4(&out->normal, normal, 0.0f);
+    set4(&out->angular_velocity, omega, 0.0f);
+    out->state.v[0] = stroke[0];
+    out->state.v[1] = pitch[0];
+    out->state.v[2] = stroke[1] * inv;
+    out->state.v[3] = pitch[1] * inv;
+}
+
+/* prescribedWingBoundaryCoordinates + prescribedWingMaximumViolation:
+ * BF.metal:1091-1142.  Positive outside the wing. */
+float or_wing_violation(const or_params* p, const or_wing* w, const or_wing_prepared* pw, const float world[3]) {
+    float rel[3] = {world[0] - pw->root.v[0], world[1] - pw->root.v[1], world[2] - pw->root.v[2]};
+    float radial = dot3(rel, pw->span.v), normal = dot3(rel, pw->normal.v), chord = dot3(rel, pw->chord.v);
+    float radius = w->geometry.v[0], chord_mean = w->root_and_chord.v[3];
+    float half = 0.5f * fmaxf(w->geometry.v[1], p->dx);
+    float fraction = clampf(radial / radius, 0.0f, 1.0f);
+    float beta_base = fmaxf(fraction * (1.0f - fraction), 0.0f);
+    float local_chord = chord_mean * w->geometry.v[3] * bfx_powf(beta_base, w->geometry.v[2]);
+    float leading = -0.25f * chord_mean;
+    float root_v = -radial, tip_v = radial - radius, normal_v = fabsf(normal) - half;
+    float lead_v = leading - chord, trail_v = chord - (leading + local_chord);
+    return fmaxf(fmaxf(root_v, tip_v), fmaxf(normal_v, fmaxf(lead_v, trail_v)));
+}
+
+/* buildPrescribedFlappingWing, classification part: BF.metal:1179-1249.
+ * Part id 1; wall = rigid rotation about the root (lattice velocity, the
+ * reference's lengths are in cells), w = -1 solid / +1 fluid, (0, 0, 0,
+ * radius) outside the bounding sphere. */
+void or_build_wing(const or_params* p, const or_wing* w, const or_wing_prepared* pw, const uint8_t* mprev,
+                   uint8_t* mnext, float* wall) {
+    float chord_mean = w->root_and_chord.v[3];
+    float radius = w->geometry.v[0] + 1.5f * chord_mean + 2.0f * p->dx;
+    float half = 0.5f * fmaxf(w->geometry.v[1], p->dx);
+#pragma omp parallel for schedule(static)
+    for (int z = 0; z < p->nz; ++z) {
+        for (int y = 0; y < p->ny; ++y) {
+            for (int x = 0; x < p->nx; ++x) {
+                int64_t gid = flat(p, x, y, z);
+                float world[3];
+                cell_world(p, x, y, z, world);
+                float rel[3] = {world[0] - pw->root.v[0], world[1] - pw->root.v[1], world[2] - pw->root.v[2]};
+                int was_solid = p->has_prev_geom && mprev[gid] != 0;
+                if (!was_solid && dot3(rel, rel) > radius * radius) {
+                    mnext[gid] = 0;
+                    wall[4 * gid] = wall[4 * gid + 1] = wall[4 * gid + 2] = 0.0f;
+                    wall[4 * gid + 3] = radius;
+                    continue;
+                }
+                float cc = dot3(rel, pw->chord.v), rc = dot3(rel, pw->span.v), nc = dot3(rel, pw->normal.v);
+                int in_radial = rc >= 0.0f && rc <= w->geometry.v[0];
+                int in_normal = fabsf(nc) <= half;
+                int is_wing = 0;
+                if (in_radial && in_normal) {
+                    float fraction = clampf(rc / w->geometry.v[0], 0.0f, 1.0f);
+                    float beta_base = fmaxf(fraction * (1.0f - fraction), 0.0f);
+                    float local_chord = chord_mean * w->geometry.v[3] * bfx_powf(beta_base, w->geometry.v[2]);
+                    float leading = -0.25f * chord_mean;
+                    float trailing = leading + local_chord;
+                    is_wing = cc >= leading && cc <= trailing;
+                }
+                mnext[gid] = is_wing ? 1 : 0;
+                float u[3];
+                cross3(pw->angular_velocity.v, rel, u);
+                wall[4 * gid] = u[0] / p->dx;
+                wall[4 * gid + 1] = u[1] / p->dx;
+                wall[4 * gid + 2] = u[2] / p->dx;
+                wall[4 * gid + 3] = is_wing ? -1.0f : 1.0f;
+            }
+        }
+    }
+}
+
+/* prescribedWingLinkFraction: BF.metal:1144-1175, with the fluid end placed
+ * the way buildPrescribedFlappingWing places it (the solid node's position
+ * plus c_q dx, BF.metal:1276-1278). */
+float or_wing_link_fraction(const or_params* p, const or_wing* w, const or_wing_prepared* pw, int q, int sx, int sy,
+                            int sz) {
+    float sw[3], fw[3];
+    cell_world(p, sx, sy, sz, sw);
+    for (int k = 0; k < 3; ++k) fw[k] = sw[k] + (float)C[q][k] * p->dx;
+    float lo = 0.0f, hi = 1.0f;
+    for (int it = 0; it < 10; ++it) {
+        float mid = 0.5f * (lo + hi);
+        float smp[3] = {mixf(fw[0], sw[0], mid), mixf(fw[1], sw[1], mid), mixf(fw[2], sw[2], mid)};
+        if (or_wing_violation(p, w, pw, smp) > 0.0f) lo = mid;
+        else hi = mid;
+    }
+    return clampf(0.5f * (lo + hi), 1.0e-4f, 1.0f);
+}
+
+/* Link fractions of a list of cut links (fluid cell, direction): the solid
+ * source of each is cell - c_q. */
+void or_wing_link_fractions(const or_params* p, const or_wing* w, const or_wing_prepared* pw, const uint32_t* cell,
+                            const uint8_t* dir, int64_t count, float* out) {
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < count; ++i) {
+        int64_t g = cell[i];
+        int x = (int)(g % p->nx), y = (int)((g / p->nx) % p->ny), z = (int)(g / ((int64_t)p->nx * p->ny));
+        int q = dir[i];
+        out[i] = or_wing_link_fraction(p, w, pw, q, x - C[q][0], y - C[q][1], z - C[q][2]);
+    }
+}
+
+/* The chord law's power, exposed for the portable-math test. */
+float or_powf(float b, float e) { return bfx_powf(b, e); }
+
+/* ------------------------------------------------------------------ */
 /* Triangle mesh: closest point BF.metal:1529-1583; raster 1638-1686;  */
 /* resolve 1697-1738/1978-2039; links 2044-2076.                        */
 /* ------------------------------------------------------------------ */
@@ -1530,8 +1726,11 @@ int64_t or_write_links(const or_params* p, int kind, const or_bird* bird, const 
                         float sd = fminf(wall[4 * s + 3], 0.0f);
                         float fd = fmaxf(wall[4 * nb + 3], 0.0f);
                         qf = clampf(fd / fmaxf(fd - sd, 1.0e-6f), 1.0e-4f, 1.0f);
-                    } else {
+                    } else if (kind == 2) {
                         qf = or_mesh_ray_root(p, mesh_pos, tris, ntris, half_thickness, keys, bx, by, bz, x, y, z);
+                    } else {
+                        qf = or_wing_link_fraction(p, (const or_wing*)(const void*)bird,
+                                                   (const or_wing_prepared*)(const void*)prep, q, x, y, z);
                     }
                     pops[q * n + s] = qf;
                     total++;

@@ -127,10 +127,32 @@ void or_build_ellipsoid(const or_params* p, const or_bird* bird, const or_prepar
 float or_ellipsoid_link_fraction(const or_params* p, const or_bird* bird, const or_prepared* prep,
                                  int fx, int fy, int fz, int sx, int sy, int sz);
 
+/* ---- prescribed flapping wing (MetalFlappingWingValidation's analytic wing) */
+typedef struct or_wing {     /* GPUFlappingWingParameters, GPUData.swift:383-388 */
+    or_f4 root_and_chord, geometry, kinematics0, kinematics1;
+} or_wing;
+typedef struct or_wing_prepared { /* GPUPreparedFlappingWing, GPUData.swift:392-399 */
+    or_f4 root, chord, span, normal, angular_velocity, state;
+} or_wing_prepared;
+/* preparePrescribedFlappingWing (BF.metal:1038-1078); time = absolute step index. */
+void or_prepare_wing(const or_wing* w, float time, or_wing_prepared* out);
+/* prescribedWingMaximumViolation of the boundary coordinates (BF.metal:1091-1142). */
+float or_wing_violation(const or_params* p, const or_wing* w, const or_wing_prepared* pw, const float world[3]);
+/* buildPrescribedFlappingWing classification (BF.metal:1179-1249). */
+void or_build_wing(const or_params* p, const or_wing* w, const or_wing_prepared* pw, const uint8_t* mprev,
+                   uint8_t* mnext, float* wall);
+/* prescribedWingLinkFraction (BF.metal:1144-1175) of the link from solid s toward s + c_q. */
+float or_wing_link_fraction(const or_params* p, const or_wing* w, const or_wing_prepared* pw, int q, int sx, int sy,
+                            int sz);
+void or_wing_link_fractions(const or_params* p, const or_wing* w, const or_wing_prepared* pw, const uint32_t* cell,
+                            const uint8_t* dir, int64_t count, float* out);
+float or_powf(float b, float e);
+
 /* Writes link fractions into pops[q*N+s] for every solid s / fluid s+c_q pair and
  * preserves newly covered momentum (BF.metal:1251-1295 pattern).  kind 0 =
  * ellipsoid bisection, 1 = mesh linear signed-distance rule (BF.metal:2044-2076),
- * 2 = mesh ray root. Returns the number of links written. */
+ * 2 = mesh ray root, 3 = prescribed-wing bisection (bird / prep then point to
+ * the or_wing / or_wing_prepared). Returns the number of links written. */
 int64_t or_write_links(const or_params* p, int kind, const or_bird* bird, const or_prepared* prep,
                        const float* mesh_pos /*4 per vertex*/, const uint32_t* tris, uint32_t ntris,
                        float half_thickness, const uint64_t* keys,

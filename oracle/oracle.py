@@ -75,6 +75,14 @@ class Prepared(ct.Structure):
         "right_root", "right_chord", "right_span", "right_normal", "right_angular_velocity")]
 
 
+class Wing(ct.Structure):
+    _fields_ = [(name, F4) for name in ("root_and_chord", "geometry", "kinematics0", "kinematics1")]
+
+
+class WingPrepared(ct.Structure):
+    _fields_ = [(name, F4) for name in ("root", "chord", "span", "normal", "angular_velocity", "state")]
+
+
 class BodyF32(ct.Structure):
     _fields_ = [("position", ct.c_float * 3), ("orientation", ct.c_float * 4),
                 ("velocity", ct.c_float * 3), ("omega_body", ct.c_float * 3)]
@@ -108,6 +116,15 @@ def lib():
         L.or_prepare_bird.argtypes = [P(Bird), P(BodyF32), ct.c_float, ct.c_float, P(Prepared)]
         L.or_build_bird.argtypes = [P(Params), P(Bird), P(Prepared), u8p, u8p, fp]
         L.or_build_ellipsoid.argtypes = [P(Params), P(Bird), P(Prepared), u8p, u8p, fp]
+        L.or_prepare_wing.argtypes = [P(Wing), ct.c_float, P(WingPrepared)]
+        L.or_build_wing.argtypes = [P(Params), P(Wing), P(WingPrepared), u8p, u8p, fp]
+        L.or_wing_link_fraction.restype = ct.c_float
+        L.or_wing_link_fraction.argtypes = [P(Params), P(Wing), P(WingPrepared)] + [ct.c_int] * 4
+        L.or_wing_violation.restype = ct.c_float
+        L.or_wing_violation.argtypes = [P(Params), P(Wing), P(WingPrepared), fp]
+        L.or_wing_link_fractions.argtypes = [P(Params), P(Wing), P(WingPrepared), P(ct.c_uint32), u8p, ct.c_int64, fp]
+        L.or_powf.restype = ct.c_float
+        L.or_powf.argtypes = [ct.c_float, ct.c_float]
         L.or_ellipsoid_link_fraction.restype = ct.c_float
         L.or_ellipsoid_link_fraction.argtypes = [P(Params), P(Bird), P(Prepared)] + [ct.c_int] * 6
         L.or_write_links.restype = ct.c_int64
@@ -227,16 +244,22 @@ class OracleSim:
     """CPU restatement of one simulation: A/B populations, masks, wall field.
 
     geometry: None (all fluid), "bird" (analytic bird, halfway links),
-    "ellipsoid" (body ellipsoid, interpolated bisection links) or "mesh"
-    (articulated triangle mesh; link_rule "linear" or "ray").
+    "ellipsoid" (body ellipsoid, interpolated bisection links), "mesh"
+    (articulated triangle mesh; link_rule "linear" or "ray") or "wing" (the
+    prescribed flapping wing of ``wing``, held at its root).
     """
 
     def __init__(self, params: Params, *, geometry=None, bird: Bird | None = None,
-                 body=None, body_f64=True, mesh=None, link_rule="linear", shear=None):
+                 body=None, body_f64=True, mesh=None, link_rule="linear", shear=None, wing: Wing | None = None):
         self.p = params
         self.n = params.nx * params.ny * params.nz
         n = self.n
         self.geometry = geometry
+        self.wing = wing
+        self.wing_prep = WingPrepared()
+        self._absolute = 0
+        if geometry == "wing":
+            body = (tuple(wing.root_and_chord.v[:3]), (0.0, 0.0, 0.0, 1.0), (0.0, 0.0, 0.0), (0.0, 0.0, 0.0))
         self.bird = bird
         self.mesh = mesh
         self.link_rule = link_rule
@@ -296,6 +319,16 @@ class OracleSim:
 
     def _geometry(self, time: float, target: np.ndarray, init: bool = False):
         L = lib()
+        if self.geometry == "wing":
+            # the validator's time is the absolute step index (MetalFlappingWingValidation.swift:3631-3634)
+            L.or_prepare_wing(ct.byref(self.wing), float(0 if init else self._absolute), ct.byref(self.wing_prep))
+            L.or_build_wing(ct.byref(self.p), ct.byref(self.wing), ct.byref(self.wing_prep), u8ptr(self.mcur),
+                            u8ptr(target), fptr(self.wall))
+            if target is not self.mcur:
+                L.or_write_links(ct.byref(self.p), 3, ct.cast(ct.byref(self.wing), ct.POINTER(Bird)),
+                                 ct.cast(ct.byref(self.wing_prep), ct.POINTER(Prepared)), None, None, 0, 0.0, None,
+                                 fptr(self.pa), u8ptr(self.mcur), u8ptr(target), fptr(self.wall), fptr(self.covered))
+            return
         L.or_prepare_bird(ct.byref(self.bird), ct.byref(self.body32), time, self.p.dx, ct.byref(self.prep))
         if self.bird.left_wing_inertia.v[3] >= 0.5:
             L.or_wing_reaction(ct.byref(self.prep), ct.byref(self.bird), self.p.dt, int(init),
@@ -355,6 +388,7 @@ class OracleSim:
         L = lib()
         self.p.capture_fields = int(capture_fields)
         absolute = self.step_index + 1
+        self._absolute = absolute
         time = np.float32(float(absolute) * float(self.p.dt))
         self.p.time = float(time)
         if self.geometry is not None:

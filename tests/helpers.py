@@ -7,7 +7,7 @@ import bfx._lib as L
 import oracle as O
 
 GEOMETRY_NAMES = {L.GEOMETRY_NONE: None, L.GEOMETRY_BIRD: "bird", L.GEOMETRY_ELLIPSOID: "ellipsoid",
-                  L.GEOMETRY_MESH: "mesh"}
+                  L.GEOMETRY_MESH: "mesh", L.GEOMETRY_FLAPPING_WING: "wing"}
 
 
 def oracle_params(cfg: L.Config) -> O.Params:
@@ -24,7 +24,15 @@ def oracle_params(cfg: L.Config) -> O.Params:
     return p
 
 
-def oracle_twin(cfg: L.Config, bird_rows=None, body=None, mesh=None) -> O.OracleSim:
+def oracle_wing(wing: L.FlappingWing) -> O.Wing:
+    w = O.Wing()
+    for name, _ in O.Wing._fields_:
+        getattr(w, name).v[:] = list(getattr(wing, name).v)
+    w.kinematics1.v[3] = 0.0  # the library drops the reference speed (not part of the geometry)
+    return w
+
+
+def oracle_twin(cfg: L.Config, bird_rows=None, body=None, mesh=None, wing=None) -> O.OracleSim:
     p = oracle_params(cfg)
     geometry = GEOMETRY_NAMES[cfg.geometry]
     bird = O.bird_from_dict(dict(zip(L.BIRD_FIELDS, bird_rows))) if bird_rows is not None else None
@@ -41,7 +49,8 @@ def oracle_twin(cfg: L.Config, bird_rows=None, body=None, mesh=None) -> O.Oracle
             om["kf_times"] = np.ascontiguousarray(mesh["kf_times"], np.float32)
             om["kf_points"] = np.ascontiguousarray(mesh["kf_points"], np.float32).ravel()
     return O.OracleSim(p, geometry=geometry, bird=bird, body=body, mesh=om,
-                       link_rule="linear" if cfg.link_rule == L.LINK_LINEAR else "ray", shear=shear)
+                       link_rule="linear" if cfg.link_rule == L.LINK_LINEAR else "ray", shear=shear,
+                       wing=oracle_wing(wing) if wing is not None else None)
 
 
 def body_struct_from_tuple(body):

@@ -28,7 +28,7 @@ def test_library_loads_and_exports_every_declared_symbol():
     for s in syms:
         assert hasattr(lib, s), s
     assert set(syms) == set(L.EXPORTED)
-    assert lib.bfx_abi_version() == 2
+    assert lib.bfx_abi_version() == 3
 
 
 def test_no_device_reports_unavailable_not_crash():
@@ -46,12 +46,12 @@ def test_struct_layout_matches_c_header():
 #include <stddef.h>
 #include "bfx.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(bfx_config), sizeof(bfx_bird),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(bfx_config), sizeof(bfx_bird),
          sizeof(bfx_body_state), sizeof(bfx_mesh), sizeof(bfx_loads), sizeof(bfx_run_sample),
          sizeof(bfx_safety_record), sizeof(bfx_snapshot_data), sizeof(bfx_advance_result),
          offsetof(bfx_config, mesh_half_thickness), sizeof(bfx_adjoint_objective), sizeof(bfx_adjoint_result),
          sizeof(bfx_ledger_sample), offsetof(bfx_ledger_sample, far_field_links), sizeof(bfx_field_frame),
-         offsetof(bfx_field_frame, geometry), offsetof(bfx_field_frame, density));
+         offsetof(bfx_field_frame, geometry), offsetof(bfx_field_frame, density), sizeof(bfx_flapping_wing));
   return 0;
 }
 '''
@@ -66,10 +66,11 @@ int main(void) {
             ct.sizeof(L.RunSample), ct.sizeof(L.SafetyRecord), ct.sizeof(L.Snapshot), ct.sizeof(L.AdvanceResult),
             L.Config.mesh_half_thickness.offset, ct.sizeof(L.AdjointObjective), ct.sizeof(L.AdjointResult),
             ct.sizeof(L.LedgerSample), L.LedgerSample.far_field_links.offset, ct.sizeof(L.FieldFrame),
-            L.FieldFrame.geometry.offset, L.FieldFrame.density.offset]
+            L.FieldFrame.geometry.offset, L.FieldFrame.density.offset, ct.sizeof(L.FlappingWing)]
     assert sizes == mine
-    # GPUBirdParameters is 13 float4 (GPUDataLayoutTests.swift:5-40)
+    # GPUBirdParameters is 13 float4, GPUFlappingWingParameters 4 (GPUDataLayoutTests.swift:5-40)
     assert ct.sizeof(L.Bird) == 13 * 16
+    assert ct.sizeof(L.FlappingWing) == 4 * 16
 
 
 def test_create_without_device_fails_cleanly():

@@ -382,3 +382,45 @@ def test_fast_math_fp32_stays_within_tolerance_of_oracle():
     err_exact = float(np.max(np.abs(runs[L.STORAGE_F32] - f64) / np.abs(f64)))
     err_fast = float(np.max(np.abs(fast - f64) / np.abs(f64)))
     assert err_fast <= 1.5 * err_exact + 1e-7, f"fast {err_fast:.3e} vs exact {err_exact:.3e} against FP64"
+
+
+# --------------------------------------------------------------------------
+# Prescribed flapping wing (MetalFlappingWingValidation's analytic wing):
+# beta-planform classification and 10-step bisection link fractions
+# --------------------------------------------------------------------------
+def _oracle_wing_fractions(osim, cell, d):
+    out = np.zeros(len(cell), np.float32)
+    cell = np.ascontiguousarray(cell, np.uint32)
+    d = np.ascontiguousarray(d, np.uint8)
+    O.lib().or_wing_link_fractions(ct.byref(osim.p), ct.byref(osim.wing), ct.byref(osim.wing_prep),
+                                   cell.ctypes.data_as(ct.POINTER(ct.c_uint32)), O.u8ptr(d), len(cell), O.fptr(out))
+    return out
+
+
+def test_prescribed_flapping_wing_matches_oracle_over_a_cycle():
+    """The Li-Nabawy wing (preparePrescribedFlappingWing +
+    buildPrescribedFlappingWing, BF.metal:940-1297) over one full cycle of
+    480 steps, so every branch of the stroke and pitch kinematics runs: masks,
+    cut-link sets and every link fraction bit-exact against the oracle each
+    step, loads within 1e-5, populations within 1e-6 every 40 steps."""
+    from helpers import oracle_wing  # noqa: F401
+    cfg, wing = cases.flapping_wing(chord=6, cycle_steps=480, viscosity=0.02)
+    lat = Lattice(cfg, wing=wing)
+    osim = oracle_twin(cfg, wing=wing)
+    assert np.array_equal(lat.mask(), osim.mcur)
+    covered = 0
+    for step in range(480):
+        lat.advance(1)
+        osim.step()
+        assert np.array_equal(lat.mask(), osim.mcur), f"mask step {step + 1}"
+        cell, d, q = lat.links()
+        oc, od = oracle_links(osim)
+        assert np.array_equal(link_set(cell, d), link_set(oc, od)), f"links step {step + 1}"
+        assert np.array_equal(q, _oracle_wing_fractions(osim, cell, d)), f"link fractions step {step + 1}"
+        compare_loads(lat, osim, f"wing step {step + 1}")
+        covered += osim.loads.covered_count + osim.loads.uncovered_count
+        if (step + 1) % 40 == 0:
+            compare_pops(lat, osim, f"wing step {step + 1}")
+    assert covered > 0
+    assert len(cell) > 100
+    lat.close()

@@ -264,3 +264,77 @@ def test_regularized_pair_order_agrees_with_literal_order(rr3):
             engaged += act_l
     assert engaged > 50
 
+
+
+def test_portable_power_matches_double_pow():
+    """bfx_powf (the beta-planform chord law's power, portable log / exp in
+    double): the correctly rounded float of the double power on the wing's
+    range of bases, pow(0, e) = 0 and pow(1, e) = 1."""
+    L = O.lib()
+    rng = np.random.default_rng(5)
+    e = np.float32(1.4891506583557845 - 1.0)
+    b = np.concatenate([rng.uniform(0.0, 0.25, 4000), np.geomspace(1e-30, 0.25, 1000)]).astype(np.float32)
+    got = np.array([L.or_powf(float(x), float(e)) for x in b], np.float32)
+    ref = (b.astype(np.float64) ** np.float64(e)).astype(np.float32)
+    assert np.max(np.abs(got.view(np.int32) - ref.view(np.int32))) <= 1
+    assert L.or_powf(0.0, float(e)) == 0.0 and L.or_powf(1.0, float(e)) == 1.0
+
+
+def _wing_kinematics_double(phase, amplitude, duration, max_rate, pitch_duration, low, high):
+    """MetalFlappingWingValidator.kinematicState (MetalFlappingWingValidation.swift:567-640),
+    the reference's double-precision form of the prescribed stroke and pitch."""
+    half = 0.5 * duration
+    if phase < half:
+        a = math.pi * (phase + half) / duration
+        stroke, rate = amplitude + max_rate * duration / math.pi * (math.sin(a) - 1), max_rate * math.cos(a)
+    elif phase < 0.5 - half:
+        stroke, rate = amplitude - max_rate * duration / math.pi - max_rate * (phase - half), -max_rate
+    elif phase < 0.5 + half:
+        a = math.pi * (phase - (0.5 - half)) / duration
+        stroke = -amplitude + max_rate * duration / math.pi - max_rate * duration / math.pi * math.sin(a)
+        rate = -max_rate * math.cos(a)
+    elif phase < 1 - half:
+        stroke, rate = -amplitude + max_rate * duration / math.pi + max_rate * (phase - (0.5 + half)), max_rate
+    else:
+        a = math.pi * (phase - (1 - half)) / duration
+        stroke, rate = amplitude - max_rate * duration / math.pi + max_rate * duration / math.pi * math.sin(a), \
+            max_rate * math.cos(a)
+    ph = 0.5 * pitch_duration
+    if phase < ph or phase >= 1 - ph:
+        w = phase + 1 if phase < ph else phase
+        x, start, change = (w - (1 - ph)) / pitch_duration, high, -(high - low)
+    elif 0.5 - ph <= phase < 0.5 + ph:
+        x, start, change = (phase - (0.5 - ph)) / pitch_duration, low, high - low
+    else:
+        return stroke, rate, (low if phase < 0.5 else high), 0.0
+    pitch = start + change * (x - math.sin(2 * math.pi * x) / (2 * math.pi))
+    prate = change / pitch_duration * (1 - math.cos(2 * math.pi * x))
+    return stroke, rate, pitch, prate
+
+
+def test_prescribed_wing_kinematics_follow_the_reference_double_form():
+    """The oracle's FP32 stroke / pitch kinematics (preparePrescribedFlappingWing,
+    BF.metal:945-1078) agree with the reference's double-precision kinematic
+    state at phases in every branch, within FP32 rounding; the span is the
+    stroke rotation of x about z and the frame is orthonormal."""
+    import bfx.cases as cases
+    from helpers import oracle_wing
+    cfg, wing = cases.flapping_wing(chord=8)
+    w = oracle_wing(wing)
+    L = O.lib()
+    cyc = w.kinematics0.v[0]
+    args = (w.kinematics0.v[1], w.kinematics0.v[2], w.kinematics1.v[2], w.kinematics0.v[3], w.kinematics1.v[0],
+            w.kinematics1.v[1])
+    for phase in (0.02, 0.1, 0.2, 0.3, 0.4, 0.45, 0.5, 0.55, 0.6, 0.7, 0.8, 0.9, 0.97):
+        t = float(np.float32(phase * cyc))
+        prep = O.WingPrepared()
+        L.or_prepare_wing(ct.byref(w), t, ct.byref(prep))
+        ph = float(np.fmod(np.float32(t) / np.float32(cyc), np.float32(1.0)))
+        stroke, rate, pitch, prate = _wing_kinematics_double(ph, *args)
+        st = list(prep.state.v)
+        assert abs(st[0] - stroke) < 2e-6 and abs(st[1] - pitch) < 2e-6, phase
+        assert abs(st[2] - rate / cyc) < 1e-7 and abs(st[3] - prate / cyc) < 1e-7, phase
+        span = np.array(prep.span.v[:3])
+        assert np.allclose(span, [math.cos(stroke), math.sin(stroke), 0.0], atol=2e-6)
+        frame = np.array([prep.chord.v[:3], prep.span.v[:3], prep.normal.v[:3]], np.float64)
+        assert np.allclose(frame @ frame.T, np.eye(3), atol=1e-6)
