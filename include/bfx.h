@@ -437,6 +437,17 @@ BFX_API int bfx_kernel_timing(bfx_sim* sim, double* total_ms, uint64_t* launches
  * device time in milliseconds. */
 BFX_API int bfx_timer_begin(bfx_sim* sim);
 BFX_API int bfx_timer_end(bfx_sim* sim, double* elapsed_ms);
+/* Test hook of the staged 16-bit fluid kernel's bounded pipeline waits; no
+ * reference counterpart.  From the next step on, the kernel's producer
+ * withholds the loads of tile `tile` (-1: none) and every pipeline wait gives
+ * up after `wait_limit` polls (0: the default limit, about a second).  The
+ * withheld tile's consumers then stop waiting, the kernel sets its error flag,
+ * waits (bounded) for its own copies still in flight and returns, and the
+ * advance fails with BFX_ERR_KERNEL, leaving the handle terminally invalid as
+ * a failed command buffer does (BirdFlowSimulation.swift:2059-2095).  The GPU
+ * and other handles stay usable.  BFX_ERR_UNSUPPORTED when the handle does not
+ * run the staged kernel (FP32 / FP64 storage or the limiter operator). */
+BFX_API int bfx_test_stall_staged_kernel(bfx_sim* sim, int32_t tile, uint32_t wait_limit);
 /* Total kernel launches issued by the library on this handle. */
 BFX_API int bfx_launch_count(bfx_sim* sim, uint64_t* launches);
 /* Bytes of device memory held by the handle. */

@@ -171,7 +171,7 @@ EXPORTED = (
     "bfx_launch_count", "bfx_device_bytes", "bfx_fluid_mass_momentum_noalloc", "bfx_adjoint", "bfx_advance_ledger",
     "bfx_last_error", "bfx_set_observation_buffers", "bfx_acquire_field_frame", "bfx_field_frame_copy",
     "bfx_release_field_frame", "bfx_release_field_frame_after", "bfx_capture_current_fields",
-    "bfx_observation_counters", "bfx_flow_diagnostics", "bfx_create_flapping_wing",
+    "bfx_observation_counters", "bfx_flow_diagnostics", "bfx_create_flapping_wing", "bfx_test_stall_staged_kernel",
 )
 
 _lib = None
@@ -197,6 +197,7 @@ def load(path: str | None = None):
     L.bfx_device_count.argtypes = [P(ct.c_int)]
     L.bfx_create.argtypes = [P(Config), P(Bird), P(BodyState), P(Mesh), P(vp)]
     L.bfx_create_flapping_wing.argtypes = [P(Config), P(FlappingWing), P(vp)]
+    L.bfx_test_stall_staged_kernel.argtypes = [vp, ct.c_int32, ct.c_uint32]
     L.bfx_destroy.argtypes = [vp]
     L.bfx_destroy.restype = None
     L.bfx_advance.argtypes = [vp, ct.c_uint64, ct.c_uint32, ct.c_uint32, P(RunSample), ct.c_size_t, P(AdvanceResult)]

@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <ctime>
@@ -145,6 +146,7 @@ struct bfx_sim {
     // side stream of the next step's geometry build, with its fork / join events
     cudaStream_t side = nullptr;
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+    cudaEvent_t halo_fork_ev = nullptr, halo_join_ev = nullptr;
     bool graphs_enabled = true;
     // pinned host staging of the device state: read-backs and body uploads
     // without a pageable-copy bounce
@@ -281,6 +283,20 @@ void encode_geometry_build(bfx_sim* s, int init, uint8_t* mprev, uint8_t* mnext,
 // cells (which read the wall field) are launched before the fork.
 bool can_pipeline(const bfx_sim* s) { return s->moving() && s->tma_ok && s->side != nullptr; }
 
+// The halo fill can run beside the link build and the link kernel when every
+// face is a far-field or velocity face: the fill then only writes constants
+// into halo slots, which no link kernel reads or writes (an out-of-domain
+// cell is never solid), and reads nothing they write.  A periodic face's fill
+// copies real cells that a link may overwrite, an outflow face's copies its
+// interior neighbour, and a link whose solid source is a periodic image writes
+// a halo slot: those keep the fill first on the main stream.
+bool halo_beside_links(const bfx_sim* s) {
+    if (!s->moving() || s->side == nullptr) return false;
+    for (int f = 0; f < 6; ++f)
+        if (s->cfg.face_bc[f] != BFX_BC_FARFIELD && s->cfg.face_bc[f] != BFX_BC_VELOCITY) return false;
+    return true;
+}
+
 void encode_links(bfx_sim* s, uint8_t* mprev, uint8_t* mnext) {
     GeomBuffers gb = geom_buffers(s, mprev, mnext);
     launch_boundary_scan(s->cfg.storage, s->rep_s, s->g, s->fp, s->box, gb, fluid_buffers(s, mnext), s->stream);
@@ -327,6 +343,17 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
     s->hstate_fresh = false;
     uint8_t* mprev = s->mask[s->cur];
     uint8_t* mnext = s->moving() ? s->mask[s->cur ^ 1] : s->mask[s->cur];
+    FluidBuffers fb = fluid_buffers(s, s->geometry() ? mnext : nullptr);
+    // the halo fill forks off here (after the previous step's fluid kernel)
+    // and joins before this step's fluid kernel
+    const bool halo_side = halo_beside_links(s) && !tape && !ledger_in;
+    if (halo_side) {
+        cudaEventRecord(s->halo_fork_ev, s->stream);
+        cudaStreamWaitEvent(s->side, s->halo_fork_ev, 0);
+        launch_halo(s->cfg.storage, s->rep_s, s->g, s->fp, fb, s->side);
+        cudaEventRecord(s->halo_join_ev, s->side);
+        s->launches += 1;
+    }
     if (s->moving() && !geometry_ready) {
         encode_geometry_build(s, 0, mprev, mnext);
     }
@@ -334,7 +361,6 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
         launch_frame_tangent(geom_buffers(s, mprev, mnext), s->cfg.time_step, 0, tape->frames, s->stream);
         s->launches += 1;
     }
-    FluidBuffers fb = fluid_buffers(s, s->geometry() ? mnext : nullptr);
     if (s->geometry() && s->moving()) encode_links(s, mprev, mnext);
     if (tape) {
         GeomBuffers gb = geom_buffers(s, mprev, mnext);
@@ -351,8 +377,10 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
     }
     // halo fill before the link writes: a link whose solid source is a periodic
     // image writes into a halo slot and must win over the periodic copy
-    launch_halo(s->cfg.storage, s->rep_s, s->g, s->fp, fb, s->stream);
-    s->launches += 1;
+    if (!halo_side) {
+        launch_halo(s->cfg.storage, s->rep_s, s->g, s->fp, fb, s->stream);
+        s->launches += 1;
+    }
     // The end-of-step body update needs only the reduced loads: it runs in the
     // link kernel's last block, except while taping (the tape records the
     // state between the loads and the body update).
@@ -369,6 +397,7 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
                            finish_fused ? &fin : nullptr, s->stream);
         s->launches += 1;
     }
+    if (halo_side) cudaStreamWaitEvent(s->stream, s->halo_join_ev, 0);
     if (tape) {
         cudaMemcpyAsync(tape->state, s->dstate, sizeof(DeviceState), cudaMemcpyDeviceToDevice, s->stream);
         cudaMemcpyAsync(tape->mask_next, mnext, (size_t)s->g.n, cudaMemcpyDeviceToDevice, s->stream);
@@ -630,6 +659,8 @@ void bfx_destroy(bfx_sim* s) {
         if (g) cudaGraphExecDestroy(g);
     if (s->fork_ev) cudaEventDestroy(s->fork_ev);
     if (s->join_ev) cudaEventDestroy(s->join_ev);
+    if (s->halo_fork_ev) cudaEventDestroy(s->halo_fork_ev);
+    if (s->halo_join_ev) cudaEventDestroy(s->halo_join_ev);
     if (s->side) cudaStreamDestroy(s->side);
     if (s->hstate) cudaFreeHost(s->hstate);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -662,7 +693,9 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
     // steps run in order on the main stream)
     if (cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&s->join_ev, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&s->join_ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->halo_fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->halo_join_ev, cudaEventDisableTiming) != cudaSuccess) {
         (void)cudaGetLastError();
         if (s->side) cudaStreamDestroy(s->side);
         s->side = nullptr;
@@ -1386,6 +1419,9 @@ int bfx_restore_state(bfx_sim* s, const void* buf, size_t size) {
     if (synced != BFX_OK) return synced;
     const char* p = (const char*)buf + sizeof(h);
     cudaError_t e = cudaMemcpy(s->dstate, p, sizeof(DeviceState), cudaMemcpyHostToDevice);
+    // a restored state never carries the staged kernel's test hook
+    if (e == cudaSuccess)
+        e = cudaMemset((char*)s->dstate + offsetof(DeviceState, test_stall_tile1), 0, 2 * sizeof(uint32_t));
     p += sizeof(DeviceState);
     if (e == cudaSuccess) e = cudaMemcpy(s->pops, p, (size_t)19 * s->g.padded * s->elem, cudaMemcpyHostToDevice);
     p += (size_t)19 * s->g.padded * s->elem;
@@ -1463,6 +1499,21 @@ int bfx_step_index(bfx_sim* s, uint64_t* step, double* time) {
     if (rc != BFX_OK) return rc;
     if (step) *step = st.step;
     if (time) *time = (double)(float)((double)st.step * (double)s->cfg.time_step);
+    return BFX_OK;
+}
+
+int bfx_test_stall_staged_kernel(bfx_sim* s, int32_t tile, uint32_t wait_limit) {
+    BFX_GUARD(s);
+    if (!s->tma_ok) return fail(s, BFX_ERR_UNSUPPORTED, "the simulation does not run the staged 16-bit fluid kernel");
+    if (tile < -1) return fail(s, BFX_ERR_INVALID_ARGUMENT, "tile must be -1 (none) or a tile index");
+    const int rc = sync_check(s, "stall hook");
+    if (rc != BFX_OK) return rc;
+    const uint32_t v[2] = {(uint32_t)(tile + 1), wait_limit};
+    static_assert(offsetof(DeviceState, test_wait_limit) == offsetof(DeviceState, test_stall_tile1) + 4,
+                  "the hook fields are adjacent");
+    const cudaError_t e = cudaMemcpy((char*)s->dstate + offsetof(DeviceState, test_stall_tile1), v, sizeof(v),
+                                     cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(s, e, "stall hook");
     return BFX_OK;
 }
 

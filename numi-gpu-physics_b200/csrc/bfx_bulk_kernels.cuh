@@ -268,6 +268,25 @@ __device__ __forceinline__ void store_cell(const BulkArgs& a, uint32_t pid, cons
     }
 }
 
+// A fluid cell's collided populations: stochastic rounding for BF16 (the
+// stream of cell gid at the step the device state counts), plain stores else.
+template <class S, int REP_S>
+__device__ __forceinline__ void store_fluid_cell(const BulkArgs& a, uint32_t gid, uint32_t pid,
+                                                 const typename S::R (&post)[19]) {
+    using T = typename S::T;
+    if constexpr (S::kStochastic) {
+        uint32_t x = sr_seed(gid, (uint32_t)a.state->step);
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            x = sr_next(x);
+            if (REP_S) S::st_rt_sr((T*)a.plane[opp(q)] + pid, opp(q), post[q], x);
+            else S::st_rt_sr((T*)a.plane[q] + (uint32_t)(pid + (uint32_t)a.doff[q]), q, post[q], x);
+        }
+    } else {
+        store_cell<S, REP_S>(a, pid, post);
+    }
+}
+
 // Moments in the reference order (rho over q = 0..18, momentum componentwise).
 template <class R>
 __device__ __forceinline__ void moments(const R (&f)[19], R& rho, R& ux, R& uy, R& uz) {
@@ -368,7 +387,7 @@ __device__ __forceinline__ void rare_cell(const BulkArgs& a, uint32_t gid, int x
         collide<R, COLL>(f, rho, vx, vy, vz, (R)a.fp.omega_p, (R)a.fp.omega_m, post, activation, restriction);
     }
     finish_cell<S, COLL>(a, gid, x, y, z, a.capture == 1, post, activation, restriction);
-    store_cell<S, REP_S>(a, pid, post);
+    store_fluid_cell<S, REP_S>(a, gid, pid, post);
 }
 
 // ---------------------------------------------------------------------------
@@ -420,7 +439,7 @@ __global__ void __launch_bounds__(256, sizeof(typename S::R) == 8 ? 1 : (COLL ==
         collide<R, COLL>(f, rho, ux, uy, uz, (R)a.fp.omega_p, (R)a.fp.omega_m, post, activation, restriction);
     }
     finish_cell<S, COLL>(a, gid, x, y, z, CAPTURE == 1, post, activation, restriction);
-    store_cell<S, REP_S>(a, pid, post);
+    store_fluid_cell<S, REP_S>(a, gid, pid, post);
 }
 
 // Solid / newly uncovered cells of the geometry box in a launch of their own

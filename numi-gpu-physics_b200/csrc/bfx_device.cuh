@@ -92,21 +92,52 @@ template <class R> __device__ __forceinline__ R feq_rt(int q, R rho, R ux, R uy,
 // Deviation formats store f - w_q (the equilibrium at rest), halving the bytes
 // per cell; FP16 additionally scales by 2^12 to keep small deviations normal.
 // ---------------------------------------------------------------------------
+//
+// Stochastic rounding (BF16).  bfloat16 keeps 8 significant bits of f - w_q, so
+// a fluid update smaller than half a unit in the last place of the stored
+// deviation (a slowly decaying low-amplitude flow changes by ~1e-4 of itself
+// per step) is lost every step under round-to-nearest and the flow freezes.
+// The BF16 fluid stores therefore round up with probability equal to the
+// discarded fraction: 16 pseudo-random bits are added to the FP32 bit pattern
+// below the kept bits before truncation, an unbiased rounding whose expected
+// value is the FP32 result.  The bits come from a hash of (cell, step) advanced
+// by the Numerical Recipes linear congruential step per direction, so a run is
+// reproducible bit for bit and independent of how steps are batched.
+__device__ __forceinline__ uint32_t sr_seed(uint32_t cell, uint32_t step) {
+    uint32_t h = cell * 0x9E3779B1u + step * 0x85EBCA77u;  // golden-ratio and Murmur3-finaliser odd constants
+    h ^= h >> 15;
+    h *= 0x2C1B3C6Du;
+    h ^= h >> 12;
+    h *= 0x297A2D39u;
+    h ^= h >> 15;
+    return h;
+}
+__device__ __forceinline__ uint32_t sr_next(uint32_t x) { return x * 1664525u + 1013904223u; }
+__device__ __forceinline__ __nv_bfloat16 bf16_stochastic(float v, uint32_t x) {
+    // the high half of the LCG state: its low bits are the weak ones
+    const uint32_t b = __float_as_uint(v) + (x >> 16);
+    return __ushort_as_bfloat16((unsigned short)(b >> 16));
+}
+
 struct StoreF32 {
     using T = float;
     using R = float;
+    static constexpr bool kStochastic = false;
     template <int Q> __device__ __forceinline__ static R ld(const T* p) { return *p; }
     template <int Q> __device__ __forceinline__ static void st(T* p, R v) { *p = v; }
     __device__ __forceinline__ static R ld_rt(const T* p, int) { return *p; }
     __device__ __forceinline__ static void st_rt(T* p, int, R v) { *p = v; }
+    __device__ __forceinline__ static void st_rt_sr(T* p, int, R v, uint32_t) { *p = v; }
 };
 struct StoreF64 {
     using T = double;
     using R = double;
+    static constexpr bool kStochastic = false;
     template <int Q> __device__ __forceinline__ static R ld(const T* p) { return *p; }
     template <int Q> __device__ __forceinline__ static void st(T* p, R v) { *p = v; }
     __device__ __forceinline__ static R ld_rt(const T* p, int) { return *p; }
     __device__ __forceinline__ static void st_rt(T* p, int, R v) { *p = v; }
+    __device__ __forceinline__ static void st_rt_sr(T* p, int, R v, uint32_t) { *p = v; }
 };
 constexpr float kF16Scale = 4096.0f;
 constexpr float kF16InvScale = 1.0f / 4096.0f;
@@ -130,10 +161,13 @@ struct StoreF16Dev {
         float w = q == 0 ? Lat<float>::w0 : (q <= 6 ? Lat<float>::w1 : Lat<float>::w2);
         *p = __float2half_rn(__fmaf_rn(v, kF16Scale, -w * kF16Scale));
     }
+    __device__ __forceinline__ static void st_rt_sr(T* p, int q, R v, uint32_t) { st_rt(p, q, v); }
     // the stored value itself: the deviation f - w_q scaled by kDevScale
     static constexpr float kDevScale = kF16Scale;
+    static constexpr bool kStochastic = false;
     __device__ __forceinline__ static float ld_dev(const T* p) { return __half2float(*p); }
     __device__ __forceinline__ static void st_dev(T* p, float v) { *p = __float2half_rn(v); }
+    __device__ __forceinline__ static void st_dev_sr(T* p, float v, uint32_t) { *p = __float2half_rn(v); }
 };
 struct StoreBF16Dev {
     using T = __nv_bfloat16;
@@ -151,9 +185,16 @@ struct StoreBF16Dev {
         float w = q == 0 ? Lat<float>::w0 : (q <= 6 ? Lat<float>::w1 : Lat<float>::w2);
         *p = __float2bfloat16_rn(v - w);
     }
+    // fluid updates: stochastic rounding with the LCG state x (see sr_seed)
+    __device__ __forceinline__ static void st_rt_sr(T* p, int q, R v, uint32_t x) {
+        float w = q == 0 ? Lat<float>::w0 : (q <= 6 ? Lat<float>::w1 : Lat<float>::w2);
+        *p = bf16_stochastic(v - w, x);
+    }
     static constexpr float kDevScale = 1.0f;
+    static constexpr bool kStochastic = true;
     __device__ __forceinline__ static float ld_dev(const T* p) { return __bfloat162float(*p); }
     __device__ __forceinline__ static void st_dev(T* p, float v) { *p = __float2bfloat16_rn(v); }
+    __device__ __forceinline__ static void st_dev_sr(T* p, float v, uint32_t x) { *p = bf16_stochastic(v, x); }
 };
 
 // ---------------------------------------------------------------------------

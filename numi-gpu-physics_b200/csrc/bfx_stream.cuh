@@ -88,9 +88,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
 }
 // Bounded wait: every iteration is a hardware-suspended try_wait, so the limit
 // ends a wait that can no longer complete after at most a few seconds.
-constexpr int kWaitLimit = 1 << 20;
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-    for (int i = 0; i < kWaitLimit; ++i)
+constexpr uint32_t kWaitLimit = 1u << 20;
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }

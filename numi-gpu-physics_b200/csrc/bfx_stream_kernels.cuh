@@ -217,19 +217,30 @@ __global__ void __launch_bounds__(StreamShape<COLL>::threads, 1)
     }
     __syncthreads();
     const Grid& g = a.g;
+    // bounded waits; the test hook can shorten them and withhold one tile
+    const uint32_t hook_limit = a.state->test_wait_limit;
+    const uint32_t wait_limit = hook_limit ? hook_limit : kWaitLimit;
     if (warp == SH::consumers) {
         // producer: one thread issues the 19 box loads of each tile
         if (lane != 0) return;
+        const int stall_tile = (int)a.state->test_stall_tile1 - 1;
         int issued = 0;
-        bool failed = false;
+        bool failed = false, stalled = false;
         for (int k = 0;; ++k) {
             const int tile = blockIdx.x + k * gridDim.x;
             if (tile >= tl.ntiles) break;
             const int s = k % NS;
-            if (k >= NS && !mbar_wait(empty0 + 8 * s, ((k / NS) + 1) & 1)) {
+            if (k >= NS && !mbar_wait(empty0 + 8 * s, ((k / NS) + 1) & 1, wait_limit)) {
                 atomicOr(&a.state->stream_error, 1u);
                 failed = true;
                 break;
+            }
+            if (tile == stall_tile) {
+                // test hook: no loads (and no arrival) for this tile, so its
+                // consumers' wait runs out; nothing is left in flight for it
+                issued = k + 1;
+                stalled = true;
+                continue;
             }
             const int txi = tile % tl.tiles_x;
             const int rest = tile / tl.tiles_x;
@@ -246,11 +257,14 @@ __global__ void __launch_bounds__(StreamShape<COLL>::threads, 1)
             }
             issued = k + 1;
         }
-        if (failed) {
-            // leave no bulk copy in flight into this CTA's shared memory: wait
-            // (bounded) for the last loads issued to complete
+        if (failed || stalled) {
+            // leave no bulk copy in flight into this CTA's shared memory (the
+            // consumers may have stopped consuming): wait (bounded) for the
+            // loads of the last NS tiles issued, the only ones that can still
+            // be in flight, to complete
             for (int k = issued - NS < 0 ? 0 : issued - NS; k < issued; ++k)
-                (void)mbar_wait(full0 + 8 * (k % NS), (k / NS) & 1);
+                if ((int)blockIdx.x + k * (int)gridDim.x != stall_tile)
+                    (void)mbar_wait(full0 + 8 * (k % NS), (k / NS) & 1, wait_limit);
         }
         return;
     }
@@ -259,6 +273,7 @@ __global__ void __launch_bounds__(StreamShape<COLL>::threads, 1)
     // The mask bytes of the next tile are loaded one tile ahead, so their HBM
     // latency overlaps the current tile's collision.
     const FluidParams& fp = a.fp;
+    const uint32_t step_seed = S::kStochastic ? (uint32_t)a.state->step : 0u;
     struct Cells {
         int xa, y, z;
         uint32_t gida;
@@ -294,7 +309,7 @@ __global__ void __launch_bounds__(StreamShape<COLL>::threads, 1)
         const uint32_t gida = cur.gida;
         bool va = cur.va, vb = cur.vb;
         const uint8_t ma = cur.ma, mb = cur.mb;
-        if (!mbar_wait(full0 + 8 * s, (k / NS) & 1)) {
+        if (!mbar_wait(full0 + 8 * s, (k / NS) & 1, wait_limit)) {
             atomicOr(&a.state->stream_error, 2u);
             break;
         }
@@ -373,11 +388,24 @@ __global__ void __launch_bounds__(StreamShape<COLL>::threads, 1)
         }
         const uint32_t pid =
             (uint32_t)(xa + 1) + (uint32_t)g.px * ((uint32_t)(y + 1) + (uint32_t)g.py * (uint32_t)(z + 1));
+        if constexpr (S::kStochastic) {
+            // BF16: stochastic rounding (sr_seed), one stream per cell
+            uint32_t ra = sr_seed(gida, step_seed), rb = sr_seed(gida + 32, step_seed);
 #pragma unroll
-        for (int q = 0; q < 19; ++q) {
-            T* p = REP_S ? (T*)a.plane[opp(q)] + pid : (T*)a.plane[q] + (uint32_t)(pid + (uint32_t)a.doff[q]);
-            if (va) S::st_dev(p, post[q].x);
-            if (vb) S::st_dev(p + 32, post[q].y);
+            for (int q = 0; q < 19; ++q) {
+                T* p = REP_S ? (T*)a.plane[opp(q)] + pid : (T*)a.plane[q] + (uint32_t)(pid + (uint32_t)a.doff[q]);
+                ra = sr_next(ra);
+                rb = sr_next(rb);
+                if (va) S::st_dev_sr(p, post[q].x, ra);
+                if (vb) S::st_dev_sr(p + 32, post[q].y, rb);
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 19; ++q) {
+                T* p = REP_S ? (T*)a.plane[opp(q)] + pid : (T*)a.plane[q] + (uint32_t)(pid + (uint32_t)a.doff[q]);
+                if (va) S::st_dev(p, post[q].x);
+                if (vb) S::st_dev(p + 32, post[q].y);
+            }
         }
     }
 }

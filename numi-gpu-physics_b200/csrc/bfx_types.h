@@ -72,6 +72,11 @@ struct DeviceState {
     uint64_t launches_device;
     double power_lattice;          // last step: sum over cut links of F_link . u_wall (lattice units)
     uint32_t stream_error;         // nonzero: a staged-kernel pipeline wait timed out (1 producer, 2 consumer)
+    // test hook of the staged kernel's bounded waits (bfx_test_stall_staged_kernel):
+    // the producer skips the loads of tile test_stall_tile1 - 1 (0: none) and
+    // every wait gives up after test_wait_limit polls (0: the default limit)
+    uint32_t test_stall_tile1;
+    uint32_t test_wait_limit;
     uint32_t apply_done;           // link-kernel blocks finished this launch (0 between launches)
     SegmentFrame seg[4];           // mesh segments 3..6: left / right middle, left / right outer
 };

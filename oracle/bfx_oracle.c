@@ -1167,6 +1167,111 @@ float or_ellipsoid_link_fraction(const or_params* p, const or_bird* bird, const 
 }
 
 /* ------------------------------------------------------------------ */
+/* Coupled momentum ledger: measureFluidMassMomentumChange and          */
+/* captureExternalFluidSources (BF.metal:4322-4552).  The reference     */
+/* forms each cell's terms in FP32 and sums FP32 threadgroup partials;  */
+/* the library (and this restatement) forms them in FP64 from the FP32  */
+/* populations and sums in FP64.                                        */
+/* ------------------------------------------------------------------ */
+void or_ledger_sources(const or_params* p, const float* pin, const float* pout, const uint8_t* mprev,
+                       const uint8_t* mcur, const float* wall, double out[24]) {
+    const int64_t n = ncells(p);
+    double acc[24] = {0};
+    const int periodic_any = axis_periodic(p, 0) || axis_periodic(p, 1) || axis_periodic(p, 2);
+#pragma omp parallel
+    {
+        double loc[24] = {0};
+#pragma omp for schedule(static)
+        for (int z = 0; z < p->nz; ++z) {
+            for (int y = 0; y < p->ny; ++y) {
+                for (int x = 0; x < p->nx; ++x) {
+                    int64_t gid = flat(p, x, y, z);
+                    int was_solid = mprev[gid] != 0, is_solid = mcur[gid] != 0;
+                    /* measureFluidMassMomentumChange: cells that were fluid before, that are fluid after */
+                    for (int q = 0; q < 19; ++q) {
+                        if (!was_solid) {
+                            double v = pin[(int64_t)q * n + gid];
+                            loc[0] += v;
+                            loc[1] += v * C[q][0];
+                            loc[2] += v * C[q][1];
+                            loc[3] += v * C[q][2];
+                        }
+                        if (!is_solid) {
+                            double v = pout[(int64_t)q * n + gid];
+                            loc[4] += v;
+                            loc[5] += v * C[q][0];
+                            loc[6] += v * C[q][1];
+                            loc[7] += v * C[q][2];
+                        }
+                    }
+                    if (was_solid != is_solid) loc[23] += 1.0;
+                    if (is_solid) continue;
+                    int persistent_target = !was_solid;
+                    double mwd = p->far[3];
+                    if (p->local_density) {
+                        mwd = 0.0;
+                        for (int q = 0; q < 19; ++q) mwd += pin[(int64_t)q * n + gid];
+                    }
+                    int interior = x > 0 && y > 0 && z > 0 && x + 1 < p->nx && y + 1 < p->ny && z + 1 < p->nz;
+                    for (int q = 0; q < 19; ++q) {
+                        int sx = x - C[q][0], sy = y - C[q][1], sz = z - C[q][2];
+                        int outside = !interior && !inside3(p, sx, sy, sz);
+                        if (outside && !periodic_any) {
+                            /* open face: the reference's far-field rule; a velocity or outflow face
+                               brings in the value the step pulls there, as the library's faces do */
+                            double incoming = outside_value(p, q, x, y, z, sx, sy, sz, pin, mcur);
+                            double outgoing = pin[(int64_t)OPP[q] * n + gid];
+                            loc[8] += incoming - outgoing;
+                            loc[9] += (incoming + outgoing) * C[q][0];
+                            loc[10] += (incoming + outgoing) * C[q][1];
+                            loc[11] += (incoming + outgoing) * C[q][2];
+                            loc[20] += 1.0;
+                            continue;
+                        }
+                        if (outside) {
+                            sx = sx < 0 ? p->nx - 1 : (sx >= p->nx ? 0 : sx);
+                            sy = sy < 0 ? p->ny - 1 : (sy >= p->ny ? 0 : sy);
+                            sz = sz < 0 ? p->nz - 1 : (sz >= p->nz ? 0 : sz);
+                        }
+                        int64_t src = flat(p, sx, sy, sz);
+                        if (persistent_target && mcur[src] != 0 && mprev[src] != 0) {
+                            /* halfway moving-wall reflection, the reference's ledger rule */
+                            double reflected = pin[(int64_t)OPP[q] * n + gid];
+                            double cu = C[q][0] * (double)wall[4 * src] + C[q][1] * (double)wall[4 * src + 1] +
+                                        C[q][2] * (double)wall[4 * src + 2];
+                            double wc = 2.0 * (double)W[q] * mwd * cu / (double)CS2;
+                            double incoming = reflected + wc;
+                            loc[12] += incoming - reflected;
+                            loc[13] += (incoming + reflected) * C[q][0];
+                            loc[14] += (incoming + reflected) * C[q][1];
+                            loc[15] += (incoming + reflected) * C[q][2];
+                            loc[22] += 1.0;
+                        }
+                    }
+                    float sponge = sponge_factor(p, x, y, z);
+                    if (sponge > 0.0f) {
+                        double inv = 1.0 / fmax(1.0 - (double)sponge, 1.0e-7);
+                        for (int q = 0; q < 19; ++q) {
+                            double actual = pout[(int64_t)q * n + gid];
+                            double far = or_equilibrium(q, p->far[3], p->far);
+                            double d = (double)sponge * (far - actual) * inv;
+                            loc[16] += d;
+                            loc[17] += d * C[q][0];
+                            loc[18] += d * C[q][1];
+                            loc[19] += d * C[q][2];
+                        }
+                        loc[21] += 1.0;
+                    }
+                }
+            }
+        }
+#pragma omp critical
+        for (int k = 0; k < 24; ++k) acc[k] += loc[k];
+    }
+    for (int k = 0; k < 24; ++k) out[k] = acc[k];
+}
+
+/* ------------------------------------------------------------------ */
 /* Prescribed flapping wing (Li-Nabawy beta planform): the analytic      */
 /* geometry of MetalFlappingWingValidation (BF.metal:940-1297).          */
 /* ------------------------------------------------------------------ */

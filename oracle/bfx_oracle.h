@@ -127,6 +127,18 @@ void or_build_ellipsoid(const or_params* p, const or_bird* bird, const or_prepar
 float or_ellipsoid_link_fraction(const or_params* p, const or_bird* bird, const or_prepared* prep,
                                  int fx, int fy, int fz, int sx, int sy, int sz);
 
+/* ---- coupled momentum ledger (BF.metal:4322-4552) ----------------------
+ * Lattice-unit sums over one step from pin (before) to pout (after) with the
+ * step's masks (mprev before, mcur after) and wall field: out[0..3] mass and
+ * momentum of the cells that were fluid (pin), [4..7] of the cells that are
+ * fluid (pout), [8..11] the open-face source (incoming - outgoing, momentum
+ * (incoming + outgoing) c), [12..15] the persistent cut-link exchange on the
+ * halfway moving-wall rule, [16..19] the sponge source recovered from
+ * f_out = (1 - s) f_post + s f_far, [20] open-face links, [21] sponge cells,
+ * [22] persistent links, [23] cells that changed occupancy. */
+void or_ledger_sources(const or_params* p, const float* pin, const float* pout, const uint8_t* mprev,
+                       const uint8_t* mcur, const float* wall, double out[24]);
+
 /* ---- prescribed flapping wing (MetalFlappingWingValidation's analytic wing) */
 typedef struct or_wing {     /* GPUFlappingWingParameters, GPUData.swift:383-388 */
     or_f4 root_and_chord, geometry, kinematics0, kinematics1;

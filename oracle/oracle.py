@@ -123,6 +123,7 @@ def lib():
         L.or_wing_violation.restype = ct.c_float
         L.or_wing_violation.argtypes = [P(Params), P(Wing), P(WingPrepared), fp]
         L.or_wing_link_fractions.argtypes = [P(Params), P(Wing), P(WingPrepared), P(ct.c_uint32), u8p, ct.c_int64, fp]
+        L.or_ledger_sources.argtypes = [P(Params), fp, fp, u8p, u8p, fp, dp]
         L.or_powf.restype = ct.c_float
         L.or_powf.argtypes = [ct.c_float, ct.c_float]
         L.or_ellipsoid_link_fraction.restype = ct.c_float
@@ -384,7 +385,9 @@ class OracleSim:
                                  self.keys.ctypes.data_as(ct.POINTER(ct.c_uint64)), fptr(self.pa),
                                  u8ptr(self.mcur), u8ptr(target), fptr(self.wall), fptr(self.covered))
 
-    def step(self, capture_fields=False, per_cell_loads=False):
+    def step(self, capture_fields=False, per_cell_loads=False, ledger=False):
+        """One step; with ``ledger`` the step's coupled-momentum ledger sums
+        (or_ledger_sources) are left in ``self.ledger``."""
         L = lib()
         self.p.capture_fields = int(capture_fields)
         absolute = self.step_index + 1
@@ -401,6 +404,10 @@ class OracleSim:
         L.or_step(ct.byref(self.p), fptr(self.pa), fptr(self.pb), u8ptr(self.mcur), u8ptr(self.mnext),
                   fptr(self.wall), fptr(self.covered), fptr(self.density), fptr(self.velocity), fptr(body_f),
                   dptr(body_d), ct.byref(self.loads), fptr(pcl))
+        if ledger:
+            self.ledger = np.zeros(24, np.float64)
+            L.or_ledger_sources(ct.byref(self.p), fptr(self.pa), fptr(self.pb), u8ptr(self.mcur), u8ptr(self.mnext),
+                                fptr(self.wall), dptr(self.ledger))
         self.load_history.append((np.array(self.loads.f64_force), np.array(self.loads.f64_torque)))
         if self.p.free_flight:
             force = np.array(self.loads.f64_force, np.float64)

@@ -526,3 +526,81 @@ def test_flow_diagnostics_of_a_leased_frame_match_numpy():
     print("exact:", np.array_equal(vort, want[0]), np.array_equal(q, want[1]))
     lease.release()
     sim.close()
+
+
+def test_staged_kernel_wait_timeout_invalidates_the_handle():
+    """The staged 16-bit kernel's bounded pipeline waits, made to run out by
+    the test hook (one tile's loads withheld, a short wait limit): the advance
+    fails with BFX_ERR_KERNEL, the handle refuses every later call with
+    BFX_ERR_INVALIDATED (the reference's terminal command-buffer failure,
+    BirdFlowSimulation.swift:2059-2095), and fresh handles on the same GPU
+    step normally and agree bit for bit."""
+    cfg, _, _, _ = cases.shear_wave(n=64, viscosity=0.02, amplitude=0.02, storage=L.STORAGE_F16_DEVIATION)
+    lat = lattice(cfg)
+    lat.advance(2)
+    lib = lat.lib
+    assert lib.bfx_test_stall_staged_kernel(lat.handle, 0, 1 << 14) == 0
+    assert lib.bfx_advance(lat.handle, 1, 1, 0, None, 0, None) == 4  # BFX_ERR_KERNEL
+    assert "timed out" in L.last_error(lat.handle)
+    assert lib.bfx_advance(lat.handle, 1, 1, 0, None, 0, None) == 6  # BFX_ERR_INVALIDATED
+    lat.close()
+    runs = []
+    for _ in range(2):
+        fresh = lattice(cfg)
+        fresh.advance(5)
+        runs.append(fresh.populations())
+        fresh.close()
+    assert np.all(np.isfinite(runs[0])) and np.array_equal(runs[0], runs[1])
+    # a handle without the staged kernel has no such hook
+    cfg32, _, _, _ = cases.shear_wave(n=16, storage=L.STORAGE_F32)
+    plain = lattice(cfg32)
+    assert lib.bfx_test_stall_staged_kernel(plain.handle, 0, 1 << 14) == 10  # BFX_ERR_UNSUPPORTED
+    plain.close()
+
+
+def test_ledger_terms_match_the_oracle_restatement():
+    """Each source term of the coupled momentum ledger (measureFluidMassMomentumChange
+    and captureExternalFluidSources, BF.metal:4322-4552) per step on the
+    compact free-flight bird, against the oracle's restatement on the same
+    populations: fluid momentum before and after, the open far-field faces,
+    the sponge, the persistent cut-link exchange and every count.  Both form
+    each cell's terms in FP64 from the same FP32 populations and sum in FP64
+    in different orders, so each term agrees to 1e-12 of its gross size (the
+    sum of the magnitudes it cancels, bounded from the term's count) plus
+    1e-9 of its value; the counts are equal."""
+    from bfx.simulation import BirdFlowSimulation
+    config, bird, state = cases.compact_bird(free_flight=True)
+    sim = BirdFlowSimulation(config, bird, state)
+    lat = sim.lattice
+    cfg = lat.config
+    rows = bird.packed()
+    body = (state.position_meters, state.orientation_body_to_world, state.linear_velocity_meters_per_second,
+            state.angular_velocity_body_radians_per_second)
+    osim = oracle_twin(cfg, rows, body)
+    mscale = float(cfg.force_to_physical) * float(cfg.time_step)
+    terms = {"fluid_momentum_before": slice(1, 4), "fluid_momentum_after": slice(5, 8),
+             "far_field_impulse": slice(9, 12), "link_exchange_impulse": slice(13, 16),
+             "sponge_impulse": slice(17, 20)}
+    n = int(cfg.nx) * int(cfg.ny) * int(cfg.nz)
+    # gross size per term (lattice units): every population and |f + f'| here is below 1
+    gross_of = {"fluid_momentum_before": lambda o: 19.0 * n, "fluid_momentum_after": lambda o: 19.0 * n,
+                "far_field_impulse": lambda o: o[20], "link_exchange_impulse": lambda o: o[22],
+                "sponge_impulse": lambda o: 19.0 * o[21]}
+    seen = {k: 0.0 for k in terms}
+    for step in range(12):
+        sample = lat.advance_ledger(1)[0]
+        osim.step(ledger=True)
+        o = osim.ledger
+        for name, sl in terms.items():
+            g = np.array(getattr(sample, name), np.float64)
+            ref = o[sl] * mscale
+            seen[name] = max(seen[name], float(np.max(np.abs(ref))))
+            tol = 1e-12 * gross_of[name](o) * mscale + 1e-9 * np.abs(ref)
+            assert np.all(np.abs(g - ref) <= tol), (step + 1, name, g, ref)
+        assert sample.far_field_links == int(o[20]), step + 1
+        assert sample.sponge_cells == int(o[21]), step + 1
+        assert sample.boundary_links == int(o[22]), step + 1
+        assert sample.topology_cells == int(o[23]), step + 1
+    # every term was exercised
+    assert all(v > 0.0 for v in seen.values()), seen
+    sim.close()
