@@ -402,3 +402,36 @@ def flapping_wing(chord=8, storage=L.STORAGE_F32, collision=L.COLLISION_TRT, cyc
                           p["pitch_duration"]]
     w.kinematics1.v[:] = [p["pitch_low"], p["pitch_high"], max_rate, p["lattice_speed"]]
     return cfg, w
+
+
+def measured_surface_replay(surface, first=60, frames=4, cell_size=0.004, steps_per_frame=5, viscosity=0.02,
+                            half_thickness_cells=0.75, margin_cells=12, storage=L.STORAGE_F32,
+                            link_rule=L.LINK_LINEAR):
+    """A keyframe replay of a measured bird surface sequence (bfx.measured),
+    frames first ... first + frames - 1, on a lattice that covers the window's
+    positions plus `margin_cells`: the body (all vertices, held at the
+    sequence's body origin) with the frames' positions as body-frame offsets,
+    half thickness 0.75 cells (MetalFlappingWingValidation's default measured
+    half thickness), `steps_per_frame` steps per frame interval, parts 1-4 from
+    the sequence's components, far-field faces."""
+    mesh = surface.keyframe_mesh(first, frames)
+    pts = surface.positions[first:first + frames].reshape(-1, 3).astype(np.float64)
+    lo = pts.min(axis=0) - margin_cells * cell_size
+    hi = pts.max(axis=0) + margin_cells * cell_size
+    n = [int(math.ceil((h - l) / cell_size)) for l, h in zip(lo, hi)]
+    interval = float(surface.times[first + 1] - surface.times[first])
+    dt = interval / steps_per_frame
+    op, om = _trt_rates(viscosity, 3.0 / 16.0)
+    rho = 1.225
+    cfg = default_config(n[0], n[1], n[2], origin=[float(v) for v in lo], cell_size=cell_size, time_step=dt,
+                         velocity_to_lattice=dt / cell_size, force_to_physical=rho * cell_size ** 4 / dt ** 2,
+                         omega_plus=op, omega_minus=om, face_bc=[L.BC_FARFIELD] * 6, geometry=L.GEOMETRY_MESH,
+                         wall_rule=L.WALL_INTERPOLATED, storage=storage, link_rule=link_rule,
+                         mesh_half_thickness=half_thickness_cells * cell_size, sponge_width=4.0,
+                         sponge_strength=0.02)
+    rows = zero_bird_rows()
+    rows[0] = (0.05, 0.03, 0.03, 0.3)
+    rows[1] = (1e-4, 1e-4, 1e-4, 0.0)
+    rows[8] = (0.0, 0.15, 0.0, 0.0)
+    body = ((0.0, 0.0, 0.0), (0.0, 0.0, 0.0, 1.0), (0.0, 0.0, 0.0), (0.0, 0.0, 0.0))
+    return cfg, rows, body, mesh
