@@ -404,20 +404,24 @@ def articulated_measure(device, steps=100, warmup=5):
     return workload_measure("articulated_bird", L.STORAGE_F16_DEVIATION, device, steps, warmup)
 
 
-def adjoint_measure(device):
-    """Discrete adjoint on the flapping-plate pair at 256x128x128 (span 40,
-    chord 8, T = 2000, one period, FP32, TRT, linear links): gradient of the
+def adjoint_measure(device, scan_points=11, scan_half_width=2e-2, fd_h=1e-3):
+    """Discrete adjoint on the flapping-plate pair of the precision workload
+    scaled to 256x128x128 (span 32, chord 6, thickness 2, 2 x 8,192
+    triangles; T = 2000, one period, FP32, TRT, linear links): gradient of the
     cycle-mean lift and aerodynamic power with respect to (stroke amplitude,
-    pitch amplitude, pitch phase, deviation amplitude); cost against a plain
-    forward pass; central differences with h = 1e-3 rad; FP32 against FP64
-    gradients at 96x48x48."""
+    pitch amplitude, pitch phase, deviation amplitude) and its cost against a
+    plain forward pass.  Checked against (a) central differences with
+    h = 1e-3 rad and (b) the least-squares slope of J over `scan_points`
+    offsets in +-2e-2 rad, with the slope's standard error (the scatter of J
+    about the line: cover / uncover events make J piecewise smooth); and the
+    FP32 against the FP64 gradient at 96x48x48."""
     import bfx._lib as L
     import bfx.cases as cases
     from bfx.simulation import Lattice, bird_struct
 
-    def plates(storage, theta=None, n=(256, 128, 128), span=40.0, chord=8.0):
+    def plates(storage, theta=None, n=(256, 128, 128), span=32.0, chord=6.0):
         cfg, rows, body, mesh = cases.flapping_plates(
-            nx=n[0], ny=n[1], nz=n[2], span=span, chord=chord, thickness=2.0, n_chord=16, n_span=64, period=2000.0,
+            nx=n[0], ny=n[1], nz=n[2], span=span, chord=chord, thickness=2.0, n_chord=32, n_span=128, period=2000.0,
             stroke_deg=60.0, pitch_deg=45.0, deviation_deg=5.0, viscosity=0.004, storage=storage,
             link_rule=L.LINK_LINEAR, sponge_width=12.0)
         if theta is not None:
@@ -438,8 +442,8 @@ def adjoint_measure(device):
     lat.advance(steps, batch_size=steps)
     fwd_ms = lat.timer_end()
     lat.close()
-    out = {"case": "flapping_plates 256x128x128, span 40, chord 8, 2x2048 triangles, T=2000, nu=0.004, TRT, "
-                   "linear links, FP32", "steps": steps,
+    out = {"case": "flapping_plates 256x128x128, span 32, chord 6, thickness 2, 2x8192 triangles, T=2000, "
+                   "nu=0.004, TRT, linear links, FP32", "steps": steps,
            "parameters": ["stroke amplitude", "pitch amplitude", "pitch phase", "deviation amplitude"],
            "theta": theta0.tolist(), "forward_ms": fwd_ms}
     for name, fw, pw in (("lift", (0.0, 0.0, 1.0), 0.0), ("power", (0.0, 0.0, 0.0), 1.0)):
@@ -450,38 +454,57 @@ def adjoint_measure(device):
                      "adjoint_reverse_ms": r.reverse_ms, "checkpoint_interval": r.checkpoint_interval,
                      "snapshots": r.snapshots, "work_bytes": r.work_bytes,
                      "cost_vs_forward": (r.forward_ms + r.reverse_ms) / fwd_ms}
-    # central differences of both objectives with h = 1e-3 rad.  Over a full
-    # period some cells change occupancy between the two runs of a pair; those
-    # cover / uncover jumps are in the differences but not in the derivative
-    # of the smooth piece the adjoint computes.
-    h = 1e-3
 
     def objectives(theta):
         lat, _ = plates(L.STORAGE_F32, theta)
-        lift, power = [], []
+        lift, power = 0.0, 0.0
         for _ in range(steps):
             lat.advance(1)
             ld = lat.loads()
-            lift.append(ld.force[2])
-            power.append(ld.power)
+            lift += ld.force[2]
+            power += ld.power
         lat.close()
-        return float(np.mean(lift)), float(np.mean(power))
+        return lift / steps, power / steps
 
-    fd_lift, fd_power = [], []
+    offsets = np.linspace(-scan_half_width, scan_half_width, scan_points)
+    fd = {"lift": [], "power": []}
+    scan = {"lift": [], "power": []}
     for k in range(4):
+        vals = []
+        for o in offsets:
+            th = theta0.copy()
+            th[k] += o
+            vals.append(objectives(th))
         tp, tm = theta0.copy(), theta0.copy()
-        tp[k] += h
-        tm[k] -= h
+        tp[k] += fd_h
+        tm[k] -= fd_h
         (lp, pp), (lm, pm) = objectives(tp), objectives(tm)
-        fd_lift.append((lp - lm) / (2 * h))
-        fd_power.append((pp - pm) / (2 * h))
-    for name, fd in (("lift", fd_lift), ("power", fd_power)):
+        fd["lift"].append((lp - lm) / (2 * fd_h))
+        fd["power"].append((pp - pm) / (2 * fd_h))
+        vals = np.array(vals)
+        A = np.vstack([np.ones_like(offsets), offsets]).T
+        for j, name in enumerate(("lift", "power")):
+            coef, *_ = np.linalg.lstsq(A, vals[:, j], rcond=None)
+            resid = vals[:, j] - A @ coef
+            sigma = float(np.sqrt(np.sum(resid ** 2) / max(len(offsets) - 2, 1)))
+            stderr = sigma / float(np.sqrt(np.sum((offsets - offsets.mean()) ** 2)))
+            scan[name].append({"slope": float(coef[1]), "slope_stderr": stderr, "residual_std": sigma,
+                               "J": vals[:, j].tolist()})
+    for name in ("lift", "power"):
         g = np.array(out[name]["gradient"])
-        out[name]["central_difference"] = fd
-        out[name]["relative_difference_vs_fd"] = float(np.max(np.abs(g - np.array(fd))) / max(np.max(np.abs(fd)), 1e-30))
-    out["central_difference_h"] = h
+        f = np.array(fd[name])
+        sl = np.array([d["slope"] for d in scan[name]])
+        se = np.array([d["slope_stderr"] for d in scan[name]])
+        out[name]["central_difference"] = f.tolist()
+        out[name]["relative_difference_vs_fd"] = float(np.max(np.abs(g - f)) / max(np.max(np.abs(f)), 1e-30))
+        out[name]["regression"] = scan[name]
+        out[name]["relative_difference_vs_regression"] = float(np.max(np.abs(g - sl)) /
+                                                                max(np.max(np.abs(sl)), 1e-30))
+        out[name]["regression_noise_relative"] = float(np.max(se) / max(np.max(np.abs(sl)), 1e-30))
+    out["central_difference_h"] = fd_h
+    out["regression_offsets"] = offsets.tolist()
     # FP64 reference gradient on a 96x48x48 lattice (the same case scaled)
-    small = dict(n=(96, 48, 48), span=15.0, chord=4.0)
+    small = dict(n=(96, 48, 48), span=12.0, chord=2.25)
     grads = {}
     for st in (L.STORAGE_F32, L.STORAGE_F64):
         lat, _ = plates(st, **small)

@@ -107,6 +107,7 @@ struct bfx_sim {
     uint32_t* scan_sums = nullptr;
     int box_blocks = 0;
     int scan_blocks = 0;
+    int topo_rows = 1;
     double* topo_partials = nullptr;
     double* link_partials = nullptr;
     int apply_blocks = 0;
@@ -242,6 +243,7 @@ GeomBuffers geom_buffers(bfx_sim* s, uint8_t* mprev, uint8_t* mnext) {
     b.scan_sums = s->scan_sums;
     b.box_blocks = s->box_blocks;
     b.scan_blocks = s->scan_blocks;
+    b.topo_rows = s->topo_rows;
     b.topo_partials = s->topo_partials;
     b.link_partials = s->link_partials;
     b.apply_blocks = s->apply_blocks;
@@ -816,7 +818,9 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
         BFX_ALLOC(s->block_counts, (size_t)s->box_blocks * sizeof(uint32_t));
         BFX_ALLOC(s->block_offsets, (size_t)s->box_blocks * sizeof(uint32_t));
         BFX_ALLOC(s->scan_sums, (size_t)((s->box_blocks + kScanSegment - 1) / kScanSegment) * sizeof(uint32_t));
-        BFX_ALLOC(s->topo_partials, (size_t)s->box_blocks * 8 * sizeof(double));
+        // the box walks (boundary scan, link emission) run four CTAs per SM
+        s->topo_rows = std::max(1, std::min(s->box_blocks, 4 * s->sm_count));
+        BFX_ALLOC(s->topo_partials, (size_t)s->topo_rows * 8 * sizeof(double));
         s->apply_blocks = 4 * s->sm_count;
         BFX_ALLOC(s->link_partials, (size_t)s->apply_blocks * 16 * sizeof(double));
         uint64_t cap = c.link_capacity ? c.link_capacity

@@ -104,7 +104,8 @@ struct GeomBuffers {
     int kf_count;            // one per kScanSegment scan blocks (two-level scan)
     int box_blocks;                 // blocks of a one-slice-per-block box launch (allocations)
     int scan_blocks;                // blocks of the link count / scan / emission launch
-    double* topo_partials;          // 8 per box block
+    double* topo_partials;          // 8 per walking CTA of the boundary scan
+    int topo_rows;                  // CTAs of the persistent box walks (boundary scan, link emission)
     double* link_partials;          // 16 per apply block (link sums, topology sums)
     int apply_blocks;
     DeviceState* state;
