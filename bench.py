@@ -455,8 +455,10 @@ def adjoint_measure(device, scan_points=11, scan_half_width=2e-2, fd_h=1e-3):
                      "snapshots": r.snapshots, "work_bytes": r.work_bytes,
                      "cost_vs_forward": (r.forward_ms + r.reverse_ms) / fwd_ms}
 
-    def objectives(theta):
+    def objectives(theta, replay=None, mode=0):
         lat, _ = plates(L.STORAGE_F32, theta)
+        if replay is not None:
+            lat.replay_topology(mode, replay.data_ptr(), steps)
         lift, power = 0.0, 0.0
         for _ in range(steps):
             lat.advance(1)
@@ -490,6 +492,27 @@ def adjoint_measure(device, scan_points=11, scan_half_width=2e-2, fd_h=1e-3):
             stderr = sigma / float(np.sqrt(np.sum((offsets - offsets.mean()) ** 2)))
             scan[name].append({"slope": float(coef[1]), "slope_stderr": stderr, "residual_std": sigma,
                                "J": vals[:, j].tolist()})
+    # Central differences at the topology of the unperturbed run (its
+    # occupancy recorded step by step and replayed in the perturbed runs):
+    # the derivative of the smooth piece of J, which the adjoint computes.
+    import torch
+    rec = torch.empty((steps, 256 * 128 * 128), dtype=torch.uint8, device=f"cuda:{device}")
+    objectives(theta0, rec, 1)
+    fd_frozen = {"lift": [], "power": []}
+    for k in range(4):
+        tp, tm = theta0.copy(), theta0.copy()
+        tp[k] += fd_h
+        tm[k] -= fd_h
+        (lp, pp), (lm, pm) = objectives(tp, rec, 2), objectives(tm, rec, 2)
+        fd_frozen["lift"].append((lp - lm) / (2 * fd_h))
+        fd_frozen["power"].append((pp - pm) / (2 * fd_h))
+    del rec
+    for name in ("lift", "power"):
+        g = np.array(out[name]["gradient"])
+        ff = np.array(fd_frozen[name])
+        out[name]["central_difference_frozen_topology"] = ff.tolist()
+        out[name]["relative_difference_vs_frozen_topology_fd"] = float(np.max(np.abs(g - ff)) /
+                                                                       max(np.max(np.abs(ff)), 1e-30))
     for name in ("lift", "power"):
         g = np.array(out[name]["gradient"])
         f = np.array(fd[name])

@@ -448,6 +448,19 @@ BFX_API int bfx_timer_end(bfx_sim* sim, double* elapsed_ms);
  * and other handles stay usable.  BFX_ERR_UNSUPPORTED when the handle does not
  * run the staged kernel (FP32 / FP64 storage or the limiter operator). */
 BFX_API int bfx_test_stall_staged_kernel(bfx_sim* sim, int32_t tile, uint32_t wait_limit);
+/* Test hook for checking the discrete adjoint against finite differences of
+ * the objective at a fixed topology; no reference counterpart.  mode 1 records
+ * the occupancy (the mask bytes, n per step) of each following step into
+ * device_masks, step k of the recording at k * nx*ny*nz; mode 2 replaces each
+ * following step's freshly classified occupancy by the recorded one (the wall
+ * field, link fractions and loads still follow this handle's geometry), so a
+ * run with perturbed kinematic parameters keeps the recorded cut-link sets;
+ * mode 0 turns it off.  The recording counts steps from the call; steps past
+ * capacity_steps are neither recorded nor replaced.  While on, steps run
+ * without CUDA graphs or the pipelined geometry build.  The buffer is the
+ * caller's and must outlive the mode.  BFX_ERR_UNSUPPORTED without moving
+ * geometry. */
+BFX_API int bfx_test_replay_topology(bfx_sim* sim, int mode, uint8_t* device_masks, uint64_t capacity_steps);
 /* Total kernel launches issued by the library on this handle. */
 BFX_API int bfx_launch_count(bfx_sim* sim, uint64_t* launches);
 /* Bytes of device memory held by the handle. */

@@ -172,6 +172,7 @@ EXPORTED = (
     "bfx_last_error", "bfx_set_observation_buffers", "bfx_acquire_field_frame", "bfx_field_frame_copy",
     "bfx_release_field_frame", "bfx_release_field_frame_after", "bfx_capture_current_fields",
     "bfx_observation_counters", "bfx_flow_diagnostics", "bfx_create_flapping_wing", "bfx_test_stall_staged_kernel",
+    "bfx_test_replay_topology",
 )
 
 _lib = None
@@ -198,6 +199,7 @@ def load(path: str | None = None):
     L.bfx_create.argtypes = [P(Config), P(Bird), P(BodyState), P(Mesh), P(vp)]
     L.bfx_create_flapping_wing.argtypes = [P(Config), P(FlappingWing), P(vp)]
     L.bfx_test_stall_staged_kernel.argtypes = [vp, ct.c_int32, ct.c_uint32]
+    L.bfx_test_replay_topology.argtypes = [vp, ct.c_int, ct.c_void_p, ct.c_uint64]
     L.bfx_destroy.argtypes = [vp]
     L.bfx_destroy.restype = None
     L.bfx_advance.argtypes = [vp, ct.c_uint64, ct.c_uint32, ct.c_uint32, P(RunSample), ct.c_size_t, P(AdvanceResult)]

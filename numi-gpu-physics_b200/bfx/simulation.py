@@ -457,6 +457,13 @@ class Lattice:
             raise C.CheckpointError("solid-mask file does not match the restart state")
         return manifest
 
+    def replay_topology(self, mode: int, device_masks_ptr: int = 0, capacity_steps: int = 0):
+        """bfx_test_replay_topology: 1 records each following step's occupancy
+        into the device buffer at device_masks_ptr (capacity_steps x n bytes), 2
+        replays a recording, 0 turns the hook off."""
+        _check(self.lib.bfx_test_replay_topology(self.handle, int(mode), ct.c_void_p(int(device_masks_ptr) or None),
+                                                 int(capacity_steps)), self.handle)
+
     def adjoint(self, steps: int, force_weight=(0.0, 0.0, 0.0), power_weight: float = 0.0, window=None,
                 checkpoint_interval: int = 0) -> L.AdjointResult:
         """Advances `steps` steps and runs the discrete adjoint backward

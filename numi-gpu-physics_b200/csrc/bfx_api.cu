@@ -107,7 +107,6 @@ struct bfx_sim {
     uint32_t* scan_sums = nullptr;
     int box_blocks = 0;
     int scan_blocks = 0;
-    int topo_rows = 1;
     double* topo_partials = nullptr;
     double* link_partials = nullptr;
     int apply_blocks = 0;
@@ -148,6 +147,12 @@ struct bfx_sim {
     cudaStream_t side = nullptr;
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     cudaEvent_t halo_fork_ev = nullptr, halo_join_ev = nullptr;
+    // topology record / replay test hook (bfx_test_replay_topology): 0 off,
+    // 1 record each step's occupancy into topo_buf, 2 replace it from there
+    int topo_mode = 0;
+    uint8_t* topo_buf = nullptr;
+    uint64_t topo_cap = 0;
+    uint64_t topo_next = 0;
     bool graphs_enabled = true;
     // pinned host staging of the device state: read-backs and body uploads
     // without a pageable-copy bounce
@@ -243,7 +248,6 @@ GeomBuffers geom_buffers(bfx_sim* s, uint8_t* mprev, uint8_t* mnext) {
     b.scan_sums = s->scan_sums;
     b.box_blocks = s->box_blocks;
     b.scan_blocks = s->scan_blocks;
-    b.topo_rows = s->topo_rows;
     b.topo_partials = s->topo_partials;
     b.link_partials = s->link_partials;
     b.apply_blocks = s->apply_blocks;
@@ -306,6 +310,23 @@ void encode_links(bfx_sim* s, uint8_t* mprev, uint8_t* mnext) {
     s->launches += 5;
 }
 
+// The pipelined path's split of encode_links.  The cut-link list (counts,
+// offsets, emission, fractions) depends on the step's geometry alone, so it is
+// built on the side stream with the geometry, beside the previous step's fluid
+// kernel; the topology impulses read the pre-step populations and run on the
+// main stream once that kernel is done.
+void encode_link_build(bfx_sim* s, uint8_t* mprev, uint8_t* mnext, cudaStream_t st) {
+    GeomBuffers gb = geom_buffers(s, mprev, mnext);
+    launch_link_count(s->g, s->fp, s->box, gb, st);
+    launch_links_emit(s->cfg.geometry, s->cfg.link_rule, s->g, s->fp, s->box, gb, st);
+    s->launches += 5;
+}
+void encode_topology(bfx_sim* s, uint8_t* mprev, uint8_t* mnext) {
+    GeomBuffers gb = geom_buffers(s, mprev, mnext);
+    launch_topology_scan(s->cfg.storage, s->rep_s, s->g, s->fp, s->box, gb, fluid_buffers(s, mnext), s->stream);
+    s->launches += 1;
+}
+
 void timing_begin(bfx_sim* s) {
     if (!s->timing) return;
     if (s->ev_used >= s->ev_start.size()) {
@@ -346,6 +367,8 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
     uint8_t* mprev = s->mask[s->cur];
     uint8_t* mnext = s->moving() ? s->mask[s->cur ^ 1] : s->mask[s->cur];
     FluidBuffers fb = fluid_buffers(s, s->geometry() ? mnext : nullptr);
+    // geometry_ready: this step's geometry and cut-link list were built on the
+    // side stream during the previous step (pipelined path)
     // the halo fill forks off here (after the previous step's fluid kernel)
     // and joins before this step's fluid kernel
     const bool halo_side = halo_beside_links(s) && !tape && !ledger_in;
@@ -359,11 +382,23 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
     if (s->moving() && !geometry_ready) {
         encode_geometry_build(s, 0, mprev, mnext);
     }
+    if (s->topo_mode && s->moving() && !tape) {
+        // the test hook's record / replay of the step's occupancy (direct steps only)
+        const uint64_t i = s->topo_next++;
+        if (i < s->topo_cap) {
+            uint8_t* rec = s->topo_buf + i * (size_t)s->g.n;
+            if (s->topo_mode == 1) cudaMemcpyAsync(rec, mnext, (size_t)s->g.n, cudaMemcpyDeviceToDevice, s->stream);
+            else cudaMemcpyAsync(mnext, rec, (size_t)s->g.n, cudaMemcpyDeviceToDevice, s->stream);
+        }
+    }
     if (tape) {
         launch_frame_tangent(geom_buffers(s, mprev, mnext), s->cfg.time_step, 0, tape->frames, s->stream);
         s->launches += 1;
     }
-    if (s->geometry() && s->moving()) encode_links(s, mprev, mnext);
+    if (s->geometry() && s->moving()) {
+        if (geometry_ready) encode_topology(s, mprev, mnext);
+        else encode_links(s, mprev, mnext);
+    }
     if (tape) {
         GeomBuffers gb = geom_buffers(s, mprev, mnext);
         gb.frames = tape->frames;
@@ -417,6 +452,7 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
         cudaEventRecord(s->fork_ev, s->stream);
         cudaStreamWaitEvent(s->side, s->fork_ev, 0);
         encode_geometry_build(s, 0, mnext, mprev, s->side);
+        encode_link_build(s, mnext, mprev, s->side);
         cudaEventRecord(s->join_ev, s->side);
         launch_bulk_stream(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, box, s->stream);
         cudaStreamWaitEvent(s->stream, s->join_ev, 0);
@@ -818,9 +854,7 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
         BFX_ALLOC(s->block_counts, (size_t)s->box_blocks * sizeof(uint32_t));
         BFX_ALLOC(s->block_offsets, (size_t)s->box_blocks * sizeof(uint32_t));
         BFX_ALLOC(s->scan_sums, (size_t)((s->box_blocks + kScanSegment - 1) / kScanSegment) * sizeof(uint32_t));
-        // the box walks (boundary scan, link emission) run four CTAs per SM
-        s->topo_rows = std::max(1, std::min(s->box_blocks, 4 * s->sm_count));
-        BFX_ALLOC(s->topo_partials, (size_t)s->topo_rows * 8 * sizeof(double));
+        BFX_ALLOC(s->topo_partials, (size_t)s->box_blocks * 8 * sizeof(double));
         s->apply_blocks = 4 * s->sm_count;
         BFX_ALLOC(s->link_partials, (size_t)s->apply_blocks * 16 * sizeof(double));
         uint64_t cap = c.link_capacity ? c.link_capacity
@@ -1030,7 +1064,7 @@ int bfx_advance(bfx_sim* s, uint64_t steps, uint32_t batch_size, uint32_t flags,
         // Pairs of plain steps replay a captured graph; steps that capture
         // fields, record samples or are individually timed are encoded directly.
         const bool last_batch = done + count == steps;
-        if (s->graphs_enabled && !record && !s->timing && can_pipeline(s) && count > 1) {
+        if (s->graphs_enabled && !record && !s->timing && !s->topo_mode && can_pipeline(s) && count > 1) {
             // Pipelined: every step but the batch's last builds the next
             // step's geometry beside its own fluid kernel.  The batch's first
             // step builds its own; pairs replay a graph while a step of the
@@ -1047,7 +1081,7 @@ int bfx_advance(bfx_sim* s, uint64_t steps, uint32_t batch_size, uint32_t flags,
                 encode_step(s, capture && last && last_batch ? 1 : 0, nullptr, 0, nullptr, nullptr, true, !last);
                 s->capture_slot = 0;
             }
-        } else if (s->graphs_enabled && !record && !s->timing) {
+        } else if (s->graphs_enabled && !record && !s->timing && !s->topo_mode) {
             uint64_t plain = capture && done + count == steps ? count - 1 : count;
             for (; k + 1 < plain; k += 2) {
                 int rc = run_pair_graph(s);
@@ -1518,6 +1552,21 @@ int bfx_test_stall_staged_kernel(bfx_sim* s, int32_t tile, uint32_t wait_limit) 
     const cudaError_t e = cudaMemcpy((char*)s->dstate + offsetof(DeviceState, test_stall_tile1), v, sizeof(v),
                                      cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_fail(s, e, "stall hook");
+    return BFX_OK;
+}
+
+int bfx_test_replay_topology(bfx_sim* s, int mode, uint8_t* device_masks, uint64_t capacity_steps) {
+    BFX_GUARD(s);
+    if (mode < 0 || mode > 2) return fail(s, BFX_ERR_INVALID_ARGUMENT, "mode must be 0 (off), 1 (record) or 2 (replay)");
+    if (mode != 0 && !s->moving()) return fail(s, BFX_ERR_UNSUPPORTED, "topology replay needs moving geometry");
+    if (mode != 0 && (!device_masks || capacity_steps == 0))
+        return fail(s, BFX_ERR_INVALID_ARGUMENT, "record and replay need a device buffer of capacity_steps masks");
+    const int rc = sync_check(s, "topology replay");
+    if (rc != BFX_OK) return rc;
+    s->topo_mode = mode;
+    s->topo_buf = mode ? device_masks : nullptr;
+    s->topo_cap = mode ? capacity_steps : 0;
+    s->topo_next = 0;
     return BFX_OK;
 }
 

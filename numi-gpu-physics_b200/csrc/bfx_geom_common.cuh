@@ -143,54 +143,6 @@ __device__ __forceinline__ bool block_inactive(const GeomArgs& a) {
     const int z = o[2] + (int)blockIdx.z;
     return x1 < lo[0] || x0 > hi[0] || y1 < lo[1] || y0 > hi[1] || z < lo[2] || z > hi[2];
 }
-// Persistent walks over the blocks of a box launch (box_shape): a grid of a
-// few CTAs per SM visits box block b = bx + gx (by + gy bz) as CTA
-// b % gridDim.x, in increasing b, with the block shape of the box launch, so
-// most of the box (inactive blocks) costs a bounds test instead of a block
-// launch.
-struct BoxGrid {
-    int gx, gy, nb;
-};
-__device__ __forceinline__ BoxGrid box_grid(const GeomArgs& a) {
-    BoxGrid r;
-    r.gx = (a.bx + (int)blockDim.x - 1) / (int)blockDim.x;
-    r.gy = (a.by + (int)blockDim.y - 1) / (int)blockDim.y;
-    r.nb = r.gx * r.gy * a.bz;
-    return r;
-}
-__device__ __forceinline__ void box_block_origin(const GeomArgs& a, const BoxGrid& bg, int b, int& lx0, int& ly0,
-                                                 int& lz) {
-    const int bxi = b % bg.gx, rest = b / bg.gx;
-    lx0 = bxi * (int)blockDim.x;
-    ly0 = (rest % bg.gy) * (int)blockDim.y;
-    lz = rest / bg.gy;
-}
-// box_cell for the thread's cell of box block b.
-__device__ __forceinline__ bool box_cell_of(const GeomArgs& a, const BoxGrid& bg, int b, int& x, int& y, int& z,
-                                            int64_t& bidx) {
-    int lx0, ly0, lz;
-    box_block_origin(a, bg, b, lx0, ly0, lz);
-    const int lx = lx0 + (int)threadIdx.x, ly = ly0 + (int)threadIdx.y;
-    if (lx >= a.bx || ly >= a.by || lz >= a.bz) return false;
-    const int32_t* o = a.b.state->box_origin;
-    x = o[0] + lx;
-    y = o[1] + ly;
-    z = o[2] + lz;
-    bidx = (int64_t)lx + (int64_t)a.bx * ((int64_t)ly + (int64_t)a.by * lz);
-    return x < a.g.nx && y < a.g.ny && z < a.g.nz;
-}
-// block_inactive for box block b.
-__device__ __forceinline__ bool block_inactive_of(const GeomArgs& a, const BoxGrid& bg, int b) {
-    int lo[3], hi[3];
-    active_bounds(a, lo, hi);
-    int lx0, ly0, lz;
-    box_block_origin(a, bg, b, lx0, ly0, lz);
-    const int32_t* o = a.b.state->box_origin;
-    const int x0 = o[0] + lx0, x1 = x0 + (int)blockDim.x - 1;
-    const int y0 = o[1] + ly0, y1 = y0 + (int)blockDim.y - 1;
-    const int z = o[2] + lz;
-    return x1 < lo[0] || x0 > hi[0] || y1 < lo[1] || y0 > hi[1] || z < lo[2] || z > hi[2];
-}
 __device__ __forceinline__ bool in_bounds(const int (&lo)[3], const int (&hi)[3], int x, int y, int z) {
     return x >= lo[0] && x <= hi[0] && y >= lo[1] && y <= hi[1] && z >= lo[2] && z <= hi[2];
 }

@@ -957,7 +957,9 @@ __device__ __forceinline__ bool may_have_links(const GeomArgs& a, int64_t bidx, 
 // ---------------------------------------------------------------------------
 // Topology impulses and cut-link count of one cell (BF.metal:2557-2609
 // covered, 2616-2666 uncovered).
-template <class S>
+// PARTS: 1 the link count (geometry only), 2 the topology impulses (reads the
+// populations), 3 both.
+template <class S, int PARTS>
 __device__ __forceinline__ void scan_cell(const GeomArgs& a, int rep_s, int x, int y, int z, int64_t bidx,
                                           double (&acc)[8], uint32_t& links) {
     using R = typename S::R;
@@ -972,7 +974,8 @@ __device__ __forceinline__ void scan_cell(const GeomArgs& a, int rep_s, int x, i
     const typename S::T* A = (const typename S::T*)a.pops;
     const double* body = a.b.state->body;
     const V3 world = cell_world(fp, x, y, z);
-    if ((m1 & kCovered) && fp.accumulate && include_topo) {
+    if (!(PARTS & 2)) {
+    } else if ((m1 & kCovered) && fp.accumulate && include_topo) {
         // newly covered: previous fluid momentum (minus the wall-moving density for estimators 0-5)
         R pd = 0, pmx = 0, pmy = 0, pmz = 0;
         for (int q = 0; q < 19; ++q) {
@@ -1017,7 +1020,7 @@ __device__ __forceinline__ void scan_cell(const GeomArgs& a, int rep_s, int x, i
         add_load<R>(acc, tx, ty, tz, (R)world.x, (R)world.y, (R)world.z, body, fp.f2p);
         acc[7] += 1.0;
     }
-    if (may_have_links(a, bidx, m1, m0)) {
+    if ((PARTS & 1) && may_have_links(a, bidx, m1, m0)) {
         for (int q = 1; q < 19; ++q) {
             int sx, sy, sz;
             if (link_source(g, a.b.mask_next, x, y, z, q, sx, sy, sz) >= 0) ++links;
@@ -1025,44 +1028,49 @@ __device__ __forceinline__ void scan_cell(const GeomArgs& a, int rep_s, int x, i
     }
 }
 
-// Persistent walk over the box blocks (box_grid): each visited block writes
-// its link count; each CTA sums the topology impulses of all its blocks' cells
-// (every thread in its fixed cell order) into one row of 8 partials.
-template <class S>
+// PARTS 3: both halves in one pass; 1: the per-block link counts alone (the
+// pipelined path builds the next step's link list from its geometry beside the
+// fluid kernel); 2: the topology impulses alone (after the fluid kernel).
+template <class S, int PARTS>
 __global__ void __launch_bounds__(256) k_boundary_scan(const GeomArgs a, int rep_s) {
     __shared__ double sh[8][256];
-    __shared__ uint32_t wcount[8];
-    const BoxGrid bg = box_grid(a);
-    const int t = linear_tid();
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int b = blockIdx.x; b < bg.nb; b += gridDim.x) {
-        if (block_inactive_of(a, bg, b)) {
-            // no key, link or topology change in this block
-            if (t == 0) a.b.block_counts[b] = 0;
-            continue;
+    uint32_t links = 0;
+    if (block_inactive(a)) {
+        // no key, link or topology change in this block
+        if (linear_tid() == 0) {
+            const int block = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+            if (PARTS & 1) a.b.block_counts[block] = 0;
+            if (PARTS & 2)
+                for (int k = 0; k < 8; ++k) a.b.topo_partials[8 * block + k] = 0.0;
         }
-        uint32_t links = 0;
+        return;
+    }
+    {
         int x, y, z;
         int64_t bidx;
-        if (box_cell_of(a, bg, b, x, y, z, bidx) && cell_active(a, x, y, z))
-            scan_cell<S>(a, rep_s, x, y, z, bidx, acc, links);
-        for (int o = 16; o > 0; o >>= 1) links += __shfl_down_sync(0xffffffffu, links, o);
-        if ((t & 31) == 0) wcount[t >> 5] = links;
-        __syncthreads();
-        if (t == 0) {
-            uint32_t tot = 0;
-            for (int w = 0; w < 8; ++w) tot += wcount[w];
-            a.b.block_counts[b] = tot;
-        }
-        __syncthreads();
+        if (box_cell(a, x, y, z, bidx) && cell_active(a, x, y, z))
+            scan_cell<S, PARTS>(a, rep_s, x, y, z, bidx, acc, links);
     }
-    // most CTAs hold no covered / uncovered cell: skip their FP64 tree
+    // most blocks hold no covered / uncovered cell: skip their FP64 tree
     bool nonzero = false;
     for (int k = 0; k < 8; ++k) nonzero = nonzero || acc[k] != 0.0;
-    const bool cta_nonzero = __syncthreads_or(nonzero) != 0;
-    if (cta_nonzero) block_sum<8>(acc, sh);
-    if (t == 0)
-        for (int k = 0; k < 8; ++k) a.b.topo_partials[8 * blockIdx.x + k] = cta_nonzero ? acc[k] : 0.0;
+    const bool block_nonzero = __syncthreads_or(nonzero) != 0;
+    if (block_nonzero) block_sum<8>(acc, sh);
+    __shared__ uint32_t wcount[8];
+    uint32_t wl = links;
+    for (int o = 16; o > 0; o >>= 1) wl += __shfl_down_sync(0xffffffffu, wl, o);
+    const int t = linear_tid();
+    if ((t & 31) == 0) wcount[t >> 5] = wl;
+    __syncthreads();
+    const int block = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    if (t == 0) {
+        uint32_t tot = 0;
+        for (int w = 0; w < 8; ++w) tot += wcount[w];
+        if (PARTS & 1) a.b.block_counts[block] = tot;
+        if (PARTS & 2)
+            for (int k = 0; k < 8; ++k) a.b.topo_partials[8 * block + k] = block_nonzero ? acc[k] : 0.0;
+    }
 }
 
 // Exclusive scan of the per-block link counts into block offsets, in two
@@ -1140,52 +1148,47 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const GeomArgs a, int nseg)
 // the preceding threads, so the list is ordered by box cell then direction.
 __global__ void __launch_bounds__(256) k_links_emit(const GeomArgs a, int geometry, int link_rule, int interpolated) {
     __shared__ uint32_t wsum[8];
+    const int block = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    // blocks without links (most of the box) emit nothing
+    if (a.b.block_counts[block] == 0) return;
     const Grid& g = a.g;
-    const BoxGrid bg = box_grid(a);
+    uint32_t mine = 0;
+    int x = 0, y = 0, z = 0;
+    int64_t bidx = 0, gid = 0;
+    bool valid = box_cell(a, x, y, z, bidx) && cell_active(a, x, y, z);
+    if (valid) {
+        gid = flat(g, x, y, z);
+        valid = may_have_links(a, bidx, a.b.mask_next[gid], a.b.mask_prev[gid]);
+    }
+    if (valid) {
+        for (int q = 1; q < 19; ++q) {
+            int sx, sy, sz;
+            if (link_source(g, a.b.mask_next, x, y, z, q, sx, sy, sz) >= 0) ++mine;
+        }
+    }
+    // block-exclusive prefix of `mine`
     const int t = linear_tid();
     const int lane = t & 31, warp = t >> 5;
-    // persistent walk over the box blocks; blocks without links (most of the
-    // box) emit nothing
-    for (int b = blockIdx.x; b < bg.nb; b += gridDim.x) {
-        if (a.b.block_counts[b] == 0) continue;
-        uint32_t mine = 0;
-        int x = 0, y = 0, z = 0;
-        int64_t bidx = 0, gid = 0;
-        bool valid = box_cell_of(a, bg, b, x, y, z, bidx) && cell_active(a, x, y, z);
-        if (valid) {
-            gid = flat(g, x, y, z);
-            valid = may_have_links(a, bidx, a.b.mask_next[gid], a.b.mask_prev[gid]);
+    uint32_t incl = mine;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    uint32_t wbase = 0;
+    for (int w = 0; w < warp; ++w) wbase += wsum[w];
+    uint32_t pos = a.b.block_offsets[block] + wbase + incl - mine;
+    if (mine == 0) return;
+    for (int q = 1; q < 19; ++q) {
+        int sx, sy, sz;
+        int64_t src = link_source(g, a.b.mask_next, x, y, z, q, sx, sy, sz);
+        if (src < 0) continue;
+        if (pos < a.b.link_capacity) {
+            a.b.link_cell[pos] = (uint32_t)gid;
+            a.b.link_meta[pos] = (uint32_t)q | ((uint32_t)(a.b.mask_next[src] & kPartMask) << 8);
         }
-        if (valid) {
-            for (int q = 1; q < 19; ++q) {
-                int sx, sy, sz;
-                if (link_source(g, a.b.mask_next, x, y, z, q, sx, sy, sz) >= 0) ++mine;
-            }
-        }
-        // block-exclusive prefix of `mine`
-        uint32_t incl = mine;
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += v;
-        }
-        if (lane == 31) wsum[warp] = incl;
-        __syncthreads();
-        uint32_t wbase = 0;
-        for (int w = 0; w < warp; ++w) wbase += wsum[w];
-        uint32_t pos = a.b.block_offsets[b] + wbase + incl - mine;
-        if (mine != 0) {
-            for (int q = 1; q < 19; ++q) {
-                int sx, sy, sz;
-                int64_t src = link_source(g, a.b.mask_next, x, y, z, q, sx, sy, sz);
-                if (src < 0) continue;
-                if (pos < a.b.link_capacity) {
-                    a.b.link_cell[pos] = (uint32_t)gid;
-                    a.b.link_meta[pos] = (uint32_t)q | ((uint32_t)(a.b.mask_next[src] & kPartMask) << 8);
-                }
-                ++pos;
-            }
-        }
-        __syncthreads();  // wsum is rewritten by the next block
+        ++pos;
     }
     (void)geometry;
     (void)link_rule;
@@ -1416,7 +1419,7 @@ __global__ void __launch_bounds__(256) k_links_apply(const GeomArgs a, int rep_s
     if (__syncthreads_or(nonzero)) block_sum<8>(acc, sh);
     double tp[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     if (with_topology) {
-        const int nb = a.b.topo_rows;
+        const int nb = a.b.scan_blocks;
         const int per = (nb + (int)gridDim.x - 1) / (int)gridDim.x;
         const int lo = (int)blockIdx.x * per;
         const int hi = lo + per < nb ? lo + per : nb;
@@ -1659,10 +1662,11 @@ void launch_classify(int geometry, int has_prev, const GridDesc& g, const FluidP
 }
 
 template <class S>
-static void scan_s(const GeomArgs& a, int rep_s, const BoxDesc& box, cudaStream_t s) {
+static void scan_s(const GeomArgs& a, int rep_s, const BoxDesc& box, int parts, cudaStream_t s) {
     dim3 grid, block;
     box_shape(box, grid, block);
-    k_boundary_scan<S><<<a.b.topo_rows, block, 0, s>>>(a, rep_s);
+    if (parts == 2) k_boundary_scan<S, 2><<<grid, block, 0, s>>>(a, rep_s);
+    else k_boundary_scan<S, 3><<<grid, block, 0, s>>>(a, rep_s);
 }
 
 #define BFX_DISPATCH_STORAGE(storage, FN, ...)                             \
@@ -1676,7 +1680,21 @@ static void scan_s(const GeomArgs& a, int rep_s, const BoxDesc& box, cudaStream_
 void launch_boundary_scan(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
                           const GeomBuffers& gb, const FluidBuffers& fb, cudaStream_t s) {
     GeomArgs a = make_geom(g, fp, box, gb, fb.pops);
-    BFX_DISPATCH_STORAGE(storage, scan_s, a, rep_s, box, s);
+    BFX_DISPATCH_STORAGE(storage, scan_s, a, rep_s, box, 3, s);
+}
+
+void launch_topology_scan(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
+                          const GeomBuffers& gb, const FluidBuffers& fb, cudaStream_t s) {
+    GeomArgs a = make_geom(g, fp, box, gb, fb.pops);
+    BFX_DISPATCH_STORAGE(storage, scan_s, a, rep_s, box, 2, s);
+}
+
+void launch_link_count(const GridDesc& g, const FluidParams& fp, const BoxDesc& box, const GeomBuffers& gb,
+                       cudaStream_t s) {
+    GeomArgs a = make_geom(g, fp, box, gb, nullptr);
+    dim3 grid, block;
+    box_shape(box, grid, block);
+    k_boundary_scan<StoreF32, 1><<<grid, block, 0, s>>>(a, 0);
 }
 
 void launch_links_emit(int geometry, int link_rule, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
@@ -1687,7 +1705,7 @@ void launch_links_emit(int geometry, int link_rule, const GridDesc& g, const Flu
     k_scan_apply<<<nseg, 1024, 0, s>>>(a, nseg);
     dim3 grid, block;
     box_shape(box, grid, block);
-    k_links_emit<<<a.b.topo_rows, block, 0, s>>>(a, geometry, link_rule, fp.interpolated);
+    k_links_emit<<<grid, block, 0, s>>>(a, geometry, link_rule, fp.interpolated);
     if (geometry == BFX_GEOMETRY_MESH && link_rule == BFX_LINK_RAY_ROOT && fp.interpolated) {
         const unsigned rblocks =
             (unsigned)std::max<int64_t>(1, std::min<int64_t>(4096, ((int64_t)gb.link_capacity * 16 + 127) / 128));

@@ -104,8 +104,7 @@ struct GeomBuffers {
     int kf_count;            // one per kScanSegment scan blocks (two-level scan)
     int box_blocks;                 // blocks of a one-slice-per-block box launch (allocations)
     int scan_blocks;                // blocks of the link count / scan / emission launch
-    double* topo_partials;          // 8 per walking CTA of the boundary scan
-    int topo_rows;                  // CTAs of the persistent box walks (boundary scan, link emission)
+    double* topo_partials;          // 8 per box block
     double* link_partials;          // 16 per apply block (link sums, topology sums)
     int apply_blocks;
     DeviceState* state;
@@ -123,6 +122,13 @@ void launch_boundary_scan(int storage, int rep_s, const GridDesc& g, const Fluid
                           const GeomBuffers& gb, const FluidBuffers& fb, cudaStream_t s);
 void launch_links_emit(int geometry, int link_rule, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
                        const GeomBuffers& gb, cudaStream_t s);
+// The two halves of the boundary scan, for the pipelined path: the per-block
+// link counts from the geometry alone, and the topology impulses (which read
+// the pre-step populations) alone.
+void launch_link_count(const GridDesc& g, const FluidParams& fp, const BoxDesc& box, const GeomBuffers& gb,
+                       cudaStream_t s);
+void launch_topology_scan(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
+                          const GeomBuffers& gb, const FluidBuffers& fb, cudaStream_t s);
 // Coupled momentum ledger passes (bfx_ledger.cu): `blocks` rows of 16 (in) or
 // 9 (out) FP64 partial sums.
 constexpr int kLedgerInWidth = 16;
