@@ -38,10 +38,12 @@ On one GPU the line also carries
   ``articulated``  the articulated bird at 768x384x384 in FP16-deviation
                 storage: GLUPS and the share of the step outside the fused kernel;
   ``ellipsoid_channel``  the RR3 channel at 256x128x128 in FP32;
-  ``adjoint``   the discrete adjoint on the plates at 256x128x128 over one
-                period: lift and power gradients, cost against a forward pass,
-                central differences (h = 1e-3 rad) and FP32 vs FP64 gradients
-                at 96x48x48.
+  ``adjoint``   the discrete adjoint on the plates of the precision workload
+                scaled to 256x128x128 over one period: lift and power
+                gradients, cost against a forward pass, central differences
+                (h = 1e-3 rad) of the full objective and at the unperturbed
+                run's topology, the least-squares slope over +-2e-2 rad, and
+                FP32 vs FP64 gradients at 96x48x48.
 (--no-variants / --no-adjoint / --no-cpu skip the extras.)
 """
 from __future__ import annotations
@@ -455,8 +457,8 @@ def adjoint_measure(device, scan_points=11, scan_half_width=2e-2, fd_h=1e-3):
                      "snapshots": r.snapshots, "work_bytes": r.work_bytes,
                      "cost_vs_forward": (r.forward_ms + r.reverse_ms) / fwd_ms}
 
-    def objectives(theta, replay=None, mode=0):
-        lat, _ = plates(L.STORAGE_F32, theta)
+    def objectives(theta, replay=None, mode=0, storage=L.STORAGE_F32):
+        lat, _ = plates(storage, theta)
         if replay is not None:
             lat.replay_topology(mode, replay.data_ptr(), steps)
         lift, power = 0.0, 0.0
@@ -493,20 +495,25 @@ def adjoint_measure(device, scan_points=11, scan_half_width=2e-2, fd_h=1e-3):
             scan[name].append({"slope": float(coef[1]), "slope_stderr": stderr, "residual_std": sigma,
                                "J": vals[:, j].tolist()})
     # Central differences at the topology of the unperturbed run (its
-    # occupancy recorded step by step and replayed in the perturbed runs):
-    # the derivative of the smooth piece of J, which the adjoint computes.
+    # occupancy recorded step by step and replayed in the perturbed runs), in
+    # FP64 with h = 1e-4 rad: the derivative of the smooth piece of J, which
+    # the adjoint computes (a larger h moves fluid cells next to the wall
+    # across the link rule's clamps, a smaller one reaches the FP32
+    # resolution of the geometry).
     import torch
     rec = torch.empty((steps, 256 * 128 * 128), dtype=torch.uint8, device=f"cuda:{device}")
-    objectives(theta0, rec, 1)
+    objectives(theta0, rec, 1, L.STORAGE_F64)
     fd_frozen = {"lift": [], "power": []}
+    hf = 1e-4
     for k in range(4):
         tp, tm = theta0.copy(), theta0.copy()
-        tp[k] += fd_h
-        tm[k] -= fd_h
-        (lp, pp), (lm, pm) = objectives(tp, rec, 2), objectives(tm, rec, 2)
-        fd_frozen["lift"].append((lp - lm) / (2 * fd_h))
-        fd_frozen["power"].append((pp - pm) / (2 * fd_h))
+        tp[k] += hf
+        tm[k] -= hf
+        (lp, pp), (lm, pm) = objectives(tp, rec, 2, L.STORAGE_F64), objectives(tm, rec, 2, L.STORAGE_F64)
+        fd_frozen["lift"].append((lp - lm) / (2 * hf))
+        fd_frozen["power"].append((pp - pm) / (2 * hf))
     del rec
+    out["frozen_topology_h"] = hf
     for name in ("lift", "power"):
         g = np.array(out[name]["gradient"])
         ff = np.array(fd_frozen[name])

@@ -310,23 +310,6 @@ void encode_links(bfx_sim* s, uint8_t* mprev, uint8_t* mnext) {
     s->launches += 5;
 }
 
-// The pipelined path's split of encode_links.  The cut-link list (counts,
-// offsets, emission, fractions) depends on the step's geometry alone, so it is
-// built on the side stream with the geometry, beside the previous step's fluid
-// kernel; the topology impulses read the pre-step populations and run on the
-// main stream once that kernel is done.
-void encode_link_build(bfx_sim* s, uint8_t* mprev, uint8_t* mnext, cudaStream_t st) {
-    GeomBuffers gb = geom_buffers(s, mprev, mnext);
-    launch_link_count(s->g, s->fp, s->box, gb, st);
-    launch_links_emit(s->cfg.geometry, s->cfg.link_rule, s->g, s->fp, s->box, gb, st);
-    s->launches += 5;
-}
-void encode_topology(bfx_sim* s, uint8_t* mprev, uint8_t* mnext) {
-    GeomBuffers gb = geom_buffers(s, mprev, mnext);
-    launch_topology_scan(s->cfg.storage, s->rep_s, s->g, s->fp, s->box, gb, fluid_buffers(s, mnext), s->stream);
-    s->launches += 1;
-}
-
 void timing_begin(bfx_sim* s) {
     if (!s->timing) return;
     if (s->ev_used >= s->ev_start.size()) {
@@ -367,8 +350,6 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
     uint8_t* mprev = s->mask[s->cur];
     uint8_t* mnext = s->moving() ? s->mask[s->cur ^ 1] : s->mask[s->cur];
     FluidBuffers fb = fluid_buffers(s, s->geometry() ? mnext : nullptr);
-    // geometry_ready: this step's geometry and cut-link list were built on the
-    // side stream during the previous step (pipelined path)
     // the halo fill forks off here (after the previous step's fluid kernel)
     // and joins before this step's fluid kernel
     const bool halo_side = halo_beside_links(s) && !tape && !ledger_in;
@@ -395,10 +376,7 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
         launch_frame_tangent(geom_buffers(s, mprev, mnext), s->cfg.time_step, 0, tape->frames, s->stream);
         s->launches += 1;
     }
-    if (s->geometry() && s->moving()) {
-        if (geometry_ready) encode_topology(s, mprev, mnext);
-        else encode_links(s, mprev, mnext);
-    }
+    if (s->geometry() && s->moving()) encode_links(s, mprev, mnext);
     if (tape) {
         GeomBuffers gb = geom_buffers(s, mprev, mnext);
         gb.frames = tape->frames;
@@ -452,7 +430,6 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
         cudaEventRecord(s->fork_ev, s->stream);
         cudaStreamWaitEvent(s->side, s->fork_ev, 0);
         encode_geometry_build(s, 0, mnext, mprev, s->side);
-        encode_link_build(s, mnext, mprev, s->side);
         cudaEventRecord(s->join_ev, s->side);
         launch_bulk_stream(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, box, s->stream);
         cudaStreamWaitEvent(s->stream, s->join_ev, 0);

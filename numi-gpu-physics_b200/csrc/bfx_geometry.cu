@@ -957,9 +957,7 @@ __device__ __forceinline__ bool may_have_links(const GeomArgs& a, int64_t bidx, 
 // ---------------------------------------------------------------------------
 // Topology impulses and cut-link count of one cell (BF.metal:2557-2609
 // covered, 2616-2666 uncovered).
-// PARTS: 1 the link count (geometry only), 2 the topology impulses (reads the
-// populations), 3 both.
-template <class S, int PARTS>
+template <class S>
 __device__ __forceinline__ void scan_cell(const GeomArgs& a, int rep_s, int x, int y, int z, int64_t bidx,
                                           double (&acc)[8], uint32_t& links) {
     using R = typename S::R;
@@ -974,8 +972,7 @@ __device__ __forceinline__ void scan_cell(const GeomArgs& a, int rep_s, int x, i
     const typename S::T* A = (const typename S::T*)a.pops;
     const double* body = a.b.state->body;
     const V3 world = cell_world(fp, x, y, z);
-    if (!(PARTS & 2)) {
-    } else if ((m1 & kCovered) && fp.accumulate && include_topo) {
+    if ((m1 & kCovered) && fp.accumulate && include_topo) {
         // newly covered: previous fluid momentum (minus the wall-moving density for estimators 0-5)
         R pd = 0, pmx = 0, pmy = 0, pmz = 0;
         for (int q = 0; q < 19; ++q) {
@@ -1020,7 +1017,7 @@ __device__ __forceinline__ void scan_cell(const GeomArgs& a, int rep_s, int x, i
         add_load<R>(acc, tx, ty, tz, (R)world.x, (R)world.y, (R)world.z, body, fp.f2p);
         acc[7] += 1.0;
     }
-    if ((PARTS & 1) && may_have_links(a, bidx, m1, m0)) {
+    if (may_have_links(a, bidx, m1, m0)) {
         for (int q = 1; q < 19; ++q) {
             int sx, sy, sz;
             if (link_source(g, a.b.mask_next, x, y, z, q, sx, sy, sz) >= 0) ++links;
@@ -1028,10 +1025,7 @@ __device__ __forceinline__ void scan_cell(const GeomArgs& a, int rep_s, int x, i
     }
 }
 
-// PARTS 3: both halves in one pass; 1: the per-block link counts alone (the
-// pipelined path builds the next step's link list from its geometry beside the
-// fluid kernel); 2: the topology impulses alone (after the fluid kernel).
-template <class S, int PARTS>
+template <class S>
 __global__ void __launch_bounds__(256) k_boundary_scan(const GeomArgs a, int rep_s) {
     __shared__ double sh[8][256];
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -1040,17 +1034,15 @@ __global__ void __launch_bounds__(256) k_boundary_scan(const GeomArgs a, int rep
         // no key, link or topology change in this block
         if (linear_tid() == 0) {
             const int block = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-            if (PARTS & 1) a.b.block_counts[block] = 0;
-            if (PARTS & 2)
-                for (int k = 0; k < 8; ++k) a.b.topo_partials[8 * block + k] = 0.0;
+            a.b.block_counts[block] = 0;
+            for (int k = 0; k < 8; ++k) a.b.topo_partials[8 * block + k] = 0.0;
         }
         return;
     }
     {
         int x, y, z;
         int64_t bidx;
-        if (box_cell(a, x, y, z, bidx) && cell_active(a, x, y, z))
-            scan_cell<S, PARTS>(a, rep_s, x, y, z, bidx, acc, links);
+        if (box_cell(a, x, y, z, bidx) && cell_active(a, x, y, z)) scan_cell<S>(a, rep_s, x, y, z, bidx, acc, links);
     }
     // most blocks hold no covered / uncovered cell: skip their FP64 tree
     bool nonzero = false;
@@ -1067,9 +1059,8 @@ __global__ void __launch_bounds__(256) k_boundary_scan(const GeomArgs a, int rep
     if (t == 0) {
         uint32_t tot = 0;
         for (int w = 0; w < 8; ++w) tot += wcount[w];
-        if (PARTS & 1) a.b.block_counts[block] = tot;
-        if (PARTS & 2)
-            for (int k = 0; k < 8; ++k) a.b.topo_partials[8 * block + k] = block_nonzero ? acc[k] : 0.0;
+        a.b.block_counts[block] = tot;
+        for (int k = 0; k < 8; ++k) a.b.topo_partials[8 * block + k] = block_nonzero ? acc[k] : 0.0;
     }
 }
 
@@ -1662,11 +1653,10 @@ void launch_classify(int geometry, int has_prev, const GridDesc& g, const FluidP
 }
 
 template <class S>
-static void scan_s(const GeomArgs& a, int rep_s, const BoxDesc& box, int parts, cudaStream_t s) {
+static void scan_s(const GeomArgs& a, int rep_s, const BoxDesc& box, cudaStream_t s) {
     dim3 grid, block;
     box_shape(box, grid, block);
-    if (parts == 2) k_boundary_scan<S, 2><<<grid, block, 0, s>>>(a, rep_s);
-    else k_boundary_scan<S, 3><<<grid, block, 0, s>>>(a, rep_s);
+    k_boundary_scan<S><<<grid, block, 0, s>>>(a, rep_s);
 }
 
 #define BFX_DISPATCH_STORAGE(storage, FN, ...)                             \
@@ -1680,21 +1670,7 @@ static void scan_s(const GeomArgs& a, int rep_s, const BoxDesc& box, int parts, 
 void launch_boundary_scan(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
                           const GeomBuffers& gb, const FluidBuffers& fb, cudaStream_t s) {
     GeomArgs a = make_geom(g, fp, box, gb, fb.pops);
-    BFX_DISPATCH_STORAGE(storage, scan_s, a, rep_s, box, 3, s);
-}
-
-void launch_topology_scan(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
-                          const GeomBuffers& gb, const FluidBuffers& fb, cudaStream_t s) {
-    GeomArgs a = make_geom(g, fp, box, gb, fb.pops);
-    BFX_DISPATCH_STORAGE(storage, scan_s, a, rep_s, box, 2, s);
-}
-
-void launch_link_count(const GridDesc& g, const FluidParams& fp, const BoxDesc& box, const GeomBuffers& gb,
-                       cudaStream_t s) {
-    GeomArgs a = make_geom(g, fp, box, gb, nullptr);
-    dim3 grid, block;
-    box_shape(box, grid, block);
-    k_boundary_scan<StoreF32, 1><<<grid, block, 0, s>>>(a, 0);
+    BFX_DISPATCH_STORAGE(storage, scan_s, a, rep_s, box, s);
 }
 
 void launch_links_emit(int geometry, int link_rule, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,

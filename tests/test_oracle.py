@@ -245,9 +245,12 @@ def test_regularized_pair_order_agrees_with_literal_order(rr3):
     direction pairs (moments from pair sums, the equilibrium's even and odd
     parts, the stress from pair non-equilibria).  The reference's literal
     per-direction order gives the same operator to FP32 rounding: within
-    1e-6 of max(|f_q|, w_q) per population, from near-equilibrium populations to ones far
-    enough out to engage the positivity admission, with the same admission
-    decisions."""
+    1e-6 relative per population (each value against its own magnitude) for
+    populations within 20 % of equilibrium, and with the same admission
+    decisions for ones far enough out (95 %) to engage the positivity
+    admission.  There the admitted outputs include populations cut to
+    ~1e-7 w_q, whose few-ulp differences (a cancellation of terms of size
+    w_q) are judged against max(|f_q|, w_q) instead."""
     _, _, w = O.lattice()
     w = w.astype(np.float64)
     rng = np.random.default_rng(5)
@@ -257,8 +260,9 @@ def test_regularized_pair_order_agrees_with_literal_order(rr3):
             f = (w * (1.0 + amp * rng.uniform(-1.0, 1.0, 19))).astype(np.float32)
             lit, act_l, res_l = O.collide_regularized(f, 1.9, rr3, 0)
             par, act_p, res_p = O.collide_regularized(f, 1.9, rr3, 1)
-            scale = np.maximum(np.abs(lit.astype(np.float64)), w)
-            assert np.max(np.abs(lit.astype(np.float64) - par) / scale) <= 1e-6
+            lit64 = lit.astype(np.float64)
+            scale = np.abs(lit64) if amp <= 0.2 else np.maximum(np.abs(lit64), w)
+            assert np.max(np.abs(lit64 - par) / scale) <= 1e-6
             assert act_l == act_p
             assert abs(res_l - res_p) <= 1e-5
             engaged += act_l
