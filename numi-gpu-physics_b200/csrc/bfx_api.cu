@@ -475,7 +475,8 @@ int run_steps_graph(bfx_sim* s, int nsteps, bool pipelined = false) {
         for (int i = 0; i < nsteps; ++i) encode_step(s, 0, nullptr, 0, nullptr, nullptr, pipelined, pipelined);
         e = cudaStreamEndCapture(s->stream, &graph);
         if (e != cudaSuccess) return cuda_fail(s, e, "graph capture end");
-        e = cudaGraphInstantiate(slot, graph, 0);
+        // kernel nodes keep the priority of the stream they were captured on
+        e = cudaGraphInstantiate(slot, graph, cudaGraphInstantiateFlagUseNodePriority);
         cudaGraphDestroy(graph);
         if (e != cudaSuccess) return cuda_fail(s, e, "graph instantiate");
         *count = s->launches - before;
@@ -699,14 +700,23 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
     s->device = config->device;
     cudaSetDevice(s->device);
     cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, s->device);
-    cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    // The main stream (fluid kernel, link build) has the device's greatest
+    // priority and the side stream (the next step's geometry, the halo fill)
+    // its least: when both have blocks waiting, the persistent fluid kernel's
+    // CTAs are placed first and the side kernels fill the resources it leaves.
+    int least_priority = 0, greatest_priority = 0;
+    if (cudaDeviceGetStreamPriorityRange(&least_priority, &greatest_priority) != cudaSuccess) {
+        (void)cudaGetLastError();
+        least_priority = greatest_priority = 0;
+    }
+    cudaError_t e = cudaStreamCreateWithPriority(&s->stream, cudaStreamNonBlocking, greatest_priority);
     if (e != cudaSuccess) {
         bfx_destroy(s);
         return cuda_fail(nullptr, e, "stream creation");
     }
     // side stream for the pipelined geometry build (optional: without it the
     // steps run in order on the main stream)
-    if (cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) != cudaSuccess ||
+    if (cudaStreamCreateWithPriority(&s->side, cudaStreamNonBlocking, least_priority) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->join_ev, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->halo_fork_ev, cudaEventDisableTiming) != cudaSuccess ||

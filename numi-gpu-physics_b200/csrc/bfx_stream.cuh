@@ -35,7 +35,7 @@ template <int COLL>
 struct StreamShape {
     static constexpr bool trt = COLL == BFX_COLLISION_TRT;
     static constexpr int W = trt ? 2 : 1;         // consumer warps per row
-    static constexpr int Y = trt ? 8 : 12;        // rows per tile
+    static constexpr int Y = trt ? 8 : 15;        // rows per tile
     static constexpr int stages = trt ? 2 : 3;    // shared-memory ring depth
     static constexpr int consumers = W * Y;
     static constexpr int threads = 32 * (consumers + 1);  // + one producer warp
