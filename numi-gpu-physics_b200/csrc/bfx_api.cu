@@ -277,7 +277,9 @@ void encode_geometry_build(bfx_sim* s, int init, uint8_t* mprev, uint8_t* mnext,
     GeomBuffers gb = geom_buffers(s, mprev, mnext);
     if (!st) st = s->stream;
     launch_prepare(s->cfg.geometry, s->cfg.time_step, s->g, s->fp, s->box, gb, init, st);
-    launch_classify(s->cfg.geometry, init ? 0 : 1, s->g, s->fp, s->box, gb, st);
+    // beside the TRT staged kernel (pipelined build): the register-lean raster
+    const bool lean = st == s->side && s->cfg.collision == BFX_COLLISION_TRT;
+    launch_classify(s->cfg.geometry, init ? 0 : 1, s->g, s->fp, s->box, gb, st, lean);
     s->launches += 1 + (s->cfg.geometry == BFX_GEOMETRY_MESH ? 4 : 1);
 }
 

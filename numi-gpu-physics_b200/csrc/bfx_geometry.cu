@@ -732,8 +732,12 @@ __global__ void k_mesh_clear(const GeomArgs a) {
 // One warp per triangle: the lanes share the triangle's voxel box (its AABB
 // grown by the half thickness plus two cells, clamped to the lattice and the
 // geometry box) and each keeps the atomic minimum of (quantised distance,
-// triangle id) per voxel.
-__global__ void __launch_bounds__(128) k_mesh_raster(const GeomArgs a) {
+// triangle id) per voxel.  LEAN caps a thread at 32 registers (a few bytes
+// spill): the pipelined build runs the raster beside the persistent TRT fluid
+// kernel, whose CTA leaves about 22 K registers of an SM free, room for five
+// lean blocks against one of the unconstrained (52-register) kernel.
+template <int LEAN>
+__global__ void __launch_bounds__(128, LEAN ? 16 : 1) k_mesh_raster(const GeomArgs a) {
     const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (t >= a.b.ntris) return;
@@ -1632,7 +1636,7 @@ void launch_prepare(int geometry, float dt, const GridDesc& g, const FluidParams
 }
 
 void launch_classify(int geometry, int has_prev, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
-                     const GeomBuffers& gb, cudaStream_t s) {
+                     const GeomBuffers& gb, cudaStream_t s, bool lean_raster) {
     GeomArgs a = make_geom(g, fp, box, gb, nullptr);
     dim3 grid, block;
     box_shape(box, grid, block);
@@ -1647,7 +1651,9 @@ void launch_classify(int geometry, int has_prev, const GridDesc& g, const FluidP
         slab_shape(box, sgrid, sblock);
         k_mesh_prepare<<<(gb.nverts + 255) / 256, 256, 0, s>>>(a);
         k_mesh_clear<<<sgrid, sblock, 0, s>>>(a);
-        k_mesh_raster<<<(unsigned)(((int64_t)gb.ntris * 32 + 127) / 128), 128, 0, s>>>(a);
+        const unsigned rblocks = (unsigned)(((int64_t)gb.ntris * 32 + 127) / 128);
+        if (lean_raster) k_mesh_raster<1><<<rblocks, 128, 0, s>>>(a);
+        else k_mesh_raster<0><<<rblocks, 128, 0, s>>>(a);
         k_mesh_resolve<<<sgrid, sblock, 0, s>>>(a, has_prev);
     }
 }

@@ -117,7 +117,7 @@ struct GeomBuffers {
 void launch_prepare(int geometry, float dt, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
                     const GeomBuffers& gb, int init, cudaStream_t s);
 void launch_classify(int geometry, int has_prev, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
-                     const GeomBuffers& gb, cudaStream_t s);
+                     const GeomBuffers& gb, cudaStream_t s, bool lean_raster = false);
 void launch_boundary_scan(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
                           const GeomBuffers& gb, const FluidBuffers& fb, cudaStream_t s);
 void launch_links_emit(int geometry, int link_rule, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,

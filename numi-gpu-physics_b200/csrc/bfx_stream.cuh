@@ -39,6 +39,11 @@ struct StreamShape {
     static constexpr int stages = trt ? 2 : 3;    // shared-memory ring depth
     static constexpr int consumers = W * Y;
     static constexpr int threads = 32 * (consumers + 1);  // + one producer warp
+    // Register cap of a thread.  The TRT step needs 80 without spilling, which
+    // leaves about 22 K of an SM's registers to the geometry kernels that the
+    // pipelined build runs beside it; the regularized operators take what one
+    // CTA of 16 warps can have.
+    static constexpr int max_regs = trt ? 80 : 65536 / threads;
 };
 
 template <class T, int COLL>

@@ -194,7 +194,7 @@ __device__ __forceinline__ void admit_dev_lane(P2 (&post)[19], int l, float rho,
 // ---------------------------------------------------------------------------
 // One CTA per SM with the operator's tile shape (StreamShape).
 template <class S, int REP_S, int COLL, int CAPTURE>
-__global__ void __launch_bounds__(StreamShape<COLL>::threads, 1)
+__global__ void __maxnreg__(StreamShape<COLL>::max_regs)
     k_stream(const __grid_constant__ CUtensorMap map, const BulkArgs a, const StreamTiles tl) {
     using T = typename S::T;
     using G = StreamGeom<T, COLL>;
