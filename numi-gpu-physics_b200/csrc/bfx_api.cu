@@ -426,11 +426,13 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
     }
     const int box[3] = {s->box.sx, s->box.sy, s->box.sz};
     if (prefetch_next && capture == 0 && !tape && !ledger_in && can_pipeline(s)) {
-        // solid / uncovered cells first (they read the wall field), then fork
-        // the next step's geometry (masks swap roles) beside the fluid kernel
-        launch_bulk_rare(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, box, s->stream);
+        // Beside the fluid kernel, on the side stream: the solid / uncovered
+        // cells (they write only their own slots, which no fluid cell reads or
+        // writes, and read the wall field), then the next step's geometry
+        // (masks swap roles), which rewrites the wall field after them.
         cudaEventRecord(s->fork_ev, s->stream);
         cudaStreamWaitEvent(s->side, s->fork_ev, 0);
+        launch_bulk_rare(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, box, s->side);
         encode_geometry_build(s, 0, mnext, mprev, s->side);
         cudaEventRecord(s->join_ev, s->side);
         launch_bulk_stream(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, box, s->stream);
