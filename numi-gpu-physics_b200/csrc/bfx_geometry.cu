@@ -732,12 +732,12 @@ __global__ void k_mesh_clear(const GeomArgs a) {
 // One warp per triangle: the lanes share the triangle's voxel box (its AABB
 // grown by the half thickness plus two cells, clamped to the lattice and the
 // geometry box) and each keeps the atomic minimum of (quantised distance,
-// triangle id) per voxel.  LEAN caps a thread at 32 registers (a few bytes
+// triangle id) per voxel.  LEAN caps a thread at 40 registers (a few bytes
 // spill): the pipelined build runs the raster beside the persistent TRT fluid
-// kernel, whose CTA leaves about 22 K registers of an SM free, room for five
-// lean blocks against one of the unconstrained (52-register) kernel.
+// kernel, whose CTA leaves about 22 K registers of an SM free, room for four
+// lean blocks against two of the unconstrained (64-register) kernel.
 template <int LEAN>
-__global__ void __launch_bounds__(128, LEAN ? 16 : 1) k_mesh_raster(const GeomArgs a) {
+__global__ void __launch_bounds__(128, LEAN ? 12 : 1) k_mesh_raster(const GeomArgs a) {
     const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (t >= a.b.ntris) return;
@@ -775,15 +775,17 @@ __global__ void __launch_bounds__(128, LEAN ? 16 : 1) k_mesh_raster(const GeomAr
     const float reach2 = reach * reach * 1.0001f;
     // voxel index -> (x, y, z) by reciprocal multiplication (exact for these small extents)
     const float inv_ex = 1.0f / (float)ex, inv_ey = 1.0f / (float)ey;
-    for (int i = lane; i < total; i += 32) {
+    auto voxel = [&](int i, int& x, int& y, int& z) {
         const int r = (int)(((float)i + 0.5f) * inv_ex);
-        const int xi = i - r * ex;
         const int zi = (int)(((float)r + 0.5f) * inv_ey);
-        const int yi = r - zi * ey;
-        const int x = lo[0] + xi, y = lo[1] + yi, z = lo[2] + zi;
+        x = lo[0] + (i - r * ex);
+        y = lo[1] + (r - zi * ey);
+        z = lo[2] + zi;
+    };
+    auto key_voxel = [&](int i) {
+        int x, y, z;
+        voxel(i, x, y, z);
         V3 w = cell_world(a.fp, x, y, z), bary;
-        const V3 dcen = w - cen;
-        if (dot(dcen, dcen) > reach2) continue;
         V3 cp = closest_point(w, A, B, C, bary);
         float dc = length(w - cp) / cs;
         float bin = roundf(dc * 65536.0f);
@@ -791,7 +793,38 @@ __global__ void __launch_bounds__(128, LEAN ? 16 : 1) k_mesh_raster(const GeomAr
         unsigned long long key = (ub << 32) | (unsigned long long)t;
         int64_t bi = (int64_t)(x - o[0]) + (int64_t)a.bx * ((int64_t)(y - o[1]) + (int64_t)a.by * (z - o[2]));
         atomicMin(&a.b.keys[bi], key);
+    };
+    // The sphere test rejects a good share of the box: queue the voxels that
+    // pass (warp ballot into a per-warp list) and run the closest-point search
+    // 32 at a time, so that its lanes are all busy.  Keys are minima, so the
+    // order of the atomics does not matter.
+    __shared__ int queue[4][64];
+    int* qw = queue[(threadIdx.x >> 5) & 3];
+    const unsigned below = (1u << lane) - 1u;
+    int qn = 0;  // warp-uniform queue length (< 32 between rounds)
+    for (int base = 0; base < total; base += 32) {
+        const int i = base + lane;
+        bool pass = false;
+        if (i < total) {
+            int x, y, z;
+            voxel(i, x, y, z);
+            const V3 dcen = cell_world(a.fp, x, y, z) - cen;
+            pass = dot(dcen, dcen) <= reach2;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, pass);
+        if (pass) qw[qn + __popc(m & below)] = i;
+        qn += __popc(m);
+        __syncwarp();
+        if (qn >= 32) {
+            const int mine = qw[lane];
+            __syncwarp();
+            if (lane < qn - 32) qw[lane] = qw[lane + 32];
+            __syncwarp();
+            qn -= 32;
+            key_voxel(mine);
+        }
     }
+    if (lane < qn) key_voxel(qw[lane]);
 }
 
 __device__ void resolve_cell(const GeomArgs& a, int has_prev, int x, int y, int z, int64_t bidx);
