@@ -29,6 +29,18 @@
 namespace bfx {
 namespace BFX_VARIANT {
 
+// sponge_factor with a fast quotient (2 ulp; the 16-bit storage quantum is far larger).
+__device__ __forceinline__ float sponge_factor_fast(const Grid& g, const FluidParams& fp, int x, int y, int z) {
+    const unsigned dx = min((unsigned)x, (unsigned)(g.nx - 1 - x));
+    const unsigned dy = min((unsigned)y, (unsigned)(g.ny - 1 - y));
+    const unsigned dz = min((unsigned)z, (unsigned)(g.nz - 1 - z));
+    const float distance = (float)min(dx, min(dy, dz));
+    const float width = fp.sponge_width;
+    if (distance >= width) return 0.0f;
+    const float nd = fminf(fmaxf(__fdividef(width - distance, fmaxf(width, 1.0f)), 0.0f), 1.0f);
+    return fp.sponge_strength * nd * nd;
+}
+
 // Collision of two cells in scaled deviation space (see above).  d: incoming
 // deviations; post: outgoing deviations.  For the regularized operators,
 // `slow` flags a lane where some outgoing population may fall below its
@@ -52,7 +64,7 @@ __device__ __forceinline__ void collide_dev2(const P2 (&d)[19], float s, float i
         float r = __fmaf_rn(Lanes<P2>::get(dsum, l), inv_s, 1.0f);
         r = r > 1.0e-8f ? r : 1.0e-8f;
         Lanes<P2>::set(rho, l, r);
-        Lanes<P2>::set(k, l, inv_s / r);
+        Lanes<P2>::set(k, l, __fdividef(inv_s, r));  // 2 ulp: far below the 16-bit storage quantum
         slow[l] = r > 1.0e3f;
     }
     ux = mx * k;
@@ -340,18 +352,15 @@ __global__ void __maxnreg__(StreamShape<COLL>::max_regs)
                                    Lanes<P2>::get(uz, l), dscale, inv_dscale, activation[l], restriction[l]);
         }
         if (fp.has_sponge) {
-            const float spa = va ? sponge_factor(g, fp, xa, y, z) : 0.0f;
-            const float spb = vb ? sponge_factor(g, fp, xb, y, z) : 0.0f;
+            const float spa = va ? sponge_factor_fast(g, fp, xa, y, z) : 0.0f;
+            const float spb = vb ? sponge_factor_fast(g, fp, xb, y, z) : 0.0f;
             if (spa > 0.0f || spb > 0.0f) {
-                // post + (far - post) * sp on the deviations, a zero factor
-                // leaving the lane unchanged
+                // post + (far - post) * sp on the deviations in packed
+                // arithmetic; a lane with a zero factor adds zero (its value
+                // is unchanged, a negative zero at most turning positive)
                 const P2 sp = make_float2(spa, spb);
 #pragma unroll
-                for (int q = 0; q < 19; ++q) {
-                    const P2 d = (pv(a.far_dev[q]) - post[q]) * sp;
-                    post[q] = make_float2(spa > 0.0f ? post[q].x + d.x : post[q].x,
-                                          spb > 0.0f ? post[q].y + d.y : post[q].y);
-                }
+                for (int q = 0; q < 19; ++q) post[q] = post[q] + (pv(a.far_dev[q]) - post[q]) * sp;
             }
         }
         if (CAPTURE) {
