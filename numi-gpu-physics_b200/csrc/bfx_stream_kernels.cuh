@@ -73,13 +73,15 @@ __device__ __forceinline__ void collide_dev2(const P2 (&d)[19], float s, float i
     const P2 t15 = 1.5f * ((ux * ux + uy * uy) + uz * uz);
     const P2 sr = s * rho;
     const P2 sr1 = Lat<float>::w1 * sr, sr2 = Lat<float>::w2 * sr;
-    const P2 wd1 = Lat<float>::w1 * dsum, wd2 = Lat<float>::w2 * dsum;
     const P2 e0 = Lat<float>::w0 * dsum - (Lat<float>::w0 * sr) * t15;
+    // per weight class: E = a + b cu^2 with a = w D - s rho w t15, b = 4.5 s rho w;
+    // O = o cu with o = 3 s rho w
+    const P2 a1 = Lat<float>::w1 * dsum - sr1 * t15, a2 = Lat<float>::w2 * dsum - sr2 * t15;
+    const P2 b1 = 4.5f * sr1, b2 = 4.5f * sr2, o1 = 3.0f * sr1, o2 = 3.0f * sr2;
     auto even_odd = [&](int q, P2& E, P2& O) {
         const P2 cu = cdot_pair(q, ux, uy, uz);
-        const P2 srw = q <= 6 ? sr1 : sr2;
-        E = (q <= 6 ? wd1 : wd2) + srw * ((4.5f * cu) * cu - t15);
-        O = srw * (3.0f * cu);
+        E = (q <= 6 ? a1 : a2) + ((q <= 6 ? b1 : b2) * cu) * cu;
+        O = (q <= 6 ? o1 : o2) * cu;
     };
     if constexpr (COLL == BFX_COLLISION_TRT) {
         // BF.metal:3063-3093 on the deviations (w_q is its own even part):
