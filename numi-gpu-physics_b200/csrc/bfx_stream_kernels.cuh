@@ -89,12 +89,14 @@ __device__ __forceinline__ void collide_dev2(const P2 (&d)[19], float s, float i
         // post_q = P + M, post_q' = P - M, P = p - w+ (p - E), M = m - w- (m - O)
         post[0] = d[0] - omega_p * (d[0] - e0);
         const float kp = 0.5f * (1.0f - omega_p), km = 0.5f * (1.0f - omega_m);
+        // w+ E = w+ a + (w+ b) cu^2 and w- O = (w- o) cu with the class factors scaled once
+        const P2 pa1 = omega_p * a1, pa2 = omega_p * a2, pb1 = omega_p * b1, pb2 = omega_p * b2;
+        const P2 mo1 = omega_m * o1, mo2 = omega_m * o2;
 #pragma unroll
         for (int q = 1; q < 19; q += 2) {
-            P2 E, O;
-            even_odd(q, E, O);
-            const P2 P = kp * ps[q] + omega_p * E;
-            const P2 M = km * md[q] + omega_m * O;
+            const P2 cu = cdot_pair(q, ux, uy, uz);
+            const P2 P = kp * ps[q] + ((q <= 6 ? pa1 : pa2) + ((q <= 6 ? pb1 : pb2) * cu) * cu);
+            const P2 M = km * md[q] + (q <= 6 ? mo1 : mo2) * cu;
             post[q] = P + M;
             post[q + 1] = P - M;
         }
