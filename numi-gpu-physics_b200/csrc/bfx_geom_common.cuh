@@ -236,6 +236,27 @@ __device__ __forceinline__ int64_t link_source(const Grid& g, const uint8_t* mas
     return (mask_next[s] & kPartMask) ? s : -1;
 }
 
+// Solid link sources of cell (x, y, z): bit q set when the source x - c_q is
+// solid, i.e. a cut link in direction q.  The 18 mask bytes are loaded in two
+// groups of nine, each group's loads issued together so their latencies
+// overlap (all 18 at once would cost the callers' occupancy in registers).
+__device__ __forceinline__ uint32_t link_sources(const Grid& g, const uint8_t* mask_next, int x, int y, int z) {
+    uint32_t bits = 0;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        uint8_t m[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            const int q = 1 + 9 * h + k;
+            int sx = x - cx(q), sy = y - cy(q), sz = z - cz(q);
+            m[k] = wrap(g, sx, sy, sz) ? mask_next[flat(g, sx, sy, sz)] : (uint8_t)0;
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) bits |= (m[k] & kPartMask) ? 1u << (1 + 9 * h + k) : 0u;
+    }
+    return bits;
+}
+
 // Ten-iteration bisection from the fluid node toward the solid node on the
 
 __device__ __forceinline__ float tri_distance(const GeomArgs& a, uint32_t t, V3 w) {

@@ -1054,12 +1054,7 @@ __device__ __forceinline__ void scan_cell(const GeomArgs& a, int rep_s, int x, i
         add_load<R>(acc, tx, ty, tz, (R)world.x, (R)world.y, (R)world.z, body, fp.f2p);
         acc[7] += 1.0;
     }
-    if (may_have_links(a, bidx, m1, m0)) {
-        for (int q = 1; q < 19; ++q) {
-            int sx, sy, sz;
-            if (link_source(g, a.b.mask_next, x, y, z, q, sx, sy, sz) >= 0) ++links;
-        }
-    }
+    if (may_have_links(a, bidx, m1, m0)) links += __popc(link_sources(g, a.b.mask_next, x, y, z));
 }
 
 template <class S>
@@ -1180,7 +1175,7 @@ __global__ void __launch_bounds__(256) k_links_emit(const GeomArgs a, int geomet
     // blocks without links (most of the box) emit nothing
     if (a.b.block_counts[block] == 0) return;
     const Grid& g = a.g;
-    uint32_t mine = 0;
+    uint32_t mine = 0, bits = 0;
     int x = 0, y = 0, z = 0;
     int64_t bidx = 0, gid = 0;
     bool valid = box_cell(a, x, y, z, bidx) && cell_active(a, x, y, z);
@@ -1189,10 +1184,8 @@ __global__ void __launch_bounds__(256) k_links_emit(const GeomArgs a, int geomet
         valid = may_have_links(a, bidx, a.b.mask_next[gid], a.b.mask_prev[gid]);
     }
     if (valid) {
-        for (int q = 1; q < 19; ++q) {
-            int sx, sy, sz;
-            if (link_source(g, a.b.mask_next, x, y, z, q, sx, sy, sz) >= 0) ++mine;
-        }
+        bits = link_sources(g, a.b.mask_next, x, y, z);
+        mine = __popc(bits);
     }
     // block-exclusive prefix of `mine`
     const int t = linear_tid();
@@ -1208,13 +1201,14 @@ __global__ void __launch_bounds__(256) k_links_emit(const GeomArgs a, int geomet
     for (int w = 0; w < warp; ++w) wbase += wsum[w];
     uint32_t pos = a.b.block_offsets[block] + wbase + incl - mine;
     if (mine == 0) return;
+#pragma unroll
     for (int q = 1; q < 19; ++q) {
-        int sx, sy, sz;
-        int64_t src = link_source(g, a.b.mask_next, x, y, z, q, sx, sy, sz);
-        if (src < 0) continue;
+        if (!(bits & (1u << q))) continue;
         if (pos < a.b.link_capacity) {
+            int sx = x - cx(q), sy = y - cy(q), sz = z - cz(q);
+            wrap(g, sx, sy, sz);  // inside: the source is solid
             a.b.link_cell[pos] = (uint32_t)gid;
-            a.b.link_meta[pos] = (uint32_t)q | ((uint32_t)(a.b.mask_next[src] & kPartMask) << 8);
+            a.b.link_meta[pos] = (uint32_t)q | ((uint32_t)(a.b.mask_next[flat(g, sx, sy, sz)] & kPartMask) << 8);
         }
         ++pos;
     }
