@@ -105,9 +105,15 @@ struct bfx_sim {
     uint32_t* block_counts = nullptr;
     uint32_t* block_offsets = nullptr;
     uint32_t* scan_sums = nullptr;
+    uint32_t* event_counts = nullptr;
+    uint32_t* event_offsets = nullptr;
+    uint32_t* event_sums = nullptr;
+    uint32_t* event_cell = nullptr;
+    uint32_t* event_total = nullptr;
     int box_blocks = 0;
     int scan_blocks = 0;
     double* topo_partials = nullptr;
+    int topo_blocks = 0;
     double* link_partials = nullptr;
     int apply_blocks = 0;
     double* mm_partials = nullptr;
@@ -246,9 +252,15 @@ GeomBuffers geom_buffers(bfx_sim* s, uint8_t* mprev, uint8_t* mnext) {
     b.block_counts = s->block_counts;
     b.block_offsets = s->block_offsets;
     b.scan_sums = s->scan_sums;
+    b.event_counts = s->event_counts;
+    b.event_offsets = s->event_offsets;
+    b.event_sums = s->event_sums;
+    b.event_cell = s->event_cell;
+    b.event_total = s->event_total;
     b.box_blocks = s->box_blocks;
     b.scan_blocks = s->scan_blocks;
     b.topo_partials = s->topo_partials;
+    b.topo_blocks = s->topo_blocks;
     b.link_partials = s->link_partials;
     b.apply_blocks = s->apply_blocks;
     b.state = s->dstate;
@@ -286,9 +298,11 @@ void encode_geometry_build(bfx_sim* s, int init, uint8_t* mprev, uint8_t* mnext,
 // The next step's geometry build can overlap this step's fluid kernel: with
 // the staged 16-bit kernel the fluid cells read only the populations and this
 // step's mask, while the build writes the other mask buffer, the wall field,
-// the keys and the pose fields of the device state; the body update it reads
-// is done by the link kernel before the fluid kernel, and the box's solid
-// cells (which read the wall field) are launched before the fork.
+// the keys, the pose fields and link count of the device state, and the
+// cut-link and event lists (this step's link kernel has read them before the
+// fork); the body update it reads is done by the link kernel before the fluid
+// kernel, and the box's solid cells (which read the wall field) are launched
+// before the fork.
 bool can_pipeline(const bfx_sim* s) { return s->moving() && s->tma_ok && s->side != nullptr; }
 
 // The halo fill can run beside the link build and the link kernel when every
@@ -305,11 +319,24 @@ bool halo_beside_links(const bfx_sim* s) {
     return true;
 }
 
-void encode_links(bfx_sim* s, uint8_t* mprev, uint8_t* mnext) {
-    GeomBuffers gb = geom_buffers(s, mprev, mnext);
-    launch_boundary_scan(s->cfg.storage, s->rep_s, s->g, s->fp, s->box, gb, fluid_buffers(s, mnext), s->stream);
-    launch_links_emit(s->cfg.geometry, s->cfg.link_rule, s->g, s->fp, s->box, gb, s->stream);
+// The cut-link and topology-event lists of a step's geometry, on the
+// simulation's stream or (pipelined path) the side stream beside the previous
+// step's fluid kernel.
+void encode_link_build(bfx_sim* s, uint8_t* mprev, uint8_t* mnext, cudaStream_t st) {
+    launch_link_build(s->cfg.geometry, s->cfg.link_rule, s->g, s->fp, s->box, geom_buffers(s, mprev, mnext), st);
     s->launches += 5;
+}
+// The topology impulses of the step's events: they read the pre-step
+// populations, so they follow the previous step's fluid kernel and precede
+// this step's link kernel on the simulation's stream.
+void encode_topology(bfx_sim* s, uint8_t* mprev, uint8_t* mnext) {
+    launch_topology(s->cfg.storage, s->rep_s, s->g, s->fp, s->box, geom_buffers(s, mprev, mnext),
+                    fluid_buffers(s, mnext), s->stream);
+    s->launches += 1;
+}
+void encode_links(bfx_sim* s, uint8_t* mprev, uint8_t* mnext) {
+    encode_link_build(s, mprev, mnext, s->stream);
+    if (s->moving()) encode_topology(s, mprev, mnext);
 }
 
 void timing_begin(bfx_sim* s) {
@@ -378,7 +405,11 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
         launch_frame_tangent(geom_buffers(s, mprev, mnext), s->cfg.time_step, 0, tape->frames, s->stream);
         s->launches += 1;
     }
-    if (s->geometry() && s->moving()) encode_links(s, mprev, mnext);
+    if (s->geometry() && s->moving()) {
+        // geometry_ready: the cut-link and event lists were built with the geometry
+        if (geometry_ready) encode_topology(s, mprev, mnext);
+        else encode_links(s, mprev, mnext);
+    }
     if (tape) {
         GeomBuffers gb = geom_buffers(s, mprev, mnext);
         gb.frames = tape->frames;
@@ -429,11 +460,13 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
         // Beside the fluid kernel, on the side stream: the solid / uncovered
         // cells (they write only their own slots, which no fluid cell reads or
         // writes, and read the wall field), then the next step's geometry
-        // (masks swap roles), which rewrites the wall field after them.
+        // (masks swap roles), which rewrites the wall field after them, and
+        // its cut-link and event lists.
         cudaEventRecord(s->fork_ev, s->stream);
         cudaStreamWaitEvent(s->side, s->fork_ev, 0);
         launch_bulk_rare(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, box, s->side);
         encode_geometry_build(s, 0, mnext, mprev, s->side);
+        if (s->geometry()) encode_link_build(s, mnext, mprev, s->side);
         cudaEventRecord(s->join_ev, s->side);
         launch_bulk_stream(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, box, s->stream);
         cudaStreamWaitEvent(s->stream, s->join_ev, 0);
@@ -844,8 +877,17 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
         s->scan_blocks = s->box_blocks;
         BFX_ALLOC(s->block_counts, (size_t)s->box_blocks * sizeof(uint32_t));
         BFX_ALLOC(s->block_offsets, (size_t)s->box_blocks * sizeof(uint32_t));
-        BFX_ALLOC(s->scan_sums, (size_t)((s->box_blocks + kScanSegment - 1) / kScanSegment) * sizeof(uint32_t));
-        BFX_ALLOC(s->topo_partials, (size_t)s->box_blocks * 8 * sizeof(double));
+        const size_t nseg = (size_t)((s->box_blocks + kScanSegment - 1) / kScanSegment);
+        BFX_ALLOC(s->scan_sums, nseg * sizeof(uint32_t));
+        BFX_ALLOC(s->event_counts, (size_t)s->box_blocks * sizeof(uint32_t));
+        BFX_ALLOC(s->event_offsets, (size_t)s->box_blocks * sizeof(uint32_t));
+        BFX_ALLOC(s->event_sums, nseg * sizeof(uint32_t));
+        BFX_ALLOC(s->event_cell, (size_t)s->box.cells * sizeof(uint32_t));
+        BFX_ALLOC(s->event_total, sizeof(uint32_t));
+        cudaMemsetAsync(s->event_total, 0, sizeof(uint32_t), s->stream);
+        s->topo_blocks = s->sm_count;
+        BFX_ALLOC(s->topo_partials, (size_t)s->topo_blocks * 8 * sizeof(double));
+        cudaMemsetAsync(s->topo_partials, 0, (size_t)s->topo_blocks * 8 * sizeof(double), s->stream);
         s->apply_blocks = 4 * s->sm_count;
         BFX_ALLOC(s->link_partials, (size_t)s->apply_blocks * 16 * sizeof(double));
         uint64_t cap = c.link_capacity ? c.link_capacity

@@ -989,163 +989,235 @@ __device__ __forceinline__ bool may_have_links(const GeomArgs& a, int64_t bidx, 
 }
 
 // ---------------------------------------------------------------------------
-// Topology impulses (BF.metal:2557-2609 covered, 2616-2666 uncovered) and the
-// per-block cut-link count.  Reads populations only; runs before any link write.
+// Topology events and impulses (BF.metal:2557-2609 covered, 2616-2666
+// uncovered).  A cell is an event when its occupancy changed this step and its
+// impulse enters the loads.  Which cells are events depends on the geometry
+// alone, so the event list is built with the cut-link list (k_link_count,
+// the offset scan, k_links_emit); the impulses read the pre-step populations
+// and run in k_topology, after the previous step's fluid kernel and before
+// the link kernel overwrites any slot they read.
 // ---------------------------------------------------------------------------
-// Topology impulses and cut-link count of one cell (BF.metal:2557-2609
-// covered, 2616-2666 uncovered).
-template <class S>
-__device__ __forceinline__ void scan_cell(const GeomArgs& a, int rep_s, int x, int y, int z, int64_t bidx,
-                                          double (&acc)[8], uint32_t& links) {
-    using R = typename S::R;
-    const FluidParams& fp = a.fp;
+__device__ __forceinline__ bool topology_event(const FluidParams& fp, uint8_t m_next) {
     const int sel = fp.interpolated;
     const int mode = sel ? fp.force_mode : 6;
-    const int include_topo = !sel || fp.load_component != 1;
-    const Grid& g = a.g;
-    const int64_t gid = flat(g, x, y, z);
-    const uint8_t m1 = a.b.mask_next[gid];
-    const uint8_t m0 = a.b.mask_prev[gid];
-    const typename S::T* A = (const typename S::T*)a.pops;
-    const double* body = a.b.state->body;
-    const V3 world = cell_world(fp, x, y, z);
-    if ((m1 & kCovered) && fp.accumulate && include_topo) {
-        // newly covered: previous fluid momentum (minus the wall-moving density for estimators 0-5)
-        R pd = 0, pmx = 0, pmy = 0, pmz = 0;
-        for (int q = 0; q < 19; ++q) {
-            R prev = canon_load<S>(A, g, rep_s, q, x, y, z);
-            pd += prev;
-            pmx += prev * (R)cx(q);
-            pmy += prev * (R)cy(q);
-            pmz += prev * (R)cz(q);
-        }
-        float4 w = a.b.wall[gid];
-        R ix = pmx, iy = pmy, iz = pmz;
-        if (mode != 6) {
-            ix = pmx - pd * (R)w.x;
-            iy = pmy - pd * (R)w.y;
-            iz = pmz - pd * (R)w.z;
-        }
-        add_load<R>(acc, ix, iy, iz, (R)world.x, (R)world.y, (R)world.z, body, fp.f2p);
-        acc[6] += 1.0;
-    } else if ((m1 & kUncovered) && fp.accumulate && include_topo && mode == 6) {
-        // newly uncovered: refill momentum plus the moving-domain stencil
-        float4 w = a.b.wall[gid];
-        R mx = 0, my = 0, mz = 0;
-        for (int q = 0; q < 19; ++q) {
-            R v = feq_rt<R>(q, R(1), (R)w.x, (R)w.y, (R)w.z);
-            mx += v * (R)cx(q);
-            my += v * (R)cy(q);
-            mz += v * (R)cz(q);
-        }
-        R tx = -mx, ty = -my, tz = -mz;
-        for (int q = 1; q < 19; ++q) {
-            int bx = x + cx(q), by = y + cy(q), bz = z + cz(q);
-            if (!inside(g, bx, by, bz)) continue;
-            int64_t nb = flat(g, bx, by, bz);
-            if (!((a.b.mask_prev[nb] & kPartMask) == 0 && (a.b.mask_next[nb] & kPartMask) == 0)) continue;
-            R old_out = canon_load<S>(A, g, rep_s, q, x, y, z);
-            R sup_in = canon_load<S>(A, g, rep_s, opp(q), bx, by, bz);
-            R sum = old_out + sup_in;
-            tx -= sum * (R)cx(q);
-            ty -= sum * (R)cy(q);
-            tz -= sum * (R)cz(q);
-        }
-        add_load<R>(acc, tx, ty, tz, (R)world.x, (R)world.y, (R)world.z, body, fp.f2p);
-        acc[7] += 1.0;
-    }
-    if (may_have_links(a, bidx, m1, m0)) links += __popc(link_sources(g, a.b.mask_next, x, y, z));
+    const bool include_topo = !sel || fp.load_component != 1;
+    if (!fp.accumulate || !include_topo) return false;
+    return (m_next & kCovered) != 0 || ((m_next & kUncovered) != 0 && mode == 6);
 }
 
+// Impulse of one event cell into acc (force 0-2, torque 3-5, covered and
+// uncovered counts 6-7), one warp per event: lane q loads direction q, then
+// every lane forms the sums in the reference's direction order from the
+// shuffled values (the same operations, in the same order, as one thread
+// summing q = 0..18), so the lanes' loads overlap instead of one thread's
+// long dependent chain.  Lane 0 adds the impulse to its acc.
 template <class S>
-__global__ void __launch_bounds__(256) k_boundary_scan(const GeomArgs a, int rep_s) {
-    __shared__ double sh[8][256];
-    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    uint32_t links = 0;
+__device__ __forceinline__ void topology_impulse_warp(const GeomArgs& a, int rep_s, int64_t gid, int lane,
+                                                      double (&acc)[8]) {
+    using R = typename S::R;
+    const FluidParams& fp = a.fp;
+    const int mode = fp.interpolated ? fp.force_mode : 6;
+    const Grid& g = a.g;
+    int x, y, z;
+    unflat(g, gid, x, y, z);
+    const uint8_t m1 = a.b.mask_next[gid];
+    const typename S::T* A = (const typename S::T*)a.pops;
+    const float4 w = a.b.wall[gid];
+    const int q = lane < 19 ? lane : 0;
+    R tx, ty, tz;
+    if (m1 & kCovered) {
+        // newly covered: previous fluid momentum (minus the wall-moving density for estimators 0-5)
+        const R mine = lane < 19 ? canon_load<S>(A, g, rep_s, q, x, y, z) : R(0);
+        R pd = 0, pmx = 0, pmy = 0, pmz = 0;
+#pragma unroll
+        for (int k = 0; k < 19; ++k) {
+            const R prev = __shfl_sync(0xffffffffu, mine, k);
+            pd += prev;
+            pmx += prev * (R)cx(k);
+            pmy += prev * (R)cy(k);
+            pmz += prev * (R)cz(k);
+        }
+        tx = pmx;
+        ty = pmy;
+        tz = pmz;
+        if (mode != 6) {
+            tx = pmx - pd * (R)w.x;
+            ty = pmy - pd * (R)w.y;
+            tz = pmz - pd * (R)w.z;
+        }
+    } else {
+        // newly uncovered: refill momentum plus the moving-domain stencil over
+        // the neighbours that are fluid before and after the step
+        const R feq_mine = lane < 19 ? feq_rt<R>(q, R(1), (R)w.x, (R)w.y, (R)w.z) : R(0);
+        R sum_mine = R(0);
+        bool live = false;
+        if (lane >= 1 && lane < 19) {
+            const int bx = x + cx(q), by = y + cy(q), bz = z + cz(q);
+            if (inside(g, bx, by, bz)) {
+                const int64_t nb = flat(g, bx, by, bz);
+                const R old_out = canon_load<S>(A, g, rep_s, q, x, y, z);
+                const R sup_in = canon_load<S>(A, g, rep_s, opp(q), bx, by, bz);
+                live = (a.b.mask_prev[nb] & kPartMask) == 0 && (a.b.mask_next[nb] & kPartMask) == 0;
+                sum_mine = old_out + sup_in;
+            }
+        }
+        const uint32_t live_bits = __ballot_sync(0xffffffffu, live);
+        R mx = 0, my = 0, mz = 0;
+#pragma unroll
+        for (int k = 0; k < 19; ++k) {
+            const R v = __shfl_sync(0xffffffffu, feq_mine, k);
+            mx += v * (R)cx(k);
+            my += v * (R)cy(k);
+            mz += v * (R)cz(k);
+        }
+        tx = -mx;
+        ty = -my;
+        tz = -mz;
+#pragma unroll
+        for (int k = 1; k < 19; ++k) {
+            const R sum = __shfl_sync(0xffffffffu, sum_mine, k);
+            if (!(live_bits & (1u << k))) continue;
+            tx -= sum * (R)cx(k);
+            ty -= sum * (R)cy(k);
+            tz -= sum * (R)cz(k);
+        }
+    }
+    if (lane == 0) {
+        const V3 world = cell_world(fp, x, y, z);
+        add_load<R>(acc, tx, ty, tz, (R)world.x, (R)world.y, (R)world.z, a.b.state->body, fp.f2p);
+        acc[(m1 & kCovered) ? 6 : 7] += 1.0;
+    }
+}
+
+// Per-block counts of cut links and topology events over the geometry box.
+// Geometry only (masks and keys), so the pipelined path runs it with the
+// next step's geometry, beside the fluid kernel.
+__global__ void __launch_bounds__(256) k_link_count(const GeomArgs a) {
+    __shared__ uint32_t wcount[8];
+    const int block = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     if (block_inactive(a)) {
         // no key, link or topology change in this block
         if (linear_tid() == 0) {
-            const int block = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
             a.b.block_counts[block] = 0;
-            for (int k = 0; k < 8; ++k) a.b.topo_partials[8 * block + k] = 0.0;
+            a.b.event_counts[block] = 0;
         }
         return;
     }
+    uint32_t links = 0, events = 0;
     {
         int x, y, z;
         int64_t bidx;
-        if (box_cell(a, x, y, z, bidx) && cell_active(a, x, y, z)) scan_cell<S>(a, rep_s, x, y, z, bidx, acc, links);
+        if (box_cell(a, x, y, z, bidx) && cell_active(a, x, y, z)) {
+            const int64_t gid = flat(a.g, x, y, z);
+            const uint8_t m1 = a.b.mask_next[gid];
+            const uint8_t m0 = a.b.mask_prev[gid];
+            events = topology_event(a.fp, m1) ? 1u : 0u;
+            if (may_have_links(a, bidx, m1, m0)) links = __popc(link_sources(a.g, a.b.mask_next, x, y, z));
+        }
     }
-    // most blocks hold no covered / uncovered cell: skip their FP64 tree
+    // links (at most 18 a cell) in the low half, events in the high half
+    uint32_t w = links | events << 16;
+    for (int o = 16; o > 0; o >>= 1) w += __shfl_down_sync(0xffffffffu, w, o);
+    const int t = linear_tid();
+    if ((t & 31) == 0) wcount[t >> 5] = w;
+    __syncthreads();
+    if (t == 0) {
+        uint32_t tl = 0, te = 0;
+        for (int k = 0; k < 8; ++k) {
+            tl += wcount[k] & 0xFFFFu;
+            te += wcount[k] >> 16;
+        }
+        a.b.block_counts[block] = tl;
+        a.b.event_counts[block] = te;
+    }
+}
+
+// Topology impulses over the event list: a fixed grid of topo_blocks blocks of
+// four warps, event i to warp i mod (4 topo_blocks) in list order, then
+// fixed-order block trees into 8 partials per block (reduced by the link
+// kernel's last block).
+template <class S>
+__global__ void __launch_bounds__(128) k_topology(const GeomArgs a, int rep_s) {
+    __shared__ double sh[8][256];
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const uint32_t count = *a.b.event_total;
+    const int lane = threadIdx.x & 31;
+    const uint32_t warps = gridDim.x * (blockDim.x / 32);
+    for (uint32_t i = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); i < count; i += warps)
+        topology_impulse_warp<S>(a, rep_s, a.b.event_cell[i], lane, acc);
+    // most blocks hold no event: skip their FP64 tree
     bool nonzero = false;
     for (int k = 0; k < 8; ++k) nonzero = nonzero || acc[k] != 0.0;
     const bool block_nonzero = __syncthreads_or(nonzero) != 0;
     if (block_nonzero) block_sum<8>(acc, sh);
-    __shared__ uint32_t wcount[8];
-    uint32_t wl = links;
-    for (int o = 16; o > 0; o >>= 1) wl += __shfl_down_sync(0xffffffffu, wl, o);
-    const int t = linear_tid();
-    if ((t & 31) == 0) wcount[t >> 5] = wl;
-    __syncthreads();
-    const int block = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-    if (t == 0) {
-        uint32_t tot = 0;
-        for (int w = 0; w < 8; ++w) tot += wcount[w];
-        a.b.block_counts[block] = tot;
-        for (int k = 0; k < 8; ++k) a.b.topo_partials[8 * block + k] = block_nonzero ? acc[k] : 0.0;
-    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 8; ++k) a.b.topo_partials[8 * blockIdx.x + k] = block_nonzero ? acc[k] : 0.0;
 }
 
-// Exclusive scan of the per-block link counts into block offsets, in two
-// levels: k_scan_reduce sums each segment of kScanSegment counts (a block per
-// segment); k_scan_apply adds the sums of the segments before its own and
-// scans its segment (eight consecutive counts per thread).  Block 0 also sets
-// the total link count and the overflow flag.  Integer sums: the offsets do
-// not depend on the split.
-__device__ __forceinline__ uint32_t block_sum_1024(uint32_t v, uint32_t* wtot) {
+// Exclusive scans of the per-block link counts (blockIdx.y 0) and event
+// counts (blockIdx.y 1) into block offsets, in two levels: k_scan_reduce sums
+// each segment of kScanSegment counts (a block per segment); k_scan_apply adds
+// the sums of the segments before its own and scans its segment (32
+// consecutive counts per thread).  Block 0 also sets the totals (and the link
+// list's overflow flag).  256-thread blocks: on the pipelined path they run
+// beside the persistent fluid kernel, in the registers it leaves free.
+// Integer sums: the offsets do not depend on the split.
+constexpr int kScanThreads = 256;
+constexpr int kScanPerThread = kScanSegment / kScanThreads;
+__device__ __forceinline__ uint32_t block_sum_scan(uint32_t v, uint32_t* wtot) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if (lane == 0) wtot[warp] = v;
     __syncthreads();
     uint32_t t = 0;
-    for (int w = 0; w < 32; ++w) t += wtot[w];
+    for (int w = 0; w < kScanThreads / 32; ++w) t += wtot[w];
     return t;
 }
 
-__global__ void __launch_bounds__(1024) k_scan_reduce(const GeomArgs a) {
-    __shared__ uint32_t wtot[32];
+__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const GeomArgs a) {
+    __shared__ uint32_t wtot[kScanThreads / 32];
+    const uint32_t* counts = blockIdx.y ? a.b.event_counts : a.b.block_counts;
+    uint32_t* sums = blockIdx.y ? a.b.event_sums : a.b.scan_sums;
     const int nb = a.b.scan_blocks;
     const int lo = blockIdx.x * kScanSegment;
     const int hi = lo + kScanSegment < nb ? lo + kScanSegment : nb;
     uint32_t t = 0;
-    for (int i = lo + threadIdx.x; i < hi; i += 1024) t += a.b.block_counts[i];
-    t = block_sum_1024(t, wtot);
-    if (threadIdx.x == 0) a.b.scan_sums[blockIdx.x] = t;
+    for (int i = lo + threadIdx.x; i < hi; i += kScanThreads) t += counts[i];
+    t = block_sum_scan(t, wtot);
+    if (threadIdx.x == 0) sums[blockIdx.x] = t;
 }
 
-__global__ void __launch_bounds__(1024) k_scan_apply(const GeomArgs a, int nseg) {
-    __shared__ uint32_t wtot[32];
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(const GeomArgs a, int nseg) {
+    __shared__ uint32_t wtot[kScanThreads / 32];
     __shared__ uint32_t seg_base;
+    const bool ev = blockIdx.y != 0;
+    const uint32_t* counts = ev ? a.b.event_counts : a.b.block_counts;
+    const uint32_t* sums = ev ? a.b.event_sums : a.b.scan_sums;
+    uint32_t* offsets = ev ? a.b.event_offsets : a.b.block_offsets;
     const int nb = a.b.scan_blocks;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
         uint32_t b = 0;
-        for (int k = 0; k < (int)blockIdx.x; ++k) b += a.b.scan_sums[k];
+        for (int k = 0; k < (int)blockIdx.x; ++k) b += sums[k];
         seg_base = b;
         if (blockIdx.x == 0) {
             uint64_t total = 0;
-            for (int k = 0; k < nseg; ++k) total += a.b.scan_sums[k];
-            a.b.state->link_count = (int64_t)total;
-            a.b.state->link_overflow = total > a.b.link_capacity ? 1u : 0u;
+            for (int k = 0; k < nseg; ++k) total += sums[k];
+            if (ev) {
+                *a.b.event_total = (uint32_t)total;  // at most one event a box cell
+            } else {
+                a.b.state->link_count = (int64_t)total;
+                a.b.state->link_overflow = total > a.b.link_capacity ? 1u : 0u;
+            }
         }
     }
-    // eight consecutive counts per thread
-    const int first = blockIdx.x * kScanSegment + 8 * threadIdx.x;
-    uint32_t c[8];
+    // kScanPerThread consecutive counts per thread
+    const int first = blockIdx.x * kScanSegment + kScanPerThread * threadIdx.x;
+    uint32_t c[kScanPerThread];
     uint32_t mine = 0;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        c[k] = first + k < nb ? a.b.block_counts[first + k] : 0u;
+    for (int k = 0; k < kScanPerThread; ++k) {
+        c[k] = first + k < nb ? counts[first + k] : 0u;
         mine += c[k];
     }
     // block-exclusive prefix of the thread sums
@@ -1160,37 +1232,41 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const GeomArgs a, int nseg)
     for (int w = 0; w < warp; ++w) base += wtot[w];
     base += incl - mine;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        if (first + k < nb) a.b.block_offsets[first + k] = base;
+    for (int k = 0; k < kScanPerThread; ++k) {
+        if (first + k < nb) offsets[first + k] = base;
         base += c[k];
     }
 }
 
-// Cut-link compaction: every persistent fluid cell appends its links (in
-// direction order) at the block offset plus the warp-ballot / shuffle prefix of
-// the preceding threads, so the list is ordered by box cell then direction.
+// Cut-link and event compaction: every persistent fluid cell appends its
+// links (in direction order) at the block offset plus the shuffle prefix of
+// the preceding threads, so the list is ordered by box cell then direction;
+// every event cell appends itself to the event list in box-cell order.
 __global__ void __launch_bounds__(256) k_links_emit(const GeomArgs a, int geometry, int link_rule, int interpolated) {
     __shared__ uint32_t wsum[8];
     const int block = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-    // blocks without links (most of the box) emit nothing
-    if (a.b.block_counts[block] == 0) return;
+    // blocks without links or events (most of the box) emit nothing
+    if (a.b.block_counts[block] == 0 && a.b.event_counts[block] == 0) return;
     const Grid& g = a.g;
-    uint32_t mine = 0, bits = 0;
+    uint32_t mine = 0, bits = 0, event = 0;
     int x = 0, y = 0, z = 0;
     int64_t bidx = 0, gid = 0;
-    bool valid = box_cell(a, x, y, z, bidx) && cell_active(a, x, y, z);
-    if (valid) {
+    if (box_cell(a, x, y, z, bidx) && cell_active(a, x, y, z)) {
         gid = flat(g, x, y, z);
-        valid = may_have_links(a, bidx, a.b.mask_next[gid], a.b.mask_prev[gid]);
+        const uint8_t m1 = a.b.mask_next[gid];
+        const uint8_t m0 = a.b.mask_prev[gid];
+        event = topology_event(a.fp, m1) ? 1u : 0u;
+        if (may_have_links(a, bidx, m1, m0)) {
+            bits = link_sources(g, a.b.mask_next, x, y, z);
+            mine = __popc(bits);
+        }
     }
-    if (valid) {
-        bits = link_sources(g, a.b.mask_next, x, y, z);
-        mine = __popc(bits);
-    }
-    // block-exclusive prefix of `mine`
+    // block-exclusive prefix of (links, events), packed low / high 16 bits
+    // (a block holds at most 256 x 18 links and 256 events)
+    const uint32_t own = mine | event << 16;
     const int t = linear_tid();
     const int lane = t & 31, warp = t >> 5;
-    uint32_t incl = mine;
+    uint32_t incl = own;
     for (int o = 1; o < 32; o <<= 1) {
         uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += v;
@@ -1199,8 +1275,10 @@ __global__ void __launch_bounds__(256) k_links_emit(const GeomArgs a, int geomet
     __syncthreads();
     uint32_t wbase = 0;
     for (int w = 0; w < warp; ++w) wbase += wsum[w];
-    uint32_t pos = a.b.block_offsets[block] + wbase + incl - mine;
+    const uint32_t excl = wbase + incl - own;
+    if (event) a.b.event_cell[a.b.event_offsets[block] + (excl >> 16)] = (uint32_t)gid;
     if (mine == 0) return;
+    uint32_t pos = a.b.block_offsets[block] + (excl & 0xFFFFu);
 #pragma unroll
     for (int q = 1; q < 19; ++q) {
         if (!(bits & (1u << q))) continue;
@@ -1441,7 +1519,7 @@ __global__ void __launch_bounds__(256) k_links_apply(const GeomArgs a, int rep_s
     if (__syncthreads_or(nonzero)) block_sum<8>(acc, sh);
     double tp[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     if (with_topology) {
-        const int nb = a.b.scan_blocks;
+        const int nb = a.b.topo_blocks;
         const int per = (nb + (int)gridDim.x - 1) / (int)gridDim.x;
         const int lo = (int)blockIdx.x * per;
         const int hi = lo + per < nb ? lo + per : nb;
@@ -1685,13 +1763,6 @@ void launch_classify(int geometry, int has_prev, const GridDesc& g, const FluidP
     }
 }
 
-template <class S>
-static void scan_s(const GeomArgs& a, int rep_s, const BoxDesc& box, cudaStream_t s) {
-    dim3 grid, block;
-    box_shape(box, grid, block);
-    k_boundary_scan<S><<<grid, block, 0, s>>>(a, rep_s);
-}
-
 #define BFX_DISPATCH_STORAGE(storage, FN, ...)                             \
     switch (storage) {                                                     \
     case BFX_STORAGE_F16_DEVIATION: FN<StoreF16Dev>(__VA_ARGS__); break;   \
@@ -1700,20 +1771,15 @@ static void scan_s(const GeomArgs& a, int rep_s, const BoxDesc& box, cudaStream_
     default: FN<StoreF32>(__VA_ARGS__); break;                             \
     }
 
-void launch_boundary_scan(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
-                          const GeomBuffers& gb, const FluidBuffers& fb, cudaStream_t s) {
-    GeomArgs a = make_geom(g, fp, box, gb, fb.pops);
-    BFX_DISPATCH_STORAGE(storage, scan_s, a, rep_s, box, s);
-}
-
-void launch_links_emit(int geometry, int link_rule, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
+void launch_link_build(int geometry, int link_rule, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
                        const GeomBuffers& gb, cudaStream_t s) {
     GeomArgs a = make_geom(g, fp, box, gb, nullptr);
-    const int nseg = (a.b.scan_blocks + kScanSegment - 1) / kScanSegment;
-    k_scan_reduce<<<nseg, 1024, 0, s>>>(a);
-    k_scan_apply<<<nseg, 1024, 0, s>>>(a, nseg);
     dim3 grid, block;
     box_shape(box, grid, block);
+    k_link_count<<<grid, block, 0, s>>>(a);
+    const int nseg = (a.b.scan_blocks + kScanSegment - 1) / kScanSegment;
+    k_scan_reduce<<<dim3(nseg, 2), kScanThreads, 0, s>>>(a);
+    k_scan_apply<<<dim3(nseg, 2), kScanThreads, 0, s>>>(a, nseg);
     k_links_emit<<<grid, block, 0, s>>>(a, geometry, link_rule, fp.interpolated);
     if (geometry == BFX_GEOMETRY_MESH && link_rule == BFX_LINK_RAY_ROOT && fp.interpolated) {
         const unsigned rblocks =
@@ -1723,6 +1789,16 @@ void launch_links_emit(int geometry, int link_rule, const GridDesc& g, const Flu
     }
     const unsigned fblocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(4096, ((int64_t)gb.link_capacity + 127) / 128));
     k_links_fraction<<<fblocks, 128, 0, s>>>(a, geometry, link_rule, fp.interpolated);
+}
+
+template <class S>
+static void topology_s(const GeomArgs& a, int rep_s, cudaStream_t s) {
+    k_topology<S><<<a.b.topo_blocks, 128, 0, s>>>(a, rep_s);
+}
+void launch_topology(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
+                     const GeomBuffers& gb, const FluidBuffers& fb, cudaStream_t s) {
+    GeomArgs a = make_geom(g, fp, box, gb, fb.pops);
+    BFX_DISPATCH_STORAGE(storage, topology_s, a, rep_s, s);
 }
 
 template <class S>

@@ -96,15 +96,22 @@ struct GeomBuffers {
     uint32_t* link_meta;            // direction | part << 8
     float* link_q;
     uint32_t link_capacity;
-    uint32_t* block_counts;         // per box block
+    uint32_t* block_counts;         // cut links per box block
     uint32_t* block_offsets;
-    uint32_t* scan_sums;
+    uint32_t* scan_sums;            // one per kScanSegment scan blocks (two-level scan)
+    // topology events (cells newly covered / uncovered whose impulse enters the loads)
+    uint32_t* event_counts;         // per box block
+    uint32_t* event_offsets;
+    uint32_t* event_sums;           // one per kScanSegment scan blocks
+    uint32_t* event_cell;           // event list (flat cell index, box-cell order); capacity: box cells
+    uint32_t* event_total;          // [1] events in the list
     const float* kf_times;          // keyframe replay: times, frames x vertices x 3 offsets (kf_count >= 2)
     const float* kf_points;
-    int kf_count;            // one per kScanSegment scan blocks (two-level scan)
+    int kf_count;
     int box_blocks;                 // blocks of a one-slice-per-block box launch (allocations)
     int scan_blocks;                // blocks of the link count / scan / emission launch
-    double* topo_partials;          // 8 per box block
+    double* topo_partials;          // 8 per topology block
+    int topo_blocks;                // blocks of the topology-impulse launch
     double* link_partials;          // 16 per apply block (link sums, topology sums)
     int apply_blocks;
     DeviceState* state;
@@ -118,10 +125,15 @@ void launch_prepare(int geometry, float dt, const GridDesc& g, const FluidParams
                     const GeomBuffers& gb, int init, cudaStream_t s);
 void launch_classify(int geometry, int has_prev, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
                      const GeomBuffers& gb, cudaStream_t s, bool lean_raster = false);
-void launch_boundary_scan(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
-                          const GeomBuffers& gb, const FluidBuffers& fb, cudaStream_t s);
-void launch_links_emit(int geometry, int link_rule, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
+// Cut-link and topology-event lists of the step's geometry (counts, offset
+// scan, emission, link fractions).  Reads only geometry: masks, keys, wall
+// field and mesh.
+void launch_link_build(int geometry, int link_rule, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
                        const GeomBuffers& gb, cudaStream_t s);
+// Topology impulses of the event list into topo_partials; reads the pre-step
+// populations, so it runs before the link kernel writes any.
+void launch_topology(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
+                     const GeomBuffers& gb, const FluidBuffers& fb, cudaStream_t s);
 // Coupled momentum ledger passes (bfx_ledger.cu): `blocks` rows of 16 (in) or
 // 9 (out) FP64 partial sums.
 constexpr int kLedgerInWidth = 16;
