@@ -120,6 +120,8 @@ struct bfx_sim {
     double* mm_result = nullptr;
     int mm_blocks = 0;
     float* scratch_f32 = nullptr;  // canonical read-out staging (lazily)
+    bool face_ready = false;       // the staged kernel takes the x faces' values (face_dev) without their fill
+    float face_dev[2 * 19] = {};   // those values (stored deviations, host copy)
     bfx_run_sample* dsamples = nullptr;
     size_t dsamples_cap = 0;
     // state
@@ -221,6 +223,7 @@ FluidBuffers fluid_buffers(bfx_sim* s, uint8_t* mask) {
     b.tape = nullptr;
     b.tmap = s->tma_ok ? &s->tmap : nullptr;
     b.sm_count = s->sm_count;
+    b.face_dev = s->face_ready ? s->face_dev : nullptr;
     return b;
 }
 
@@ -305,6 +308,15 @@ void encode_geometry_build(bfx_sim* s, int init, uint8_t* mprev, uint8_t* mnext,
 // before the fork.
 bool can_pipeline(const bfx_sim* s) { return s->moving() && s->tma_ok && s->side != nullptr; }
 
+// Faces f0..f1 are far-field or velocity faces: the values the halo fill
+// writes there depend only on the face and the direction.
+bool faces_constant(const bfx_config& c, int f0 = 0, int f1 = 5) {
+    for (int f = f0; f <= f1; ++f)
+        if (c.face_bc[f] != BFX_BC_FARFIELD && c.face_bc[f] != BFX_BC_VELOCITY) return false;
+    return true;
+}
+bool x_faces_constant(const bfx_config& c) { return faces_constant(c, 0, 1); }
+
 // The halo fill can run beside the link build and the link kernel when every
 // face is a far-field or velocity face: the fill then only writes constants
 // into halo slots, which no link kernel reads or writes (an out-of-domain
@@ -313,10 +325,7 @@ bool can_pipeline(const bfx_sim* s) { return s->moving() && s->tma_ok && s->side
 // interior neighbour, and a link whose solid source is a periodic image writes
 // a halo slot: those keep the fill first on the main stream.
 bool halo_beside_links(const bfx_sim* s) {
-    if (!s->moving() || s->side == nullptr) return false;
-    for (int f = 0; f < 6; ++f)
-        if (s->cfg.face_bc[f] != BFX_BC_FARFIELD && s->cfg.face_bc[f] != BFX_BC_VELOCITY) return false;
-    return true;
+    return s->moving() && s->side != nullptr && faces_constant(s->cfg);
 }
 
 // The cut-link and topology-event lists of a step's geometry, on the
@@ -379,13 +388,16 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
     uint8_t* mprev = s->mask[s->cur];
     uint8_t* mnext = s->moving() ? s->mask[s->cur ^ 1] : s->mask[s->cur];
     FluidBuffers fb = fluid_buffers(s, s->geometry() ? mnext : nullptr);
-    // the halo fill forks off here (after the previous step's fluid kernel)
-    // and joins before this step's fluid kernel
+    // The halo fill forks off here (after the previous step's fluid kernel)
+    // and joins before this step's fluid kernel; without the x faces when
+    // the staged kernel takes their values from its table
+    const bool yz_only = s->face_ready && bulk_staged(s->cfg.storage, s->cfg.collision, tape ? 2 : capture, s->tma_ok);
     const bool halo_side = halo_beside_links(s) && !tape && !ledger_in;
     if (halo_side) {
         cudaEventRecord(s->halo_fork_ev, s->stream);
         cudaStreamWaitEvent(s->side, s->halo_fork_ev, 0);
-        launch_halo(s->cfg.storage, s->rep_s, s->g, s->fp, fb, s->side);
+        if (yz_only) launch_halo_yz(s->cfg.storage, s->rep_s, s->g, s->fp, fb, s->side);
+        else launch_halo(s->cfg.storage, s->rep_s, s->g, s->fp, fb, s->side);
         cudaEventRecord(s->halo_join_ev, s->side);
         s->launches += 1;
     }
@@ -426,7 +438,8 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
     // halo fill before the link writes: a link whose solid source is a periodic
     // image writes into a halo slot and must win over the periodic copy
     if (!halo_side) {
-        launch_halo(s->cfg.storage, s->rep_s, s->g, s->fp, fb, s->stream);
+        if (yz_only) launch_halo_yz(s->cfg.storage, s->rep_s, s->g, s->fp, fb, s->stream);
+        else launch_halo(s->cfg.storage, s->rep_s, s->g, s->fp, fb, s->stream);
         s->launches += 1;
     }
     // The end-of-step body update needs only the reduced loads: it runs in the
@@ -445,6 +458,15 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
                            finish_fused ? &fin : nullptr, s->stream);
         s->launches += 1;
     }
+    const bool pipelined = prefetch_next && capture == 0 && !tape && !ledger_in && can_pipeline(s);
+    const int box[3] = {s->box.sx, s->box.sy, s->box.sz};
+    if (pipelined) {
+        // The solid / uncovered cells right after the link kernel, beside the
+        // halo fill: they write only their own slots, which no fluid cell
+        // reads or writes, and read the wall field, which the next step's
+        // geometry rewrites after the fork below.
+        launch_bulk_rare(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, box, s->stream);
+    }
     if (halo_side) cudaStreamWaitEvent(s->stream, s->halo_join_ev, 0);
     if (tape) {
         cudaMemcpyAsync(tape->state, s->dstate, sizeof(DeviceState), cudaMemcpyDeviceToDevice, s->stream);
@@ -455,16 +477,11 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
         fb.tape = tape->moments;
         capture = 2;
     }
-    const int box[3] = {s->box.sx, s->box.sy, s->box.sz};
-    if (prefetch_next && capture == 0 && !tape && !ledger_in && can_pipeline(s)) {
-        // Beside the fluid kernel, on the side stream: the solid / uncovered
-        // cells (they write only their own slots, which no fluid cell reads or
-        // writes, and read the wall field), then the next step's geometry
-        // (masks swap roles), which rewrites the wall field after them, and
-        // its cut-link and event lists.
+    if (pipelined) {
+        // Beside the fluid kernel, on the side stream: the next step's
+        // geometry (masks swap roles) and its cut-link and event lists.
         cudaEventRecord(s->fork_ev, s->stream);
         cudaStreamWaitEvent(s->side, s->fork_ev, 0);
-        launch_bulk_rare(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, box, s->side);
         encode_geometry_build(s, 0, mnext, mprev, s->side);
         if (s->geometry()) encode_link_build(s, mnext, mprev, s->side);
         cudaEventRecord(s->join_ev, s->side);
@@ -830,6 +847,23 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
                 staged_collision(c.collision) &&
                 encode_population_map(&s->tmap, s->pops, c.storage, c.collision, g.px, g.ny + 2, g.nz + 2);
     if (s->tma_ok) prepare_stream(c.storage, c.collision);
+    // Both x faces far-field or velocity faces: what the halo fill writes
+    // there depends on the face and the direction only, so the staged kernel
+    // takes it from a table and its steps skip the x faces' fill (one
+    // scattered store per lattice row and direction).
+    if (s->tma_ok && x_faces_constant(c)) {
+        float* dvals = nullptr;
+        BFX_ALLOC(dvals, sizeof(s->face_dev));
+        launch_halo_values(c.storage, s->g, s->fp, dvals, s->stream);
+        cudaError_t fe = cudaMemcpyAsync(s->face_dev, dvals, sizeof(s->face_dev), cudaMemcpyDeviceToHost, s->stream);
+        if (fe == cudaSuccess) fe = cudaStreamSynchronize(s->stream);
+        if (fe != cudaSuccess) {
+            int code = cuda_fail(nullptr, fe, "face values");
+            bfx_destroy(s);
+            return code;
+        }
+        s->face_ready = true;
+    }
     BFX_ALLOC(s->density, (size_t)g.n * sizeof(float));
     BFX_ALLOC(s->velocity, (size_t)g.n * sizeof(float4));
     s->slot_density[0] = s->density;

@@ -19,6 +19,12 @@ struct BulkArgs {
     float far_eq_f[19];     // equilibrium(q, far density, far velocity), FP32
     double far_eq_d[19];    // same in FP64 (FP64 storage)
     float far_dev[19];      // (far_eq_f - w_q) x the storage's deviation scale (16-bit formats)
+    // x-face values of the staged kernel (face_values 1; the halo fill then
+    // skips the x faces): the stored deviation of what the fill writes for
+    // direction q across face f (0: -x, 1: +x), read back as the kernel reads
+    // a population
+    int face_values;
+    float face_dev[2][19];
     int box[3];             // geometry box extent (origin in DeviceState); rare-cell launch
     void* pops;
     const uint8_t* mask;

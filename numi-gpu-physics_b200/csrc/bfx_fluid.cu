@@ -97,6 +97,28 @@ __global__ void __launch_bounds__(128) k_halo(const BulkArgs a, int rep_s, int64
     }
 }
 
+// The values k_halo writes across a far-field or velocity face depend only on
+// the face and the direction.  When both x faces are of those kinds the
+// staged kernel takes their values from this table instead of the x-halo
+// slots, whose fill (one scattered store per row and direction) it skips:
+// out[19 f + q] = the stored value of direction q across face f (0: -x,
+// 1: +x), read back as the staged kernel reads a population (scaled deviation).
+template <class S>
+__global__ void k_halo_values(const BulkArgs a, float* out) {
+    using T = typename S::T;
+    using R = typename S::R;
+    const int t = threadIdx.x;
+    if (t >= 2 * 19) return;
+    const int f = t / 19, q = t % 19;
+    const FluidParams& fp = a.fp;
+    R val = sizeof(R) == 8 ? (R)a.far_eq_d[q] : (R)a.far_eq_f[q];
+    if (fp.face_bc[f] == BFX_BC_VELOCITY)
+        val = feq_rt<R>(q, (R)fp.far[3], (R)fp.face_u[f][0], (R)fp.face_u[f][1], (R)fp.face_u[f][2]);
+    T stored;
+    S::st_rt(&stored, q, val);
+    out[t] = S::ld_dev(&stored);
+}
+
 // ---------------------------------------------------------------------------
 // Initialisation (rep E), canonical read-out / write-in, macroscopic fields.
 // ---------------------------------------------------------------------------
@@ -281,6 +303,9 @@ BulkArgs make_bulk_args(const GridDesc& gd, const FluidParams& fp, const FluidBu
         const double scale = storage == BFX_STORAGE_F16_DEVIATION ? (double)StoreF16Dev::kDevScale : 1.0;
         a.far_dev[q] = (float)((a.far_eq_d[q] - wq<double>(q)) * scale);
     }
+    a.face_values = b.face_dev ? 1 : 0;
+    for (int f = 0; f < 2; ++f)
+        for (int q = 0; q < 19; ++q) a.face_dev[f][q] = b.face_dev ? b.face_dev[19 * f + q] : 0.0f;
     a.pops = b.pops;
     a.mask = b.mask;
     a.wall = b.wall;
@@ -361,6 +386,9 @@ static bool use_staged(int storage, int collision, int capture, bool tma_ok) {
     const bool sixteen = storage == BFX_STORAGE_F16_DEVIATION || storage == BFX_STORAGE_BF16_DEVIATION;
     return tma_ok && sixteen && staged_collision(collision) && capture != 2;
 }
+bool bulk_staged(int storage, int collision, int capture, bool tma_ok) {
+    return use_staged(storage, collision, capture, tma_ok);
+}
 
 int launch_bulk_count(int storage, int collision, int capture, bool tma_ok, bool geometry) {
     return use_staged(storage, collision, capture, tma_ok) && geometry ? 2 : 1;
@@ -419,6 +447,26 @@ static void halo_s(const BulkArgs& a, int rep_s, cudaStream_t s) {
     const int64_t halo = a.g.pn - a.g.n;
     k_halo<S><<<(unsigned)((halo + 127) / 128), 128, 0, s>>>(a, rep_s, halo);
 }
+// The z planes and y rows of the shell come first in padded_shell_cell's
+// order, the x columns last: the first 2 (fz + fy) cells are the y / z faces.
+template <class S>
+static void halo_yz_s(const BulkArgs& a, int rep_s, cudaStream_t s) {
+    const int64_t yz = 2 * ((int64_t)a.g.px * a.g.py + (int64_t)a.g.px * (a.g.pz - 2));
+    k_halo<S><<<(unsigned)((yz + 127) / 128), 128, 0, s>>>(a, rep_s, yz);
+}
+void launch_halo_values(int storage, const GridDesc& g, const FluidParams& fp, float* out, cudaStream_t s) {
+    FluidBuffers b = {};
+    BulkArgs a = make_bulk_args(g, fp, b, 0, storage);
+    if (storage == BFX_STORAGE_F16_DEVIATION) k_halo_values<StoreF16Dev><<<1, 128, 0, s>>>(a, out);
+    else if (storage == BFX_STORAGE_BF16_DEVIATION) k_halo_values<StoreBF16Dev><<<1, 128, 0, s>>>(a, out);
+}
+
+void launch_halo_yz(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const FluidBuffers& b,
+                    cudaStream_t s) {
+    BulkArgs a = make_bulk_args(g, fp, b, 0, storage);
+    BFX_DISPATCH_STORAGE(storage, halo_yz_s, a, rep_s, s);
+}
+
 void launch_halo(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const FluidBuffers& b,
                  cudaStream_t s) {
     BulkArgs a = make_bulk_args(g, fp, b, 0, storage);

@@ -28,6 +28,8 @@ struct FluidBuffers {
     void* tape;             // pre-collision (rho, u) per cell when the step is taped (capture == 2)
     const void* tmap;       // CUtensorMap of the population array for the staged kernel (null: k_bulk)
     int sm_count;
+    const float* face_dev;  // host copy of the x-face values [2][19] for the staged kernel (null: the halo
+                            // fill covers the x faces)
 };
 
 // Fused stream + collide of every cell: fluid cells collide, solid cells take
@@ -37,6 +39,17 @@ struct FluidBuffers {
 // to a second launch over the box.
 void launch_bulk(int storage, int collision, int rep_s, const GridDesc& g, const FluidParams& fp,
                  const FluidBuffers& b, int capture, const int* box, cudaStream_t s);
+// The step runs the TMA-staged kernel (16-bit storage, staged operator, a
+// population tensor map, not taped).
+bool bulk_staged(int storage, int collision, int capture, bool tma_ok);
+// x-face values for the staged kernel when both x faces are far-field or
+// velocity faces (BulkArgs::face_dev): out[2 * 19], computed as the halo fill
+// computes and stores them, read back as stored deviations.
+void launch_halo_values(int storage, const GridDesc& g, const FluidParams& fp, float* out, cudaStream_t s);
+// Halo fill of the z and y faces only (the staged kernel takes the x faces'
+// values from BulkArgs::face_dev).
+void launch_halo_yz(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const FluidBuffers& b,
+                    cudaStream_t s);
 // The staged path's two launches (k_rare over the geometry box, then k_stream)
 // for callers that queue work between them; only for a simulation whose
 // population tensor map was encoded (16-bit storage, staged operator).

@@ -174,6 +174,20 @@ __device__ __forceinline__ void collide_dev2(const P2 (&d)[19], float s, float i
     }
 }
 
+// x faces without their halo fill (BulkArgs::face_values): at x = 0 (SGN +1)
+// every direction with c_x > 0 comes from beyond the -x face, at x = nx - 1
+// (SGN -1) every direction with c_x < 0 from beyond the +x face; the halo
+// fill takes the x face first for a source outside in several axes, so these
+// are its values for every such direction, rows at the y / z faces included.
+// The values are kernel parameters: no load waits on memory.
+template <int SGN>
+__device__ __forceinline__ void x_face_values(const BulkArgs& a, int l, P2 (&dv)[19]) {
+    constexpr int f = SGN > 0 ? 0 : 1;
+#pragma unroll
+    for (int q = 1; q < 19; ++q)
+        if (cx(q) == SGN) Lanes<P2>::set(dv[q], l, a.face_dev[f][q]);
+}
+
 // Exact positivity admission of one lane (BF.metal:3035-3052) on absolute
 // populations f = w_q + d / s: the admissible scale over every direction, and
 // the scaled blend feq + scale (cand - feq) when it is below 1.
@@ -340,6 +354,16 @@ __global__ void __maxnreg__(StreamShape<COLL>::max_regs)
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(empty0 + 8 * s);
+        if (a.face_values) {
+            // no x-halo fill: the warp's cells at x = 0 or x = nx - 1 take the
+            // x-face values (one warp-uniform test for the warp's 64 cells)
+            const int xbase = xa - lane;
+            if (xbase == 0 || xbase + kTileX >= g.nx) {
+                if (xa == 0) x_face_values<1>(a, 0, dv);
+                if (xa == g.nx - 1) x_face_values<-1>(a, 0, dv);
+                if (xb == g.nx - 1) x_face_values<-1>(a, 1, dv);
+            }
+        }
         // solid and newly uncovered cells (mask byte set) are left to k_rare
         va = va && ma == 0;
         vb = vb && mb == 0;
