@@ -827,31 +827,45 @@ __global__ void __launch_bounds__(128, LEAN ? 12 : 1) k_mesh_raster(const GeomAr
     if (lane < qn) key_voxel(qw[lane]);
 }
 
-__device__ void resolve_cell(const GeomArgs& a, int has_prev, int x, int y, int z, int64_t bidx);
+__device__ bool resolve_cell(const GeomArgs& a, int has_prev, int x, int y, int z, int64_t bidx);
 
 // Mask byte and wall value of every active cell (cells outside the active
-// bounds keep mask 0; their wall value is never read); slab launch.
+// bounds keep mask 0; their wall value is never read); slab launch.  With
+// block_live, every slab also records for each of its kSlabZ slices (one
+// block of the link count's box launch) whether any cell holds a key or a
+// changed occupancy: only such blocks can hold a cut link (its fluid cell is
+// keyed) or a topology event, so the link count skips the others.
 __global__ void k_mesh_resolve(const GeomArgs a, int has_prev) {
-    if (slab_inactive(a)) return;
+    const bool inactive = slab_inactive(a);
     int lo[3], hi[3];
     active_bounds(a, lo, hi);
 #pragma unroll
     for (int k = 0; k < kSlabZ; ++k) {
         int x, y, z;
         int64_t bidx;
-        if (slab_cell(a, k, x, y, z, bidx) && in_bounds(lo, hi, x, y, z)) resolve_cell(a, has_prev, x, y, z, bidx);
+        bool live = false;
+        if (!inactive && slab_cell(a, k, x, y, z, bidx) && in_bounds(lo, hi, x, y, z))
+            live = resolve_cell(a, has_prev, x, y, z, bidx);
+        if (a.b.block_live) {
+            const int any = __syncthreads_or(live);
+            const int lz = (int)blockIdx.z * kSlabZ + k;
+            if (linear_tid() == 0 && lz < a.bz)
+                a.b.block_live[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * lz)] = any ? 1 : 0;
+        }
     }
 }
 
-__device__ void resolve_cell(const GeomArgs& a, int has_prev, int x, int y, int z, int64_t bidx) {
+// Resolves one cell; true when it holds a key or its occupancy changed.
+__device__ bool resolve_cell(const GeomArgs& a, int has_prev, int x, int y, int z, int64_t bidx) {
     const int64_t gid = flat(a.g, x, y, z);
     uint8_t prev_part = a.b.mask_prev[gid] & kPartMask;
     unsigned long long key = a.b.keys[bidx];
     uint32_t t = (uint32_t)(key & 0xFFFFFFFFull);
     if (key == 0xFFFFFFFFFFFFFFFFull || t >= a.b.ntris) {
-        a.b.mask_next[gid] = topo_flags(0, prev_part, has_prev);
+        const uint8_t m = topo_flags(0, prev_part, has_prev);
+        a.b.mask_next[gid] = m;
         a.b.wall[gid] = make_float4(0.0f, 0.0f, 0.0f, 16.0f);
-        return;
+        return m != 0;
     }
     V3 w = cell_world(a.fp, x, y, z);
     V3 A, B, C, bary;
@@ -865,6 +879,7 @@ __device__ void resolve_cell(const GeomArgs& a, int has_prev, int x, int y, int 
     uint8_t part = sd <= 0.0f ? a.b.mesh_tri_part[t] : (uint8_t)0;
     a.b.mask_next[gid] = topo_flags(part, prev_part, has_prev);
     a.b.wall[gid] = make_float4(v.x, v.y, v.z, sd / a.fp.dx);
+    return true;
 }
 
 __global__ void k_fill_wall_w(float4* wall, int64_t n, float w) {
@@ -1095,7 +1110,7 @@ __device__ __forceinline__ void topology_impulse_warp(const GeomArgs& a, int rep
 __global__ void __launch_bounds__(256) k_link_count(const GeomArgs a) {
     __shared__ uint32_t wcount[8];
     const int block = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-    if (block_inactive(a)) {
+    if (block_inactive(a) || (a.b.block_live && !a.b.block_live[block])) {
         // no key, link or topology change in this block
         if (linear_tid() == 0) {
             a.b.block_counts[block] = 0;

@@ -121,6 +121,7 @@ struct GeomBuffers {
     const float* kf_times;          // keyframe replay: times, frames x vertices x 3 offsets (kf_count >= 2)
     const float* kf_points;
     int kf_count;
+    uint8_t* block_live;            // per box block: a key or an occupancy change (mesh resolve), or null
     int box_blocks;                 // blocks of a one-slice-per-block box launch (allocations)
     int scan_blocks;                // blocks of the link count / scan / emission launch
     double* topo_partials;          // 8 per topology block
