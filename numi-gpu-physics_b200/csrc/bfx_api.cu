@@ -110,7 +110,9 @@ struct bfx_sim {
     uint32_t* event_sums = nullptr;
     uint32_t* event_cell = nullptr;
     uint32_t* event_total = nullptr;
-    uint8_t* block_live = nullptr;
+    uint32_t* live_list = nullptr;
+    uint32_t* live_count = nullptr;
+    uint32_t* cell_bits = nullptr;
     int box_blocks = 0;
     int scan_blocks = 0;
     double* topo_partials = nullptr;
@@ -262,7 +264,9 @@ GeomBuffers geom_buffers(bfx_sim* s, uint8_t* mprev, uint8_t* mnext) {
     b.event_cell = s->event_cell;
     b.event_total = s->event_total;
     // the occupancy test hook's replayed masks are not what the resolve saw
-    b.block_live = s->topo_mode ? nullptr : s->block_live;
+    b.live_list = s->topo_mode ? nullptr : s->live_list;
+    b.live_count = s->live_count;
+    b.cell_bits = s->cell_bits;
     b.box_blocks = s->box_blocks;
     b.scan_blocks = s->scan_blocks;
     b.topo_partials = s->topo_partials;
@@ -921,9 +925,11 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
         BFX_ALLOC(s->event_sums, nseg * sizeof(uint32_t));
         BFX_ALLOC(s->event_cell, (size_t)s->box.cells * sizeof(uint32_t));
         BFX_ALLOC(s->event_total, sizeof(uint32_t));
+        BFX_ALLOC(s->cell_bits, (size_t)s->box.cells * sizeof(uint32_t));
         if (c.geometry == BFX_GEOMETRY_MESH) {
-            BFX_ALLOC(s->block_live, (size_t)s->box_blocks);
-            cudaMemsetAsync(s->block_live, 0, (size_t)s->box_blocks, s->stream);
+            BFX_ALLOC(s->live_list, (size_t)s->box_blocks * sizeof(uint32_t));
+            BFX_ALLOC(s->live_count, sizeof(uint32_t));
+            cudaMemsetAsync(s->live_count, 0, sizeof(uint32_t), s->stream);
         }
         cudaMemsetAsync(s->event_total, 0, sizeof(uint32_t), s->stream);
         s->topo_blocks = s->sm_count;

@@ -77,6 +77,20 @@ __device__ __forceinline__ V3 normalize3(V3 v) {
     return v3(v.x / l, v.y / l, v.z / l);
 }
 
+// Cell of this thread in box block (bxi, byi, bzi) of a box launch.
+__device__ __forceinline__ bool box_cell_at(const GeomArgs& a, int bxi, int byi, int bzi, int& x, int& y, int& z,
+                                            int64_t& bidx) {
+    int lx = bxi * blockDim.x + threadIdx.x;
+    int ly = byi * blockDim.y + threadIdx.y;
+    int lz = bzi;
+    if (lx >= a.bx || ly >= a.by || lz >= a.bz) return false;
+    const int32_t* o = a.b.state->box_origin;
+    x = o[0] + lx;
+    y = o[1] + ly;
+    z = o[2] + lz;
+    bidx = (int64_t)lx + (int64_t)a.bx * ((int64_t)ly + (int64_t)a.by * lz);
+    return x < a.g.nx && y < a.g.ny && z < a.g.nz;
+}
 __device__ __forceinline__ bool box_cell(const GeomArgs& a, int& x, int& y, int& z, int64_t& bidx) {
     int lx = blockIdx.x * blockDim.x + threadIdx.x;
     int ly = blockIdx.y * blockDim.y + threadIdx.y;
@@ -134,14 +148,17 @@ __device__ __forceinline__ bool slab_inactive(const GeomArgs& a) {
 
 // The cells of box_cell's block all lie outside the active bounds (uniform
 // over the block).
-__device__ __forceinline__ bool block_inactive(const GeomArgs& a) {
+__device__ __forceinline__ bool block_inactive_at(const GeomArgs& a, int bxi, int byi, int bzi) {
     int lo[3], hi[3];
     active_bounds(a, lo, hi);
     const int32_t* o = a.b.state->box_origin;
-    const int x0 = o[0] + (int)(blockIdx.x * blockDim.x), x1 = x0 + (int)blockDim.x - 1;
-    const int y0 = o[1] + (int)(blockIdx.y * blockDim.y), y1 = y0 + (int)blockDim.y - 1;
-    const int z = o[2] + (int)blockIdx.z;
+    const int x0 = o[0] + bxi * (int)blockDim.x, x1 = x0 + (int)blockDim.x - 1;
+    const int y0 = o[1] + byi * (int)blockDim.y, y1 = y0 + (int)blockDim.y - 1;
+    const int z = o[2] + bzi;
     return x1 < lo[0] || x0 > hi[0] || y1 < lo[1] || y0 > hi[1] || z < lo[2] || z > hi[2];
+}
+__device__ __forceinline__ bool block_inactive(const GeomArgs& a) {
+    return block_inactive_at(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 __device__ __forceinline__ bool in_bounds(const int (&lo)[3], const int (&hi)[3], int x, int y, int z) {
     return x >= lo[0] && x <= hi[0] && y >= lo[1] && y <= hi[1] && z >= lo[2] && z <= hi[2];

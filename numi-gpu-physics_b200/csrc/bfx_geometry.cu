@@ -830,11 +830,13 @@ __global__ void __launch_bounds__(128, LEAN ? 12 : 1) k_mesh_raster(const GeomAr
 __device__ bool resolve_cell(const GeomArgs& a, int has_prev, int x, int y, int z, int64_t bidx);
 
 // Mask byte and wall value of every active cell (cells outside the active
-// bounds keep mask 0; their wall value is never read); slab launch.  With
-// block_live, every slab also records for each of its kSlabZ slices (one
-// block of the link count's box launch) whether any cell holds a key or a
-// changed occupancy: only such blocks can hold a cut link (its fluid cell is
-// keyed) or a topology event, so the link count skips the others.
+// bounds keep mask 0; their wall value is never read); slab launch.  With a
+// live list, every slab also appends each of its kSlabZ slices (one block of
+// the link count's box launch) in which a cell holds a key or a changed
+// occupancy: only such blocks can hold a cut link (its fluid cell is keyed)
+// or a topology event, so the link count and emission visit those alone.  The
+// list's order is not fixed, and nothing depends on it: the counts are stored
+// by block index and the emission writes at offsets scanned in block order.
 __global__ void k_mesh_resolve(const GeomArgs a, int has_prev) {
     const bool inactive = slab_inactive(a);
     int lo[3], hi[3];
@@ -846,11 +848,11 @@ __global__ void k_mesh_resolve(const GeomArgs a, int has_prev) {
         bool live = false;
         if (!inactive && slab_cell(a, k, x, y, z, bidx) && in_bounds(lo, hi, x, y, z))
             live = resolve_cell(a, has_prev, x, y, z, bidx);
-        if (a.b.block_live) {
+        if (a.b.live_list) {
             const int any = __syncthreads_or(live);
             const int lz = (int)blockIdx.z * kSlabZ + k;
-            if (linear_tid() == 0 && lz < a.bz)
-                a.b.block_live[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * lz)] = any ? 1 : 0;
+            if (any && linear_tid() == 0 && lz < a.bz)
+                a.b.live_list[atomicAdd(a.b.live_count, 1u)] = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * lz);
         }
     }
 }
@@ -1106,11 +1108,13 @@ __device__ __forceinline__ void topology_impulse_warp(const GeomArgs& a, int rep
 
 // Per-block counts of cut links and topology events over the geometry box.
 // Geometry only (masks and keys), so the pipelined path runs it with the
-// next step's geometry, beside the fluid kernel.
-__global__ void __launch_bounds__(256) k_link_count(const GeomArgs a) {
-    __shared__ uint32_t wcount[8];
-    const int block = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-    if (block_inactive(a) || (a.b.block_live && !a.b.block_live[block])) {
+// next step's geometry, beside the fluid kernel.  Each active cell of a counted
+// block also stores its link sources (bits 1-18) and event flag (bit 0) in
+// cell_bits, so the emission reads one word instead of the 20 mask and key
+// loads again.
+__device__ __forceinline__ void count_block(const GeomArgs& a, int bxi, int byi, int bzi, int block,
+                                            uint32_t* wcount) {
+    if (block_inactive_at(a, bxi, byi, bzi)) {
         // no key, link or topology change in this block
         if (linear_tid() == 0) {
             a.b.block_counts[block] = 0;
@@ -1122,12 +1126,14 @@ __global__ void __launch_bounds__(256) k_link_count(const GeomArgs a) {
     {
         int x, y, z;
         int64_t bidx;
-        if (box_cell(a, x, y, z, bidx) && cell_active(a, x, y, z)) {
+        if (box_cell_at(a, bxi, byi, bzi, x, y, z, bidx) && cell_active(a, x, y, z)) {
             const int64_t gid = flat(a.g, x, y, z);
             const uint8_t m1 = a.b.mask_next[gid];
             const uint8_t m0 = a.b.mask_prev[gid];
             events = topology_event(a.fp, m1) ? 1u : 0u;
-            if (may_have_links(a, bidx, m1, m0)) links = __popc(link_sources(a.g, a.b.mask_next, x, y, z));
+            const uint32_t sources = may_have_links(a, bidx, m1, m0) ? link_sources(a.g, a.b.mask_next, x, y, z) : 0u;
+            links = __popc(sources);
+            a.b.cell_bits[bidx] = sources | events;
         }
     }
     // links (at most 18 a cell) in the low half, events in the high half
@@ -1144,6 +1150,23 @@ __global__ void __launch_bounds__(256) k_link_count(const GeomArgs a) {
         }
         a.b.block_counts[block] = tl;
         a.b.event_counts[block] = te;
+    }
+}
+__global__ void __launch_bounds__(256) k_link_count(const GeomArgs a) {
+    __shared__ uint32_t wcount[8];
+    count_block(a, blockIdx.x, blockIdx.y, blockIdx.z, blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z),
+                wcount);
+}
+// The same over the live list of the mesh resolve (the other blocks' counts
+// are zeroed before): a fixed grid, list entry i to block i mod gridDim.x;
+// (gx, gy) are the box launch's grid extents.
+__global__ void __launch_bounds__(256) k_link_count_live(const GeomArgs a, int gx, int gy) {
+    __shared__ uint32_t wcount[8];
+    const uint32_t n = *a.b.live_count;
+    for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+        const int b = (int)a.b.live_list[i];
+        count_block(a, b % gx, (b / gx) % gy, b / (gx * gy), b, wcount);
+        __syncthreads();
     }
 }
 
@@ -1257,24 +1280,20 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(const GeomArgs a, i
 // links (in direction order) at the block offset plus the shuffle prefix of
 // the preceding threads, so the list is ordered by box cell then direction;
 // every event cell appends itself to the event list in box-cell order.
-__global__ void __launch_bounds__(256) k_links_emit(const GeomArgs a, int geometry, int link_rule, int interpolated) {
-    __shared__ uint32_t wsum[8];
-    const int block = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-    // blocks without links or events (most of the box) emit nothing
+__device__ __forceinline__ void emit_block(const GeomArgs& a, int bxi, int byi, int bzi, int block, uint32_t* wsum) {
+    // blocks without links or events (most of the box) emit nothing; the
+    // others were counted, so their active cells' bits are this step's
     if (a.b.block_counts[block] == 0 && a.b.event_counts[block] == 0) return;
     const Grid& g = a.g;
     uint32_t mine = 0, bits = 0, event = 0;
     int x = 0, y = 0, z = 0;
     int64_t bidx = 0, gid = 0;
-    if (box_cell(a, x, y, z, bidx) && cell_active(a, x, y, z)) {
+    if (box_cell_at(a, bxi, byi, bzi, x, y, z, bidx) && cell_active(a, x, y, z)) {
         gid = flat(g, x, y, z);
-        const uint8_t m1 = a.b.mask_next[gid];
-        const uint8_t m0 = a.b.mask_prev[gid];
-        event = topology_event(a.fp, m1) ? 1u : 0u;
-        if (may_have_links(a, bidx, m1, m0)) {
-            bits = link_sources(g, a.b.mask_next, x, y, z);
-            mine = __popc(bits);
-        }
+        const uint32_t cb = a.b.cell_bits[bidx];
+        event = cb & 1u;
+        bits = cb & ~1u;
+        mine = __popc(bits);
     }
     // block-exclusive prefix of (links, events), packed low / high 16 bits
     // (a block holds at most 256 x 18 links and 256 events)
@@ -1305,9 +1324,21 @@ __global__ void __launch_bounds__(256) k_links_emit(const GeomArgs a, int geomet
         }
         ++pos;
     }
-    (void)geometry;
-    (void)link_rule;
-    (void)interpolated;
+}
+__global__ void __launch_bounds__(256) k_links_emit(const GeomArgs a) {
+    __shared__ uint32_t wsum[8];
+    emit_block(a, blockIdx.x, blockIdx.y, blockIdx.z, blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z),
+               wsum);
+}
+// The same over the live list (k_link_count_live).
+__global__ void __launch_bounds__(256) k_links_emit_live(const GeomArgs a, int gx, int gy) {
+    __shared__ uint32_t wsum[8];
+    const uint32_t n = *a.b.live_count;
+    for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+        const int b = (int)a.b.live_list[i];
+        emit_block(a, b % gx, (b / gx) % gy, b / (gx * gy), b, wsum);
+        __syncthreads();
+    }
 }
 
 // Link fractions, one thread per emitted link (the bisections and ray roots
@@ -1774,6 +1805,7 @@ void launch_classify(int geometry, int has_prev, const GridDesc& g, const FluidP
         const unsigned rblocks = (unsigned)(((int64_t)gb.ntris * 32 + 127) / 128);
         if (lean_raster) k_mesh_raster<1><<<rblocks, 128, 0, s>>>(a);
         else k_mesh_raster<0><<<rblocks, 128, 0, s>>>(a);
+        if (gb.live_list) cudaMemsetAsync(gb.live_count, 0, sizeof(uint32_t), s);
         k_mesh_resolve<<<sgrid, sblock, 0, s>>>(a, has_prev);
     }
 }
@@ -1791,11 +1823,20 @@ void launch_link_build(int geometry, int link_rule, const GridDesc& g, const Flu
     GeomArgs a = make_geom(g, fp, box, gb, nullptr);
     dim3 grid, block;
     box_shape(box, grid, block);
-    k_link_count<<<grid, block, 0, s>>>(a);
+    // with the mesh resolve's live list: count and emit over those blocks only
+    const unsigned live_grid = (unsigned)std::min<int64_t>((int64_t)grid.x * grid.y * grid.z, 1024);
+    if (gb.live_list) {
+        cudaMemsetAsync(gb.block_counts, 0, (size_t)gb.scan_blocks * sizeof(uint32_t), s);
+        cudaMemsetAsync(gb.event_counts, 0, (size_t)gb.scan_blocks * sizeof(uint32_t), s);
+        k_link_count_live<<<live_grid, block, 0, s>>>(a, (int)grid.x, (int)grid.y);
+    } else {
+        k_link_count<<<grid, block, 0, s>>>(a);
+    }
     const int nseg = (a.b.scan_blocks + kScanSegment - 1) / kScanSegment;
     k_scan_reduce<<<dim3(nseg, 2), kScanThreads, 0, s>>>(a);
     k_scan_apply<<<dim3(nseg, 2), kScanThreads, 0, s>>>(a, nseg);
-    k_links_emit<<<grid, block, 0, s>>>(a, geometry, link_rule, fp.interpolated);
+    if (gb.live_list) k_links_emit_live<<<live_grid, block, 0, s>>>(a, (int)grid.x, (int)grid.y);
+    else k_links_emit<<<grid, block, 0, s>>>(a);
     if (geometry == BFX_GEOMETRY_MESH && link_rule == BFX_LINK_RAY_ROOT && fp.interpolated) {
         const unsigned rblocks =
             (unsigned)std::max<int64_t>(1, std::min<int64_t>(4096, ((int64_t)gb.link_capacity * 16 + 127) / 128));

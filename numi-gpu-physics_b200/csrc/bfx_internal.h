@@ -121,7 +121,9 @@ struct GeomBuffers {
     const float* kf_times;          // keyframe replay: times, frames x vertices x 3 offsets (kf_count >= 2)
     const float* kf_points;
     int kf_count;
-    uint8_t* block_live;            // per box block: a key or an occupancy change (mesh resolve), or null
+    uint32_t* live_list;            // box blocks with a key or an occupancy change (mesh resolve), or null
+    uint32_t* live_count;           // [1] entries in live_list
+    uint32_t* cell_bits;            // per box cell of a counted block: link sources (bits 1-18), event (bit 0)
     int box_blocks;                 // blocks of a one-slice-per-block box launch (allocations)
     int scan_blocks;                // blocks of the link count / scan / emission launch
     double* topo_partials;          // 8 per topology block
