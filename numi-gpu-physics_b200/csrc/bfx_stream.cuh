@@ -64,6 +64,7 @@ struct StreamGeom {
 struct StreamTiles {
     int tiles_x, tiles_y;
     int ntiles;
+    int step_x, step_y, step_z;  // the grid stride (CTAs) in tile coordinates
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
