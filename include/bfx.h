@@ -526,7 +526,8 @@ typedef struct bfx_adjoint_result {
     uint32_t checkpoint_interval;
     uint32_t snapshots;
     double forward_ms;              /* device time of the forward pass with its snapshots */
-    double reverse_ms;              /* device time of the recomputation and the reverse sweep */
+    double reverse_ms;              /* device time of the recomputation and the reverse sweep, from its first
+                                       launch (the allocation of its work memory is not included) */
     uint64_t max_links;             /* largest cut-link count of the run */
     uint64_t work_bytes;            /* device memory of snapshots, tape and adjoint fields */
 } bfx_adjoint_result;

@@ -1934,7 +1934,10 @@ int bfx_adjoint(bfx_sim* s, uint64_t steps, const bfx_adjoint_objective* objecti
                              s->stream);
     }
 
-    cudaEvent_t ev[3];
+    // ev: forward start and end, reverse end, reverse start (after the
+    // reverse pass's work memory is allocated: those host-side allocations
+    // leave the device idle for a varying time that is not the pass's work)
+    cudaEvent_t ev[4];
     for (auto& e : ev) cudaEventCreate(&e);
     cudaEventRecord(ev[0], s->stream);
     // pass 1: forward with snapshots
@@ -1986,6 +1989,7 @@ int bfx_adjoint(bfx_sim* s, uint64_t steps, const bfx_adjoint_objective* objecti
     BFX_ADJ_ALLOC(p_rare, (size_t)s->box_blocks * 4 * sizeof(double));
     BFX_ADJ_ALLOC(p_links, (size_t)s->apply_blocks * 4 * sizeof(double));
 #undef BFX_ADJ_ALLOC
+    cudaEventRecord(ev[3], s->stream);
     cudaMemsetAsync(lam, 0, pop_bytes, s->stream);
     const int32_t off = 0;
     cudaMemcpyAsync(&s->dobjective->enabled, &off, sizeof(off), cudaMemcpyHostToDevice, s->stream);
@@ -2063,7 +2067,7 @@ int bfx_adjoint(bfx_sim* s, uint64_t steps, const bfx_adjoint_objective* objecti
     s->step = st_end.step;
     float f_ms = 0.0f, r_ms = 0.0f;
     cudaEventElapsedTime(&f_ms, ev[0], ev[1]);
-    cudaEventElapsedTime(&r_ms, ev[1], ev[2]);
+    cudaEventElapsedTime(&r_ms, ev[3], ev[2]);
     for (auto& e : ev) cudaEventDestroy(e);
     if (result) {
         std::memset(result, 0, sizeof(*result));
