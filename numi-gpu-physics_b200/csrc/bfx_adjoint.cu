@@ -764,7 +764,7 @@ __global__ void __launch_bounds__(128) k_adj_halo(const AdjArgs a, int rep_s, in
     }
 }
 
-// Cover / uncover impulses (k_boundary_scan): pass 0 covered, pass 1 uncovered.
+// Cover / uncover impulses (the forward k_topology): pass 0 covered, pass 1 uncovered.
 template <class R>
 __global__ void __launch_bounds__(256) k_adj_topology(const AdjArgs a, int rep_s, int pass) {
     const GeomArgs& ga = a.ga;
