@@ -103,9 +103,9 @@ __global__ void k_prepare(const GeomArgs a, int init, float dt, float box_radius
     float phase = af * time;
     // The step's sines and cosines (portable FP64 series, bit-identical to the
     // host) are independent of one another: the lanes evaluate them in two
-    // rounds, the phase angles and then the rotation angles built from them.
-    //   round 1: phase, phase + pitch phase, 2 phase, phase + joint phase (2)
-    //   round 2: +/- stroke, deviation, +/- pitch, +/- each joint angle
+    // passes, the phase angles and then the rotation angles built from them.
+    //   pass 1: phase, phase + pitch phase, 2 phase, phase + joint phase (2)
+    //   pass 2: +/- stroke, deviation, +/- pitch, +/- each joint angle
     const int njoints = a.b.joint_count < 2 ? a.b.joint_count : 2;
     __shared__ SinCos sc1[5], sc2[9];
     {
