@@ -156,7 +156,7 @@ struct bfx_sim {
     uint64_t pipe_launches[2] = {0, 0};
     // side stream of the next step's geometry build, with its fork / join events
     cudaStream_t side = nullptr;
-    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr, lists_ev = nullptr;
     cudaEvent_t halo_fork_ev = nullptr, halo_join_ev = nullptr;
     // topology record / replay test hook (bfx_test_replay_topology): 0 off,
     // 1 record each step's occupancy into topo_buf, 2 replace it from there
@@ -338,8 +338,9 @@ bool halo_beside_links(const bfx_sim* s) {
 // The cut-link and topology-event lists of a step's geometry, on the
 // simulation's stream or (pipelined path) the side stream beside the previous
 // step's fluid kernel.
-void encode_link_build(bfx_sim* s, uint8_t* mprev, uint8_t* mnext, cudaStream_t st) {
-    launch_link_build(s->cfg.geometry, s->cfg.link_rule, s->g, s->fp, s->box, geom_buffers(s, mprev, mnext), st);
+void encode_link_build(bfx_sim* s, uint8_t* mprev, uint8_t* mnext, cudaStream_t st, cudaEvent_t lists_done = nullptr) {
+    launch_link_build(s->cfg.geometry, s->cfg.link_rule, s->g, s->fp, s->box, geom_buffers(s, mprev, mnext), st,
+                      lists_done);
     s->launches += 5;
 }
 // The topology impulses of the step's events: they read the pre-step
@@ -424,11 +425,9 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
         launch_frame_tangent(geom_buffers(s, mprev, mnext), s->cfg.time_step, 0, tape->frames, s->stream);
         s->launches += 1;
     }
-    if (s->geometry() && s->moving()) {
-        // geometry_ready: the cut-link and event lists were built with the geometry
-        if (geometry_ready) encode_topology(s, mprev, mnext);
-        else encode_links(s, mprev, mnext);
-    }
+    // geometry_ready: the previous step built this step's cut-link and event
+    // lists with its geometry and ran its topology impulses
+    if (s->geometry() && s->moving() && !geometry_ready) encode_links(s, mprev, mnext);
     if (tape) {
         GeomBuffers gb = geom_buffers(s, mprev, mnext);
         gb.frames = tape->frames;
@@ -490,10 +489,10 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
         cudaEventRecord(s->fork_ev, s->stream);
         cudaStreamWaitEvent(s->side, s->fork_ev, 0);
         encode_geometry_build(s, 0, mnext, mprev, s->side);
-        if (s->geometry()) encode_link_build(s, mnext, mprev, s->side);
+        if (s->geometry()) encode_link_build(s, mnext, mprev, s->side, s->lists_ev);
+        else cudaEventRecord(s->lists_ev, s->side);
         cudaEventRecord(s->join_ev, s->side);
         launch_bulk_stream(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, box, s->stream);
-        cudaStreamWaitEvent(s->stream, s->join_ev, 0);
     } else {
         timing_begin(s);
         launch_bulk(s->cfg.storage, s->cfg.collision, s->rep_s, s->g, s->fp, fb, capture,
@@ -513,6 +512,15 @@ void encode_step(bfx_sim* s, int capture, bfx_run_sample* sample_slot_base, uint
     }
     s->rep_s ^= 1;
     if (s->moving()) s->cur ^= 1;
+    if (pipelined) {
+        // The next step's topology impulses, as soon as its event list is
+        // written (they read the populations after this step's fluid kernel,
+        // before the next link kernel), beside its link fractions; then the
+        // join.  Inside this step's encoding, so a captured graph holds both.
+        cudaStreamWaitEvent(s->stream, s->lists_ev, 0);
+        if (s->geometry()) encode_topology(s, s->mask[s->cur], s->mask[s->cur ^ 1]);
+        cudaStreamWaitEvent(s->stream, s->join_ev, 0);
+    }
 }
 
 // Replays (capturing on first use) the graph of `nsteps` (1 or 2) plain steps
@@ -736,6 +744,7 @@ void bfx_destroy(bfx_sim* s) {
         if (g) cudaGraphExecDestroy(g);
     if (s->fork_ev) cudaEventDestroy(s->fork_ev);
     if (s->join_ev) cudaEventDestroy(s->join_ev);
+    if (s->lists_ev) cudaEventDestroy(s->lists_ev);
     if (s->halo_fork_ev) cudaEventDestroy(s->halo_fork_ev);
     if (s->halo_join_ev) cudaEventDestroy(s->halo_join_ev);
     if (s->side) cudaStreamDestroy(s->side);
@@ -780,6 +789,7 @@ int bfx_create(const bfx_config* config, const bfx_bird* bird, const bfx_body_st
     if (cudaStreamCreateWithPriority(&s->side, cudaStreamNonBlocking, least_priority) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->join_ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->lists_ev, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->halo_fork_ev, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->halo_join_ev, cudaEventDisableTiming) != cudaSuccess) {
         (void)cudaGetLastError();

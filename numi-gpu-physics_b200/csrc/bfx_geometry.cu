@@ -1819,7 +1819,7 @@ void launch_classify(int geometry, int has_prev, const GridDesc& g, const FluidP
     }
 
 void launch_link_build(int geometry, int link_rule, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
-                       const GeomBuffers& gb, cudaStream_t s) {
+                       const GeomBuffers& gb, cudaStream_t s, cudaEvent_t lists_done) {
     GeomArgs a = make_geom(g, fp, box, gb, nullptr);
     dim3 grid, block;
     box_shape(box, grid, block);
@@ -1837,6 +1837,7 @@ void launch_link_build(int geometry, int link_rule, const GridDesc& g, const Flu
     k_scan_apply<<<dim3(nseg, 2), kScanThreads, 0, s>>>(a, nseg);
     if (gb.live_list) k_links_emit_live<<<live_grid, block, 0, s>>>(a, (int)grid.x, (int)grid.y);
     else k_links_emit<<<grid, block, 0, s>>>(a);
+    if (lists_done) cudaEventRecord(lists_done, s);
     if (geometry == BFX_GEOMETRY_MESH && link_rule == BFX_LINK_RAY_ROOT && fp.interpolated) {
         const unsigned rblocks =
             (unsigned)std::max<int64_t>(1, std::min<int64_t>(4096, ((int64_t)gb.link_capacity * 16 + 127) / 128));

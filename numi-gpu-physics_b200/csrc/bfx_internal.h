@@ -144,8 +144,10 @@ void launch_classify(int geometry, int has_prev, const GridDesc& g, const FluidP
 // Cut-link and topology-event lists of the step's geometry (counts, offset
 // scan, emission, link fractions).  Reads only geometry: masks, keys, wall
 // field and mesh.
+// lists_done (optional) is recorded once the lists are written, before the
+// link fractions.
 void launch_link_build(int geometry, int link_rule, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
-                       const GeomBuffers& gb, cudaStream_t s);
+                       const GeomBuffers& gb, cudaStream_t s, cudaEvent_t lists_done = nullptr);
 // Topology impulses of the event list into topo_partials; reads the pre-step
 // populations, so it runs before the link kernel writes any.
 void launch_topology(int storage, int rep_s, const GridDesc& g, const FluidParams& fp, const BoxDesc& box,
